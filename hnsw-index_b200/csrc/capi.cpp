@@ -1,0 +1,788 @@
+// C ABI: the drop-in boundary (include/hnsw_gpu.h).
+//
+// Host-side work here is plumbing: validating the file (host loader),
+// flattening the graph into the device layout, staging buffers, choosing a
+// scratch geometry per call and launching the kernels. No search result is
+// ever computed on the host.
+#include "hnsw_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <functional>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device.hpp"
+#include "host_index.hpp"
+
+using namespace hnswgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+std::string format_error_message(const Err& e) {
+    char buf[256];
+    switch (e.status) {
+        case HNSW_ERR_FORMAT_BAD_MAGIC: return "invalid index file: missing HNSWIDX magic bytes";
+        case HNSW_ERR_FORMAT_UNSUPPORTED_VERSION:
+            std::snprintf(buf, sizeof buf, "invalid index file: unsupported format version %llu", (unsigned long long)e.a);
+            return buf;
+        case HNSW_ERR_FORMAT_TRUNCATED: return "invalid index file: unexpected end of input";
+        case HNSW_ERR_FORMAT_CHECKSUM:
+            std::snprintf(buf, sizeof buf, "invalid index file: checksum mismatch: stored %#010llx, computed %#010llx",
+                          (unsigned long long)e.a, (unsigned long long)e.b);
+            return buf;
+        case HNSW_ERR_FORMAT_TRAILING_BYTES: return "invalid index file: unexpected bytes after the last section";
+        case HNSW_ERR_FORMAT_INVALID: return "invalid index file: invalid field: " + e.what;
+        case HNSW_ERR_MEMORY_LIMIT_EXCEEDED:
+            std::snprintf(buf, sizeof buf,
+                          "loading the index needs %llu bytes of memory, more than the limit of %llu",
+                          (unsigned long long)e.a, (unsigned long long)e.b);
+            return buf;
+        case HNSW_ERR_DUPLICATE_KEY:
+            std::snprintf(buf, sizeof buf, "key %llu is already present", (unsigned long long)e.a);
+            return buf;
+        case HNSW_ERR_NON_FINITE_VECTOR: return "vector contains NaN or infinite values";
+        case HNSW_ERR_ZERO_VECTOR: return "zero vector has no direction under cosine distance";
+        case HNSW_ERR_CAPACITY_EXCEEDED: return "index capacity exceeded";
+        case HNSW_ERR_DIMENSION_MISMATCH: return "dimension mismatch";
+        default: return e.what;
+    }
+}
+
+int from_err(const Err& e) { return e ? set_error(e.status, format_error_message(e)) : HNSW_OK; }
+
+int cuda_fail(cudaError_t e, const char* where) {
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(HNSW_ERR_OUT_OF_DEVICE_MEMORY, std::string(where) + ": " + cudaGetErrorString(e));
+    return set_error(HNSW_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CU(call, where)                             \
+    do {                                            \
+        cudaError_t _e = (call);                    \
+        if (_e != cudaSuccess) return cuda_fail(_e, where); \
+    } while (0)
+
+uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+// Growable device buffer.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, need);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// One concurrent call's stream and scratch.
+struct Slot {
+    cudaStream_t stream = nullptr;
+    DBuf q, ks, efs, fbits, fused, okeys, odist, ocount, ostatus, work, overflow, counters;
+    DBuf g_results, g_cands, g_visited;
+    uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
+    uint64_t g_words = 0;
+    size_t last_nq = 0;
+    ~Slot() {
+        for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
+                        &g_results, &g_cands, &g_visited})
+            b->release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct SlotPool {
+    std::mutex mu;
+    std::vector<std::unique_ptr<Slot>> free;
+    int device = 0;
+    int acquire(Slot** out) {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            if (!free.empty()) {
+                *out = free.back().release();
+                free.pop_back();
+                return HNSW_OK;
+            }
+        }
+        auto* s = new (std::nothrow) Slot();
+        if (!s) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out of host memory");
+        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete s;
+            return cuda_fail(e, "cudaStreamCreate");
+        }
+        *out = s;
+        return HNSW_OK;
+    }
+    void release(Slot* s) {
+        std::lock_guard<std::mutex> g(mu);
+        free.emplace_back(s);
+    }
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Scratch geometry per (ef bound): results, candidates and the visited
+// hash sized so that a typical traversal at that ef stays in shared memory.
+// Queries whose ef exceeds the fast kernel's 1024 go to the retry pass.
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc) {
+    constexpr uint32_t kSmemBudget = 220 * 1024;
+    SearchGeometry g;
+    g.ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_max, 32)));
+    g.cand_cap = 2 * g.ef_cap + 32;
+    uint32_t want = g.ef_cap * 48;
+    uint32_t h = 2048;
+    while (h < want && h < 32768) h <<= 1;
+    g.hash_cap = h;
+    while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget && g.hash_cap > 1024) g.hash_cap >>= 1;
+    const uint32_t bpw = geometry_bytes_per_warp(g, dp, dc);
+    g.warps_per_block = std::max<uint32_t>(1, std::min<uint32_t>(4, kSmemBudget / bpw));
+    return g;
+}
+
+}  // namespace
+
+struct hnsw_gpu_index {
+    int device = 0;
+    int num_sms = 148;
+    hnsw_index_info info{};
+    DeviceIndexView view;
+    DBuf vec, codes, norms, offset, adj0, upoff, adjU, keys, dead;
+    SlotPool slots;
+    bool counters = false;
+    std::mutex counters_mu;
+    std::vector<uint32_t> last_counters;
+    ~hnsw_gpu_index() {
+        DeviceGuard g(device);
+        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead}) b->release();
+        std::lock_guard<std::mutex> l(slots.mu);
+        slots.free.clear();
+    }
+};
+
+struct hnsw_gpu_brute {
+    int device = 0;
+    uint32_t n = 0, dim = 0, dp = 0;
+    int metric = 0;
+    DBuf base, keys;
+    SlotPool slots;
+    std::mutex mu;
+    DBuf qprep, part, okeys, odist, ocount, ostatus, q;
+    cudaStream_t stream = nullptr;
+    ~hnsw_gpu_brute() {
+        DeviceGuard g(device);
+        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q}) b->release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct hnsw_builder {
+    std::unique_ptr<Builder> b;
+};
+
+extern "C" {
+
+const char* hnsw_last_error(void) { return g_last_error.c_str(); }
+
+uint32_t hnsw_crc32(const uint8_t* bytes, size_t len) { return crc32(bytes, len); }
+
+static void fill_info(const HostIndex& ix, uint64_t required, hnsw_index_info* out) {
+    std::memset(out, 0, sizeof *out);
+    out->dim = ix.dim;
+    out->metric = uint32_t(ix.metric);
+    out->m = ix.params.m;
+    out->m0 = ix.params.m0;
+    out->ef_construction = ix.params.ef_construction;
+    out->quantized = ix.quantized ? 1 : 0;
+    out->nodes = uint32_t(ix.node_count());
+    out->live = uint32_t(ix.key_to_id.size());
+    out->top_level = ix.has_entry() ? ix.top_level() : 0;
+    out->entry = ix.has_entry() ? ix.entry_id() : kSentinel;
+    out->seed = ix.params.seed;
+    out->level_multiplier = ix.params.level_multiplier;
+    out->required_memory = required;
+}
+
+int hnsw_validate_bytes(const uint8_t* bytes, size_t len, uint64_t max_memory, hnsw_index_info* info) {
+    if (!bytes && len) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    static const uint8_t empty = 0;
+    HostIndex ix;
+    uint64_t required = 0;
+    Err e = load_index(bytes ? bytes : &empty, len, max_memory, &ix, &required);
+    if (e) return from_err(e);
+    if (info) fill_info(ix, required, info);
+    return HNSW_OK;
+}
+
+// Flattens a loaded index into the device layout (see device.hpp).
+static int upload(hnsw_gpu_index* gi, const HostIndex& ix) {
+    DeviceIndexView& v = gi->view;
+    const uint32_t n = uint32_t(ix.node_count());
+    v.n = n;
+    v.dim = ix.dim;
+    v.dp = round_up(ix.dim, 32);
+    v.dc = round_up(ix.dim, 16);
+    v.m = ix.params.m;
+    v.m0 = ix.params.m0;
+    v.mp = round_up(ix.params.m, 32);
+    v.m0p = round_up(ix.params.m0, 32);
+    v.metric = ix.metric;
+    v.quantized = ix.quantized ? 1 : 0;
+    v.scale = ix.q_scale;
+    v.live = uint32_t(ix.key_to_id.size());
+    v.entry = ix.has_entry() ? ix.entry_id() : kSentinel;
+    v.top = ix.has_entry() ? ix.top_level() : 0;
+    const size_t nn = std::max<size_t>(n, 1);
+    cudaStream_t st = nullptr;
+
+    CU(gi->vec.ensure(nn * v.dp * 4), "cudaMalloc vectors");
+    if (v.dp == v.dim) {
+        CU(cudaMemcpy(gi->vec.p, ix.vectors.data(), size_t(n) * v.dim * 4, cudaMemcpyHostToDevice), "copy vectors");
+    } else {
+        CU(cudaMemset(gi->vec.p, 0, nn * v.dp * 4), "memset vectors");
+        if (n)
+            CU(cudaMemcpy2D(gi->vec.p, size_t(v.dp) * 4, ix.vectors.data(), size_t(v.dim) * 4, size_t(v.dim) * 4, n,
+                            cudaMemcpyHostToDevice),
+               "copy vectors");
+    }
+    v.vec = gi->vec.as<float>();
+
+    // Layer-0 rows: ids then sentinel.
+    {
+        std::vector<uint32_t> rows(nn * v.m0p, kSentinel);
+        for (uint32_t id = 0; id < n; ++id) {
+            const uint32_t* blk = ix.block(id, 0);
+            std::copy(blk + 1, blk + 1 + blk[0], rows.begin() + size_t(id) * v.m0p);
+        }
+        CU(gi->adj0.ensure(rows.size() * 4), "cudaMalloc adj0");
+        CU(cudaMemcpy(gi->adj0.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice), "copy adj0");
+        v.adj0 = gi->adj0.as<uint32_t>();
+    }
+    // Upper layers: one block of mp ids per (node, layer >= 1).
+    {
+        std::vector<uint32_t> off(nn, 0);
+        size_t blocks = 0;
+        for (uint32_t id = 0; id < n; ++id) {
+            off[id] = uint32_t(blocks);
+            blocks += ix.levels[id];
+        }
+        std::vector<uint32_t> adj(std::max<size_t>(blocks, 1) * v.mp, kSentinel);
+        for (uint32_t id = 0; id < n; ++id)
+            for (unsigned layer = 1; layer <= ix.levels[id]; ++layer) {
+                const uint32_t* blk = ix.block(id, layer);
+                std::copy(blk + 1, blk + 1 + blk[0], adj.begin() + size_t(off[id] + layer - 1) * v.mp);
+            }
+        CU(gi->upoff.ensure(off.size() * 4), "cudaMalloc up_off");
+        CU(cudaMemcpy(gi->upoff.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice), "copy up_off");
+        CU(gi->adjU.ensure(adj.size() * 4), "cudaMalloc adjU");
+        CU(cudaMemcpy(gi->adjU.p, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice), "copy adjU");
+        v.up_off = gi->upoff.as<uint32_t>();
+        v.adjU = gi->adjU.as<uint32_t>();
+    }
+    // Keys and tombstones.
+    {
+        CU(gi->keys.ensure(nn * 8), "cudaMalloc keys");
+        if (n) CU(cudaMemcpy(gi->keys.p, ix.keys.data(), size_t(n) * 8, cudaMemcpyHostToDevice), "copy keys");
+        v.keys = gi->keys.as<uint64_t>();
+        bool ids = true;
+        for (uint32_t id = 0; id < n && ids; ++id) ids = ix.keys[id] == id;
+        v.keys_are_ids = ids ? 1 : 0;
+        std::vector<uint32_t> dead((nn + 31) / 32, 0);
+        for (uint32_t id = 0; id < n; ++id)
+            if (ix.deleted[id]) dead[id >> 5] |= 1u << (id & 31);
+        CU(gi->dead.ensure(dead.size() * 4), "cudaMalloc dead");
+        CU(cudaMemcpy(gi->dead.p, dead.data(), dead.size() * 4, cudaMemcpyHostToDevice), "copy dead");
+        v.dead = gi->dead.as<uint32_t>();
+    }
+    // Quantizer: offsets, then codes derived on the device.
+    if (ix.quantized) {
+        std::vector<float> off(v.dp, 0.0f);
+        std::copy(ix.q_offset.begin(), ix.q_offset.end(), off.begin());
+        CU(gi->offset.ensure(off.size() * 4), "cudaMalloc offsets");
+        CU(cudaMemcpy(gi->offset.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice), "copy offsets");
+        CU(gi->codes.ensure(nn * v.dc), "cudaMalloc codes");
+        CU(gi->norms.ensure(nn * 4), "cudaMalloc code norms");
+        CU(launch_encode_codes(v.vec, n, v.dim, v.dp, v.dc, gi->offset.as<float>(), v.scale, gi->codes.as<int8_t>(),
+                               gi->norms.as<int32_t>(), st),
+           "encode codes");
+        CU(cudaDeviceSynchronize(), "encode codes");
+        v.q_offset = gi->offset.as<float>();
+        v.codes = gi->codes.as<int8_t>();
+        v.code_norm = gi->norms.as<int32_t>();
+    }
+    gi->info.device_bytes = gi->vec.bytes + gi->adj0.bytes + gi->upoff.bytes + gi->adjU.bytes + gi->keys.bytes +
+                            gi->dead.bytes + gi->offset.bytes + gi->codes.bytes + gi->norms.bytes;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_index_open(const uint8_t* bytes, size_t len, uint64_t max_memory, int device, hnsw_gpu_index** out) {
+    if (!out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (!bytes && len) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    static const uint8_t empty = 0;
+    HostIndex ix;
+    uint64_t required = 0;
+    Err e = load_index(bytes ? bytes : &empty, len, max_memory, &ix, &required);
+    if (e) return from_err(e);
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0)
+        return set_error(HNSW_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
+    if (device < 0 || device >= ndev) return set_error(HNSW_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (ix.dim > 8192) return set_error(HNSW_ERR_INVALID_ARGUMENT, "dimension above the device path's limit of 8192");
+    DeviceGuard dg(device);
+    std::unique_ptr<hnsw_gpu_index> gi(new hnsw_gpu_index());
+    gi->device = device;
+    gi->slots.device = device;
+    cudaDeviceGetAttribute(&gi->num_sms, cudaDevAttrMultiProcessorCount, device);
+    fill_info(ix, required, &gi->info);
+    int s = upload(gi.get(), ix);
+    if (s != HNSW_OK) return s;
+    *out = gi.release();
+    return HNSW_OK;
+}
+
+void hnsw_gpu_index_close(hnsw_gpu_index* index) { delete index; }
+
+int hnsw_gpu_index_info(const hnsw_gpu_index* index, hnsw_index_info* out) {
+    if (!index || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    *out = index->info;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_set_tombstones(hnsw_gpu_index* index, const uint8_t* deleted, size_t nodes) {
+    if (!index || (!deleted && nodes)) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (nodes != index->view.n) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "tombstone column length != node count");
+    DeviceGuard dg(index->device);
+    std::vector<uint32_t> dead((std::max<size_t>(nodes, 1) + 31) / 32, 0);
+    uint32_t live = 0;
+    for (size_t id = 0; id < nodes; ++id) {
+        if (deleted[id] > 1) return set_error(HNSW_ERR_INVALID_ARGUMENT, "tombstone flags must be 0 or 1");
+        if (deleted[id]) dead[id >> 5] |= 1u << (id & 31);
+        else ++live;
+    }
+    CU(cudaMemcpy(index->dead.p, dead.data(), dead.size() * 4, cudaMemcpyHostToDevice), "copy tombstones");
+    index->view.live = live;
+    index->info.live = live;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_set_counters(hnsw_gpu_index* index, int enabled) {
+    if (!index) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null index");
+    index->counters = enabled != 0;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq) {
+    if (!index || !host_out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(index->counters_mu);
+    if (index->last_counters.size() < nq * 4) return set_error(HNSW_ERR_INVALID_ARGUMENT, "no counters for that many queries");
+    std::memcpy(host_out, index->last_counters.data(), nq * 16);
+    return HNSW_OK;
+}
+
+// Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
+static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
+    const uint32_t warps = 64;
+    const uint32_t cand_cap = std::max<uint32_t>(1u << 16, 4 * ef_cap);
+    const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
+    CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
+    CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
+    CU(s->g_visited.ensure(size_t(warps) * words * 4), "cudaMalloc retry visited");
+    s->g_warps = warps;
+    s->g_ef_cap = ef_cap;
+    s->g_cand_cap = cand_cap;
+    s->g_words = words;
+    return HNSW_OK;
+}
+
+// Enqueues one search on `stream` with device pointers. ef_max bounds every
+// per-query max(ef, k) of the batch.
+static int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
+                          const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
+                          uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
+                          uint32_t out_stride, cudaStream_t stream) {
+    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc);
+    CU(s->work.ensure(16), "cudaMalloc work counters");
+    CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
+    CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
+    int r = ensure_retry(gi, s, std::max(geo.ef_cap, round_up(ef_max, 32)));
+    if (r != HNSW_OK) return r;
+    SearchArgs a;
+    a.ix = gi->view;
+    a.queries = d_q;
+    a.nq = uint32_t(nq);
+    a.k = o.k;
+    a.ef = o.ef;
+    a.ks = d_ks;
+    a.efs = d_efs;
+    a.quantized = o.quantized;
+    a.filter_bits = d_fbits;
+    a.filter_nbits = o.filter_nbits;
+    a.filter_stride = o.filter_stride;
+    a.filter_used = d_fused;
+    a.out_keys = d_keys;
+    a.out_dist = d_dist;
+    a.out_count = d_count;
+    a.out_status = d_status;
+    a.out_stride = out_stride;
+    if (gi->counters) {
+        CU(s->counters.ensure(std::max<size_t>(nq, 1) * 16), "cudaMalloc counters");
+        a.counters = s->counters.as<uint32_t>();
+    }
+    a.work_next = s->work.as<uint32_t>();
+    a.overflow_count = s->work.as<uint32_t>() + 1;
+    a.overflow_list = s->overflow.as<uint32_t>();
+    a.persistent = o.mode == HNSW_MODE_PERSISTENT ? 1 : 0;
+    a.g_results = s->g_results.as<uint64_t>();
+    a.g_cands = s->g_cands.as<uint64_t>();
+    a.g_visited = s->g_visited.as<uint32_t>();
+    a.g_ef_cap = s->g_ef_cap;
+    a.g_cand_cap = s->g_cand_cap;
+    a.g_visited_words = s->g_words;
+    CU(launch_search(a, geo, gi->num_sms, stream), "search kernel");
+    CU(launch_search_retry(a, s->g_warps, stream), "search retry kernel");
+    return HNSW_OK;
+}
+
+int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim,
+                          const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                          int32_t* out_status) {
+    if (!gi || !opts) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != gi->view.dim) {
+        return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(gi->view.dim) +
+                                                          ", got " + std::to_string(dim));
+    }
+    if (nq == 0) return HNSW_OK;
+    if (!queries || !out_keys || !out_dist || !out_count || !out_status)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    if (nq > 0x7FFFFFFFu) return set_error(HNSW_ERR_INVALID_ARGUMENT, "batch too large");
+    const hnsw_search_opts& o = *opts;
+    uint32_t kmax = o.k, efmax = o.ef;
+    if (o.ks)
+        for (size_t i = 0; i < nq; ++i) kmax = std::max(kmax, o.ks[i]);
+    else
+        kmax = o.k;
+    if (o.efs)
+        for (size_t i = 0; i < nq; ++i) efmax = std::max(efmax, o.efs[i]);
+    uint32_t ef_bound = std::max(kmax, efmax);
+    if (ef_bound > 65536) return set_error(HNSW_ERR_INVALID_ARGUMENT, "ef and k above 65536 are not supported on the device");
+    const uint32_t stride = o.out_stride ? o.out_stride : std::max<uint32_t>(kmax, 1);
+    if (stride < kmax) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out_stride below k");
+    if (o.filter_bits && o.filter_nbits == 0) return set_error(HNSW_ERR_INVALID_ARGUMENT, "filter bitmap has no bits");
+    DeviceGuard dg(gi->device);
+    Slot* s = nullptr;
+    int r = gi->slots.acquire(&s);
+    if (r != HNSW_OK) return r;
+    std::unique_ptr<Slot, std::function<void(Slot*)>> hold(s, [gi](Slot* p) { gi->slots.release(p); });
+    cudaStream_t st = s->stream;
+    CU(s->q.ensure(nq * dim * 4), "cudaMalloc queries");
+    CU(cudaMemcpyAsync(s->q.p, queries, nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    const uint32_t* d_ks = nullptr;
+    const uint32_t* d_efs = nullptr;
+    const uint64_t* d_fb = nullptr;
+    const uint8_t* d_fu = nullptr;
+    if (o.ks) {
+        CU(s->ks.ensure(nq * 4), "cudaMalloc ks");
+        CU(cudaMemcpyAsync(s->ks.p, o.ks, nq * 4, cudaMemcpyHostToDevice, st), "copy ks");
+        d_ks = s->ks.as<uint32_t>();
+    }
+    if (o.efs) {
+        CU(s->efs.ensure(nq * 4), "cudaMalloc efs");
+        CU(cudaMemcpyAsync(s->efs.p, o.efs, nq * 4, cudaMemcpyHostToDevice, st), "copy efs");
+        d_efs = s->efs.as<uint32_t>();
+    }
+    if (o.filter_bits) {
+        const uint64_t words = (o.filter_nbits + 63) / 64;
+        const uint64_t total = o.filter_stride ? o.filter_stride * (nq - 1) + words : words;
+        CU(s->fbits.ensure(total * 8), "cudaMalloc filter");
+        CU(cudaMemcpyAsync(s->fbits.p, o.filter_bits, total * 8, cudaMemcpyHostToDevice, st), "copy filter");
+        d_fb = s->fbits.as<uint64_t>();
+        if (o.filter_used) {
+            CU(s->fused.ensure(nq), "cudaMalloc filter flags");
+            CU(cudaMemcpyAsync(s->fused.p, o.filter_used, nq, cudaMemcpyHostToDevice, st), "copy filter flags");
+            d_fu = s->fused.as<uint8_t>();
+        }
+    }
+    CU(s->okeys.ensure(nq * stride * 8), "cudaMalloc out keys");
+    CU(s->odist.ensure(nq * stride * 4), "cudaMalloc out dist");
+    CU(s->ocount.ensure(nq * 4), "cudaMalloc out count");
+    CU(s->ostatus.ensure(nq * 4), "cudaMalloc out status");
+    r = enqueue_search(gi, s, s->q.as<float>(), nq, o, d_ks, d_efs, d_fb, d_fu, s->okeys.as<uint64_t>(),
+                       s->odist.as<float>(), s->ocount.as<uint32_t>(), s->ostatus.as<int32_t>(), ef_bound, stride, st);
+    if (r != HNSW_OK) return r;
+    CU(cudaMemcpyAsync(out_count, s->ocount.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    CU(cudaMemcpyAsync(out_status, s->ostatus.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
+    CU(cudaMemcpyAsync(out_keys, s->okeys.p, nq * stride * 8, cudaMemcpyDeviceToHost, st), "copy keys");
+    CU(cudaMemcpyAsync(out_dist, s->odist.p, nq * stride * 4, cudaMemcpyDeviceToHost, st), "copy distances");
+    CU(cudaStreamSynchronize(st), "search");
+    if (gi->counters) {
+        std::lock_guard<std::mutex> g(gi->counters_mu);
+        gi->last_counters.resize(nq * 4);
+        CU(cudaMemcpy(gi->last_counters.data(), s->counters.p, nq * 16, cudaMemcpyDeviceToHost), "copy counters");
+    }
+    for (size_t i = 0; i < nq; ++i)
+        if (out_status[i] != HNSW_OK) {
+            const int32_t code = out_status[i];
+            std::string msg = code == HNSW_ERR_NON_FINITE_VECTOR ? "vector contains NaN or infinite values"
+                              : code == HNSW_ERR_ZERO_VECTOR     ? "zero vector has no direction under cosine distance"
+                              : code == HNSW_ERR_QUANTIZATION_DISABLED
+                                  ? "quantized search requested but quantization is not enabled"
+                              : code == HNSW_ERR_SCRATCH_OVERFLOW ? "a query outgrew the device scratch"
+                                                                  : "query failed";
+            return set_error(code, msg);
+        }
+    return HNSW_OK;
+}
+
+int hnsw_gpu_search_batch_device(hnsw_gpu_index* gi, const float* d_queries, size_t nq, size_t dim,
+                                 const hnsw_search_opts* o, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
+                                 int32_t* d_status, void* stream) {
+    if (!gi || !o) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != gi->view.dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return HNSW_OK;
+    const uint32_t ef_bound = std::max(o->k, o->ef);
+    const uint32_t stride = o->out_stride ? o->out_stride : std::max<uint32_t>(o->k, 1);
+    DeviceGuard dg(gi->device);
+    Slot* s = nullptr;
+    int r = gi->slots.acquire(&s);
+    if (r != HNSW_OK) return r;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    r = enqueue_search(gi, s, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used, d_keys, d_dist, d_count,
+                       d_status, ef_bound, stride, st);
+    // The slot's buffers are in use until the stream reaches this point.
+    cudaStreamSynchronize(st);
+    gi->slots.release(s);
+    return r;
+}
+
+// ------------------------------------------------------------------------
+// Brute force
+// ------------------------------------------------------------------------
+int hnsw_gpu_brute_open(const float* vectors, const uint64_t* keys, size_t n, size_t dim, int metric, int device,
+                        hnsw_gpu_brute** out) {
+    if (!out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (dim == 0 || dim > kMaxDim) return set_error(HNSW_ERR_INVALID_DIMENSION, "invalid dimension");
+    if (metric < 0 || metric > 2) return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown metric");
+    if (n && !vectors) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null vectors");
+    if (n > 0xFFFFFFF0ull) return set_error(HNSW_ERR_CAPACITY_EXCEEDED, "too many vectors");
+    // insert_batch: prepare every row, keys unique (src/brute.rs:103-115).
+    const uint32_t dp = round_up(uint32_t(dim), 32);
+    std::vector<float> rows(std::max<size_t>(n, 1) * dp, 0.0f);
+    for (size_t i = 0; i < n; ++i) {
+        double norm;
+        int s = check_vector(vectors + i * dim, dim, &norm);
+        if (s) return set_error(s, "vector contains NaN or infinite values");
+        if (metric == HNSW_METRIC_COSINE) {
+            if (norm == 0.0) return set_error(HNSW_ERR_ZERO_VECTOR, "zero vector has no direction under cosine distance");
+            double inv = 1.0 / std::sqrt(norm);
+            for (size_t j = 0; j < dim; ++j) rows[i * dp + j] = float(double(vectors[i * dim + j]) * inv);
+        } else {
+            std::memcpy(&rows[i * dp], vectors + i * dim, dim * 4);
+        }
+    }
+    std::vector<uint64_t> kv(std::max<size_t>(n, 1));
+    for (size_t i = 0; i < n; ++i) kv[i] = keys ? keys[i] : uint64_t(i);
+    if (keys) {
+        std::vector<uint64_t> sorted(kv.begin(), kv.begin() + n);
+        std::sort(sorted.begin(), sorted.end());
+        auto it = std::adjacent_find(sorted.begin(), sorted.end());
+        if (it != sorted.end()) return set_error(HNSW_ERR_DUPLICATE_KEY, "key " + std::to_string(*it) + " is already present");
+    }
+    DeviceGuard dg(device);
+    std::unique_ptr<hnsw_gpu_brute> b(new hnsw_gpu_brute());
+    b->device = device;
+    b->n = uint32_t(n);
+    b->dim = uint32_t(dim);
+    b->dp = dp;
+    b->metric = metric;
+    CU(b->base.ensure(rows.size() * 4), "cudaMalloc base");
+    CU(cudaMemcpy(b->base.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice), "copy base");
+    CU(b->keys.ensure(kv.size() * 8), "cudaMalloc keys");
+    CU(cudaMemcpy(b->keys.p, kv.data(), kv.size() * 8, cudaMemcpyHostToDevice), "copy keys");
+    CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+    *out = b.release();
+    return HNSW_OK;
+}
+
+void hnsw_gpu_brute_close(hnsw_gpu_brute* brute) { delete brute; }
+
+int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
+                                int precision, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                                int32_t* out_status) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return HNSW_OK;
+    if (precision != HNSW_PRECISION_FP32)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "precision not available in this build");
+    if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
+    std::lock_guard<std::mutex> lock(b->mu);
+    DeviceGuard dg(b->device);
+    cudaStream_t st = b->stream;
+    const uint32_t kk = std::max<uint32_t>(k, 1);
+    BruteArgs a;
+    a.base = b->base.as<float>();
+    a.keys = b->keys.as<uint64_t>();
+    a.n = b->n;
+    a.dim = b->dim;
+    a.dp = b->dp;
+    a.metric = b->metric;
+    a.nq = uint32_t(nq);
+    a.k = k;
+    a.tiles = std::max<uint32_t>(1, std::min<uint32_t>(64, (b->n + 8191) / 8192));
+    CU(b->q.ensure(nq * dim * 4), "cudaMalloc queries");
+    CU(cudaMemcpyAsync(b->q.p, queries, nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    CU(b->qprep.ensure(nq * b->dp * 4), "cudaMalloc qprep");
+    CU(b->part.ensure(size_t(nq) * a.tiles * kk * 8), "cudaMalloc partial");
+    CU(b->okeys.ensure(nq * kk * 8), "cudaMalloc out keys");
+    CU(b->odist.ensure(nq * kk * 4), "cudaMalloc out dist");
+    CU(b->ocount.ensure(nq * 4), "cudaMalloc out count");
+    CU(b->ostatus.ensure(nq * 4), "cudaMalloc out status");
+    a.queries = b->q.as<float>();
+    a.qprep = b->qprep.as<float>();
+    a.part = b->part.as<uint64_t>();
+    a.out_keys = b->okeys.as<uint64_t>();
+    a.out_dist = b->odist.as<float>();
+    a.out_count = b->ocount.as<uint32_t>();
+    a.out_status = b->ostatus.as<int32_t>();
+    CU(launch_brute_fp32(a, st), "brute kernel");
+    CU(cudaMemcpyAsync(out_count, b->ocount.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    CU(cudaMemcpyAsync(out_status, b->ostatus.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
+    if (k) {
+        CU(cudaMemcpyAsync(out_keys, b->okeys.p, nq * size_t(k) * 8, cudaMemcpyDeviceToHost, st), "copy keys");
+        CU(cudaMemcpyAsync(out_dist, b->odist.p, nq * size_t(k) * 4, cudaMemcpyDeviceToHost, st), "copy distances");
+    }
+    CU(cudaStreamSynchronize(st), "brute search");
+    for (size_t i = 0; i < nq; ++i)
+        if (out_status[i] != HNSW_OK) return set_error(out_status[i], "query failed validation");
+    return HNSW_OK;
+}
+
+// ------------------------------------------------------------------------
+// Builder and synthetic data
+// ------------------------------------------------------------------------
+void hnsw_params_default(uint32_t m, hnsw_params* out) {
+    Params p = default_params(m);
+    out->m = p.m;
+    out->m0 = p.m0;
+    out->ef_construction = p.ef_construction;
+    out->level_multiplier = p.level_multiplier;
+    out->selection = p.selection;
+    out->extend_candidates = p.extend_candidates;
+    out->keep_pruned = p.keep_pruned;
+    out->seed = p.seed;
+}
+
+int hnsw_builder_new(size_t dim, int metric, const hnsw_params* params, hnsw_builder** out) {
+    if (!out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null output handle");
+    *out = nullptr;
+    if (dim == 0 || dim > kMaxDim)
+        return set_error(HNSW_ERR_INVALID_DIMENSION,
+                         "invalid dimension " + std::to_string(dim) + ": must be between 1 and 65536");
+    if (metric < 0 || metric > 2) return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown metric");
+    Params p = params ? Params{} : default_params(16);
+    if (params) {
+        p.m = params->m;
+        p.m0 = params->m0;
+        p.ef_construction = params->ef_construction;
+        p.level_multiplier = params->level_multiplier;
+        p.selection = params->selection ? 1 : 0;
+        p.extend_candidates = params->extend_candidates != 0;
+        p.keep_pruned = params->keep_pruned != 0;
+        p.seed = params->seed;
+    }
+    const char* bad = validate_params(p);
+    if (*bad) return set_error(HNSW_ERR_INVALID_PARAMETER, std::string("invalid parameter `") + bad + "`");
+    auto* h = new hnsw_builder();
+    h->b.reset(new Builder(uint32_t(dim), metric, p));
+    *out = h;
+    return HNSW_OK;
+}
+
+void hnsw_builder_free(hnsw_builder* b) { delete b; }
+
+int hnsw_builder_insert(hnsw_builder* b, uint64_t key, const float* v, size_t dim) {
+    if (!b || !v) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != b->b->index().dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    return from_err(b->b->insert(key, v));
+}
+
+int hnsw_builder_insert_batch(hnsw_builder* b, const uint64_t* keys, const float* v, size_t n, size_t dim, int threads) {
+    if (!b || (n && (!keys || !v))) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != b->b->index().dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    return from_err(b->b->insert_batch(keys, v, n, threads));
+}
+
+int hnsw_builder_remove(hnsw_builder* b, uint64_t key, int* removed) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    bool r = b->b->remove(key);
+    if (removed) *removed = r ? 1 : 0;
+    return HNSW_OK;
+}
+
+int hnsw_builder_enable_quantization(hnsw_builder* b) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    b->b->enable_quantization();
+    return HNSW_OK;
+}
+
+int hnsw_builder_to_bytes(const hnsw_builder* b, uint8_t** out, size_t* len) {
+    if (!b || !out || !len) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint8_t> bytes = write_index(b->b->index());
+    auto* p = static_cast<uint8_t*>(std::malloc(std::max<size_t>(bytes.size(), 1)));
+    if (!p) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out of host memory");
+    std::memcpy(p, bytes.data(), bytes.size());
+    *out = p;
+    *len = bytes.size();
+    return HNSW_OK;
+}
+
+void hnsw_bytes_free(uint8_t* p) { std::free(p); }
+
+void hnsw_synthetic_gaussian(size_t nb, size_t nq, size_t dim, uint64_t seed, float* base, float* queries) {
+    synthetic_gaussian(nb, nq, dim, seed, base, queries);
+}
+
+void hnsw_synthetic_mixture(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t seed,
+                            float* base, float* queries) {
+    synthetic_mixture(nb, nq, dim, clusters, sigma, seed, base, queries);
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// Device-resident index and the launch interface of the search kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace hnswgpu {
+
+constexpr uint32_t kSentinel = 0xFFFFFFFFu;
+
+// Flattened HNSW index in HBM. Rows of vectors are padded to a multiple of 32
+// floats (128 B), int8 code rows to a multiple of 16 bytes (zero fill, so
+// integer dot products and norms are unchanged), neighbor rows to a multiple
+// of 32 ids with kSentinel after the live prefix.
+struct DeviceIndexView {
+    uint32_t n = 0, dim = 0, dp = 0, dc = 0;
+    uint32_t m = 0, m0 = 0, mp = 0, m0p = 0;
+    uint32_t top = 0, entry = kSentinel, live = 0;
+    int metric = 0;
+    int quantized = 0;
+    int keys_are_ids = 0;
+    float scale = 1.0f;
+    const float* vec = nullptr;        // n * dp
+    const int8_t* codes = nullptr;     // n * dc
+    const int32_t* code_norm = nullptr;// n  (sum of squared codes)
+    const float* q_offset = nullptr;   // dp (quantizer offsets)
+    const uint32_t* adj0 = nullptr;    // n * m0p
+    const uint32_t* up_off = nullptr;  // n: block index of the node's layer-1 list
+    const uint32_t* adjU = nullptr;    // blocks * mp
+    const uint64_t* keys = nullptr;    // n
+    const uint32_t* dead = nullptr;    // ceil(n/32) tombstone bitmap
+};
+
+// Per-launch scratch geometry (picked by the launcher per call).
+struct SearchGeometry {
+    uint32_t ef_cap = 64;     // results capacity (>= every ef of the batch)
+    uint32_t cand_cap = 160;  // candidate queue capacity
+    uint32_t hash_cap = 4096; // visited hash entries (power of two)
+    uint32_t warps_per_block = 4;
+    uint32_t bytes_per_warp = 0;
+};
+
+struct SearchArgs {
+    DeviceIndexView ix;
+    const float* queries = nullptr;  // nq * dim
+    uint32_t nq = 0;
+    uint32_t k = 10, ef = 64;
+    const uint32_t* ks = nullptr;
+    const uint32_t* efs = nullptr;
+    int quantized = 0;
+    const uint64_t* filter_bits = nullptr;
+    uint64_t filter_nbits = 0;
+    uint64_t filter_stride = 0;
+    const uint8_t* filter_used = nullptr;
+    uint64_t* out_keys = nullptr;
+    float* out_dist = nullptr;
+    uint32_t* out_count = nullptr;
+    int32_t* out_status = nullptr;
+    uint32_t out_stride = 10;
+    uint32_t* counters = nullptr;  // optional nq * 4
+    // Work distribution: persistent mode drains work_next; the overflow
+    // list collects queries that outgrew the fast scratch.
+    uint32_t* work_next = nullptr;
+    uint32_t* overflow_list = nullptr;
+    uint32_t* overflow_count = nullptr;
+    int persistent = 0;
+    // Fallback workspaces in global memory (retry kernel only).
+    uint64_t* g_results = nullptr;
+    uint64_t* g_cands = nullptr;
+    uint32_t* g_visited = nullptr;  // bitmap, ceil(n/32) words per warp
+    uint32_t g_ef_cap = 0, g_cand_cap = 0;
+    uint64_t g_visited_words = 0;
+};
+
+// Launches the fast search (plain or persistent) followed by the retry pass
+// for queries that overflowed. All on `stream`.
+cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo, int num_sms, cudaStream_t stream);
+// Retry pass only (global-memory scratch); `warps` warps.
+cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream);
+// Scratch bytes per warp of a geometry for dimension dp (floats) / dc (bytes).
+uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t dc);
+
+// Derives int8 codes and their squared norms from offsets and scale
+// (ScalarQuantizer::encode_into, src/quantization.rs:73-81).
+cudaError_t launch_encode_codes(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, uint32_t dc,
+                                const float* offset, float scale, int8_t* codes, int32_t* norms,
+                                cudaStream_t stream);
+
+// Exact FP32 brute force in the reference kernel order (K1 per row) with a
+// per-query top-k merge.
+struct BruteArgs {
+    const float* base = nullptr;  // n * dp, prepared
+    const uint64_t* keys = nullptr;
+    uint32_t n = 0, dim = 0, dp = 0;
+    int metric = 0;
+    const float* queries = nullptr;  // nq * dim raw
+    uint32_t nq = 0, k = 10;
+    uint64_t* out_keys = nullptr;
+    float* out_dist = nullptr;
+    uint32_t* out_count = nullptr;
+    int32_t* out_status = nullptr;
+    // scratch
+    float* qprep = nullptr;         // nq * dp
+    uint64_t* part = nullptr;       // nq * tiles * k partial top-k (packed dist key, row)
+    uint32_t tiles = 0;
+};
+cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream);
+
+}  // namespace hnswgpu

@@ -1,0 +1,596 @@
+// HNSW query traversal on sm_100a: one warp per query.
+//
+// Restates, with identical results, HnswIndex::search_impl / search_graph /
+// greedy_closest / search_layer (src/hnsw/mod.rs:460-511,
+// src/hnsw/search.rs:49-161):
+//   * distances in the AVX2 summation order (common.cuh), so every
+//     comparison sees the reference's bits;
+//   * the layer-0 beam processes each neighbor list in list order, applying
+//     the visited test, the `improves` rule (strict IEEE <) and admission
+//     exactly as the sequential loop does;
+//   * heaps are sorted arrays ordered by (total_cmp distance, id), the
+//     reference's Candidate order; the results max is the array's last entry.
+// Candidates worse than the worst result once ef results exist can never be
+// expanded (the loop would stop at them), so they are pruned when the
+// candidate array fills; that does not change the result.
+//
+// Scratch per warp: the prepared query (and its int8 code), the results
+// array, the candidate array, and an open-addressing visited hash over node
+// ids (exact: ids are stored, not hashed away). A query that outgrows the
+// warp's scratch is pushed to an overflow list and re-run by a retry kernel
+// whose scratch lives in global memory (visited bitmap over all nodes).
+#include "common.cuh"
+#include "device.hpp"
+
+namespace hnswgpu {
+namespace dev {
+
+enum : int32_t { ST_OK = 0, ST_NON_FINITE = 3, ST_ZERO = 4, ST_QDISABLED = 7, ST_OVERFLOW = 25 };
+
+struct Counters {
+    uint32_t dist0 = 0, exp0 = 0, dist_up = 0, exp_up = 0;
+};
+
+// Per-warp workspace (shared memory in the fast kernel, global memory in
+// the retry kernel).
+struct Ws {
+    float* qf;         // dp floats: prepared query
+    int8_t* qc;        // dc bytes: query code
+    uint64_t* R;       // ef_cap + 1
+    uint64_t* C;       // cand_cap + 1
+    uint32_t* H;       // hash_cap entries, or a bitmap when bitmap_mode
+    uint32_t* fr;      // 32: fresh neighbor positions
+    float* fd;         // 32: distances of fresh neighbors
+    uint32_t ef_cap, cand_cap, hash_cap;
+    bool bitmap_mode;  // H is a bitmap over node ids (retry kernel)
+    uint32_t bitmap_words;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Inserts x into the ascending array A[lo, hi) (capacity permitting one more
+// entry). Returns the insertion position.
+__device__ __forceinline__ uint32_t sorted_insert(uint64_t* A, uint32_t lo, uint32_t hi, uint64_t x) {
+    const int lane = lane_id();
+    uint32_t pos = lo;
+    for (uint32_t base = lo; base < hi; base += 32) {
+        uint32_t i = base + lane;
+        bool lt = i < hi && A[i] < x;
+        pos += __popc(__ballot_sync(kFull, lt));
+    }
+    // Shift [pos, hi) up by one, highest chunk first.
+    if (hi > pos) {
+        uint32_t n = hi - pos;
+        for (int c = int((n - 1) >> 5); c >= 0; --c) {
+            uint32_t i = pos + uint32_t(c) * 32 + lane;
+            bool mv = i < hi;
+            uint64_t v = mv ? A[i] : 0;
+            __syncwarp();
+            if (mv) A[i + 1] = v;
+            __syncwarp();
+        }
+    }
+    if (lane == 0) A[pos] = x;
+    __syncwarp();
+    return pos;
+}
+
+// Visited test-and-set. Returns true if id was not visited before.
+// *full is set when the hash passes its load limit.
+__device__ __forceinline__ bool visit(Ws& w, uint32_t id) {
+    if (w.bitmap_mode) {
+        uint32_t bit = 1u << (id & 31);
+        uint32_t old = atomicOr(&w.H[id >> 5], bit);
+        return (old & bit) == 0;
+    }
+    const uint32_t mask = w.hash_cap - 1;
+    uint32_t h = uint32_t((uint64_t(id * 0x9E3779B1u) * w.hash_cap) >> 32);
+    for (uint32_t probe = 0; probe < w.hash_cap; ++probe) {
+        uint32_t old = atomicCAS(&w.H[h], kEmpty, id);
+        if (old == kEmpty) return true;
+        if (old == id) return false;
+        h = (h + 1) & mask;
+    }
+    return true;  // unreachable while the load limit holds
+}
+
+struct QueryCtx {
+    const SearchArgs* a;
+    Ws* w;
+    uint32_t qi;
+    int metric;
+    bool quant;
+    float s2;
+    int qnorm;  // squared norm of the query code (L2 on codes)
+    bool use_filter;
+    const uint64_t* fbits;
+    uint64_t fnbits;
+    Counters cnt;
+};
+
+__device__ __forceinline__ bool admit(const QueryCtx& c, uint32_t id) {
+    const DeviceIndexView& ix = c.a->ix;
+    if ((__ldg(ix.dead + (id >> 5)) >> (id & 31)) & 1u) return false;
+    if (!c.use_filter) return true;
+    uint64_t key = ix.keys_are_ids ? uint64_t(id) : __ldg(ix.keys + id);
+    return key < c.fnbits && ((__ldg(c.fbits + (key >> 6)) >> (key & 63)) & 1ull);
+}
+
+// Distance from the query to node `id` for the group of 8 lanes (valid in
+// every lane of the group). All 32 lanes call; `id` may differ per group.
+__device__ __forceinline__ float group_distance(const QueryCtx& c, uint32_t id, int g8) {
+    const DeviceIndexView& ix = c.a->ix;
+    if (c.quant) {
+        int dot = group_i8dot(ix.codes + size_t(id) * ix.dc, c.w->qc, int(ix.dc), g8);
+        long long l2 = 0;
+        if (c.metric == 0) l2 = (long long)c.qnorm + (long long)__ldg(ix.code_norm + id) - 2ll * (long long)dot;
+        return sq_distance(c.metric, dot, l2, c.s2);
+    }
+    const float* row = ix.vec + size_t(id) * ix.dp;
+    float s = c.metric == 0 ? group_sum<true>(row, c.w->qf, int(ix.dim), g8)
+                            : group_sum<false>(row, c.w->qf, int(ix.dim), g8);
+    s = __shfl_sync(kFull, s, (lane_id() & ~7));
+    return metric_from_sum(c.metric, s);
+}
+
+// Exact f32 distance (for the re-rank), valid in every lane of the group.
+__device__ __forceinline__ float group_exact(const QueryCtx& c, uint32_t id, int g8) {
+    const DeviceIndexView& ix = c.a->ix;
+    const float* row = ix.vec + size_t(id) * ix.dp;
+    float s = c.metric == 0 ? group_sum<true>(row, c.w->qf, int(ix.dim), g8)
+                            : group_sum<false>(row, c.w->qf, int(ix.dim), g8);
+    s = __shfl_sync(kFull, s, (lane_id() & ~7));
+    return metric_from_sum(c.metric, s);
+}
+
+// Computes distances for the neighbors at positions fr[0..nf) of the
+// current chunk (ids in lane order `ids`), writing fd[pos].
+__device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uint32_t F) {
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    const int g = lane >> 3, g8 = lane & 7;
+    // Ranks of fresh lanes -> compact list of positions.
+    if ((F >> lane) & 1u) w.fr[__popc(F & ((1u << lane) - 1u))] = uint32_t(lane);
+    __syncwarp();
+    const uint32_t nf = __popc(F);
+    for (uint32_t r = 0; r < nf; r += 4) {
+        uint32_t slot = r + uint32_t(g);
+        bool active = slot < nf;
+        uint32_t pos = active ? w.fr[slot] : w.fr[0];
+        uint32_t id = __shfl_sync(kFull, my_id, int(pos));
+        float d = group_distance(c, id, g8);
+        if (active && g8 == 0) w.fd[pos] = d;
+    }
+    __syncwarp();
+}
+
+// greedy_closest (src/hnsw/search.rs:49-68) on an upper layer.
+__device__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    for (;;) {
+        const uint32_t from = pid(best);
+        const uint32_t* blk = ix.adjU + size_t(__ldg(ix.up_off + from) + (layer - 1)) * ix.mp;
+        c.cnt.exp_up++;
+        float bd = pdist(best);
+        uint32_t bid = from;
+        for (uint32_t base = 0; base < ix.m; base += 32) {
+            uint32_t id = (base + lane < ix.m) ? __ldg(blk + base + lane) : kEmpty;
+            uint32_t V = __ballot_sync(kFull, id != kEmpty);
+            if (V == 0) break;
+            chunk_distances(c, id, V);
+            c.cnt.dist_up += __popc(V);
+            // First strict minimum in list order (IEEE comparison, as d < best.distance).
+            float d = ((V >> lane) & 1u) ? w.fd[lane] : __int_as_float(0x7f800000);
+            int idx = lane;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                float od = __shfl_down_sync(kFull, d, off);
+                int oi = __shfl_down_sync(kFull, idx, off);
+                if (od < d || (od == d && oi < idx)) {
+                    d = od;
+                    idx = oi;
+                }
+            }
+            d = __shfl_sync(kFull, d, 0);
+            idx = __shfl_sync(kFull, idx, 0);
+            if (((V >> idx) & 1u) && d < bd) {
+                bd = d;
+                bid = __shfl_sync(kFull, id, idx);
+            }
+            if (V != kFull) break;
+        }
+        if (bid == from) return best;
+        best = (uint64_t(fkey(bd)) << 32) | bid;
+    }
+}
+
+// search_layer on layer 0 (src/hnsw/search.rs:81-142). Returns the number of
+// results in w.R (sorted ascending), or -1 on scratch overflow.
+__device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    // Reset the visited set.
+    if (w.bitmap_mode) {
+        for (uint32_t i = lane; i < w.bitmap_words; i += 32) w.H[i] = 0;
+    } else {
+        for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
+    }
+    __syncwarp();
+    const uint32_t hash_limit = (w.hash_cap >> 2) * 3;
+    uint32_t visited = 0;
+    uint32_t rs = 0, head = 0, tail = 0;
+    if (lane == 0) visit(w, pid(ep));
+    visited = 1;
+    if (lane == 0) w.C[0] = ep;
+    tail = 1;
+    if (admit(c, pid(ep))) {
+        if (lane == 0) w.R[0] = ep;
+        rs = 1;
+    }
+    __syncwarp();
+    while (head < tail) {
+        const uint64_t cur = w.C[head];
+        ++head;
+        const float worst0 = rs > 0 ? pdist(w.R[rs - 1]) : 0.0f;
+        if (rs >= ef && pdist(cur) > worst0) break;
+        c.cnt.exp0++;
+        const uint32_t* row = ix.adj0 + size_t(pid(cur)) * ix.m0p;
+        for (uint32_t base = 0; base < ix.m0; base += 32) {
+            uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+            const bool valid = id != kEmpty;
+            const uint32_t V = __ballot_sync(kFull, valid);
+            if (V == 0) break;
+            if (!w.bitmap_mode && visited + __popc(V) > hash_limit) return -1;
+            const bool fresh = valid && visit(w, id);
+            const uint32_t F = __ballot_sync(kFull, fresh);
+            visited += __popc(F);
+            if (F != 0) {
+                chunk_distances(c, id, F);
+                c.cnt.dist0 += __popc(F);
+                const bool adm = fresh && admit(c, id);
+                const uint32_t A = __ballot_sync(kFull, adm);
+                float my_d = fresh ? w.fd[lane] : 0.0f;
+                uint32_t P = F;
+                if (rs >= ef) {
+                    float wd = pdist(w.R[rs - 1]);
+                    P &= __ballot_sync(kFull, fresh && my_d < wd);
+                }
+                while (P) {
+                    const int i = __ffs(P) - 1;
+                    P &= P - 1;
+                    const float d = __shfl_sync(kFull, my_d, i);
+                    const uint32_t nid = __shfl_sync(kFull, id, i);
+                    const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
+                    if (!improves) continue;
+                    const uint64_t x = pack(d, nid);
+                    // Candidate queue: make room if needed.
+                    if (tail == w.cand_cap) {
+                        if (head > 0) {
+                            const uint32_t n = tail - head;
+                            for (uint32_t b = 0; b < n; b += 32) {
+                                uint32_t j = b + lane;
+                                uint64_t v = j < n ? w.C[head + j] : 0;
+                                __syncwarp();
+                                if (j < n) w.C[j] = v;
+                                __syncwarp();
+                            }
+                            head = 0;
+                            tail = n;
+                        }
+                        if (tail == w.cand_cap && rs >= ef) {
+                            // Drop candidates that can never be expanded.
+                            const float wd = pdist(w.R[rs - 1]);
+                            uint32_t keep = head;
+                            for (uint32_t b = head; b < tail; b += 32) {
+                                uint32_t j = b + lane;
+                                bool ok = j < tail && !(pdist(w.C[j]) > wd);
+                                keep += __popc(__ballot_sync(kFull, ok));
+                            }
+                            tail = keep;
+                        }
+                        if (tail == w.cand_cap) return -1;
+                    }
+                    sorted_insert(w.C, head, tail, x);
+                    ++tail;
+                    if ((A >> i) & 1u) {
+                        sorted_insert(w.R, 0, rs, x);
+                        ++rs;
+                        if (rs > ef) rs = ef;
+                    }
+                }
+            }
+            if (V != kFull) break;
+        }
+    }
+    return int(rs);
+}
+
+// Prepares the query (vector::check + normalisation, src/vector.rs:22-45,
+// 90-104; and the int8 code, src/quantization.rs:73-81) into the workspace.
+// Returns a status.
+__device__ int32_t prepare(QueryCtx& c, const float* q) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    const uint32_t dim = ix.dim;
+    bool bad = false;
+    for (uint32_t i = lane; i < ix.dp; i += 32) {
+        float x = i < dim ? q[i] : 0.0f;
+        bad |= !isfinite(x);
+        w.qf[i] = x;
+    }
+    bad = __any_sync(kFull, bad);
+    __syncwarp();
+    if (bad) return ST_NON_FINITE;
+    double norm = 0.0;
+    if (lane == 0)
+        for (uint32_t i = 0; i < dim; ++i) {
+            double x = double(w.qf[i]);
+            norm = __dadd_rn(norm, __dmul_rn(x, x));
+        }
+    norm = __shfl_sync(kFull, norm, 0);
+    if (norm > 4.2535295865117308e37 /* f32::MAX / 8 */) return ST_NON_FINITE;
+    if (c.metric == 2) {
+        if (norm == 0.0) return ST_ZERO;
+        const double inv = __ddiv_rn(1.0, __dsqrt_rn(norm));
+        for (uint32_t i = lane; i < dim; i += 32) w.qf[i] = __double2float_rn(__dmul_rn(double(w.qf[i]), inv));
+        __syncwarp();
+    }
+    if (c.quant) {
+        const float inv = __fdiv_rn(1.0f, ix.scale);
+        int sq = 0;
+        for (uint32_t i = lane; i < ix.dc; i += 32) {
+            int8_t code = i < dim ? sq_encode1(w.qf[i], __ldg(ix.q_offset + i), inv) : int8_t(0);
+            w.qc[i] = code;
+            sq += int(code) * int(code);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(kFull, sq, off);
+        c.qnorm = sq;
+        __syncwarp();
+    }
+    return ST_OK;
+}
+
+// One query, start to finish. Returns the status written.
+__device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
+    const DeviceIndexView& ix = a.ix;
+    const int lane = lane_id();
+    QueryCtx c;
+    c.a = &a;
+    c.w = &w;
+    c.qi = qi;
+    c.metric = ix.metric;
+    // Codes exist only on quantized indexes; a quantized request on any
+    // other index fails with QuantizationDisabled after validation.
+    c.quant = a.quantized != 0 && ix.quantized != 0;
+    c.s2 = __fmul_rn(ix.scale, ix.scale);
+    c.qnorm = 0;
+    c.use_filter = a.filter_bits != nullptr && (a.filter_used == nullptr || a.filter_used[qi] != 0);
+    c.fbits = a.filter_bits + (a.filter_stride ? size_t(qi) * a.filter_stride : 0);
+    c.fnbits = a.filter_nbits;
+    const uint32_t k = min(a.ks ? a.ks[qi] : a.k, a.out_stride);
+    uint32_t ef = a.efs ? a.efs[qi] : a.ef;
+    uint32_t count = 0;
+    int32_t st = prepare(c, a.queries + size_t(qi) * ix.dim);
+    if (st == ST_OK && a.quantized && !ix.quantized) st = ST_QDISABLED;
+    if (st == ST_OK && k != 0 && ix.live != 0 && ix.entry != kEmpty) {
+        ef = max(ef, k);
+        if (ef > w.ef_cap) return ST_OVERFLOW;
+        // search_graph (src/hnsw/search.rs:146-161)
+        float d0;
+        {
+            const int g8 = lane & 7;
+            d0 = group_distance(c, ix.entry, g8);
+        }
+        c.cnt.dist_up++;
+        uint64_t ep = pack(d0, ix.entry);
+        for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
+        int rs = layer0(c, ep, ef);
+        if (rs < 0) return ST_OVERFLOW;
+        // Quantized: exact distances for the survivors (src/hnsw/mod.rs:494-498).
+        if (c.quant) {
+            const int g = lane >> 3, g8 = lane & 7;
+            for (int r = 0; r < rs; r += 4) {
+                int slot = r + g;
+                uint32_t id = pid(w.R[slot < rs ? slot : 0]);
+                float d = group_exact(c, id, g8);
+                __syncwarp();
+                if (slot < rs && g8 == 0) w.C[slot] = pack(d, id);
+                __syncwarp();
+            }
+            for (int i = lane; i < rs; i += 32) w.R[i] = w.C[i];
+            __syncwarp();
+        }
+        // Sort by (total_cmp distance, key) and keep k (src/hnsw/mod.rs:501-510).
+        uint64_t* key_of = w.C;
+        for (int i = lane; i < rs; i += 32) key_of[i] = ix.keys_are_ids ? uint64_t(pid(w.R[i])) : __ldg(ix.keys + pid(w.R[i]));
+        __syncwarp();
+        count = min(uint32_t(rs), k);
+        for (int i = lane; i < rs; i += 32) {
+            const uint32_t dk = uint32_t(w.R[i] >> 32);
+            const uint64_t key = key_of[i];
+            uint32_t rank = 0;
+            for (int j = 0; j < rs; ++j) {
+                const uint32_t ok = uint32_t(w.R[j] >> 32);
+                const uint64_t okey = key_of[j];
+                rank += (ok < dk || (ok == dk && okey < key)) ? 1u : 0u;
+            }
+            if (rank < k) {
+                const size_t o = size_t(qi) * a.out_stride + rank;
+                a.out_keys[o] = key;
+                a.out_dist[o] = kdec(dk);
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        a.out_count[qi] = st == ST_OK ? count : 0u;
+        a.out_status[qi] = st;
+        if (a.counters) {
+            a.counters[4 * size_t(qi) + 0] = c.cnt.dist0;
+            a.counters[4 * size_t(qi) + 1] = c.cnt.exp0;
+            a.counters[4 * size_t(qi) + 2] = c.cnt.dist_up;
+            a.counters[4 * size_t(qi) + 3] = c.cnt.exp_up;
+        }
+    }
+    return st;
+}
+
+__device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
+
+__device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_cap, uint32_t cand_cap,
+                      uint32_t hash_cap) {
+    size_t off = 0;
+    w.qf = reinterpret_cast<float*>(base + off);
+    off = align_up(off + size_t(ix.dp) * 4, 16);
+    w.qc = reinterpret_cast<int8_t*>(base + off);
+    off = align_up(off + size_t(ix.dc), 16);
+    w.R = reinterpret_cast<uint64_t*>(base + off);
+    off = align_up(off + size_t(ef_cap + 1) * 8, 16);
+    w.C = reinterpret_cast<uint64_t*>(base + off);
+    off = align_up(off + size_t(cand_cap + 1) * 8, 16);
+    w.fr = reinterpret_cast<uint32_t*>(base + off);
+    off += 32 * 4;
+    w.fd = reinterpret_cast<float*>(base + off);
+    off += 32 * 4;
+    w.H = reinterpret_cast<uint32_t*>(base + off);
+    w.ef_cap = ef_cap;
+    w.cand_cap = cand_cap;
+    w.hash_cap = hash_cap;
+    w.bitmap_mode = false;
+    w.bitmap_words = 0;
+}
+
+__global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
+    extern __shared__ __align__(16) char smem[];
+    const uint32_t warp = threadIdx.x >> 5;
+    Ws w;
+    carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g.ef_cap, g.cand_cap, g.hash_cap);
+    const int lane = lane_id();
+    if (a.persistent) {
+        for (;;) {
+            uint32_t qi = 0;
+            if (lane == 0) qi = atomicAdd(a.work_next, 1u);
+            qi = __shfl_sync(kFull, qi, 0);
+            if (qi >= a.nq) break;
+            if (run_query(a, w, qi) == ST_OVERFLOW && lane == 0) {
+                a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
+                a.out_status[qi] = ST_OVERFLOW;
+            }
+        }
+    } else {
+        const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
+        if (qi >= a.nq) return;
+        if (run_query(a, w, qi) == ST_OVERFLOW && lane == 0) {
+            a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
+            a.out_status[qi] = ST_OVERFLOW;
+        }
+    }
+}
+
+// Retry pass: each warp owns a global-memory workspace with a visited bitmap
+// over all nodes and large heaps; it takes overflowed queries in turn.
+__global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) char smem[];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + warp;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    const DeviceIndexView& ix = a.ix;
+    Ws w;
+    // Query vectors and small buffers in shared memory; heaps and visited
+    // set in global memory.
+    size_t per = align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256;
+    char* base = smem + size_t(warp) * per;
+    w.qf = reinterpret_cast<float*>(base);
+    w.qc = reinterpret_cast<int8_t*>(base + align_up(size_t(ix.dp) * 4, 16));
+    w.fr = reinterpret_cast<uint32_t*>(base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16));
+    w.fd = reinterpret_cast<float*>(w.fr + 32);
+    w.R = a.g_results + size_t(gw) * (a.g_ef_cap + 1);
+    w.C = a.g_cands + size_t(gw) * (a.g_cand_cap + 1);
+    w.H = a.g_visited + size_t(gw) * a.g_visited_words;
+    w.ef_cap = a.g_ef_cap;
+    w.cand_cap = a.g_cand_cap;
+    w.hash_cap = 0;
+    w.bitmap_mode = true;
+    w.bitmap_words = uint32_t(a.g_visited_words);
+    const uint32_t total = *a.overflow_count;
+    for (uint32_t t = gw; t < total; t += nwarps) {
+        const uint32_t qi = a.overflow_list[t];
+        run_query(a, w, qi);  // writes ST_OVERFLOW again if even this scratch is too small
+    }
+}
+
+__global__ void encode_codes_kernel(const float* __restrict__ vec, uint32_t n, uint32_t dim, uint32_t dp,
+                                    uint32_t dc, const float* __restrict__ offset, float scale,
+                                    int8_t* __restrict__ codes, int32_t* __restrict__ norms) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const float inv = __fdiv_rn(1.0f, scale);
+    int sq = 0;
+    for (uint32_t i = lane; i < dc; i += 32) {
+        int8_t code = i < dim ? sq_encode1(vec[size_t(warp) * dp + i], offset[i], inv) : int8_t(0);
+        codes[size_t(warp) * dc + i] = code;
+        sq += int(code) * int(code);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(kFull, sq, off);
+    if (lane == 0) norms[warp] = sq;
+}
+
+}  // namespace dev
+
+uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t dc) {
+    auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+    size_t b = al(size_t(dp) * 4) + al(dc) + al(size_t(g.ef_cap + 1) * 8) + al(size_t(g.cand_cap + 1) * 8) + 256 +
+               size_t(g.hash_cap) * 4;
+    return uint32_t(al(b));
+}
+
+cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, int num_sms, cudaStream_t stream) {
+    SearchGeometry geo = geo_in;
+    geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
+    const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
+    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    dim3 block(32 * geo.warps_per_block);
+    dim3 grid;
+    if (args.persistent) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::search_kernel, int(block.x), smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        grid = dim3(uint32_t(num_sms * per_sm));
+    } else {
+        grid = dim3((args.nq + geo.warps_per_block - 1) / geo.warps_per_block);
+    }
+    if (grid.x == 0) return cudaSuccess;
+    dev::search_kernel<<<grid, block, smem, stream>>>(args, geo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream) {
+    const uint32_t wpb = 4;
+    auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+    size_t per = al(size_t(args.ix.dp) * 4) + al(args.ix.dc) + 256;
+    size_t smem = per * wpb;
+    cudaError_t e = cudaFuncSetAttribute(dev::search_retry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    dev::search_retry_kernel<<<(warps + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_encode_codes(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, uint32_t dc,
+                                const float* offset, float scale, int8_t* codes, int32_t* norms, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t threads = 256;
+    const uint64_t blocks = (uint64_t(n) * 32 + threads - 1) / threads;
+    dev::encode_codes_kernel<<<uint32_t(blocks), threads, 0, stream>>>(vec, n, dim, dp, dc, offset, scale, codes, norms);
+    return cudaGetLastError();
+}
+
+}  // namespace hnswgpu

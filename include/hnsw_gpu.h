@@ -1,0 +1,224 @@
+/*
+ * hnsw_gpu.h — C ABI of the B200-native query path of the hnsw-index crate.
+ *
+ * Plain pointers and sizes only. Every entry point returns an hnsw_status
+ * (0 = success) and never throws or aborts across the boundary; the message
+ * of the last failure on the calling thread is available from
+ * hnsw_last_error(). Each declaration names the reference interface it stands
+ * in for (paths within the hnsw-index crate).
+ *
+ * Buffers: the caller owns every host buffer; they are read or written only
+ * during the call. The library owns device memory per handle. Functions whose
+ * name ends in _device take device pointers and a cudaStream_t passed as
+ * void*, and return once the work is enqueued.
+ *
+ * Threading: an hnsw_gpu_index / hnsw_gpu_brute handle may be searched from
+ * many host threads at once (the reference's HnswIndex is Send + Sync,
+ * src/hnsw/tests.rs:82-86); each call takes its own scratch slot and stream.
+ */
+#ifndef HNSW_GPU_H
+#define HNSW_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error kinds. Mirrors Error and FormatError (src/error.rs:9-74); the
+ * values from HNSW_ERR_CUDA on are new to the device path. */
+typedef enum hnsw_status {
+    HNSW_OK = 0,
+    HNSW_ERR_DIMENSION_MISMATCH = 1,   /* Error::DimensionMismatch */
+    HNSW_ERR_INVALID_DIMENSION = 2,    /* Error::InvalidDimension */
+    HNSW_ERR_NON_FINITE_VECTOR = 3,    /* Error::NonFiniteVector */
+    HNSW_ERR_ZERO_VECTOR = 4,          /* Error::ZeroVector */
+    HNSW_ERR_DUPLICATE_KEY = 5,        /* Error::DuplicateKey */
+    HNSW_ERR_CAPACITY_EXCEEDED = 6,    /* Error::CapacityExceeded */
+    HNSW_ERR_QUANTIZATION_DISABLED = 7,/* Error::QuantizationDisabled */
+    HNSW_ERR_INVALID_PARAMETER = 8,    /* Error::InvalidParameter */
+    HNSW_ERR_FORMAT_BAD_MAGIC = 10,    /* FormatError::BadMagic */
+    HNSW_ERR_FORMAT_UNSUPPORTED_VERSION = 11, /* FormatError::UnsupportedVersion */
+    HNSW_ERR_FORMAT_TRUNCATED = 12,    /* FormatError::Truncated */
+    HNSW_ERR_FORMAT_CHECKSUM = 13,     /* FormatError::ChecksumMismatch */
+    HNSW_ERR_FORMAT_TRAILING_BYTES = 14, /* FormatError::TrailingBytes */
+    HNSW_ERR_FORMAT_INVALID = 15,      /* FormatError::Invalid(what); what = hnsw_last_error() */
+    HNSW_ERR_MEMORY_LIMIT_EXCEEDED = 16, /* Error::MemoryLimitExceeded */
+    HNSW_ERR_CUDA = 20,                /* a CUDA call failed */
+    HNSW_ERR_OUT_OF_DEVICE_MEMORY = 21,
+    HNSW_ERR_TIMEOUT = 22,             /* a bounded device wait ran out */
+    HNSW_ERR_ADMISSION_REJECTED = 23,  /* no scratch slot free for a request */
+    HNSW_ERR_INVALID_ARGUMENT = 24,    /* null pointer, size out of the device path's range */
+    HNSW_ERR_SCRATCH_OVERFLOW = 25     /* a query outgrew its device scratch; retried internally */
+} hnsw_status;
+
+/* Metric tags, as in the file format (src/metric.rs:44-60). */
+enum { HNSW_METRIC_L2 = 0, HNSW_METRIC_INNER_PRODUCT = 1, HNSW_METRIC_COSINE = 2 };
+
+/* Thread-local text of the last error ("invalid field: metric", ...). */
+const char* hnsw_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* HNSW index on the device                                            */
+/* ------------------------------------------------------------------ */
+
+typedef struct hnsw_gpu_index hnsw_gpu_index;
+
+typedef struct hnsw_index_info {
+    uint32_t dim, metric, m, m0, ef_construction, quantized;
+    uint32_t nodes;        /* tombstones included */
+    uint32_t live;         /* HnswIndex::len */
+    uint32_t top_level;
+    uint32_t entry;        /* entry point id, 0xFFFFFFFF if empty */
+    uint64_t seed;
+    double level_multiplier;
+    uint64_t required_memory; /* io.rs required_memory() of the file */
+    uint64_t device_bytes;    /* device memory held by the handle */
+} hnsw_index_info;
+
+/* Validates a format-v1 file with every check of HnswIndex::from_bytes /
+ * from_bytes_with_limit (src/hnsw/io.rs:236-540). Host only: needs no GPU.
+ * max_memory == 0 means the default limit (64 x len, at least 64 MiB,
+ * io.rs:269-275). info may be NULL. */
+int hnsw_validate_bytes(const uint8_t* bytes, size_t len, uint64_t max_memory, hnsw_index_info* info);
+
+/* Loads and validates a file (as hnsw_validate_bytes), then flattens it
+ * into device memory on `device`. Replaces HnswIndex::from_bytes
+ * (src/hnsw/mod.rs:666-700) for the device path. `bytes` may be freed after
+ * the call. */
+int hnsw_gpu_index_open(const uint8_t* bytes, size_t len, uint64_t max_memory, int device,
+                        hnsw_gpu_index** out);
+void hnsw_gpu_index_close(hnsw_gpu_index* index);
+int hnsw_gpu_index_info(const hnsw_gpu_index* index, hnsw_index_info* out);
+
+/* Replaces the tombstone column (deleted flags per node id, 0 or 1), the
+ * device-side form of HnswIndex::remove (src/hnsw/mod.rs:357-365). */
+int hnsw_gpu_set_tombstones(hnsw_gpu_index* index, const uint8_t* deleted, size_t nodes);
+
+/* Options of one search call. Mirrors SearchOptions (src/hnsw/mod.rs:56-98)
+ * plus the batch arguments of search_batch (mod.rs:520-536). The reference
+ * filter is a closure over keys; here it is a key bitmap: key `x` passes iff
+ * x < filter_nbits and bit x is set. */
+typedef struct hnsw_search_opts {
+    uint32_t k;                 /* results per query (when ks == NULL) */
+    uint32_t ef;                /* candidate list size (when efs == NULL); raised to k */
+    const uint32_t* ks;         /* optional per-query k */
+    const uint32_t* efs;        /* optional per-query ef */
+    int32_t quantized;          /* SearchOptions::quantized */
+    const uint64_t* filter_bits;/* optional key bitmap(s) */
+    uint64_t filter_nbits;      /* bits per bitmap */
+    uint64_t filter_stride;     /* words between per-query bitmaps; 0 = one shared bitmap */
+    const uint8_t* filter_used; /* optional per-query flag: 0 = no filter for that query */
+    uint32_t out_stride;        /* entries per query row of the outputs; 0 = max k */
+    int32_t mode;               /* HNSW_MODE_* */
+} hnsw_search_opts;
+
+enum {
+    HNSW_MODE_PLAIN = 0,      /* one warp per query, one launch per call */
+    HNSW_MODE_PERSISTENT = 1  /* persistent CTAs draining a device work queue */
+};
+
+/* Batched search: HnswIndex::search_batch / search_with / search_filtered
+ * (src/hnsw/mod.rs:412-536). Host buffers. queries: nq x dim row-major.
+ * Outputs: out_keys/out_dist nq x out_stride, out_count[nq] results per
+ * query (sorted by distance, then key), out_status[nq] per-query status
+ * (HNSW_ERR_NON_FINITE_VECTOR, HNSW_ERR_ZERO_VECTOR, ...). The return value
+ * is HNSW_OK when every query succeeded, else the first failing status. */
+int hnsw_gpu_search_batch(hnsw_gpu_index* index, const float* queries, size_t nq, size_t dim,
+                          const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist,
+                          uint32_t* out_count, int32_t* out_status);
+
+/* Same with every pointer (queries, ks, efs, filter bits, outputs) in device
+ * memory, enqueued on `stream` (a cudaStream_t; NULL = the handle's stream).
+ * Per-query statuses are written asynchronously. */
+int hnsw_gpu_search_batch_device(hnsw_gpu_index* index, const float* d_queries, size_t nq, size_t dim,
+                                 const hnsw_search_opts* d_opts, uint64_t* d_keys, float* d_dist,
+                                 uint32_t* d_count, int32_t* d_status, void* stream);
+
+/* Per-query traversal counters of the last search on this thread's slot
+ * (device pointer, nq x 4 u32: layer-0 distances, layer-0 expansions,
+ * upper-layer distances, upper-layer list reads). Enabled by
+ * hnsw_gpu_set_counters(index, 1). */
+int hnsw_gpu_set_counters(hnsw_gpu_index* index, int enabled);
+int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq);
+
+/* ------------------------------------------------------------------ */
+/* Exact brute-force k-NN on the device                                */
+/* ------------------------------------------------------------------ */
+
+typedef struct hnsw_gpu_brute hnsw_gpu_brute;
+
+enum {
+    HNSW_PRECISION_FP32 = 0,   /* CUDA-core FP32 in the AVX2 kernel order: bit-identical distances */
+    HNSW_PRECISION_BF16 = 1,   /* tcgen05 BF16 scoring, FP32 accumulate, FP32 re-rank */
+    HNSW_PRECISION_BF16X3 = 2  /* 3-term BF16 split (compensated), FP32 re-rank */
+};
+
+/* BruteForceIndex::new + insert_batch (src/brute.rs:66-115): validates and
+ * prepares rows (unit length for cosine) and uploads them. keys may be NULL
+ * (keys 0..n-1). */
+int hnsw_gpu_brute_open(const float* vectors, const uint64_t* keys, size_t n, size_t dim, int metric,
+                        int device, hnsw_gpu_brute** out);
+void hnsw_gpu_brute_close(hnsw_gpu_brute* brute);
+
+/* BruteForceIndex::search_batch (src/brute.rs:169-180): exact top-k by
+ * (distance total order, key). Outputs as hnsw_gpu_search_batch with
+ * out_stride = k. */
+int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* brute, const float* queries, size_t nq, size_t dim,
+                                uint32_t k, int precision, uint64_t* out_keys, float* out_dist,
+                                uint32_t* out_count, int32_t* out_status);
+
+/* ------------------------------------------------------------------ */
+/* Host-side index construction (produces format-v1 files)             */
+/* ------------------------------------------------------------------ */
+
+typedef struct hnsw_builder hnsw_builder;
+
+typedef struct hnsw_params {
+    uint32_t m, m0, ef_construction;
+    double level_multiplier;
+    uint32_t selection;          /* 0 = simple, 1 = heuristic */
+    uint32_t extend_candidates;  /* heuristic flags */
+    uint32_t keep_pruned;
+    uint64_t seed;
+} hnsw_params;
+
+/* HnswParams::new(m) defaults (src/params.rs:78-87). */
+void hnsw_params_default(uint32_t m, hnsw_params* out);
+
+/* HnswIndex::new (src/hnsw/mod.rs:181-187). */
+int hnsw_builder_new(size_t dim, int metric, const hnsw_params* params, hnsw_builder** out);
+void hnsw_builder_free(hnsw_builder* b);
+/* HnswIndex::insert (mod.rs:290-302): sequential, deterministic. */
+int hnsw_builder_insert(hnsw_builder* b, uint64_t key, const float* vector, size_t dim);
+/* HnswIndex::insert_batch (mod.rs:318-349): parallel link on `threads`
+ * host threads (0 = all cores). */
+int hnsw_builder_insert_batch(hnsw_builder* b, const uint64_t* keys, const float* vectors, size_t n,
+                              size_t dim, int threads);
+/* HnswIndex::remove (mod.rs:357-365). *removed = 1 if the key was live. */
+int hnsw_builder_remove(hnsw_builder* b, uint64_t key, int* removed);
+/* HnswIndex::enable_quantization (mod.rs:544-547). */
+int hnsw_builder_enable_quantization(hnsw_builder* b);
+/* HnswIndex::to_bytes (mod.rs:639-643). Free the buffer with hnsw_bytes_free. */
+int hnsw_builder_to_bytes(const hnsw_builder* b, uint8_t** out, size_t* len);
+void hnsw_bytes_free(uint8_t* p);
+
+/* ------------------------------------------------------------------ */
+/* Synthetic data (src/synthetic.rs:81-124)                            */
+/* ------------------------------------------------------------------ */
+
+/* Dataset::gaussian: base then queries from one SplitMix64 stream. */
+void hnsw_synthetic_gaussian(size_t n_base, size_t n_query, size_t dim, uint64_t seed, float* base,
+                             float* queries);
+/* Dataset::clustered with the spread (sigma) as a parameter: centers first,
+ * then per point next_below(clusters) and dim Gaussians. */
+void hnsw_synthetic_mixture(size_t n_base, size_t n_query, size_t dim, size_t clusters, double sigma,
+                            uint64_t seed, float* base, float* queries);
+/* CRC-32 (IEEE) of a buffer (src/crc32.rs). */
+uint32_t hnsw_crc32(const uint8_t* bytes, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HNSW_GPU_H */

@@ -1,0 +1,769 @@
+// CPU ORACLE — test infrastructure, not product code.
+//
+// A plain C++ restatement of the hnsw-index crate's query path, used only by
+// tests/, __graft_entry__.smoke() and the CPU-baseline / reference legs of
+// bench.py, as the checker the CUDA path is compared against. Nothing in the
+// product library links or calls this file.
+//
+// Every function names the reference file:line it restates (paths are within
+// the hnsw-index crate). Pinned by the reference's own known answers (see
+// tests/test_oracle_golden.py): SplitMix64 outputs, the Python-generator golden
+// components, CRC-32 check values, scalar kernel known answers, metric known
+// answers (IP -0.0), brute-force tie breaking, the complete-graph exactness
+// case and the recall pins.
+//
+// Compile with -ffp-contract=off: the reference (Rust) never contracts a*b+c,
+// and every FMA below is explicit.
+
+#include <immintrin.h>
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <queue>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// f32 kernels in the AVX2 backend's summation order
+// (src/kernels/x86.rs:32-131): four FMA chains of eight lanes over 32-float
+// steps, an 8-wide tail into chain 0, lane-wise (c0+c1)+(c2+c3), the
+// horizontal sum ((l0+l4)+(l1+l5))+((l2+l6)+(l3+l7)) (x86.rs:19-26), then a
+// scalar tail without FMA.
+// ---------------------------------------------------------------------------
+
+inline float hsum8(const float* v) {
+    return ((v[0] + v[4]) + (v[1] + v[5])) + ((v[2] + v[6]) + (v[3] + v[7]));
+}
+
+// Portable restatement (fmaf per lane is exactly what _mm256_fmadd_ps does).
+float dot_avx2order_portable(const float* a, const float* b, size_t len) {
+    float acc[4][8] = {};
+    size_t i = 0;
+    for (; i + 32 <= len; i += 32)
+        for (int c = 0; c < 4; ++c)
+            for (int l = 0; l < 8; ++l)
+                acc[c][l] = std::fmaf(a[i + 8 * c + l], b[i + 8 * c + l], acc[c][l]);
+    for (; i + 8 <= len; i += 8)
+        for (int l = 0; l < 8; ++l) acc[0][l] = std::fmaf(a[i + l], b[i + l], acc[0][l]);
+    float v[8];
+    for (int l = 0; l < 8; ++l) v[l] = (acc[0][l] + acc[1][l]) + (acc[2][l] + acc[3][l]);
+    float sum = hsum8(v);
+    for (; i < len; ++i) sum += a[i] * b[i];
+    return sum;
+}
+
+float l2_avx2order_portable(const float* a, const float* b, size_t len) {
+    float acc[4][8] = {};
+    size_t i = 0;
+    for (; i + 32 <= len; i += 32)
+        for (int c = 0; c < 4; ++c)
+            for (int l = 0; l < 8; ++l) {
+                float d = a[i + 8 * c + l] - b[i + 8 * c + l];
+                acc[c][l] = std::fmaf(d, d, acc[c][l]);
+            }
+    for (; i + 8 <= len; i += 8)
+        for (int l = 0; l < 8; ++l) {
+            float d = a[i + l] - b[i + l];
+            acc[0][l] = std::fmaf(d, d, acc[0][l]);
+        }
+    float v[8];
+    for (int l = 0; l < 8; ++l) v[l] = (acc[0][l] + acc[1][l]) + (acc[2][l] + acc[3][l]);
+    float sum = hsum8(v);
+    for (; i < len; ++i) {
+        float d = a[i] - b[i];
+        sum += d * d;
+    }
+    return sum;
+}
+
+// Intrinsics version (same bits; used when the CPU has AVX2+FMA).
+__attribute__((target("avx2,fma"))) float dot_avx2(const float* a, const float* b, size_t len) {
+    __m256 acc0 = _mm256_setzero_ps(), acc1 = _mm256_setzero_ps();
+    __m256 acc2 = _mm256_setzero_ps(), acc3 = _mm256_setzero_ps();
+    size_t i = 0;
+    for (; i + 32 <= len; i += 32) {
+        acc0 = _mm256_fmadd_ps(_mm256_loadu_ps(a + i), _mm256_loadu_ps(b + i), acc0);
+        acc1 = _mm256_fmadd_ps(_mm256_loadu_ps(a + i + 8), _mm256_loadu_ps(b + i + 8), acc1);
+        acc2 = _mm256_fmadd_ps(_mm256_loadu_ps(a + i + 16), _mm256_loadu_ps(b + i + 16), acc2);
+        acc3 = _mm256_fmadd_ps(_mm256_loadu_ps(a + i + 24), _mm256_loadu_ps(b + i + 24), acc3);
+    }
+    for (; i + 8 <= len; i += 8)
+        acc0 = _mm256_fmadd_ps(_mm256_loadu_ps(a + i), _mm256_loadu_ps(b + i), acc0);
+    float v[8];
+    _mm256_storeu_ps(v, _mm256_add_ps(_mm256_add_ps(acc0, acc1), _mm256_add_ps(acc2, acc3)));
+    float sum = hsum8(v);
+    for (; i < len; ++i) sum += a[i] * b[i];
+    return sum;
+}
+
+__attribute__((target("avx2,fma"))) float l2_avx2(const float* a, const float* b, size_t len) {
+    __m256 acc0 = _mm256_setzero_ps(), acc1 = _mm256_setzero_ps();
+    __m256 acc2 = _mm256_setzero_ps(), acc3 = _mm256_setzero_ps();
+    size_t i = 0;
+    for (; i + 32 <= len; i += 32) {
+        __m256 d0 = _mm256_sub_ps(_mm256_loadu_ps(a + i), _mm256_loadu_ps(b + i));
+        __m256 d1 = _mm256_sub_ps(_mm256_loadu_ps(a + i + 8), _mm256_loadu_ps(b + i + 8));
+        __m256 d2 = _mm256_sub_ps(_mm256_loadu_ps(a + i + 16), _mm256_loadu_ps(b + i + 16));
+        __m256 d3 = _mm256_sub_ps(_mm256_loadu_ps(a + i + 24), _mm256_loadu_ps(b + i + 24));
+        acc0 = _mm256_fmadd_ps(d0, d0, acc0);
+        acc1 = _mm256_fmadd_ps(d1, d1, acc1);
+        acc2 = _mm256_fmadd_ps(d2, d2, acc2);
+        acc3 = _mm256_fmadd_ps(d3, d3, acc3);
+    }
+    for (; i + 8 <= len; i += 8) {
+        __m256 d = _mm256_sub_ps(_mm256_loadu_ps(a + i), _mm256_loadu_ps(b + i));
+        acc0 = _mm256_fmadd_ps(d, d, acc0);
+    }
+    float v[8];
+    _mm256_storeu_ps(v, _mm256_add_ps(_mm256_add_ps(acc0, acc1), _mm256_add_ps(acc2, acc3)));
+    float sum = hsum8(v);
+    for (; i < len; ++i) {
+        float d = a[i] - b[i];
+        sum += d * d;
+    }
+    return sum;
+}
+
+bool have_avx2() {
+    static const bool ok = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
+    return ok;
+}
+
+inline float k_dot(const float* a, const float* b, size_t n) {
+    return have_avx2() ? dot_avx2(a, b, n) : dot_avx2order_portable(a, b, n);
+}
+inline float k_l2(const float* a, const float* b, size_t n) {
+    return have_avx2() ? l2_avx2(a, b, n) : l2_avx2order_portable(a, b, n);
+}
+
+// Scalar backend: one accumulator, strict left to right (src/kernels/scalar.rs:7-22).
+float dot_scalar(const float* a, const float* b, size_t n) {
+    float s = 0.0f;
+    for (size_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+float l2_scalar(const float* a, const float* b, size_t n) {
+    float s = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+        float d = a[i] - b[i];
+        s += d * d;
+    }
+    return s;
+}
+
+enum Metric : uint8_t { L2 = 0, IP = 1, COS = 2 };
+
+// Metric::distance (src/metric.rs:35-41).
+inline float metric_distance(int metric, const float* a, const float* b, size_t n) {
+    switch (metric) {
+        case L2: return k_l2(a, b, n);
+        case IP: return -k_dot(a, b, n);
+        default: return 1.0f - k_dot(a, b, n);
+    }
+}
+
+// int8 kernels: exact integer sums (src/kernels/int8.rs:13-48).
+int64_t i8_dot(const int8_t* a, const int8_t* b, size_t n) {
+    int64_t s = 0;
+    for (size_t i = 0; i < n; ++i) s += int64_t(a[i]) * int64_t(b[i]);
+    return s;
+}
+int64_t i8_l2(const int8_t* a, const int8_t* b, size_t n) {
+    int64_t s = 0;
+    for (size_t i = 0; i < n; ++i) {
+        int64_t d = int64_t(a[i]) - int64_t(b[i]);
+        s += d * d;
+    }
+    return s;
+}
+
+// ScalarQuantizer::encode_into (src/quantization.rs:73-81): inv = 1/scale in
+// f32, code = clamp(round_half_away((x - o) * inv), -127, 127).
+void sq_encode(const float* x, const float* offset, float scale, size_t dim, int8_t* out) {
+    float inv = 1.0f / scale;
+    for (size_t i = 0; i < dim; ++i) {
+        float v = std::round((x[i] - offset[i]) * inv);
+        v = std::min(127.0f, std::max(-127.0f, v));
+        out[i] = int8_t(v);
+    }
+}
+
+// ScalarQuantizer::distance (src/quantization.rs:85-92).
+inline float sq_distance(int metric, float scale, const int8_t* a, const int8_t* b, size_t n) {
+    float s2 = scale * scale;
+    switch (metric) {
+        case L2: return float(i8_l2(a, b, n)) * s2;
+        case IP: return -float(i8_dot(a, b, n)) * s2;
+        default: return 1.0f - float(i8_dot(a, b, n)) * s2;
+    }
+}
+
+// total_cmp of f32 (Rust core::f32::total_cmp).
+inline int32_t total_key(float f) {
+    int32_t b;
+    std::memcpy(&b, &f, 4);
+    b ^= int32_t(uint32_t(b >> 31) >> 1);
+    return b;
+}
+
+// Candidate ordering: (total_cmp distance, id) (src/hnsw/search.rs:36-44).
+struct Cand {
+    float d;
+    uint32_t id;
+};
+inline bool cand_less(const Cand& a, const Cand& b) {
+    int32_t ka = total_key(a.d), kb = total_key(b.d);
+    return ka != kb ? ka < kb : a.id < b.id;
+}
+struct CandLess {
+    bool operator()(const Cand& a, const Cand& b) const { return cand_less(a, b); }
+};
+struct CandGreater {
+    bool operator()(const Cand& a, const Cand& b) const { return cand_less(b, a); }
+};
+
+// ---------------------------------------------------------------------------
+// SplitMix64 + Box-Muller + Lemire (src/synthetic.rs:23-60).
+// ---------------------------------------------------------------------------
+inline uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+struct SplitMix64 {
+    uint64_t s;
+    uint64_t next() {
+        s += 0x9E3779B97F4A7C15ULL;
+        return mix64(s);
+    }
+    double next_f64() { return double(next() >> 11) * (1.0 / double(1ULL << 53)); }
+    uint64_t below(uint64_t n) { return uint64_t((__uint128_t(next()) * n) >> 64); }
+    double gaussian() {
+        double u1 = 1.0 - next_f64();
+        double u2 = next_f64();
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// A loaded index (format v1, src/hnsw/io.rs:3-28). The oracle trusts files
+// that the validating loader of the product library has accepted; it checks
+// only the envelope and lengths.
+// ---------------------------------------------------------------------------
+struct Index {
+    int metric = 0;
+    uint32_t dim = 0, m = 0, m0 = 0, n = 0, entry = 0xFFFFFFFFu;
+    uint8_t top = 0;
+    bool quantized = false;
+    std::vector<uint64_t> keys;
+    std::vector<uint8_t> levels, deleted;
+    std::vector<float> vectors;
+    // layer 0: (m0+1) words per node (count, ids)
+    std::vector<uint32_t> l0;
+    // upper layers: per node, level*(m+1) words
+    std::vector<std::vector<uint32_t>> upper;
+    std::vector<float> offset;
+    float scale = 1.0f;
+    std::vector<int8_t> codes;
+    size_t live = 0;
+
+    const float* vec(uint32_t id) const { return vectors.data() + size_t(id) * dim; }
+    const uint32_t* list(uint32_t id, unsigned layer, uint32_t* count) const {
+        if (layer == 0) {
+            const uint32_t* b = l0.data() + size_t(id) * (m0 + 1);
+            *count = std::min(b[0], m0);
+            return b + 1;
+        }
+        const uint32_t* b = upper[id].data() + size_t(layer - 1) * (m + 1);
+        *count = std::min(b[0], m);
+        return b + 1;
+    }
+};
+
+uint32_t crc_table[256];
+bool crc_ready = false;
+uint32_t crc32(const uint8_t* p, size_t n) {
+    if (!crc_ready) {
+        for (uint32_t i = 0; i < 256; ++i) {
+            uint32_t c = i;
+            for (int k = 0; k < 8; ++k) c = (c & 1) ? (c >> 1) ^ 0xEDB88320u : (c >> 1);
+            crc_table[i] = c;
+        }
+        crc_ready = true;
+    }
+    uint32_t c = 0xFFFFFFFFu;
+    for (size_t i = 0; i < n; ++i) c = (c >> 8) ^ crc_table[(c ^ p[i]) & 0xFF];
+    return ~c;
+}
+
+struct Rd {
+    const uint8_t* p;
+    size_t n, pos;
+    bool ok = true;
+    const uint8_t* take(size_t k) {
+        if (!ok || k > n - pos) {
+            ok = false;
+            return nullptr;
+        }
+        const uint8_t* r = p + pos;
+        pos += k;
+        return r;
+    }
+    template <class T>
+    T get() {
+        T v{};
+        const uint8_t* b = take(sizeof(T));
+        if (b) std::memcpy(&v, b, sizeof(T));
+        return v;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Search (src/hnsw/search.rs:49-161, src/hnsw/mod.rs:460-511).
+// ---------------------------------------------------------------------------
+struct Stats {
+    uint64_t dist0 = 0, exp0 = 0, dist_up = 0, exp_up = 0;
+};
+
+struct Scratch {
+    std::vector<uint16_t> marks;
+    uint16_t epoch = 0;
+    void reset(size_t n) {  // VisitedSet::reset (src/hnsw/scratch.rs:25-33)
+        if (marks.size() < n) marks.resize(n, 0);
+        epoch = uint16_t(epoch + 1);
+        if (epoch == 0) {
+            std::fill(marks.begin(), marks.end(), 0);
+            epoch = 1;
+        }
+    }
+    bool insert(uint32_t id) {
+        if (marks[id] == epoch) return false;
+        marks[id] = epoch;
+        return true;
+    }
+};
+
+struct Filter {
+    // Key bitmap: key admitted iff key < nbits and bit set. nullptr = no filter.
+    const uint64_t* bits = nullptr;
+    uint64_t nbits = 0;
+    bool accept(uint64_t key) const {
+        if (!bits) return true;
+        return key < nbits && ((bits[key >> 6] >> (key & 63)) & 1);
+    }
+};
+
+template <class Dist, class Admit>
+Cand greedy_closest(const Index& ix, Cand start, unsigned layer, const Dist& dist, Stats& st) {
+    Cand best = start;
+    for (;;) {
+        uint32_t from = best.id, cnt;
+        const uint32_t* ids = ix.list(from, layer, &cnt);
+        st.exp_up++;
+        for (uint32_t j = 0; j < cnt; ++j) {
+            float d = dist(ids[j]);
+            st.dist_up++;
+            if (d < best.d) best = Cand{d, ids[j]};
+        }
+        if (best.id == from) return best;
+    }
+}
+
+template <class Dist, class Admit>
+std::vector<Cand> search_layer0(const Index& ix, Scratch& sc, Cand ep, size_t ef, const Dist& dist,
+                                const Admit& admit, Stats& st) {
+    sc.reset(ix.n);
+    std::priority_queue<Cand, std::vector<Cand>, CandGreater> cands;  // min-heap
+    std::priority_queue<Cand, std::vector<Cand>, CandLess> results;   // max-heap
+    if (sc.insert(ep.id)) {
+        cands.push(ep);
+        if (admit(ep.id)) {
+            results.push(ep);
+            if (results.size() > ef) results.pop();
+        }
+    }
+    while (!cands.empty()) {
+        Cand cur = cands.top();
+        cands.pop();
+        if (results.size() >= ef && !results.empty() && cur.d > results.top().d) break;
+        uint32_t cnt;
+        const uint32_t* ids = ix.list(cur.id, 0, &cnt);
+        st.exp0++;
+        for (uint32_t j = 0; j < cnt; ++j) {
+            uint32_t nb = ids[j];
+            if (!sc.insert(nb)) continue;
+            float d = dist(nb);
+            st.dist0++;
+            bool improves = results.size() < ef || (!results.empty() && d < results.top().d);
+            if (improves) {
+                Cand c{d, nb};
+                cands.push(c);
+                if (admit(nb)) {
+                    results.push(c);
+                    if (results.size() > ef) results.pop();
+                }
+            }
+        }
+    }
+    std::vector<Cand> out;
+    out.reserve(results.size());
+    while (!results.empty()) {
+        out.push_back(results.top());
+        results.pop();
+    }
+    std::sort(out.begin(), out.end(), CandLess());
+    return out;
+}
+
+enum Status : int32_t {
+    OK = 0,
+    DIMENSION_MISMATCH = 1,
+    NON_FINITE_VECTOR = 3,
+    ZERO_VECTOR = 4,
+    QUANTIZATION_DISABLED = 7,
+};
+
+// check + normalized + prepare_query (src/vector.rs:22-45,90-104).
+int32_t prepare_query(int metric, const float* q, size_t dim, float* out) {
+    double norm = 0.0;
+    for (size_t i = 0; i < dim; ++i) {
+        if (!std::isfinite(q[i])) return NON_FINITE_VECTOR;
+        norm += double(q[i]) * double(q[i]);
+    }
+    if (norm > double(3.40282346638528859812e+38F) / 8.0) return NON_FINITE_VECTOR;
+    if (metric == COS) {
+        if (norm == 0.0) return ZERO_VECTOR;
+        double inv = 1.0 / std::sqrt(norm);
+        for (size_t i = 0; i < dim; ++i) out[i] = float(double(q[i]) * inv);
+    } else {
+        std::memcpy(out, q, dim * 4);
+    }
+    return OK;
+}
+
+struct Hit {
+    uint64_t key;
+    float d;
+};
+inline bool hit_less(const Hit& a, const Hit& b) {  // Neighbor::cmp_by_distance (src/neighbor.rs:17-21)
+    int32_t ka = total_key(a.d), kb = total_key(b.d);
+    return ka != kb ? ka < kb : a.key < b.key;
+}
+
+// HnswIndex::search_impl (src/hnsw/mod.rs:460-511), one query.
+int32_t search_one(const Index& ix, Scratch& sc, const float* query, size_t k, size_t ef, bool quantized,
+                   const Filter& filter, std::vector<Hit>& out, Stats& st) {
+    out.clear();
+    std::vector<float> q(ix.dim);
+    int32_t s = prepare_query(ix.metric, query, ix.dim, q.data());
+    if (s != OK) return s;
+    if (quantized && !ix.quantized) return QUANTIZATION_DISABLED;
+    if (k == 0 || ix.live == 0) return OK;
+    ef = std::max(ef, k);
+    auto admit = [&](uint32_t id) { return !ix.deleted[id] && filter.accept(ix.keys[id]); };
+    auto exact = [&](uint32_t id) { return metric_distance(ix.metric, q.data(), ix.vec(id), ix.dim); };
+    std::vector<Cand> found;
+    if (ix.entry == 0xFFFFFFFFu) return OK;
+    if (!quantized) {
+        Cand ep{exact(ix.entry), ix.entry};
+        st.dist_up++;
+        for (int layer = ix.top; layer >= 1; --layer)
+            ep = greedy_closest<decltype(exact), decltype(admit)>(ix, ep, unsigned(layer), exact, st);
+        found = search_layer0(ix, sc, ep, ef, exact, admit, st);
+    } else {
+        std::vector<int8_t> code(ix.dim);
+        sq_encode(q.data(), ix.offset.data(), ix.scale, ix.dim, code.data());
+        auto approx = [&](uint32_t id) {
+            return sq_distance(ix.metric, ix.scale, code.data(), ix.codes.data() + size_t(id) * ix.dim, ix.dim);
+        };
+        Cand ep{approx(ix.entry), ix.entry};
+        st.dist_up++;
+        for (int layer = ix.top; layer >= 1; --layer)
+            ep = greedy_closest<decltype(approx), decltype(admit)>(ix, ep, unsigned(layer), approx, st);
+        found = search_layer0(ix, sc, ep, ef, approx, admit, st);
+        for (auto& c : found) c.d = exact(c.id);
+    }
+    out.reserve(found.size());
+    for (auto& c : found) out.push_back(Hit{ix.keys[c.id], c.d});
+    std::sort(out.begin(), out.end(), hit_less);
+    if (out.size() > k) out.resize(k);
+    return OK;
+}
+
+template <class F>
+void parallel_for(size_t n, int threads, F&& f) {
+    if (threads <= 0) threads = int(std::max(1u, std::thread::hardware_concurrency()));
+    if (threads == 1 || n < 2) {
+        for (size_t i = 0; i < n; ++i) f(0, i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] {
+            for (;;) {
+                size_t i = next.fetch_add(1, std::memory_order_relaxed);
+                if (i >= n) break;
+                f(t, i);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- kernels ----
+float orc_dot(const float* a, const float* b, size_t n) { return k_dot(a, b, n); }
+float orc_l2(const float* a, const float* b, size_t n) { return k_l2(a, b, n); }
+float orc_dot_portable(const float* a, const float* b, size_t n) { return dot_avx2order_portable(a, b, n); }
+float orc_l2_portable(const float* a, const float* b, size_t n) { return l2_avx2order_portable(a, b, n); }
+float orc_dot_scalar(const float* a, const float* b, size_t n) { return dot_scalar(a, b, n); }
+float orc_l2_scalar(const float* a, const float* b, size_t n) { return l2_scalar(a, b, n); }
+float orc_distance(int metric, const float* a, const float* b, size_t n) { return metric_distance(metric, a, b, n); }
+int64_t orc_i8_dot(const int8_t* a, const int8_t* b, size_t n) { return i8_dot(a, b, n); }
+int64_t orc_i8_l2(const int8_t* a, const int8_t* b, size_t n) { return i8_l2(a, b, n); }
+void orc_sq_encode(const float* x, const float* offset, float scale, size_t dim, int8_t* out) {
+    sq_encode(x, offset, scale, dim, out);
+}
+float orc_sq_distance(int metric, float scale, const int8_t* a, const int8_t* b, size_t n) {
+    return sq_distance(metric, scale, a, b, n);
+}
+int32_t orc_prepare_query(int metric, const float* q, size_t dim, float* out) {
+    return prepare_query(metric, q, dim, out);
+}
+uint32_t orc_crc32(const uint8_t* p, size_t n) { return crc32(p, n); }
+int orc_have_avx2() { return have_avx2() ? 1 : 0; }
+
+// ---- generator ----
+void orc_splitmix(uint64_t seed, uint64_t* out, size_t n) {
+    SplitMix64 r{seed};
+    for (size_t i = 0; i < n; ++i) out[i] = r.next();
+}
+// Dataset::gaussian (src/synthetic.rs:81-92): one stream, base then queries.
+void orc_gaussian(size_t nb, size_t nq, size_t dim, uint64_t seed, float* base, float* queries) {
+    SplitMix64 r{seed};
+    for (size_t i = 0; i < nb * dim; ++i) base[i] = float(r.gaussian());
+    for (size_t i = 0; i < nq * dim; ++i) queries[i] = float(r.gaussian());
+}
+// Dataset::clustered (src/synthetic.rs:102-124) with the spread as a parameter.
+void orc_clustered(size_t nb, size_t nq, size_t dim, size_t clusters, double spread, uint64_t seed,
+                   float* base, float* queries) {
+    SplitMix64 r{seed};
+    std::vector<double> centers(clusters * dim);
+    for (auto& c : centers) c = r.gaussian();
+    auto sample = [&](size_t count, float* out) {
+        for (size_t p = 0; p < count; ++p) {
+            size_t c = size_t(r.below(clusters));
+            for (size_t j = 0; j < dim; ++j) out[p * dim + j] = float(centers[c * dim + j] + spread * r.gaussian());
+        }
+    };
+    sample(nb, base);
+    sample(nq, queries);
+}
+
+// ---- index ----
+void* orc_index_load(const uint8_t* p, size_t len) {
+    if (len < 60 || std::memcmp(p, "HNSWIDX\0", 8) != 0) return nullptr;
+    uint32_t stored;
+    std::memcpy(&stored, p + len - 4, 4);
+    if (crc32(p, len - 4) != stored) return nullptr;
+    Rd r{p, len - 4, 8};
+    auto* ix = new Index();
+    if (r.get<uint32_t>() != 1) { delete ix; return nullptr; }
+    ix->metric = r.get<uint8_t>();
+    r.get<uint8_t>();
+    r.get<uint8_t>();
+    ix->quantized = r.get<uint8_t>() == 1;
+    ix->dim = r.get<uint32_t>();
+    ix->m = r.get<uint32_t>();
+    ix->m0 = r.get<uint32_t>();
+    r.get<uint32_t>();
+    r.get<double>();
+    r.get<uint64_t>();
+    ix->n = r.get<uint32_t>();
+    ix->entry = r.get<uint32_t>();
+    size_t n = ix->n, dim = ix->dim;
+    const uint8_t* kb = r.take(n * 8);
+    const uint8_t* lb = r.take(n);
+    const uint8_t* fb = r.take(n);
+    const uint8_t* vb = r.take(n * dim * 4);
+    if (!r.ok) { delete ix; return nullptr; }
+    ix->keys.resize(n);
+    std::memcpy(ix->keys.data(), kb, n * 8);
+    ix->levels.assign(lb, lb + n);
+    ix->deleted.assign(fb, fb + n);
+    ix->vectors.resize(n * dim);
+    std::memcpy(ix->vectors.data(), vb, n * dim * 4);
+    ix->l0.assign(n * (ix->m0 + 1), 0);
+    ix->upper.resize(n);
+    for (size_t id = 0; id < n; ++id) {
+        ix->top = std::max(ix->top, ix->levels[id]);
+        ix->upper[id].assign(size_t(ix->levels[id]) * (ix->m + 1), 0);
+        for (unsigned layer = 0; layer <= ix->levels[id]; ++layer) {
+            uint32_t cnt = r.get<uint32_t>();
+            uint32_t cap = layer == 0 ? ix->m0 : ix->m;
+            if (!r.ok || cnt > cap) { delete ix; return nullptr; }
+            uint32_t* blk = layer == 0 ? ix->l0.data() + id * (ix->m0 + 1)
+                                       : ix->upper[id].data() + (layer - 1) * (ix->m + 1);
+            blk[0] = cnt;
+            for (uint32_t j = 0; j < cnt; ++j) blk[1 + j] = r.get<uint32_t>();
+        }
+    }
+    if (ix->quantized) {
+        ix->offset.resize(dim);
+        for (size_t j = 0; j < dim; ++j) ix->offset[j] = r.get<float>();
+        ix->scale = r.get<float>();
+        ix->codes.resize(n * dim);
+        // Codes are re-derived from offsets and scale (src/hnsw/mod.rs:769-775).
+        for (size_t id = 0; id < n; ++id)
+            sq_encode(ix->vec(uint32_t(id)), ix->offset.data(), ix->scale, dim, ix->codes.data() + id * dim);
+    }
+    if (!r.ok || r.pos != r.n) { delete ix; return nullptr; }
+    for (size_t id = 0; id < n; ++id) ix->live += ix->deleted[id] ? 0 : 1;
+    if (n == 0) ix->entry = 0xFFFFFFFFu;
+    return ix;
+}
+
+void orc_index_free(void* ix) { delete static_cast<Index*>(ix); }
+uint32_t orc_index_nodes(void* ix) { return static_cast<Index*>(ix)->n; }
+uint32_t orc_index_dim(void* ix) { return static_cast<Index*>(ix)->dim; }
+int orc_index_metric(void* ix) { return static_cast<Index*>(ix)->metric; }
+const int8_t* orc_index_codes(void* ix) { return static_cast<Index*>(ix)->codes.data(); }
+
+// HnswIndex::search_batch / search_with / search_filtered
+// (src/hnsw/mod.rs:412-536). `filter_bits` (optional) is a key bitmap of
+// `filter_nbits` bits, shared by all queries when filter_stride == 0, else
+// query i uses filter_bits + i*filter_stride (in u64 words). Outputs are
+// nq*k arrays; counts[i] results for query i. Per-query counters (optional):
+// stats[4*i + {0,1,2,3}] = layer-0 distances, layer-0 expansions, upper-layer
+// distances, upper-layer list reads.
+void orc_search_batch(void* handle, const float* queries, size_t nq, size_t k, const size_t* ks,
+                      size_t ef, const size_t* efs, int quantized, const uint64_t* filter_bits,
+                      uint64_t filter_nbits, size_t filter_stride, const uint8_t* use_filter,
+                      uint64_t* out_keys, float* out_dist, uint32_t* counts, int32_t* status,
+                      uint64_t* stats, int threads, size_t out_stride) {
+    const Index& ix = *static_cast<Index*>(handle);
+    int nt = threads <= 0 ? int(std::max(1u, std::thread::hardware_concurrency())) : threads;
+    std::vector<Scratch> scratch(static_cast<size_t>(nt));
+    if (out_stride == 0) out_stride = k;
+    parallel_for(nq, nt, [&](int t, size_t i) {
+        Filter f;
+        if (filter_bits && (!use_filter || use_filter[i])) {
+            f.bits = filter_bits + (filter_stride ? i * filter_stride : 0);
+            f.nbits = filter_nbits;
+        }
+        std::vector<Hit> hits;
+        Stats st;
+        size_t ki = ks ? ks[i] : k, efi = efs ? efs[i] : ef;
+        status[i] = search_one(ix, scratch[size_t(t)], queries + i * ix.dim, ki, efi, quantized != 0, f, hits, st);
+        counts[i] = uint32_t(hits.size());
+        for (size_t j = 0; j < hits.size(); ++j) {
+            out_keys[i * out_stride + j] = hits[j].key;
+            out_dist[i * out_stride + j] = hits[j].d;
+        }
+        if (stats) {
+            stats[4 * i + 0] = st.dist0;
+            stats[4 * i + 1] = st.exp0;
+            stats[4 * i + 2] = st.dist_up;
+            stats[4 * i + 3] = st.exp_up;
+        }
+    });
+}
+
+// BruteForceIndex::search_filtered / search_batch (src/brute.rs:122-180) over
+// rows already prepared (unit length for cosine, src/vector.rs:50-66): a
+// bounded max-heap of (total_cmp distance, key), into_sorted_vec ascending.
+void orc_brute_batch(int metric, const float* base, const uint64_t* keys, size_t nb, size_t dim,
+                     const float* queries, size_t nq, size_t k, uint64_t* out_keys, float* out_dist,
+                     uint32_t* counts, int32_t* status, int threads) {
+    parallel_for(nq, threads, [&](int, size_t i) {
+        std::vector<float> q(dim);
+        status[i] = prepare_query(metric, queries + i * dim, dim, q.data());
+        counts[i] = 0;
+        if (status[i] != OK || k == 0) return;
+        size_t kk = std::min(k, nb);
+        auto less = [](const Hit& a, const Hit& b) { return hit_less(a, b); };
+        std::priority_queue<Hit, std::vector<Hit>, decltype(less)> heap(less);
+        for (size_t r = 0; r < nb; ++r) {
+            Hit h{keys ? keys[r] : uint64_t(r), metric_distance(metric, q.data(), base + r * dim, dim)};
+            if (heap.size() < kk) heap.push(h);
+            else if (hit_less(h, heap.top())) {
+                heap.pop();
+                heap.push(h);
+            }
+        }
+        size_t c = heap.size();
+        counts[i] = uint32_t(c);
+        for (size_t j = c; j-- > 0;) {
+            out_keys[i * k + j] = heap.top().key;
+            out_dist[i * k + j] = heap.top().d;
+            heap.pop();
+        }
+    });
+}
+
+// Double-precision scoring for the precision study of brute force: exact
+// top-k by (f64 distance, key). Used as the FP64 oracle.
+void orc_brute_f64(int metric, const float* base, size_t nb, size_t dim, const float* queries, size_t nq,
+                   size_t k, uint64_t* out_keys, double* out_dist, int threads) {
+    parallel_for(nq, threads, [&](int, size_t i) {
+        const float* q = queries + i * dim;
+        std::vector<std::pair<double, uint64_t>> best;
+        best.reserve(k + 1);
+        auto cmp = [](const std::pair<double, uint64_t>& a, const std::pair<double, uint64_t>& b) {
+            return a.first != b.first ? a.first < b.first : a.second < b.second;
+        };
+        std::priority_queue<std::pair<double, uint64_t>, std::vector<std::pair<double, uint64_t>>, decltype(cmp)> heap(cmp);
+        for (size_t r = 0; r < nb; ++r) {
+            const float* x = base + r * dim;
+            double s = 0.0;
+            if (metric == L2) {
+                for (size_t j = 0; j < dim; ++j) {
+                    double d = double(q[j]) - double(x[j]);
+                    s += d * d;
+                }
+            } else {
+                for (size_t j = 0; j < dim; ++j) s += double(q[j]) * double(x[j]);
+                s = metric == IP ? -s : 1.0 - s;
+            }
+            std::pair<double, uint64_t> h{s, uint64_t(r)};
+            if (heap.size() < k) heap.push(h);
+            else if (cmp(h, heap.top())) {
+                heap.pop();
+                heap.push(h);
+            }
+        }
+        size_t c = heap.size();
+        for (size_t j = c; j-- > 0;) {
+            out_keys[i * k + j] = heap.top().second;
+            out_dist[i * k + j] = heap.top().first;
+            heap.pop();
+        }
+    });
+}
+
+// eval::recall_at_k (src/eval.rs:25-47) over fixed-stride key arrays.
+double orc_recall_at_k(const uint64_t* truth, const uint32_t* truth_counts, size_t truth_stride,
+                       const uint64_t* found, const uint32_t* found_counts, size_t found_stride, size_t nq,
+                       size_t k) {
+    size_t hits = 0, expected = 0;
+    for (size_t i = 0; i < nq; ++i) {
+        size_t tn = std::min<size_t>(k, truth_counts[i]), fn = std::min<size_t>(k, found_counts[i]);
+        expected += tn;
+        for (size_t a = 0; a < fn; ++a)
+            for (size_t b = 0; b < tn; ++b)
+                if (found[i * found_stride + a] == truth[i * truth_stride + b]) {
+                    ++hits;
+                    break;
+                }
+    }
+    return expected == 0 ? 1.0 : double(hits) / double(expected);
+}
+
+}  // extern "C"

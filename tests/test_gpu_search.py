@@ -1,0 +1,291 @@
+"""GPU HNSW search vs the CPU oracle, through the C ABI.
+
+The bar is bit-exact: the same keys, the same f32 distance bits and the same
+counts as the oracle's restatement of HnswIndex::search_batch / search_with
+(src/hnsw/mod.rs:412-536) on the same index file and queries. The integer
+and visited/filter/tombstone logic is exact by construction, and distances
+are computed in the reference AVX2 kernel order, so no tolerance is needed.
+"""
+
+import numpy as np
+import pytest
+
+import hnsw_gpu as H
+import oracle as O
+from conftest import build_index
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_same(gpu, ref, label=""):
+    gk, gd, gc, gs = gpu
+    rk, rd, rc, rs = ref
+    np.testing.assert_array_equal(gs, rs, err_msg=f"{label}: status")
+    np.testing.assert_array_equal(gc, rc, err_msg=f"{label}: counts")
+    for i in range(len(gc)):
+        c = int(gc[i])
+        np.testing.assert_array_equal(gk[i, :c], rk[i, :c], err_msg=f"{label}: keys of query {i}")
+        np.testing.assert_array_equal(gd[i, :c].view(np.uint32), rd[i, :c].view(np.uint32),
+                                      err_msg=f"{label}: distance bits of query {i}")
+
+
+@pytest.fixture(scope="module")
+def gaussian_10k():
+    """Config 1: 10k x 128 N(0,1) seed 42, queries seed 43, L2, M=16, seed 7."""
+    base, _ = H.gaussian(10_000, 0, 128, 42)
+    _, queries = H.gaussian(0, 1000, 128, 43)
+    data = build_index(base, metric=0, m=16, seed=7)
+    return base, queries, data
+
+
+def test_config1_bit_exact(gaussian_10k):
+    base, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    gpu = gi.search_arrays(queries, 10, 64)
+    ref = oi.search(queries, 10, 64)
+    assert_same(gpu, ref, "config 1")
+    tk, _, tc, _ = O.brute(0, base, queries, 10)
+    r_gpu = O.recall_at_k(tk, tc, gpu[0], gpu[2], 10)
+    r_ref = O.recall_at_k(tk, tc, ref[0], ref[2], 10)
+    assert r_gpu == r_ref
+
+
+@pytest.mark.parametrize("ef", [1, 10, 16, 32, 100, 128, 256, 512])
+def test_ef_sweep_bit_exact(gaussian_10k, ef):
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    assert_same(gi.search_arrays(queries[:300], 10, ef), oi.search(queries[:300], 10, ef), f"ef={ef}")
+
+
+def test_persistent_mode_matches_plain(gaussian_10k):
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    a = gi.search_arrays(queries, 10, 64, mode=0)
+    b = gi.search_arrays(queries, 10, 64, mode=1)
+    assert_same(a, b, "persistent")
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("dim", [1, 7, 8, 31, 33, 40, 96])
+def test_metrics_and_dims(metric, dim):
+    base, queries = H.gaussian(1500, 40, dim, 100 + dim)
+    if metric == 2:
+        base[:, 0] += np.where(base[:, 0] >= 0, 1.0, -1.0)
+        queries[:, 0] += 1.0
+    data = build_index(base, metric=metric, m=8, seed=3)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    assert_same(gi.search_arrays(queries, 7, 20), oi.search(queries, 7, 20), f"metric={metric} dim={dim}")
+
+
+def test_m0_above_32_and_large_k():
+    base, queries = H.mixture(4000, 60, 24, 40, 0.4, 9)
+    data = build_index(base, metric=1, m=24, seed=5)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    for k, ef in [(1, 16), (10, 64), (100, 100), (100, 300)]:
+        assert_same(gi.search_arrays(queries, k, ef), oi.search(queries, k, ef), f"k={k} ef={ef}")
+
+
+def test_complete_graph_equals_brute_force():
+    """src/hnsw/tests.rs:113-127: n <= M with simple selection is exhaustive."""
+    base, queries = H.gaussian(16, 20, 8, 3)
+    data = build_index(base, metric=0, m=16, seed=0, parallel=False,
+                       selection=H.NeighborSelection.simple())
+    gi = H.HnswIndex.from_bytes(data)
+    got = gi.search_arrays(queries, 5, 5)
+    tk, td, tc, ts = O.brute(0, base, queries, 5)
+    np.testing.assert_array_equal(got[0], tk)
+    np.testing.assert_array_equal(got[1].view(np.uint32), td.view(np.uint32))
+
+
+def test_tombstones_including_entry_point():
+    """src/hnsw/tests.rs:220-248."""
+    base, queries = H.gaussian(300, 5, 8, 9)
+    data0 = build_index(base, metric=0, m=16, seed=0, parallel=False)
+    info = H.validate_bytes(data0)
+    entry_key = info.entry  # keys are ids here
+    deleted = set(range(0, 300, 2)) | {entry_key}
+    data = build_index(base, metric=0, m=16, seed=0, parallel=False, deleted_keys=sorted(deleted))
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    got = gi.search_arrays(queries, 20, 50)
+    assert_same(got, oi.search(queries, 20, 50), "tombstones")
+    for i in range(len(queries)):
+        assert got[2][i] == 20
+        assert all(int(k) % 2 == 1 and int(k) != entry_key for k in got[0][i, :20])
+
+
+def test_removing_everything_gives_empty_results():
+    base, queries = H.gaussian(50, 1, 4, 4)
+    data = build_index(base, metric=0, parallel=False, deleted_keys=range(50))
+    gi = H.HnswIndex.from_bytes(data)
+    assert gi.search(queries[0], 5, 10) == []
+
+
+def test_filters_during_traversal():
+    """src/hnsw/tests.rs:293-313, plus the retry path for selective filters."""
+    base, queries = H.gaussian(2000, 10, 8, 8)
+    data = build_index(base, metric=0, parallel=False)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    nbits = 2000
+    keys = np.arange(2000, dtype=np.uint64)
+    for accepted, k, ef in [(keys[keys % 10 == 3], 10, 64), (np.array([1234], np.uint64), 3, 10),
+                            (np.zeros(0, np.uint64), 3, 10), (keys[keys % 100 == 7], 10, 32),
+                            (keys[keys % 3 == 0], 50, 200)]:
+        bits = H.key_bitmap(accepted, nbits)
+        got = gi.search_arrays(queries, k, ef, filter_bits=bits, filter_nbits=nbits)
+        ref = oi.search(queries, k, ef, filter_bits=bits, filter_nbits=nbits)
+        assert_same(got, ref, f"filter {accepted.size} keys")
+    only = gi.search_filtered(queries[0], 3, 10, lambda k: k == 1234)
+    assert [n.key for n in only] == [1234]
+    assert gi.search_filtered(queries[0], 3, 10, lambda k: False) == []
+
+
+def test_per_query_filters_k_ef():
+    base, queries = H.mixture(3000, 64, 16, 20, 0.5, 4)
+    data = build_index(base, metric=0, m=12, seed=2)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    rng = np.random.default_rng(0)
+    nbits = 3000
+    words = (nbits + 63) // 64
+    bits = np.zeros((64, words), np.uint64)
+    for i in range(64):
+        sel = rng.random(3000) < rng.uniform(0.01, 0.9)
+        bits[i] = H.key_bitmap(np.nonzero(sel)[0].astype(np.uint64), nbits)
+    used = (rng.random(64) < 0.7).astype(np.uint8)
+    ks = rng.choice([1, 10, 100], 64).astype(np.uint32)
+    efs = rng.choice([16, 32, 64, 128, 256], 64).astype(np.uint32)
+    got = gi.search_arrays(queries, 100, 16, filter_bits=bits, filter_nbits=nbits, filter_stride=words,
+                           filter_used=used, ks=ks, efs=efs)
+    ref = oi.search(queries, 100, 16, filter_bits=bits, filter_nbits=nbits, filter_stride=words,
+                    filter_used=used, ks=ks, efs=efs)
+    assert_same(got, ref, "per-query")
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+def test_quantized_traversal_and_exact_rerank(metric):
+    """src/hnsw/tests.rs:336-368: reported distances are exact."""
+    base, queries = H.gaussian(2000, 20, 32, 12)
+    data = build_index(base, metric=metric, parallel=False, quantize=True)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    got = gi.search_arrays(queries, 10, 64, quantized=True)
+    assert_same(got, oi.search(queries, 10, 64, quantized=True), "quantized")
+    # Distances equal the exact metric recomputed by the reference kernel.
+    pq = queries if metric != 2 else O.normalize_rows(queries)
+    stored = base if metric != 2 else O.normalize_rows(base)
+    for i in range(len(queries)):
+        for j in range(int(got[2][i])):
+            want = O.distance(metric, pq[i], stored[int(got[0][i, j])])
+            assert np.float32(got[1][i, j]).view(np.uint32) == want.view(np.uint32)
+
+
+def test_quantization_disabled_status():
+    base, queries = H.gaussian(200, 2, 8, 1)
+    data = build_index(base)
+    gi = H.HnswIndex.from_bytes(data)
+    with pytest.raises(H.Error) as e:
+        gi.search_arrays(queries, 5, 10, quantized=True)
+    assert e.value.status == H.Status.QUANTIZATION_DISABLED
+
+
+def test_invalid_queries_have_statuses():
+    base, _ = H.gaussian(300, 0, 4, 2)
+    data = build_index(base, metric=2)
+    gi = H.HnswIndex.from_bytes(data)
+    q = np.array([[1, 0, 0, 0], [np.nan, 1, 0, 0], [0, 0, 0, 0], [3e19, 0, 0, 0], [np.inf, 0, 0, 0]],
+                 np.float32)
+    keys, dist, count, status = gi.search_arrays(q, 3, 10, raise_on_error=False)
+    assert list(status) == [0, 3, 4, 3, 3]
+    assert count[0] == 3 and all(count[1:] == 0)
+    with pytest.raises(H.Error):
+        gi.search(q[1], 3, 10)
+    with pytest.raises(H.Error) as e:
+        gi.search_batch(np.zeros(6, np.float32), 3, 10)
+    assert e.value.status == H.Status.DIMENSION_MISMATCH
+
+
+def test_k_and_ef_edge_cases():
+    """src/hnsw/tests.rs:208-218."""
+    base, queries = H.gaussian(100, 1, 4, 2)
+    data = build_index(base, parallel=False)
+    gi = H.HnswIndex.from_bytes(data)
+    assert gi.search(queries[0], 0, 10) == []
+    assert len(gi.search(queries[0], 10, 1)) == 10
+    assert len(gi.search(queries[0], 500, 500)) == 100
+
+
+def test_inner_product_and_cosine_known_answers():
+    """src/hnsw/tests.rs:370-388."""
+    b = H.IndexBuilder(2, H.Metric.InnerProduct)
+    b.insert_batch(np.array([1, 2, 3], np.uint64), np.array([[1, 0], [3, 0], [0, 1]], np.float32))
+    ip = H.HnswIndex.from_bytes(b.to_bytes())
+    hits = ip.search([1.0, 0.0], 3, 10)
+    assert [h.key for h in hits] == [2, 1, 3]
+    assert hits[0].distance == -3.0
+    c = H.IndexBuilder(2, H.Metric.Cosine)
+    c.insert_batch(np.array([1, 2], np.uint64), np.array([[10, 0], [1, 1]], np.float32))
+    cos = H.HnswIndex.from_bytes(c.to_bytes())
+    hits = cos.search([0.1, 0.0], 2, 10)
+    assert hits[0].key == 1 and abs(hits[0].distance) < 1e-6
+    assert abs(hits[1].distance - (1.0 - np.float32(np.sqrt(0.5)))) < 1e-6
+
+
+def test_empty_index():
+    b = H.IndexBuilder(3, H.Metric.L2)
+    gi = H.HnswIndex.from_bytes(b.to_bytes())
+    assert gi.search([0.0, 0.0, 0.0], 5, 10) == []
+
+
+def test_concurrent_searches_match(gaussian_10k):
+    """tests/concurrency.rs:22-58: many host threads on one handle."""
+    import threading
+
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    want = gi.search_arrays(queries[:200], 10, 48)
+    errors = []
+
+    def worker(t):
+        try:
+            for _ in range(3):
+                got = gi.search_arrays(queries[:200], 10, 48)
+                assert_same(got, want, f"thread {t}")
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(6)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors[0]
+
+
+def test_search_batch_equals_individual_searches():
+    """tests/concurrency.rs:61-70."""
+    base, queries = H.gaussian(2000, 50, 16, 5)
+    data = build_index(base, parallel=False)
+    gi = H.HnswIndex.from_bytes(data)
+    batch = gi.search_batch(queries, 10, 40)
+    for i in range(len(queries)):
+        assert batch[i] == gi.search(queries[i], 10, 40)
+    with pytest.raises(H.Error):
+        gi.search_batch(queries.reshape(-1)[:15], 10, 40)
+
+
+def test_set_tombstones_on_device():
+    base, queries = H.gaussian(1000, 30, 16, 21)
+    data = build_index(base, parallel=False)
+    gi = H.HnswIndex.from_bytes(data)
+    dead = np.zeros(1000, np.uint8)
+    dead[::3] = 1
+    gi.set_tombstones(dead)
+    data2 = build_index(base, parallel=False, deleted_keys=range(0, 1000, 3))
+    oi = O.Index(data2)
+    assert_same(gi.search_arrays(queries, 10, 40), oi.search(queries, 10, 40), "device tombstones")
