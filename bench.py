@@ -1,0 +1,416 @@
+"""Benchmark of the device HNSW query path on the plain-GPU config.
+
+Workload (the configuration the headline metric is quoted on): 1,000,000
+base vectors, dim 128, f32, Gaussian mixture of 1,000 centers (centers
+N(0,1), points center + N(0, 0.3^2) per coordinate, seed 1); 10,000 queries
+from the same mixture (seed 2); L2, M=16, M0=32, efConstruction=200; k=10;
+ef swept over {16, 32, 64, 128, 256}. The headline ef is the smallest whose
+recall@10 (against exact brute force on the GPU) is >= 0.95.
+
+A step is one search_batch of the 10,000 queries. `value` is QPS with the
+queries already resident in HBM (CUDA events on the launching stream); `e2e`
+is QPS through the public host-buffer entry point (hnsw_gpu_search_batch),
+host<->device copies included. Inputs (index and vectors, ~650 MB) are far
+larger than L2, so no flush is needed between steps.
+
+`--impl reference` times the CPU restatement of the reference's
+search_batch (the oracle; the Rust crate cannot be built here) on all host
+cores for the same config, metric and unit.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hnsw-index_b200"))
+
+N_BASE, N_QUERY, DIM = 1_000_000, 10_000, 128
+CLUSTERS, SIGMA, BASE_SEED, QUERY_SEED = 1000, 0.3, 1, 2
+M, EF_CONSTRUCTION, LEVEL_SEED = 16, 200, 0
+K = 10
+EF_SWEEP = (16, 32, 64, 128, 256)
+RECALL_TARGET = 0.95
+SELECT_QUERIES = 1000  # ef is chosen on the first 1000 queries (both arms)
+CACHE = os.environ.get("HNSW_BENCH_CACHE", "/tmp/hnsw_b200_bench")
+METRIC = "QPS at recall@10>=0.95 (1M x 128 clustered, k=10)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def workload_tag():
+    s = f"{N_BASE}-{N_QUERY}-{DIM}-{CLUSTERS}-{SIGMA}-{BASE_SEED}-{QUERY_SEED}-{M}-{EF_CONSTRUCTION}-{LEVEL_SEED}"
+    return hashlib.sha1(s.encode()).hexdigest()[:12]
+
+
+def load_data():
+    import hnsw_gpu as H
+
+    return H.mixture_split(N_BASE, N_QUERY, DIM, CLUSTERS, SIGMA, BASE_SEED, QUERY_SEED)
+
+
+def index_file(base, rank, barrier):
+    """Builds the index once per box (host builder, all cores) and caches it."""
+    import hnsw_gpu as H
+
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"index-{workload_tag()}.hnsw")
+    build_s = None
+    if rank == 0 and not os.path.exists(path):
+        t = time.time()
+        b = H.IndexBuilder(DIM, H.Metric.L2, H.HnswParams(m=M, ef_construction=EF_CONSTRUCTION, seed=LEVEL_SEED))
+        b.insert_batch(np.arange(N_BASE, dtype=np.uint64), base)
+        data = b.to_bytes()
+        build_s = time.time() - t
+        tmp = path + f".tmp{os.getpid()}"
+        with open(tmp, "wb") as f:
+            f.write(data)
+        os.replace(tmp, path)
+        log(f"built index in {build_s:.1f} s ({len(data) / 1e6:.0f} MB)")
+    barrier()
+    with open(path, "rb") as f:
+        return f.read(), build_s
+
+
+def start_clock_sampler(device_index: int, path: str):
+    try:
+        return subprocess.Popen(
+            ["nvidia-smi", "-i", str(device_index),
+             "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def stop_clock_sampler(proc, path: str):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+    except OSError:
+        return None
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "search_kernel_1Mx128_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def algorithmic_bytes(counters: np.ndarray, k: int) -> float:
+    """Bytes one search must touch (f32 rows, adjacency lists, query, results):
+    4D per distance, 4(M0+1) per layer-0 list read, 4(M+1) per upper list
+    read, 4D for the query, 12k for the output."""
+    dist = counters[:, 0].astype(np.float64) + counters[:, 2]
+    return float((4 * DIM * dist + 4 * (2 * M + 1) * counters[:, 1] + 4 * (M + 1) * counters[:, 3]
+                  + 4 * DIM + 12 * k).sum())
+
+
+def choose_ef(recalls):
+    for ef in EF_SWEEP:
+        if recalls[ef] >= RECALL_TARGET:
+            return ef
+    return EF_SWEEP[-1]
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the oracle's search_batch on the host cores.
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    base, queries = load_data()
+    data, _ = index_file(base, 0, lambda: None)
+    ix = O.Index(data)
+    cores = os.cpu_count() or 1
+    # ef choice on the first 1000 queries, as in the GPU arm.
+    sel = queries[:SELECT_QUERIES]
+    tk, _, tc, _ = O.brute(0, base, sel, K, threads=cores)
+    recalls = {}
+    for ef in EF_SWEEP:
+        k_, d_, c_, s_ = ix.search(sel, K, ef, threads=cores)
+        recalls[ef] = O.recall_at_k(tk, tc, k_, c_, K)
+    ef = choose_ef(recalls)
+    sample = queries[:2000]
+    for _ in range(args.warmup):
+        ix.search(sample, K, ef, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        ix.search(sample, K, ef, threads=cores)
+        times.append(time.perf_counter() - t)
+    qps = len(sample) * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "plain-1Mx128-clustered", "ef": ef, "k": K, "recall_at_10": recalls[ef],
+                   "sweep_recall_1000q": recalls, "sample_queries": len(sample)},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"{len(sample)} queries per step at ef={ef}, {args.steps} steps"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import hnsw_gpu as H
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+
+        def barrier():
+            dist.barrier()
+    else:
+        torch.cuda.set_device(local)
+
+        def barrier():
+            pass
+
+    dev = torch.device("cuda", local)
+    t0 = time.time()
+    base, queries = load_data()
+    log(f"[rank {rank}] data in {time.time() - t0:.1f} s")
+    data, build_s = index_file(base, rank, barrier)
+    index = H.HnswIndex.from_bytes(data, device=local)
+
+    # Exact ground truth on the GPU (FP32, reference kernel order).
+    truth_path = os.path.join(CACHE, f"truth-{workload_tag()}.npz")
+    if os.path.exists(truth_path):
+        z = np.load(truth_path)
+        tk, tc = z["keys"], z["counts"]
+    else:
+        bf = H.BruteForceIndex(DIM, H.Metric.L2, device=local)
+        bf.insert_batch(np.arange(N_BASE, dtype=np.uint64), base)
+        t = time.time()
+        tk, _, tc, _ = bf.search_arrays(queries, K)
+        log(f"[rank {rank}] ground truth in {time.time() - t:.1f} s")
+        bf.close()
+        if rank == 0:
+            np.savez(truth_path + ".tmp.npz", keys=tk, counts=tc)
+            os.replace(truth_path + ".tmp.npz", truth_path)
+    del base
+
+    # ef sweep: recall on all queries and on the selection subset.
+    recalls, recalls_sel = {}, {}
+    for ef in EF_SWEEP:
+        kk, dd, cc, ss = index.search_arrays(queries, K, ef)
+        recalls[ef] = H.recall_at_k(tk, tc, kk, cc, K)
+        recalls_sel[ef] = H.recall_at_k(tk[:SELECT_QUERIES], tc[:SELECT_QUERIES], kk[:SELECT_QUERIES],
+                                        cc[:SELECT_QUERIES], K)
+    ef = choose_ef(recalls_sel)
+
+    # Traversal counters for the algorithmic byte count (one untimed pass).
+    index.set_counters(True)
+    index.search_arrays(queries, K, ef)
+    counters = index.read_counters(N_QUERY)
+    index.set_counters(False)
+    alg_bytes = algorithmic_bytes(counters, K)
+
+    # Device-resident timing.
+    q_dev = torch.from_numpy(queries).to(dev)
+    o_keys = torch.empty((N_QUERY, K), dtype=torch.int64, device=dev)
+    o_dist = torch.empty((N_QUERY, K), dtype=torch.float32, device=dev)
+    o_cnt = torch.empty(N_QUERY, dtype=torch.int32, device=dev)
+    o_st = torch.empty(N_QUERY, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def step(ef_, mode):
+        index.search_device(q_dev.data_ptr(), N_QUERY, K, ef_, o_keys.data_ptr(), o_dist.data_ptr(),
+                            o_cnt.data_ptr(), o_st.data_ptr(), stream=stream.cuda_stream, mode=mode)
+
+    def timed(ef_, mode, steps, warmup):
+        for _ in range(warmup):
+            step(ef_, mode)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            barrier()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for i in range(steps):
+            starts[i].record(stream)
+            step(ef_, mode)
+            ends[i].record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            barrier()
+        return [s.elapsed_time(e) for s, e in zip(starts, ends)]
+
+    # Plain (one launch per call, warp per query) vs persistent work queue.
+    sweep_qps = {}
+    for e in EF_SWEEP:
+        ms = timed(e, 1, 3, 1)
+        sweep_qps[e] = N_QUERY / (statistics.median(ms) / 1e3)
+    plain_ms = timed(ef, 0, max(3, args.steps // 2), 1)
+    plain_qps = N_QUERY / (statistics.median(plain_ms) / 1e3)
+
+    clock_path = f"/tmp/hnsw_bench_clocks_{rank}.csv"
+    sampler = start_clock_sampler(local, clock_path)
+    step_ms = timed(ef, 1, args.steps, args.warmup)
+    clocks = stop_clock_sampler(sampler, clock_path)
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * N_QUERY * args.steps / (total_ms / 1e3)
+
+    # End to end through the host-buffer API (pinned host memory).
+    q_pin = torch.from_numpy(queries).pin_memory()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        kk, dd, cc, ss = index.search_arrays(q_pin.numpy(), K, ef, mode=1)
+        if i >= args.warmup:
+            e2e_times.append(time.perf_counter() - t)
+    e2e_total = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_qps = world * N_QUERY * len(e2e_times) / e2e_total
+    h2d = N_QUERY * DIM * 4
+    d2h = N_QUERY * K * 12 + N_QUERY * 8
+
+    mean_s = statistics.mean(step_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / mean_s / 1e9
+    traffic = profiled_traffic()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        oi = O.Index(data)
+        cores = os.cpu_count() or 1
+        sample = queries[:2000]
+        oi.search(sample[:200], K, ef, threads=cores)
+        times = []
+        for _ in range(2):
+            t = time.perf_counter()
+            oi.search(sample, K, ef, threads=cores)
+            times.append(time.perf_counter() - t)
+        cpu = {"value": len(sample) / statistics.median(times), "unit": "queries/s", "cores": cores,
+               "kind": "port", "sample": f"{len(sample)} of the {N_QUERY} queries at ef={ef}, median of 2 passes"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        srt = sorted(step_ms)
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": "plain-1Mx128-clustered", "n_base": N_BASE, "n_queries_per_gpu": N_QUERY, "dim": DIM,
+                "clusters": CLUSTERS, "sigma": SIGMA, "M": M, "M0": 2 * M, "ef_construction": EF_CONSTRUCTION,
+                "k": K, "ef": ef, "recall_at_10": recalls[ef], "sweep_recall": recalls, "sweep_qps": sweep_qps,
+                "plain_qps": plain_qps, "persistent_over_plain": value / world / plain_qps,
+                "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
+                "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush",
+                "parallelism": f"replicas x{world}", "index_build_s": build_s,
+            },
+            "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    index.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -188,8 +188,18 @@ struct hnsw_gpu_index {
     bool counters = false;
     std::mutex counters_mu;
     std::vector<uint32_t> last_counters;
+    // Scratch of the device-pointer entry point: one slot, ordered on the
+    // device (an event joins each call after the previous one).
+    std::mutex dev_mu;
+    std::unique_ptr<Slot> dev_slot;
+    cudaEvent_t dev_done = nullptr;
     ~hnsw_gpu_index() {
         DeviceGuard g(device);
+        if (dev_done) {
+            cudaEventSynchronize(dev_done);
+            cudaEventDestroy(dev_done);
+        }
+        dev_slot.reset();
         for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead}) b->release();
         std::lock_guard<std::mutex> l(slots.mu);
         slots.free.clear();
@@ -580,15 +590,22 @@ int hnsw_gpu_search_batch_device(hnsw_gpu_index* gi, const float* d_queries, siz
     const uint32_t ef_bound = std::max(o->k, o->ef);
     const uint32_t stride = o->out_stride ? o->out_stride : std::max<uint32_t>(o->k, 1);
     DeviceGuard dg(gi->device);
-    Slot* s = nullptr;
-    int r = gi->slots.acquire(&s);
-    if (r != HNSW_OK) return r;
+    std::lock_guard<std::mutex> lock(gi->dev_mu);
+    if (!gi->dev_slot) {
+        Slot* s = nullptr;
+        int r = gi->slots.acquire(&s);
+        if (r != HNSW_OK) return r;
+        gi->dev_slot.reset(s);
+        CU(cudaEventCreateWithFlags(&gi->dev_done, cudaEventDisableTiming), "cudaEventCreate");
+        CU(cudaEventRecord(gi->dev_done, s->stream), "cudaEventRecord");
+    }
+    Slot* s = gi->dev_slot.get();
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
-    r = enqueue_search(gi, s, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used, d_keys, d_dist, d_count,
-                       d_status, ef_bound, stride, st);
-    // The slot's buffers are in use until the stream reaches this point.
-    cudaStreamSynchronize(st);
-    gi->slots.release(s);
+    // The slot's buffers may still be in use by the previous call on another stream.
+    CU(cudaStreamWaitEvent(st, gi->dev_done, 0), "cudaStreamWaitEvent");
+    int r = enqueue_search(gi, s, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used, d_keys, d_dist,
+                           d_count, d_status, ef_bound, stride, st);
+    CU(cudaEventRecord(gi->dev_done, st), "cudaEventRecord");
     return r;
 }
 
@@ -783,6 +800,11 @@ void hnsw_synthetic_gaussian(size_t nb, size_t nq, size_t dim, uint64_t seed, fl
 void hnsw_synthetic_mixture(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t seed,
                             float* base, float* queries) {
     synthetic_mixture(nb, nq, dim, clusters, sigma, seed, base, queries);
+}
+
+void hnsw_synthetic_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t base_seed,
+                                  uint64_t query_seed, float* base, float* queries) {
+    synthetic_mixture_split(nb, nq, dim, clusters, sigma, base_seed, query_seed, base, queries);
 }
 
 }  // extern "C"

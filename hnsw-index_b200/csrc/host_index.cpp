@@ -510,6 +510,22 @@ void synthetic_mixture(size_t nb, size_t nq, size_t dim, size_t clusters, double
     sample(nq, queries);
 }
 
+void synthetic_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t base_seed,
+                             uint64_t query_seed, float* base, float* queries) {
+    SplitMix64 r{base_seed};
+    std::vector<double> centers(clusters * dim);
+    for (auto& c : centers) c = r.gaussian();
+    auto sample = [&](SplitMix64& g, size_t count, float* out) {
+        for (size_t p = 0; p < count; ++p) {
+            size_t c = size_t(g.below(clusters));
+            for (size_t j = 0; j < dim; ++j) out[p * dim + j] = float(centers[c * dim + j] + sigma * g.gaussian());
+        }
+    };
+    sample(r, nb, base);
+    SplitMix64 rq{query_seed};
+    sample(rq, nq, queries);
+}
+
 // ---------------------------------------------------------------------------
 // Construction (src/hnsw/mod.rs:290-400, src/hnsw/build.rs:19-222)
 // ---------------------------------------------------------------------------

@@ -117,5 +117,7 @@ private:
 void synthetic_gaussian(size_t nb, size_t nq, size_t dim, uint64_t seed, float* base, float* queries);
 void synthetic_mixture(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t seed,
                        float* base, float* queries);
+void synthetic_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t base_seed,
+                             uint64_t query_seed, float* base, float* queries);
 
 }  // namespace hnswgpu

@@ -332,7 +332,7 @@ __device__ int32_t prepare(QueryCtx& c, const float* q) {
             norm = __dadd_rn(norm, __dmul_rn(x, x));
         }
     norm = __shfl_sync(kFull, norm, 0);
-    if (norm > 4.2535295865117308e37 /* f32::MAX / 8 */) return ST_NON_FINITE;
+    if (norm > double(3.40282346638528859812e+38F) / 8.0) return ST_NON_FINITE;  // f32::MAX / 8
     if (c.metric == 2) {
         if (norm == 0.0) return ST_ZERO;
         const double inv = __ddiv_rn(1.0, __dsqrt_rn(norm));

@@ -175,6 +175,8 @@ _lib.hnsw_synthetic_gaussian.argtypes = [_sz, _sz, _sz, C.c_uint64, _vp, _vp]
 _lib.hnsw_synthetic_gaussian.restype = None
 _lib.hnsw_synthetic_mixture.argtypes = [_sz, _sz, _sz, _sz, C.c_double, C.c_uint64, _vp, _vp]
 _lib.hnsw_synthetic_mixture.restype = None
+_lib.hnsw_synthetic_mixture_split.argtypes = [_sz, _sz, _sz, _sz, C.c_double, C.c_uint64, C.c_uint64, _vp, _vp]
+_lib.hnsw_synthetic_mixture_split.restype = None
 _lib.hnsw_crc32.argtypes = [_vp, _sz]
 _lib.hnsw_crc32.restype = C.c_uint32
 
@@ -186,7 +188,7 @@ EXPORTED_SYMBOLS = (
     "hnsw_params_default", "hnsw_builder_new", "hnsw_builder_free", "hnsw_builder_insert",
     "hnsw_builder_insert_batch", "hnsw_builder_remove", "hnsw_builder_enable_quantization",
     "hnsw_builder_to_bytes", "hnsw_bytes_free", "hnsw_synthetic_gaussian",
-    "hnsw_synthetic_mixture", "hnsw_crc32",
+    "hnsw_synthetic_mixture", "hnsw_synthetic_mixture_split", "hnsw_crc32",
 )
 
 LIBRARY_PATH = _LIB_PATH
@@ -456,7 +458,7 @@ class HnswIndex:
         return out
 
     def search_device(self, d_queries: int, nq: int, k: int, ef: int, d_keys: int, d_dist: int,
-                      d_count: int, d_status: int, stream: int = 0, quantized: bool = False,
+                      d_count: int, d_status: int, stream: Optional[int] = None, quantized: bool = False,
                       mode: int = 0, out_stride: int = 0):
         """hnsw_gpu_search_batch_device with raw device pointers."""
         o = _Opts()
@@ -464,8 +466,10 @@ class HnswIndex:
         o.quantized = int(quantized)
         o.out_stride = out_stride or k
         o.mode = mode
+        # stream None = the library's own stream; 0 = the legacy default stream.
+        handle = None if stream is None else (stream if stream != 0 else 1)
         _check(_lib.hnsw_gpu_search_batch_device(self._h, d_queries, nq, self.dim(), C.byref(o), d_keys,
-                                                 d_dist, d_count, d_status, stream or None))
+                                                 d_dist, d_count, d_status, handle))
 
 
 def validate_bytes(data: bytes, max_memory: Optional[int] = None) -> _Info:
@@ -635,6 +639,16 @@ def mixture(n_base: int, n_query: int, dim: int, clusters: int, sigma: float, se
     base = np.empty((n_base, dim), np.float32)
     queries = np.empty((n_query, dim), np.float32)
     _lib.hnsw_synthetic_mixture(n_base, n_query, dim, clusters, sigma, seed, _ptr(base), _ptr(queries))
+    return base, queries
+
+
+def mixture_split(n_base: int, n_query: int, dim: int, clusters: int, sigma: float, base_seed: int,
+                  query_seed: int):
+    """Mixture with base (and centers) from base_seed and queries from query_seed."""
+    base = np.empty((n_base, dim), np.float32)
+    queries = np.empty((n_query, dim), np.float32)
+    _lib.hnsw_synthetic_mixture_split(n_base, n_query, dim, clusters, sigma, base_seed, query_seed, _ptr(base),
+                                      _ptr(queries))
     return base, queries
 
 

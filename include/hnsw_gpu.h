@@ -130,8 +130,11 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* index, const float* queries, size_t nq
                           uint32_t* out_count, int32_t* out_status);
 
 /* Same with every pointer (queries, ks, efs, filter bits, outputs) in device
- * memory, enqueued on `stream` (a cudaStream_t; NULL = the handle's stream).
- * Per-query statuses are written asynchronously. */
+ * memory, enqueued on `stream` (a cudaStream_t; NULL = the handle's own
+ * stream; cudaStreamLegacy for the legacy default stream). Returns once the
+ * work is enqueued; per-query statuses are written asynchronously. opts->k
+ * and opts->ef bound every per-query k and ef. Calls on one handle share one
+ * scratch area and are ordered on the device in call order. */
 int hnsw_gpu_search_batch_device(hnsw_gpu_index* index, const float* d_queries, size_t nq, size_t dim,
                                  const hnsw_search_opts* d_opts, uint64_t* d_keys, float* d_dist,
                                  uint32_t* d_count, int32_t* d_status, void* stream);
@@ -215,6 +218,12 @@ void hnsw_synthetic_gaussian(size_t n_base, size_t n_query, size_t dim, uint64_t
  * then per point next_below(clusters) and dim Gaussians. */
 void hnsw_synthetic_mixture(size_t n_base, size_t n_query, size_t dim, size_t clusters, double sigma,
                             uint64_t seed, float* base, float* queries);
+/* The same mixture with the queries drawn from their own stream: centers
+ * and base points from SplitMix64(base_seed) as hnsw_synthetic_mixture,
+ * then queries (next_below(clusters) and dim Gaussians each) from
+ * SplitMix64(query_seed) around the same centers. */
+void hnsw_synthetic_mixture_split(size_t n_base, size_t n_query, size_t dim, size_t clusters, double sigma,
+                                  uint64_t base_seed, uint64_t query_seed, float* base, float* queries);
 /* CRC-32 (IEEE) of a buffer (src/crc32.rs). */
 uint32_t hnsw_crc32(const uint8_t* bytes, size_t len);
 

@@ -198,10 +198,12 @@ def test_invalid_queries_have_statuses():
     base, _ = H.gaussian(300, 0, 4, 2)
     data = build_index(base, metric=2)
     gi = H.HnswIndex.from_bytes(data)
-    q = np.array([[1, 0, 0, 0], [np.nan, 1, 0, 0], [0, 0, 0, 0], [3e19, 0, 0, 0], [np.inf, 0, 0, 0]],
-                 np.float32)
+    # 6.521909e18 squared lies between f32::MAX / 8 and 2^125: rejected (src/vector.rs:16,36-38).
+    q = np.array([[1, 0, 0, 0], [np.nan, 1, 0, 0], [0, 0, 0, 0], [3e19, 0, 0, 0], [np.inf, 0, 0, 0],
+                  [6.521909e18, 0, 0, 0]], np.float32)
     keys, dist, count, status = gi.search_arrays(q, 3, 10, raise_on_error=False)
-    assert list(status) == [0, 3, 4, 3, 3]
+    assert list(status) == [0, 3, 4, 3, 3, 3]
+    assert O.prepare_query(2, q[5])[0] == 3
     assert count[0] == 3 and all(count[1:] == 0)
     with pytest.raises(H.Error):
         gi.search(q[1], 3, 10)

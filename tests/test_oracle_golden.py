@@ -158,6 +158,9 @@ def test_prepare_query_validation():
     assert O.prepare_query(0, [np.finfo(np.float32).max] * 2)[0] == 3
     assert O.prepare_query(2, [0.0, 0.0])[0] == 4
     assert O.prepare_query(0, [1.3e19])[0] == 3
+    # Squared norm just above f32::MAX / 8 (and below 2^125) is rejected.
+    assert O.prepare_query(0, [6.521909e18])[0] == 3
+    assert O.prepare_query(0, [6.5219e18])[0] == 0
     assert O.prepare_query(0, [0.0, 0.0])[0] == 0
 
 
