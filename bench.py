@@ -96,7 +96,7 @@ def start_clock_sampler(device_index: int, path: str):
              "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "200"],
+             "--format=csv,noheader,nounits", "-lms", "100"],
             stdout=open(path, "w"), stderr=subprocess.DEVNULL)
     except Exception:
         return None
@@ -276,6 +276,9 @@ def run_gpu(args):
     counters = index.read_counters(N_QUERY)
     index.set_counters(False)
     alg_bytes = algorithmic_bytes(counters, K)
+    visited = counters[:, 0].astype(np.float64)
+    visit_stats = {"p50": float(np.percentile(visited, 50)), "p99": float(np.percentile(visited, 99)),
+                   "max": float(visited.max()), "expansions_p50": float(np.percentile(counters[:, 1], 50))}
 
     # Device-resident timing.
     q_dev = torch.from_numpy(queries).to(dev)
@@ -381,6 +384,7 @@ def run_gpu(args):
                 "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
                 "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush",
                 "parallelism": f"replicas x{world}", "index_build_s": build_s,
+                "layer0_distances_per_query": visit_stats,
             },
             "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
@@ -400,7 +404,7 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -11,6 +11,8 @@
 // bit 1 = the horizontal sum), leaving one pair's distance per lane.
 // Each block keeps a per-query top-k (by total_cmp distance, then key) of its
 // row slice; a merge kernel combines the slices.
+#include <algorithm>
+
 #include "common.cuh"
 #include "device.hpp"
 

@@ -109,10 +109,11 @@ struct Slot {
     DBuf g_results, g_cands, g_visited;
     uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_words = 0;
+    DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
     size_t last_nq = 0;
     ~Slot() {
         for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
-                        &g_results, &g_cands, &g_visited})
+                        &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands})
             b->release();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -161,18 +162,33 @@ struct DeviceGuard {
 // Scratch geometry per (ef bound): results, candidates and the visited
 // hash sized so that a typical traversal at that ef stays in shared memory.
 // Queries whose ef exceeds the fast kernel's 1024 go to the retry pass.
-SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc) {
+// Persistent warps spill to global memory instead of restarting, so their
+// visited hash is sized near the typical visit count (about 12 per unit of
+// ef on the 1M x 128 workload, p99 about 25); plain warps size it for the tail.
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent) {
     constexpr uint32_t kSmemBudget = 220 * 1024;
     SearchGeometry g;
     g.ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_max, 32)));
     g.cand_cap = 2 * g.ef_cap + 32;
-    uint32_t want = g.ef_cap * 48;
+    uint32_t want = g.ef_cap * (persistent ? 32 : 48);
     uint32_t h = 2048;
     while (h < want && h < 32768) h <<= 1;
     g.hash_cap = h;
     while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget && g.hash_cap > 1024) g.hash_cap >>= 1;
-    const uint32_t bpw = geometry_bytes_per_warp(g, dp, dc);
-    g.warps_per_block = std::max<uint32_t>(1, std::min<uint32_t>(4, kSmemBudget / bpw));
+    // Warps per block that maximise resident warps per SM.
+    uint32_t best_warps = 0, best_wpb = 1;
+    for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
+        SearchGeometry t = g;
+        t.warps_per_block = wpb;
+        if (size_t(geometry_bytes_per_warp(t, dp, dc)) * wpb > kSmemBudget) continue;
+        uint32_t warps = 0;
+        if (persistent_warps(t, dp, dc, 1, &warps) != cudaSuccess) continue;
+        if (warps >= best_warps) {
+            best_warps = warps;
+            best_wpb = wpb;
+        }
+    }
+    g.warps_per_block = best_wpb;
     return g;
 }
 
@@ -334,8 +350,12 @@ static int upload(hnsw_gpu_index* gi, const HostIndex& ix) {
         for (uint32_t id = 0; id < n && ids; ++id) ids = ix.keys[id] == id;
         v.keys_are_ids = ids ? 1 : 0;
         std::vector<uint32_t> dead((nn + 31) / 32, 0);
+        v.has_dead = 0;
         for (uint32_t id = 0; id < n; ++id)
-            if (ix.deleted[id]) dead[id >> 5] |= 1u << (id & 31);
+            if (ix.deleted[id]) {
+                dead[id >> 5] |= 1u << (id & 31);
+                v.has_dead = 1;
+            }
         CU(gi->dead.ensure(dead.size() * 4), "cudaMalloc dead");
         CU(cudaMemcpy(gi->dead.p, dead.data(), dead.size() * 4, cudaMemcpyHostToDevice), "copy dead");
         v.dead = gi->dead.as<uint32_t>();
@@ -409,6 +429,7 @@ int hnsw_gpu_set_tombstones(hnsw_gpu_index* index, const uint8_t* deleted, size_
     }
     CU(cudaMemcpy(index->dead.p, dead.data(), dead.size() * 4, cudaMemcpyHostToDevice), "copy tombstones");
     index->view.live = live;
+    index->view.has_dead = live != nodes ? 1 : 0;
     index->info.live = live;
     return HNSW_OK;
 }
@@ -429,8 +450,8 @@ int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq)
 
 // Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
 static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
-    const uint32_t warps = 64;
-    const uint32_t cand_cap = std::max<uint32_t>(1u << 16, 4 * ef_cap);
+    const uint32_t warps = uint32_t(gi->num_sms) * 4;
+    const uint32_t cand_cap = std::max<uint32_t>(1u << 14, 4 * ef_cap);
     const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
     CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
     CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
@@ -448,7 +469,7 @@ static int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t 
                           const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
                           uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
                           uint32_t out_stride, cudaStream_t stream) {
-    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc);
+    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
     CU(s->work.ensure(16), "cudaMalloc work counters");
     CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
     CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
@@ -480,6 +501,23 @@ static int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t 
     a.overflow_count = s->work.as<uint32_t>() + 1;
     a.overflow_list = s->overflow.as<uint32_t>();
     a.persistent = o.mode == HNSW_MODE_PERSISTENT ? 1 : 0;
+    if (a.persistent) {
+        uint32_t warps = 0;
+        CU(persistent_warps(geo, gi->view.dp, gi->view.dc, gi->num_sms, &warps), "occupancy");
+        const uint32_t words = ((gi->view.n + 31) / 32 + 3) & ~3u;
+        const uint32_t cand_cap = std::max<uint32_t>(8192, 4 * geo.ef_cap);
+        const size_t bits_bytes = size_t(warps) * words * 4;
+        if (bits_bytes > s->spill_bits.bytes) {
+            CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
+            CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
+        }
+        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
+        a.spill_bits = s->spill_bits.as<uint32_t>();
+        a.spill_words = words;
+        a.spill_cands = s->spill_cands.as<uint64_t>();
+        a.spill_cand_cap = cand_cap;
+        a.spill_slots = warps;
+    }
     a.g_results = s->g_results.as<uint64_t>();
     a.g_cands = s->g_cands.as<uint64_t>();
     a.g_visited = s->g_visited.as<uint32_t>();

@@ -36,6 +36,12 @@ __device__ __forceinline__ uint32_t pid(uint64_t p) { return uint32_t(p); }
 
 __device__ __forceinline__ float4 ldg_f4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
+// Asks the memory system to bring `bytes` (multiple of 16, 16-byte aligned
+// source) into L2 without occupying registers or shared memory.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // One 32-float step of four AVX2 lanes held by this GPU lane.
 template <bool L2>
 __device__ __forceinline__ void acc4(const float4 x, const float4 y, float (&a)[4]) {

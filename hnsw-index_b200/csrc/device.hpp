@@ -21,6 +21,7 @@ struct DeviceIndexView {
     int metric = 0;
     int quantized = 0;
     int keys_are_ids = 0;
+    int has_dead = 0;  // any tombstone set
     float scale = 1.0f;
     const float* vec = nullptr;        // n * dp
     const int8_t* codes = nullptr;     // n * dc
@@ -72,6 +73,12 @@ struct SearchArgs {
     uint32_t* g_visited = nullptr;  // bitmap, ceil(n/32) words per warp
     uint32_t g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_visited_words = 0;
+    // Per-warp spill areas of the persistent kernel (slot = global warp index).
+    uint32_t* spill_bits = nullptr;   // spill_slots * spill_words (multiple of 4 words)
+    uint32_t spill_words = 0;
+    uint64_t* spill_cands = nullptr;  // spill_slots * (spill_cand_cap + 1)
+    uint32_t spill_cand_cap = 0;
+    uint32_t spill_slots = 0;
 };
 
 // Launches the fast search (plain or persistent) followed by the retry pass
@@ -81,6 +88,8 @@ cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo, int
 cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream);
 // Scratch bytes per warp of a geometry for dimension dp (floats) / dc (bytes).
 uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t dc);
+// Resident warps of the persistent kernel for a geometry (spill slots needed).
+cudaError_t persistent_warps(const SearchGeometry& g, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps);
 
 // Derives int8 codes and their squared norms from offsets and scale
 // (ScalarQuantizer::encode_into, src/quantization.rs:73-81).
@@ -107,5 +116,6 @@ struct BruteArgs {
     uint32_t tiles = 0;
 };
 cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream);
+
 
 }  // namespace hnswgpu

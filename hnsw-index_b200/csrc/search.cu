@@ -19,6 +19,8 @@
 // ids (exact: ids are stored, not hashed away). A query that outgrows the
 // warp's scratch is pushed to an overflow list and re-run by a retry kernel
 // whose scratch lives in global memory (visited bitmap over all nodes).
+#include <algorithm>
+
 #include "common.cuh"
 #include "device.hpp"
 
@@ -42,8 +44,20 @@ struct Ws {
     uint32_t* fr;      // 32: fresh neighbor positions
     float* fd;         // 32: distances of fresh neighbors
     uint32_t ef_cap, cand_cap, hash_cap;
-    bool bitmap_mode;  // H is a bitmap over node ids (retry kernel)
+    bool bitmap_mode;  // H is a bitmap over node ids (retry kernel, or after a spill)
     uint32_t bitmap_words;
+    // Persistent warps own spill areas in global memory: when the shared
+    // visited hash or candidate array fills, the query continues there
+    // instead of restarting. Null in the plain and retry kernels.
+    uint32_t* spill_bits;   // bitmap over node ids (spill_words words, zero between queries)
+    uint32_t spill_words;
+    uint64_t* spill_cands;  // spill_cand_cap + 1 entries
+    uint32_t spill_cand_cap;
+    // The shared-memory arrays, restored after a spilled query.
+    uint32_t* H0;
+    uint64_t* C0;
+    uint32_t cand_cap0;
+    bool spilled_bits, spilled_cands;
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -110,7 +124,7 @@ struct QueryCtx {
 
 __device__ __forceinline__ bool admit(const QueryCtx& c, uint32_t id) {
     const DeviceIndexView& ix = c.a->ix;
-    if ((__ldg(ix.dead + (id >> 5)) >> (id & 31)) & 1u) return false;
+    if (ix.has_dead && ((__ldg(ix.dead + (id >> 5)) >> (id & 31)) & 1u)) return false;
     if (!c.use_filter) return true;
     uint64_t key = ix.keys_are_ids ? uint64_t(id) : __ldg(ix.keys + id);
     return key < c.fnbits && ((__ldg(c.fbits + (key >> 6)) >> (key & 63)) & 1ull);
@@ -206,13 +220,103 @@ __device__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
     }
 }
 
+// First index in the ascending A[lo, hi) whose entry is not below x (one lane).
+__device__ __forceinline__ uint32_t lower_bound(const uint64_t* A, uint32_t lo, uint32_t hi, uint64_t x) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Merges the entries x held by the lanes in S into the ascending A[lo, hi),
+// keeping only positions below `limit` (truncation of the results array to
+// ef). Entries are distinct. All lanes call.
+__device__ __forceinline__ void batch_merge(uint64_t* A, uint32_t lo, uint32_t hi, uint32_t S, uint64_t x,
+                                            uint32_t limit) {
+    const int lane = lane_id();
+    const bool in = (S >> lane) & 1u;
+    uint32_t rank_s = 0;
+    for (uint32_t bits = S; bits; bits &= bits - 1) {
+        const int j = __ffs(bits) - 1;
+        rank_s += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
+    }
+    const uint32_t pa = in ? lower_bound(A, lo, hi, x) : hi;
+    // The smallest new entry sits at the lowest insertion point.
+    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
+    if (hi > pmin) {
+        for (int base = int((hi - 1) & ~31u); base >= int(pmin & ~31u); base -= 32) {
+            const uint32_t k = uint32_t(base) + uint32_t(lane);
+            const bool mv = k >= pmin && k < hi;
+            const uint64_t v = mv ? A[k] : 0;
+            uint32_t shift = 0;
+            for (uint32_t bits = S; bits; bits &= bits - 1) {
+                const int j = __ffs(bits) - 1;
+                shift += (__shfl_sync(kFull, x, j) < v) ? 1u : 0u;
+            }
+            __syncwarp();
+            if (mv && k + shift < limit) A[k + shift] = v;
+            __syncwarp();
+        }
+    }
+    if (in && pa + rank_s < limit) A[pa + rank_s] = x;
+    __syncwarp();
+}
+
+// Makes room for `need` more candidates: compacts the queue to the front,
+// then drops candidates worse than the worst of ef results (they can never be
+// expanded). Returns false if the queue is still too small.
+__device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail, uint32_t need, uint32_t rs,
+                                          uint32_t ef) {
+    if (tail + need <= w.cand_cap) return true;
+    const int lane = lane_id();
+    if (head > 0) {
+        const uint32_t n = tail - head;
+        for (uint32_t b = 0; b < n; b += 32) {
+            const uint32_t j = b + lane;
+            const uint64_t v = j < n ? w.C[head + j] : 0;
+            __syncwarp();
+            if (j < n) w.C[j] = v;
+            __syncwarp();
+        }
+        head = 0;
+        tail = n;
+    }
+    if (tail + need > w.cand_cap && rs >= ef) {
+        const float wd = pdist(w.R[rs - 1]);
+        uint32_t keep = head;
+        for (uint32_t b = head; b < tail; b += 32) {
+            const uint32_t j = b + lane;
+            const bool ok = j < tail && !(pdist(w.C[j]) > wd);
+            keep += __popc(__ballot_sync(kFull, ok));
+        }
+        tail = keep;
+    }
+    if (tail + need > w.cand_cap && w.spill_cands && !w.spilled_cands && w.spill_cand_cap > w.cand_cap) {
+        // Move the queue to the warp's global spill array.
+        const uint32_t n = tail - head;
+        for (uint32_t b = 0; b < n; b += 32) {
+            const uint32_t j = b + lane;
+            if (j < n) w.spill_cands[j] = w.C[head + j];
+        }
+        __syncwarp();
+        w.C = w.spill_cands;
+        w.cand_cap = w.spill_cand_cap;
+        w.spilled_cands = true;
+        head = 0;
+        tail = n;
+    }
+    return tail + need <= w.cand_cap;
+}
+
 // search_layer on layer 0 (src/hnsw/search.rs:81-142). Returns the number of
 // results in w.R (sorted ascending), or -1 on scratch overflow.
 __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
     const int lane = lane_id();
-    // Reset the visited set.
+    // Reset the visited set (a spill bitmap is cleared when its query ends).
     if (w.bitmap_mode) {
         for (uint32_t i = lane; i < w.bitmap_words; i += 32) w.H[i] = 0;
     } else {
@@ -238,13 +342,31 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
         if (rs >= ef && pdist(cur) > worst0) break;
         c.cnt.exp0++;
         const uint32_t* row = ix.adj0 + size_t(pid(cur)) * ix.m0p;
+        // The next candidate in the queue is usually the next expansion.
+        if (lane == 0 && head < tail) prefetch_l2(ix.adj0 + size_t(pid(w.C[head])) * ix.m0p, ix.m0p * 4);
         for (uint32_t base = 0; base < ix.m0; base += 32) {
             uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
             const bool valid = id != kEmpty;
             const uint32_t V = __ballot_sync(kFull, valid);
             if (V == 0) break;
-            if (!w.bitmap_mode && visited + __popc(V) > hash_limit) return -1;
+            if (!w.bitmap_mode && visited + __popc(V) > hash_limit) {
+                if (!w.spill_bits) return -1;
+                // Move the visited set into the warp's global bitmap.
+                for (uint32_t i = lane; i < w.hash_cap; i += 32) {
+                    const uint32_t v = w.H[i];
+                    if (v != kEmpty) atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
+                }
+                __syncwarp();
+                w.H = w.spill_bits;
+                w.bitmap_mode = true;
+                w.bitmap_words = w.spill_words;
+                w.spilled_bits = true;
+            }
             const bool fresh = valid && visit(w, id);
+            if (fresh) {
+                if (c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
+                else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
+            }
             const uint32_t F = __ballot_sync(kFull, fresh);
             visited += __popc(F);
             if (F != 0) {
@@ -258,47 +380,63 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                     float wd = pdist(w.R[rs - 1]);
                     P &= __ballot_sync(kFull, fresh && my_d < wd);
                 }
-                while (P) {
-                    const int i = __ffs(P) - 1;
-                    P &= P - 1;
-                    const float d = __shfl_sync(kFull, my_d, i);
-                    const uint32_t nid = __shfl_sync(kFull, id, i);
-                    const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
-                    if (!improves) continue;
-                    const uint64_t x = pack(d, nid);
-                    // Candidate queue: make room if needed.
-                    if (tail == w.cand_cap) {
-                        if (head > 0) {
-                            const uint32_t n = tail - head;
-                            for (uint32_t b = 0; b < n; b += 32) {
-                                uint32_t j = b + lane;
-                                uint64_t v = j < n ? w.C[head + j] : 0;
-                                __syncwarp();
-                                if (j < n) w.C[j] = v;
-                                __syncwarp();
-                            }
-                            head = 0;
-                            tail = n;
-                        }
-                        if (tail == w.cand_cap && rs >= ef) {
-                            // Drop candidates that can never be expanded.
-                            const float wd = pdist(w.R[rs - 1]);
-                            uint32_t keep = head;
-                            for (uint32_t b = head; b < tail; b += 32) {
-                                uint32_t j = b + lane;
-                                bool ok = j < tail && !(pdist(w.C[j]) > wd);
-                                keep += __popc(__ballot_sync(kFull, ok));
-                            }
-                            tail = keep;
-                        }
-                        if (tail == w.cand_cap) return -1;
+                if (P == 0) {
+                    if (V != kFull) break;
+                    continue;
+                }
+                const bool inP = (P >> lane) & 1u;
+                const uint64_t my_x = pack(my_d, id);
+                // Equal distances (IEEE, so -0 == +0) among the improving
+                // neighbors, or with a current result, make the order of
+                // evaluation matter: take the sequential path for this list.
+                const float dz = __fadd_rn(my_d, 0.0f);
+                const unsigned same =
+                    __match_any_sync(kFull, inP ? __float_as_uint(dz) : (0x7FC00000u | uint32_t(lane)));
+                uint32_t pr = 0;  // results below my_x
+                bool tie = inP && __popc(same) > 1;
+                if (inP) {
+                    pr = lower_bound(w.R, 0, rs, my_x);
+                    if (pr < rs && pdist(w.R[pr]) == my_d) tie = true;
+                    if (pr > 0 && pdist(w.R[pr - 1]) == my_d) tie = true;
+                }
+                if (!__any_sync(kFull, tie)) {
+                    // Rank of each neighbor among the results and the admitted
+                    // neighbors before it in list order; it improves iff the
+                    // rank is below ef (src/hnsw/search.rs:125).
+                    uint32_t before = 0;
+                    for (uint32_t bits = A & P; bits; bits &= bits - 1) {
+                        const int j = __ffs(bits) - 1;
+                        const uint64_t xj = __shfl_sync(kFull, my_x, j);
+                        before += (j < lane && xj < my_x) ? 1u : 0u;
                     }
-                    sorted_insert(w.C, head, tail, x);
-                    ++tail;
-                    if ((A >> i) & 1u) {
-                        sorted_insert(w.R, 0, rs, x);
-                        ++rs;
-                        if (rs > ef) rs = ef;
+                    const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
+                    const uint32_t IR = I & A;
+                    if (IR) {
+                        batch_merge(w.R, 0, rs, IR, my_x, ef);
+                        rs = min(rs + uint32_t(__popc(IR)), ef);
+                    }
+                    if (I) {
+                        if (!make_room(w, head, tail, uint32_t(__popc(I)), rs, ef)) return -1;
+                        batch_merge(w.C, head, tail, I, my_x, w.cand_cap);
+                        tail += uint32_t(__popc(I));
+                    }
+                } else {
+                    while (P) {
+                        const int i = __ffs(P) - 1;
+                        P &= P - 1;
+                        const float d = __shfl_sync(kFull, my_d, i);
+                        const uint32_t nid = __shfl_sync(kFull, id, i);
+                        const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
+                        if (!improves) continue;
+                        const uint64_t x = pack(d, nid);
+                        if (!make_room(w, head, tail, 1, rs, ef)) return -1;
+                        sorted_insert(w.C, head, tail, x);
+                        ++tail;
+                        if ((A >> i) & 1u) {
+                            sorted_insert(w.R, 0, rs, x);
+                            ++rs;
+                            if (rs > ef) rs = ef;
+                        }
                     }
                 }
             }
@@ -463,6 +601,34 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_
     w.hash_cap = hash_cap;
     w.bitmap_mode = false;
     w.bitmap_words = 0;
+    w.spill_bits = nullptr;
+    w.spill_words = 0;
+    w.spill_cands = nullptr;
+    w.spill_cand_cap = 0;
+    w.H0 = w.H;
+    w.C0 = w.C;
+    w.cand_cap0 = cand_cap;
+    w.spilled_bits = w.spilled_cands = false;
+}
+
+// Clears a spill bitmap and points the workspace back at shared memory.
+__device__ void end_spill(Ws& w) {
+    const int lane = lane_id();
+    if (w.spilled_bits) {
+        uint4* b = reinterpret_cast<uint4*>(w.spill_bits);
+        for (uint32_t i = lane; i < (w.spill_words >> 2); i += 32) b[i] = make_uint4(0, 0, 0, 0);
+        __threadfence_block();
+        __syncwarp();
+        w.H = w.H0;
+        w.bitmap_mode = false;
+        w.bitmap_words = 0;
+        w.spilled_bits = false;
+    }
+    if (w.spilled_cands) {
+        w.C = w.C0;
+        w.cand_cap = w.cand_cap0;
+        w.spilled_cands = false;
+    }
 }
 
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
@@ -472,12 +638,21 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g.ef_cap, g.cand_cap, g.hash_cap);
     const int lane = lane_id();
     if (a.persistent) {
+        const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
+        if (a.spill_bits && slot < a.spill_slots) {
+            w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;
+            w.spill_words = a.spill_words;
+            w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
+            w.spill_cand_cap = a.spill_cand_cap;
+        }
         for (;;) {
             uint32_t qi = 0;
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
             qi = __shfl_sync(kFull, qi, 0);
             if (qi >= a.nq) break;
-            if (run_query(a, w, qi) == ST_OVERFLOW && lane == 0) {
+            const int32_t st = run_query(a, w, qi);
+            end_spill(w);
+            if (st == ST_OVERFLOW && lane == 0) {
                 a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
                 a.out_status[qi] = ST_OVERFLOW;
             }
@@ -517,6 +692,14 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.hash_cap = 0;
     w.bitmap_mode = true;
     w.bitmap_words = uint32_t(a.g_visited_words);
+    w.spill_bits = nullptr;
+    w.spill_words = 0;
+    w.spill_cands = nullptr;
+    w.spill_cand_cap = 0;
+    w.H0 = w.H;
+    w.C0 = w.C;
+    w.cand_cap0 = w.cand_cap;
+    w.spilled_bits = w.spilled_cands = false;
     const uint32_t total = *a.overflow_count;
     for (uint32_t t = gw; t < total; t += nwarps) {
         const uint32_t qi = a.overflow_list[t];
@@ -565,12 +748,27 @@ cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, 
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         grid = dim3(uint32_t(num_sms * per_sm));
+        // Warps beyond the spill slots run without spill areas (overflow -> retry).
+        (void)0;
     } else {
         grid = dim3((args.nq + geo.warps_per_block - 1) / geo.warps_per_block);
     }
     if (grid.x == 0) return cudaSuccess;
     dev::search_kernel<<<grid, block, smem, stream>>>(args, geo);
     return cudaGetLastError();
+}
+
+cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps) {
+    SearchGeometry g = g_in;
+    g.bytes_per_warp = geometry_bytes_per_warp(g, dp, dc);
+    const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
+    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::search_kernel, int(32 * g.warps_per_block), smem);
+    if (e != cudaSuccess) return e;
+    *warps = uint32_t(std::max(per_sm, 1)) * g.warps_per_block * uint32_t(num_sms);
+    return cudaSuccess;
 }
 
 cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream) {

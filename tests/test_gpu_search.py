@@ -291,3 +291,46 @@ def test_set_tombstones_on_device():
     data2 = build_index(base, parallel=False, deleted_keys=range(0, 1000, 3))
     oi = O.Index(data2)
     assert_same(gi.search_arrays(queries, 10, 40), oi.search(queries, 10, 40), "device tombstones")
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_visited_and_candidate_overflow_paths(mode):
+    """A 0.5%-selective filter with ef=32 cannot fill the results, so every
+    query visits the whole connected graph: the shared-memory visited hash and
+    candidate array overflow. Plain mode re-runs such queries in the retry
+    kernel; persistent mode continues them in per-warp global spill areas."""
+    base, queries = H.gaussian(5000, 48, 16, 77)
+    data = build_index(base, metric=0, m=8, seed=1)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    keys = np.arange(5000, dtype=np.uint64)
+    for accepted, k, ef in [(keys[keys % 200 == 11], 10, 32), (keys[keys % 7 == 0], 10, 32),
+                            (keys[keys % 50 == 3], 25, 64)]:
+        bits = H.key_bitmap(accepted, 5000)
+        got = gi.search_arrays(queries, k, ef, filter_bits=bits, filter_nbits=5000, mode=mode)
+        ref = oi.search(queries, k, ef, filter_bits=bits, filter_nbits=5000)
+        assert_same(got, ref, f"mode={mode} filter={accepted.size}")
+    # The same handle keeps giving exact answers after spilled queries.
+    assert_same(gi.search_arrays(queries, 10, 40, mode=mode), oi.search(queries, 10, 40), "after spill")
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_modes_on_quantized_filtered_tombstoned_mixture(mode):
+    base, queries = H.mixture(6000, 96, 32, 30, 0.4, 8)
+    rng = np.random.default_rng(5)
+    dead = np.nonzero(rng.random(6000) < 0.05)[0]
+    data = build_index(base, metric=1, m=12, seed=4, deleted_keys=dead, quantize=True)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    words = (6000 + 63) // 64
+    bits = np.zeros((96, words), np.uint64)
+    for i in range(96):
+        sel = rng.random(6000) < np.exp(rng.uniform(np.log(0.01), np.log(0.9)))
+        bits[i] = H.key_bitmap(np.nonzero(sel)[0].astype(np.uint64), 6000)
+    ks = rng.choice([1, 10, 100], 96).astype(np.uint32)
+    efs = rng.choice([16, 32, 64, 128, 256, 512], 96).astype(np.uint32)
+    got = gi.search_arrays(queries, 100, 16, quantized=True, filter_bits=bits, filter_nbits=6000,
+                           filter_stride=words, ks=ks, efs=efs, mode=mode)
+    ref = oi.search(queries, 100, 16, quantized=True, filter_bits=bits, filter_nbits=6000,
+                    filter_stride=words, ks=ks, efs=efs)
+    assert_same(got, ref, f"config-4-like mode={mode}")
