@@ -12,6 +12,7 @@
 // Each block keeps a per-query top-k (by total_cmp distance, then key) of its
 // row slice; a merge kernel combines the slices.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "device.hpp"
@@ -304,6 +305,49 @@ cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     dev::brute_merge_kernel<<<(a.nq * 32 + 127) / 128, 128, 0, stream>>>(a, kk, nslices);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Scratch for the allocation-free entry point
+// (hnsw_gpu_brute_search_batch_noalloc). The prepared queries and the
+// per-slice top-k lists live in this fixed array instead of memory the call
+// allocates. Every GPU that loads the library holds it until the process
+// exits. Host code must not pass the array's name to a kernel: on the host it
+// is only a stand-in, so its device address is looked up once per device.
+// ---------------------------------------------------------------------------
+namespace {
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+cudaError_t noalloc_scratch_address(void** out) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+
+bool noalloc_layout(uint32_t nq, uint32_t dp, uint32_t kk, uint32_t want_slices, size_t* qprep_bytes,
+                    uint32_t* slices) {
+    const size_t q = (size_t(nq) * dp * 4 + 255) & ~size_t(255);
+    if (q >= kNoAllocScratchBytes) return false;
+    const size_t per_slice = size_t(nq) * kk * 8;
+    const size_t fit = (kNoAllocScratchBytes - q) / per_slice;
+    if (fit < 1) return false;
+    *qprep_bytes = q;
+    *slices = uint32_t(std::min<size_t>(fit, std::max<uint32_t>(1, want_slices)));
+    return true;
 }
 
 }  // namespace hnswgpu

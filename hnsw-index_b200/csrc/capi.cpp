@@ -750,6 +750,51 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t 
     return HNSW_OK;
 }
 
+// For callers that must not allocate device memory once they are running:
+// all scratch comes from a fixed 8 MiB array compiled into the library.
+int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* b, const float* d_queries, size_t nq, size_t dim,
+                                        uint32_t k, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
+                                        int32_t* d_status, void* stream) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return HNSW_OK;
+    if (!d_queries || !d_count || !d_status || (k && (!d_keys || !d_dist)))
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
+    if (nq > 0x7FFFFFFFu) return set_error(HNSW_ERR_INVALID_ARGUMENT, "batch too large");
+    DeviceGuard dg(b->device);
+    void* scratch = nullptr;
+    CU(noalloc_scratch_address(&scratch), "no-alloc scratch address");
+    const uint32_t kk = std::max<uint32_t>(1, std::min<uint32_t>(k, b->n ? b->n : 1));
+    const uint32_t want = std::max<uint32_t>(1, std::min<uint32_t>(64, (b->n + 8191) / 8192));
+    size_t qbytes = 0;
+    uint32_t slices = 0;
+    if (!noalloc_layout(uint32_t(nq), b->dp, kk, want, &qbytes, &slices))
+        return set_error(HNSW_ERR_INVALID_ARGUMENT,
+                         "batch too large for the no-alloc scratch: nq * (4 * padded dim + 8 * min(k, n)) must "
+                         "stay below 8 MiB");
+    BruteArgs a;
+    a.base = b->base.as<float>();
+    a.keys = b->keys.as<uint64_t>();
+    a.n = b->n;
+    a.dim = b->dim;
+    a.dp = b->dp;
+    a.metric = b->metric;
+    a.queries = d_queries;
+    a.nq = uint32_t(nq);
+    a.k = k;
+    a.out_keys = d_keys;
+    a.out_dist = d_dist;
+    a.out_count = d_count;
+    a.out_status = d_status;
+    a.qprep = static_cast<float*>(scratch);
+    a.part = reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(scratch) + qbytes);
+    a.tiles = slices;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+    CU(launch_brute_fp32(a, st), "brute kernel (no-alloc)");
+    return HNSW_OK;
+}
+
 // ------------------------------------------------------------------------
 // Builder and synthetic data
 // ------------------------------------------------------------------------

@@ -117,5 +117,15 @@ struct BruteArgs {
 };
 cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream);
 
+// Fixed device scratch of the allocation-free brute-force entry point.
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device
+constexpr int kMaxDevices = 64;
+// Device address of that scratch on the current device (looked up once per
+// device with cudaGetSymbolAddress, then cached).
+cudaError_t noalloc_scratch_address(void** out);
+// Splits the scratch into prepared queries and per-slice top-k lists for a
+// batch; false when even one slice does not fit.
+bool noalloc_layout(uint32_t nq, uint32_t dp, uint32_t kk, uint32_t want_slices, size_t* qprep_bytes,
+                    uint32_t* slices);
 
 }  // namespace hnswgpu

@@ -172,6 +172,27 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* brute, const float* queries, siz
                                 uint32_t k, int precision, uint64_t* out_keys, float* out_dist,
                                 uint32_t* out_count, int32_t* out_status);
 
+/* Allocation-free variant of hnsw_gpu_brute_search_batch, FP32 precision,
+ * for callers that cannot allocate device memory while they run: code on a
+ * latency-critical path, in a process whose memory policy forbids cudaMalloc
+ * after start-up, or any caller that must not synchronise the device, which
+ * cudaMalloc and cudaFree may do. It has no counterpart in the reference.
+ * Inputs and outputs are device pointers the caller owns (queries nq x dim;
+ * keys/dist nq x k; count and status nq). Scratch comes from one fixed
+ * 8 MiB array in the library's device memory, held by every GPU that loads
+ * the library until the process exits; a batch must satisfy
+ * nq * (4 * round_up(dim, 32) + 8 * min(k, n)) < 8 MiB, otherwise the call
+ * returns HNSW_ERR_INVALID_ARGUMENT without launching. The first call on a
+ * device looks up the array's device address (once per device, with that
+ * device current); make that first call before any stream capture. All calls
+ * share the one array, so calls whose work overlaps on the GPU (different
+ * streams, no ordering between them) race and corrupt each other's results;
+ * order them on one stream. Enqueued on `stream` (NULL = the handle's
+ * stream); returns once enqueued. */
+int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* brute, const float* d_queries, size_t nq, size_t dim,
+                                        uint32_t k, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
+                                        int32_t* d_status, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Host-side index construction (produces format-v1 files)             */
 /* ------------------------------------------------------------------ */
