@@ -277,7 +277,91 @@ __global__ void brute_merge_kernel(BruteArgs a, uint32_t kk, uint32_t nslices) {
     if (lane == 0) a.out_count[q] = got;
 }
 
+// Exact re-rank of tensor-core candidates (one warp per query): every
+// candidate whose approximate distance is <= thr2[q] gets its FP32 distance
+// in the reference kernel order; a top-k list ordered by (total_cmp distance,
+// key) keeps the best (src/brute.rs:131-160). A query whose candidate list
+// overflowed gets status 25 and is re-run by the exact FP32 kernels.
+__global__ void brute_rerank_kernel(BruteArgs a, const uint64_t* __restrict__ cand,
+                                    const uint32_t* __restrict__ cand_count, uint32_t cand_cap,
+                                    const float* __restrict__ thr2, uint32_t kk) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + uint32_t(warp);
+    uint64_t* L = reinterpret_cast<uint64_t*>(smem) + size_t(warp) * (kk + 1);
+    uint32_t* pos = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(smem) + size_t(blockDim.x >> 5) * (kk + 1)) +
+                    warp * 32;
+    if (q >= a.nq) return;
+    if (a.out_status[q] != 0) {
+        if (lane == 0) a.out_count[q] = 0;
+        return;
+    }
+    const uint32_t total = cand_count[q];
+    if (total > cand_cap) {
+        if (lane == 0) a.out_status[q] = 25;
+        return;
+    }
+    const float t2 = thr2[q];
+    const float* qv = a.qprep + size_t(q) * a.dp;
+    const uint64_t* C = cand + size_t(q) * cand_cap;
+    const int g = lane >> 3, g8 = lane & 7;
+    uint32_t size = 0;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t i = base + uint32_t(lane);
+        uint32_t row = 0;
+        bool pass = false;
+        if (i < total) {
+            const uint64_t c = C[i];
+            pass = __uint_as_float(uint32_t(c >> 32)) <= t2;
+            row = uint32_t(c);
+        }
+        const uint32_t P = __ballot_sync(kFull, pass);
+        if (pass) pos[__popc(P & ((1u << lane) - 1u))] = row;
+        __syncwarp();
+        const uint32_t np = __popc(P);
+        for (uint32_t r = 0; r < np; r += 4) {
+            const uint32_t slot = r + uint32_t(g);
+            const uint32_t rrow = pos[slot < np ? slot : 0];
+            const float* xr = a.base + size_t(rrow) * a.dp;
+            float sum = a.metric == 0 ? group_sum<true>(xr, qv, int(a.dim), g8) : group_sum<false>(xr, qv, int(a.dim), g8);
+            const float d = metric_from_sum(a.metric, sum);
+            const uint64_t e = (uint64_t(fkey(d)) << 32) | rrow;
+            // Insert the (up to) four new entries one after another.
+            for (int gg = 0; gg < 4; ++gg) {
+                if (r + uint32_t(gg) >= np) break;
+                const uint64_t x = __shfl_sync(kFull, e, gg * 8);
+                if (size >= kk && !entry_less(x, L[size - 1], a.keys)) continue;
+                list_insert(L, size, x, a.keys);
+                size = min(size + 1, kk);
+            }
+        }
+        __syncwarp();
+    }
+    const uint32_t want = min(a.k, a.n);
+    for (uint32_t i = lane; i < size && i < want; i += 32) {
+        a.out_keys[size_t(q) * a.k + i] = __ldg(a.keys + uint32_t(L[i]));
+        a.out_dist[size_t(q) * a.k + i] = kdec(uint32_t(L[i] >> 32));
+    }
+    if (lane == 0) a.out_count[q] = min(size, want);
+}
+
 }  // namespace dev
+
+cudaError_t launch_brute_prep(const BruteArgs& a, cudaStream_t stream) {
+    dev::brute_prep_kernel<<<(a.nq * 32 + 127) / 128, 128, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_brute_rerank(const BruteArgs& a, const uint64_t* cand, const uint32_t* cand_count, uint32_t cand_cap,
+                                const float* thr2, cudaStream_t stream) {
+    const uint32_t kk = std::max<uint32_t>(1, std::min<uint32_t>(a.k, a.n ? a.n : 1));
+    const uint32_t wpb = 4;
+    const size_t smem = size_t(wpb) * (kk + 1) * 8 + size_t(wpb) * 32 * 4;
+    cudaError_t e = cudaFuncSetAttribute(dev::brute_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    dev::brute_rerank_kernel<<<(a.nq + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(a, cand, cand_count, cand_cap, thr2, kk);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream) {
     const uint32_t kk = std::max<uint32_t>(1, std::min<uint32_t>(a.k, a.n ? a.n : 1));

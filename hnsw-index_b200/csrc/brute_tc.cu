@@ -1,0 +1,467 @@
+// Tensor-core brute-force scoring on sm_100a (tcgen05 + TMA + TMEM).
+//
+// Scores q . x for every (query, row) pair as one BF16 GEMM with FP32
+// accumulation in tensor memory, either plainly (K' = D, operands rounded to
+// BF16) or with the 3-term split (K' = 3D: queries [q_hi | q_hi | q_lo],
+// rows [x_hi | x_lo | x_hi], so the sum is q_hi.x_hi + q_hi.x_lo + q_lo.x_hi,
+// i.e. q.x up to the dropped q_lo.x_lo term). The epilogue turns each score
+// into the metric's distance and either writes it densely (threshold sample)
+// or keeps only (row, distance) pairs at or below a per-query threshold
+// (candidate pass). Exact FP32 re-ranking of the survivors happens in
+// brute_tc_rerank (K1 order), so the final results are those of
+// BruteForceIndex::search_batch (src/brute.rs:169-180).
+//
+// Kernel structure (one CTA per SM, persistent over 128 x 256 output tiles):
+//   warp 0      TMA producer: A (128 queries x 64 K) and B (256 rows x 64 K)
+//               tiles into a 4-stage shared-memory ring (128-byte swizzle);
+//   warp 1      allocates 512 TMEM columns; one thread issues
+//               tcgen05.mma (M=128, N=256, K=16) and tcgen05.commit;
+//   warps 2..5  epilogue: tcgen05.ld of a 128 x 256 FP32 accumulator (two
+//               accumulators alternate so the epilogue overlaps the next tile).
+// Every mbarrier wait is bounded by a clock budget; on expiry the CTA sets an
+// error word, drains, frees its TMEM and returns. No cluster multicast.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "brute_tc.hpp"
+#include "common.cuh"
+
+namespace hnswgpu {
+namespace tc {
+
+constexpr int kStages = 4;
+constexpr uint32_t kTileM = 128, kTileN = 256, kTileK = 64;
+constexpr uint32_t kABytes = kTileM * kTileK * 2;   // 16 KB
+constexpr uint32_t kBBytes = kTileN * kTileK * 2;   // 32 KB
+constexpr uint32_t kStageBytes = kABytes + kBBytes;  // 48 KB
+constexpr uint32_t kTmemCols = 512;                   // two 256-column accumulators
+constexpr int kThreads = 192;
+constexpr long long kWaitBudget = 4000000000ll;       // clock cycles (~2 s)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase with the given parity; false (and the error word set)
+// if the clock budget runs out or another role already failed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err) {
+    const long long t0 = clock64();
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255) == 255) {
+            if (*reinterpret_cast<volatile uint32_t*>(err)) return false;
+            if (clock64() - t0 > kWaitBudget) {
+                atomicExch(err, 1u);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor of a K-major tile with 128-byte swizzle:
+// rows of 128 B, 8-row groups 1024 B apart (SBO), version 1, layout 2.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= uint64_t((smem_addr >> 4) & 0x3FFF);        // start address
+    d |= uint64_t(1) << 16;                          // leading byte offset (unused with swizzle)
+    d |= uint64_t(1024 >> 4) << 32;                  // stride byte offset
+    d |= uint64_t(1) << 46;                          // descriptor version
+    d |= uint64_t(2) << 61;                          // 128-byte swizzle
+    return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M=128, N=256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTileN >> 3) << 17) | ((kTileM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__global__ void __launch_bounds__(kThreads, 1)
+    score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte alignment for the swizzled tiles.
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + kStages * kABytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    uint64_t* empty = full + kStages;
+    uint64_t* acc_full = empty + kStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* mma_done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t q_tiles = a.q_tiles;
+    const uint32_t n_tiles = a.n_tile_end - a.n_tile_begin;
+    const uint32_t total = q_tiles * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+        }
+        mbar_init(mma_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; ok && t < total; t += gridDim.x) {
+                const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
+                for (uint32_t k = 0; k < a.k_chunks; ++k) {
+                    const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                    if (!mbar_wait(&empty[s], ph ^ 1u, a.err)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], kStageBytes);
+                    tma_load_2d(sA + s * kABytes, &tmA, &full[s], int(k * kTileK), int(qt * kTileM));
+                    tma_load_2d(sB + s * kBBytes, &tmB, &full[s], int(k * kTileK), int(nt * kTileN));
+                    ++it;
+                }
+            }
+            // Let the copies still in flight land before the CTA can exit
+            // (bounded waits; on the normal path these phases are complete).
+            const uint32_t inflight = it < uint32_t(kStages) ? it : uint32_t(kStages);
+            for (uint32_t j = 0; j < inflight; ++j) {
+                const uint32_t i2 = it - 1 - j;
+                const long long t0 = clock64();
+                while (!mbar_try(&full[i2 % kStages], (i2 / kStages) & 1u) && clock64() - t0 < kWaitBudget) {
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            uint32_t it = 0, tile_it = 0;
+            for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
+                const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+                if (!mbar_wait(&acc_empty[b], (use & 1u) ^ 1u, a.err)) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + b * kTileN;
+                bool ok = true;
+                for (uint32_t k = 0; k < a.k_chunks; ++k, ++it) {
+                    const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                    if (!mbar_wait(&full[s], ph, a.err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ad = umma_desc(smem_u32(sA + s * kABytes));
+                    const uint64_t bd = umma_desc(smem_u32(sB + s * kBBytes));
+#pragma unroll
+                    for (uint32_t j = 0; j < kTileK / 16; ++j)
+                        umma_bf16(d, ad + 2 * j, bd + 2 * j, (k | j) != 0 ? 1u : 0u);
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&acc_full[b]);
+            }
+            // Every MMA this thread issued has completed before TMEM is freed.
+            umma_commit(mma_done);
+            const long long t0 = clock64();
+            while (!mbar_try(mma_done, 0) && clock64() - t0 < kWaitBudget) {
+            }
+        }
+    } else {
+        // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, i.e. those query rows.
+        const uint32_t lane_base = 32u * uint32_t(warp & 3);
+        uint32_t tile_it = 0;
+        for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
+            const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
+            const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+            const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err));
+            if (!got) break;
+            tc_fence_after();
+            const uint32_t q = qt * kTileM + lane_base + uint32_t(lane);
+            const bool qvalid = q < a.nq;
+            const float thr = (qvalid && a.thr) ? a.thr[q] : 0.0f;
+            const float qn = (qvalid && a.qnorm2) ? a.qnorm2[q] : 0.0f;
+            for (uint32_t c = 0; c < kTileN / 32; ++c) {
+                uint32_t v[32];
+                __syncwarp();
+                tmem_ld32(tmem_base + (lane_base << 16) + b * kTileN + c * 32, v);
+                const uint32_t row0 = nt * kTileN + c * 32;
+#pragma unroll
+                for (int j = 0; j < 32 && qvalid; ++j) {
+                    const uint32_t row = row0 + uint32_t(j);
+                    const float s = __uint_as_float(v[j]);
+                    float dist;
+                    if (a.metric == 0) dist = qn + (row < a.n ? a.xnorm2[row] : 0.0f) - 2.0f * s;
+                    else if (a.metric == 1) dist = -s;
+                    else dist = 1.0f - s;
+                    if (a.dense) {
+                        if (row >= a.row0 && row < a.row0 + a.ld) a.dense[size_t(q) * a.ld + (row - a.row0)] =
+                            row < a.n ? dist : __int_as_float(0x7f800000);
+                    } else if (row < a.n && dist <= thr) {
+                        const uint32_t slot = atomicAdd(a.cand_count + q, 1u);
+                        if (slot < a.cand_cap) {
+                            a.cand[size_t(q) * a.cand_cap + slot] = (uint64_t(__float_as_uint(dist)) << 32) | row;
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[b]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols));
+    }
+}
+
+// Splits rows of fp32 values into BF16 operand rows: plain (K' = D, hi) or
+// 3-term (K' = 3D; query layout hi|hi|lo, row layout hi|lo|hi). Rows are
+// zero padded to kp columns; rows >= n are zero.
+__global__ void split_bf16_kernel(const float* __restrict__ src, uint32_t n, uint32_t dim, uint32_t src_stride,
+                                  __nv_bfloat16* __restrict__ dst, uint32_t rows_padded, uint32_t kp, int terms,
+                                  int query_side) {
+    const size_t total = size_t(rows_padded) * kp;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const uint32_t r = uint32_t(i / kp), c = uint32_t(i % kp);
+        float out = 0.0f;
+        if (r < n) {
+            const uint32_t seg = c / dim, j = c % dim;
+            if (seg < uint32_t(terms)) {
+                const float x = src[size_t(r) * src_stride + j];
+                const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+                const float lo = __bfloat162float(__float2bfloat16_rn(x - __bfloat162float(hi)));
+                // query: hi, hi, lo; row: hi, lo, hi
+                const bool use_lo = terms == 3 && (query_side ? seg == 2 : seg == 1);
+                out = use_lo ? lo : __bfloat162float(hi);
+            }
+        }
+        dst[i] = __float2bfloat16_rn(out);
+    }
+}
+
+// Squared norms of fp32 rows (for the L2 epilogue).
+__global__ void row_norms_kernel(const float* __restrict__ src, uint32_t n, uint32_t dim, uint32_t stride,
+                                 float* __restrict__ out) {
+    const uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    float s = 0.0f;
+    for (uint32_t j = lane; j < dim; j += 32) {
+        const float x = src[size_t(r) * stride + j];
+        s = fmaf(x, x, s);
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, off);
+    if (lane == 0) out[r] = s;
+}
+
+// k-th smallest value of each query's row of `vals` (count entries, +inf
+// padding allowed) by a 4-pass radix select on the order-preserving key; the
+// threshold written is that value + margin[q] (or +inf when count < k).
+__global__ void kth_threshold_kernel(const float* __restrict__ vals, uint32_t ld, const uint32_t* __restrict__ counts,
+                                     const uint64_t* __restrict__ packed, uint32_t packed_cap, uint32_t nq, uint32_t k,
+                                     const float* __restrict__ margin, float* __restrict__ thr_out) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t s_prefix, s_rank;
+    const uint32_t q = blockIdx.x;
+    if (q >= nq) return;
+    const uint32_t n = counts ? min(counts[q], packed_cap) : ld;
+    if (n < k || k == 0) {
+        if (threadIdx.x == 0) thr_out[q] = __int_as_float(0x7f800000);
+        return;
+    }
+    auto key_at = [&](uint32_t i) -> uint32_t {
+        const float v = packed ? __uint_as_float(uint32_t(packed[size_t(q) * packed_cap + i] >> 32))
+                               : vals[size_t(q) * ld + i];
+        return dev::fkey(v);
+    };
+    uint32_t prefix = 0, rank = k;  // find the rank-th smallest key (1-based)
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+        for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const uint32_t mask_hi = pass == 0 ? 0u : (0xFFFFFFFFu << (32 - 8 * pass));
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t key = key_at(i);
+            if ((key & mask_hi) == (prefix & mask_hi)) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0, digit = 0;
+            for (; digit < 256; ++digit) {
+                if (acc + hist[digit] >= rank) break;
+                acc += hist[digit];
+            }
+            s_prefix = prefix | (digit << shift);
+            s_rank = rank - acc;
+        }
+        __syncthreads();
+        prefix = s_prefix;
+        rank = s_rank;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) thr_out[q] = dev::kdec(prefix) + margin[q];
+}
+
+// Per-query error margin 2E in distance units (see tc_margins).
+__global__ void margins_kernel(const float* __restrict__ qnorm2, uint32_t nq, float max_xnorm, float eps, int metric,
+                               uint32_t dim, float max_xnorm2, float* __restrict__ out) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const float qn2 = qnorm2[q];
+    const float qn = sqrtf(qn2);
+    float e = eps * qn * max_xnorm;  // bound on |approx dot - fp32 dot|
+    if (metric == 0) e = 2.0f * e + float(dim + 4) * 5.96e-8f * (qn2 + max_xnorm2);
+    out[q] = 2.0f * e * 1.0001f + 1e-30f;
+}
+
+}  // namespace tc
+
+cudaError_t tc_margins(const float* qnorm2, uint32_t nq, float max_xnorm, float eps, int metric, uint32_t dim,
+                       float* out, cudaStream_t stream) {
+    if (nq == 0) return cudaSuccess;
+    tc::margins_kernel<<<(nq + 255) / 256, 256, 0, stream>>>(qnorm2, nq, max_xnorm, eps, metric, dim,
+                                                            max_xnorm * max_xnorm, out);
+    return cudaGetLastError();
+}
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+bool make_map(CUtensorMap* map, const void* base, uint64_t rows, uint64_t kp, uint32_t box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {kp, rows};
+    cuuint64_t strides[1] = {kp * 2};
+    cuuint32_t box[2] = {tc::kTileK, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+}  // namespace
+
+uint32_t tc_k_padded(uint32_t dim, int terms) { return (dim * uint32_t(terms) + tc::kTileK - 1) / tc::kTileK * tc::kTileK; }
+uint32_t tc_rows_padded(uint32_t n, bool query_side) {
+    const uint32_t t = query_side ? tc::kTileM : tc::kTileN;
+    return (std::max<uint32_t>(n, 1) + t - 1) / t * t;
+}
+
+cudaError_t tc_split(const float* src, uint32_t n, uint32_t dim, uint32_t src_stride, __nv_bfloat16* dst,
+                     uint32_t rows_padded, uint32_t kp, int terms, bool query_side, cudaStream_t stream) {
+    const size_t total = size_t(rows_padded) * kp;
+    const uint32_t blocks = uint32_t(std::min<size_t>((total + 255) / 256, 148 * 64));
+    tc::split_bf16_kernel<<<blocks, 256, 0, stream>>>(src, n, dim, src_stride, dst, rows_padded, kp, terms,
+                                                      query_side ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_row_norms(const float* src, uint32_t n, uint32_t dim, uint32_t stride, float* out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    tc::row_norms_kernel<<<(n * 32 + 255) / 256, 256, 0, stream>>>(src, n, dim, stride, out);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B, uint32_t np_, uint32_t kp,
+                     const TcScoreArgs& args_in, int num_sms, cudaStream_t stream) {
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, A, qp, kp, tc::kTileM) || !make_map(&mb, B, np_, kp, tc::kTileN)) return cudaErrorInvalidValue;
+    TcScoreArgs a = args_in;
+    a.q_tiles = qp / tc::kTileM;
+    a.k_chunks = kp / tc::kTileK;
+    const size_t smem = 1024 + size_t(tc::kStages) * tc::kStageBytes + 256;
+    cudaError_t e = cudaFuncSetAttribute(tc::score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    const uint32_t total = a.q_tiles * (a.n_tile_end - a.n_tile_begin);
+    if (total == 0) return cudaSuccess;
+    const uint32_t grid = std::min<uint32_t>(total, uint32_t(num_sms));
+    tc::score_kernel<<<grid, tc::kThreads, smem, stream>>>(ma, mb, a);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_kth_threshold(const float* vals, uint32_t ld, const uint32_t* counts, const uint64_t* packed,
+                             uint32_t packed_cap, uint32_t nq, uint32_t k, const float* margin, float* thr_out,
+                             cudaStream_t stream) {
+    if (nq == 0) return cudaSuccess;
+    tc::kth_threshold_kernel<<<nq, 256, 0, stream>>>(vals, ld, counts, packed, packed_cap, nq, k, margin, thr_out);
+    return cudaGetLastError();
+}
+
+}  // namespace hnswgpu

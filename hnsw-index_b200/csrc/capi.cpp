@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "brute_tc.hpp"
 #include "device.hpp"
 #include "host_index.hpp"
 
@@ -224,16 +225,25 @@ struct hnsw_gpu_index {
 
 struct hnsw_gpu_brute {
     int device = 0;
+    int num_sms = 148;
     uint32_t n = 0, dim = 0, dp = 0;
     int metric = 0;
+    float max_xnorm = 0.0f;  // largest row norm (error margins of the tensor-core path)
     DBuf base, keys;
     SlotPool slots;
     std::mutex mu;
     DBuf qprep, part, okeys, odist, ocount, ostatus, q;
+    // Tensor-core path: BF16 operand rows per term count (index 0: 1 term, 1: 3 terms).
+    DBuf bop[2], xnorm2;
+    uint32_t bop_kp[2] = {0, 0};
+    DBuf aop, dense, thr1, thr2, margin, qnorm2, ccount, cand, err;
+    uint64_t last_candidates = 0, last_queries = 0;
     cudaStream_t stream = nullptr;
     ~hnsw_gpu_brute() {
         DeviceGuard g(device);
-        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q}) b->release();
+        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &bop[0], &bop[1], &xnorm2,
+                        &aop, &dense, &thr1, &thr2, &margin, &qnorm2, &ccount, &cand, &err})
+            b->release();
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -684,6 +694,16 @@ int hnsw_gpu_brute_open(const float* vectors, const uint64_t* keys, size_t n, si
     DeviceGuard dg(device);
     std::unique_ptr<hnsw_gpu_brute> b(new hnsw_gpu_brute());
     b->device = device;
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
+    {
+        double mx = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            double s2 = 0.0;
+            for (size_t j = 0; j < dim; ++j) s2 += double(rows[i * dp + j]) * double(rows[i * dp + j]);
+            mx = std::max(mx, s2);
+        }
+        b->max_xnorm = float(std::sqrt(mx) * (1.0 + 1e-6));
+    }
     b->n = uint32_t(n);
     b->dim = uint32_t(dim);
     b->dp = dp;
@@ -699,15 +719,173 @@ int hnsw_gpu_brute_open(const float* vectors, const uint64_t* keys, size_t n, si
 
 void hnsw_gpu_brute_close(hnsw_gpu_brute* brute) { delete brute; }
 
+// Tensor-core brute force: BF16 (1 term) or compensated BF16 (3 terms)
+// scoring with FP32 accumulation, then exact FP32 re-ranking.
+//   1. queries: validate/normalise (FP32), split into BF16 operand rows;
+//   2. sample pass: dense approximate distances to the first rows; the k-th
+//      smallest plus 2E (E bounds |approximate - FP32| distance) is a
+//      threshold every true top-k row passes;
+//   3. candidate pass over all rows: (row, approximate distance) <= threshold;
+//   4. a tighter threshold: k-th smallest candidate + 2E;
+//   5. exact FP32 distances (reference order) of those candidates, top-k by
+//      (distance, key). Queries whose candidate list overflowed are re-run
+//      with the exact FP32 kernels.
+static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t nq, uint32_t k, int precision,
+                               uint64_t* out_keys, float* out_dist, uint32_t* out_count, int32_t* out_status) {
+    std::lock_guard<std::mutex> lock(b->mu);
+    DeviceGuard dg(b->device);
+    cudaStream_t st = b->stream;
+    const int terms = precision == HNSW_PRECISION_BF16X3 ? 3 : 1;
+    const int ti = terms == 3 ? 1 : 0;
+    const uint32_t kp = tc_k_padded(b->dim, terms);
+    const uint32_t np = tc_rows_padded(b->n, false);
+    const uint32_t qp = tc_rows_padded(uint32_t(nq), true);
+    if (b->bop_kp[ti] != kp) {
+        CU(b->bop[ti].ensure(size_t(np) * kp * 2), "cudaMalloc BF16 rows");
+        CU(tc_split(b->base.as<float>(), b->n, b->dim, b->dp, b->bop[ti].as<__nv_bfloat16>(), np, kp, terms, false, st),
+           "split rows");
+        b->bop_kp[ti] = kp;
+    }
+    if (b->metric == HNSW_METRIC_L2 && b->xnorm2.bytes < size_t(np) * 4) {
+        CU(b->xnorm2.ensure(size_t(np) * 4), "cudaMalloc row norms");
+        CU(tc_row_norms(b->base.as<float>(), b->n, b->dim, b->dp, b->xnorm2.as<float>(), st), "row norms");
+    }
+    BruteArgs a;
+    a.base = b->base.as<float>();
+    a.keys = b->keys.as<uint64_t>();
+    a.n = b->n;
+    a.dim = b->dim;
+    a.dp = b->dp;
+    a.metric = b->metric;
+    a.nq = uint32_t(nq);
+    a.k = k;
+    CU(b->q.ensure(nq * b->dim * 4), "cudaMalloc queries");
+    CU(cudaMemcpyAsync(b->q.p, queries, nq * b->dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
+    CU(b->qprep.ensure(size_t(qp) * b->dp * 4), "cudaMalloc qprep");
+    CU(b->okeys.ensure(nq * size_t(k) * 8), "cudaMalloc out keys");
+    CU(b->odist.ensure(nq * size_t(k) * 4), "cudaMalloc out dist");
+    CU(b->ocount.ensure(nq * 4), "cudaMalloc out count");
+    CU(b->ostatus.ensure(nq * 4), "cudaMalloc out status");
+    a.queries = b->q.as<float>();
+    a.qprep = b->qprep.as<float>();
+    a.out_keys = b->okeys.as<uint64_t>();
+    a.out_dist = b->odist.as<float>();
+    a.out_count = b->ocount.as<uint32_t>();
+    a.out_status = b->ostatus.as<int32_t>();
+    CU(launch_brute_prep(a, st), "query prep");
+    // Query norms (L2 epilogue and margins) and BF16 query operands.
+    CU(b->qnorm2.ensure(size_t(qp) * 4), "cudaMalloc query norms");
+    CU(tc_row_norms(a.qprep, uint32_t(nq), b->dim, b->dp, b->qnorm2.as<float>(), st), "query norms");
+    CU(b->aop.ensure(size_t(qp) * kp * 2), "cudaMalloc BF16 queries");
+    CU(tc_split(a.qprep, uint32_t(nq), b->dim, b->dp, b->aop.as<__nv_bfloat16>(), qp, kp, terms, true, st), "split queries");
+    const double u24 = 5.9604644775390625e-8;
+    const double eps = terms == 3 ? (3.1 * 1.52587890625e-5 + double(kp + b->dim + 8) * u24)
+                                  : (2.0 * 3.90625e-3 + 1.52587890625e-5 + double(kp + b->dim + 8) * u24);
+    CU(b->margin.ensure(size_t(qp) * 4), "cudaMalloc margins");
+    CU(tc_margins(b->qnorm2.as<float>(), uint32_t(nq), b->max_xnorm, float(eps), b->metric, b->dim,
+                  b->margin.as<float>(), st),
+       "margins");
+    CU(b->err.ensure(16), "cudaMalloc error word");
+    CU(cudaMemsetAsync(b->err.p, 0, 16, st), "memset error word");
+    // Sample pass.
+    const uint32_t sample_rows = std::min<uint32_t>(np, 16384);
+    CU(b->dense.ensure(size_t(qp) * sample_rows * 4), "cudaMalloc sample");
+    CU(b->thr1.ensure(size_t(qp) * 4), "cudaMalloc thresholds");
+    CU(b->thr2.ensure(size_t(qp) * 4), "cudaMalloc thresholds");
+    TcScoreArgs t;
+    t.nq = uint32_t(nq);
+    t.n = b->n;
+    t.metric = b->metric;
+    t.qnorm2 = b->qnorm2.as<float>();
+    t.xnorm2 = b->metric == HNSW_METRIC_L2 ? b->xnorm2.as<float>() : nullptr;
+    t.err = b->err.as<uint32_t>();
+    t.n_tile_begin = 0;
+    t.n_tile_end = sample_rows / 256;
+    t.dense = b->dense.as<float>();
+    t.row0 = 0;
+    t.ld = sample_rows;
+    CU(tc_score(b->aop.as<__nv_bfloat16>(), qp, b->bop[ti].as<__nv_bfloat16>(), np, kp, t, b->num_sms, st), "sample pass");
+    const uint32_t kk = std::min<uint32_t>(k, b->n);
+    CU(tc_kth_threshold(b->dense.as<float>(), sample_rows, nullptr, nullptr, 0, uint32_t(nq), kk, b->margin.as<float>(),
+                        b->thr1.as<float>(), st),
+       "sample threshold");
+    // Candidate pass.
+    const uint32_t cap = 32768;
+    CU(b->ccount.ensure(size_t(qp) * 4), "cudaMalloc candidate counts");
+    CU(b->cand.ensure(size_t(nq) * cap * 8), "cudaMalloc candidates");
+    CU(cudaMemsetAsync(b->ccount.p, 0, size_t(qp) * 4, st), "memset candidate counts");
+    t.dense = nullptr;
+    t.n_tile_begin = 0;
+    t.n_tile_end = np / 256;
+    t.thr = b->thr1.as<float>();
+    t.cand_count = b->ccount.as<uint32_t>();
+    t.cand = b->cand.as<uint64_t>();
+    t.cand_cap = cap;
+    CU(tc_score(b->aop.as<__nv_bfloat16>(), qp, b->bop[ti].as<__nv_bfloat16>(), np, kp, t, b->num_sms, st),
+       "candidate pass");
+    CU(tc_kth_threshold(nullptr, 0, b->ccount.as<uint32_t>(), b->cand.as<uint64_t>(), cap, uint32_t(nq), kk,
+                        b->margin.as<float>(), b->thr2.as<float>(), st),
+       "candidate threshold");
+    CU(launch_brute_rerank(a, b->cand.as<uint64_t>(), b->ccount.as<uint32_t>(), cap, b->thr2.as<float>(), st),
+       "re-rank");
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(&err, b->err.p, 4, cudaMemcpyDeviceToHost, st), "copy error word");
+    CU(cudaMemcpyAsync(out_count, a.out_count, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
+    CU(cudaMemcpyAsync(out_status, a.out_status, nq * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
+    CU(cudaMemcpyAsync(out_keys, a.out_keys, nq * size_t(k) * 8, cudaMemcpyDeviceToHost, st), "copy keys");
+    CU(cudaMemcpyAsync(out_dist, a.out_dist, nq * size_t(k) * 4, cudaMemcpyDeviceToHost, st), "copy distances");
+    CU(cudaStreamSynchronize(st), "tensor brute force");
+    if (err) return set_error(HNSW_ERR_TIMEOUT, "tensor-core scoring: a bounded wait ran out");
+    // Queries whose candidate list overflowed: exact FP32 kernels.
+    std::vector<uint32_t> redo;
+    for (size_t i = 0; i < nq; ++i)
+        if (out_status[i] == HNSW_ERR_SCRATCH_OVERFLOW) redo.push_back(uint32_t(i));
+    if (!redo.empty()) {
+        std::vector<float> sub(redo.size() * b->dim);
+        for (size_t j = 0; j < redo.size(); ++j)
+            std::memcpy(&sub[j * b->dim], queries + size_t(redo[j]) * b->dim, b->dim * 4);
+        std::vector<uint64_t> sk(redo.size() * k);
+        std::vector<float> sd(redo.size() * k);
+        std::vector<uint32_t> sc(redo.size());
+        std::vector<int32_t> ss(redo.size());
+        b->mu.unlock();
+        int r = hnsw_gpu_brute_search_batch(b, sub.data(), redo.size(), b->dim, k, HNSW_PRECISION_FP32, sk.data(),
+                                            sd.data(), sc.data(), ss.data());
+        b->mu.lock();
+        if (r != HNSW_OK) return r;
+        for (size_t j = 0; j < redo.size(); ++j) {
+            const size_t i = redo[j];
+            out_count[i] = sc[j];
+            out_status[i] = ss[j];
+            std::memcpy(out_keys + i * k, &sk[j * k], size_t(k) * 8);
+            std::memcpy(out_dist + i * k, &sd[j * k], size_t(k) * 4);
+        }
+    }
+    {
+        std::vector<uint32_t> counts(nq);
+        if (cudaMemcpy(counts.data(), b->ccount.p, nq * 4, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            uint64_t total = 0;
+            for (uint32_t c : counts) total += c;
+            b->last_candidates = total;
+            b->last_queries = nq;
+        }
+    }
+    for (size_t i = 0; i < nq; ++i)
+        if (out_status[i] != HNSW_OK) return set_error(out_status[i], "query failed validation");
+    return HNSW_OK;
+}
+
 int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
                                 int precision, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
                                 int32_t* out_status) {
     if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
     if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
     if (nq == 0) return HNSW_OK;
-    if (precision != HNSW_PRECISION_FP32)
-        return set_error(HNSW_ERR_INVALID_ARGUMENT, "precision not available in this build");
+    if (precision < HNSW_PRECISION_FP32 || precision > HNSW_PRECISION_BF16X3)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown precision");
     if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
+    if (precision != HNSW_PRECISION_FP32 && b->n > 0 && k > 0)
+        return brute_search_tensor(b, queries, nq, k, precision, out_keys, out_dist, out_count, out_status);
     std::lock_guard<std::mutex> lock(b->mu);
     DeviceGuard dg(b->device);
     cudaStream_t st = b->stream;
@@ -747,6 +925,13 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t 
     CU(cudaStreamSynchronize(st), "brute search");
     for (size_t i = 0; i < nq; ++i)
         if (out_status[i] != HNSW_OK) return set_error(out_status[i], "query failed validation");
+    return HNSW_OK;
+}
+
+int hnsw_gpu_brute_stats(const hnsw_gpu_brute* b, hnsw_brute_stats* out) {
+    if (!b || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    out->candidates = b->last_candidates;
+    out->queries = b->last_queries;
     return HNSW_OK;
 }
 

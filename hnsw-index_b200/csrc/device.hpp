@@ -116,6 +116,13 @@ struct BruteArgs {
     uint32_t tiles = 0;
 };
 cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream);
+// Query preparation only (vector::check, cosine normalisation) into a.qprep.
+cudaError_t launch_brute_prep(const BruteArgs& a, cudaStream_t stream);
+// Exact FP32 re-rank of packed (approx distance bits << 32 | row) candidates
+// whose approximate distance is <= thr2[q]; writes a.out_* (status 25 when a
+// query's candidate list overflowed).
+cudaError_t launch_brute_rerank(const BruteArgs& a, const uint64_t* cand, const uint32_t* cand_count, uint32_t cand_cap,
+                                const float* thr2, cudaStream_t stream);
 
 // Fixed device scratch of the allocation-free brute-force entry point.
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device

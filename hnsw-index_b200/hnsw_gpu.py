@@ -159,6 +159,11 @@ _lib.hnsw_gpu_brute_open.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, C.POI
 _lib.hnsw_gpu_brute_close.argtypes = [_vp]
 _lib.hnsw_gpu_brute_close.restype = None
 _lib.hnsw_gpu_brute_search_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_uint32, C.c_int, _vp, _vp, _vp, _vp]
+class _BruteStats(C.Structure):
+    _fields_ = [("candidates", C.c_uint64), ("queries", C.c_uint64)]
+
+
+_lib.hnsw_gpu_brute_stats.argtypes = [_vp, C.POINTER(_BruteStats)]
 _lib.hnsw_params_default.argtypes = [C.c_uint32, C.POINTER(_Params)]
 _lib.hnsw_params_default.restype = None
 _lib.hnsw_builder_new.argtypes = [_sz, C.c_int, C.POINTER(_Params), C.POINTER(_vp)]
@@ -547,6 +552,12 @@ class BruteForceIndex:
         if st != 0 and raise_on_error:
             _raise(st)
         return keys, dist, count, status
+
+    def last_candidates_per_query(self) -> float:
+        """Mean candidates kept by the threshold in the last tensor-core search."""
+        st = _BruteStats()
+        _check(_lib.hnsw_gpu_brute_stats(self._h, C.byref(st)))
+        return st.candidates / max(st.queries, 1)
 
     def search(self, query, k: int, precision: Precision = Precision.FP32):
         keys, dist, count, _ = self.search_arrays(np.asarray(query, np.float32).reshape(1, -1), k, precision)

@@ -172,6 +172,14 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* brute, const float* queries, siz
                                 uint32_t k, int precision, uint64_t* out_keys, float* out_dist,
                                 uint32_t* out_count, int32_t* out_status);
 
+/* Counters of the last tensor-core search on this handle: candidates kept
+ * by the scoring threshold, summed over the batch's queries. */
+typedef struct hnsw_brute_stats {
+    uint64_t candidates;
+    uint64_t queries;
+} hnsw_brute_stats;
+int hnsw_gpu_brute_stats(const hnsw_gpu_brute* brute, hnsw_brute_stats* out);
+
 /* Allocation-free variant of hnsw_gpu_brute_search_batch, FP32 precision,
  * for callers that cannot allocate device memory while they run: code on a
  * latency-critical path, in a process whose memory policy forbids cudaMalloc
