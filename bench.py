@@ -401,6 +401,114 @@ def run_gpu(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Brute-force precision workload (not the default line): 1M x 768 cosine.
+# ---------------------------------------------------------------------------
+def run_brute(args):
+    import hnsw_gpu as H
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nb, nq, dim, k = args.brute_n, args.brute_nq, 768, 100
+    t = time.time()
+    base, queries = H.mixture_split(nb, nq, dim, 4096, 0.5, 3, 4)
+    log(f"data in {time.time() - t:.1f} s")
+    t = time.time()
+    bf = H.BruteForceIndex(dim, H.Metric.Cosine)
+    bf.insert_batch(np.arange(nb, dtype=np.uint64), base)
+    log(f"brute open in {time.time() - t:.1f} s")
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+    out = {}
+    results = {}
+    for prec in (H.Precision.BF16X3, H.Precision.BF16, H.Precision.FP32):
+        steps = args.steps if prec != H.Precision.FP32 else 1
+        bf.search_arrays(queries, k, prec)  # warm-up (also builds the BF16 rows)
+        times, stats = [], []
+        for _ in range(steps):
+            t = time.perf_counter()
+            res = bf.search_arrays(queries, k, prec)
+            times.append(time.perf_counter() - t)
+            if prec != H.Precision.FP32:
+                stats.append(bf.last_stats())
+        results[prec.name] = res
+        entry = {"qps_e2e": nq / statistics.median(times), "ms_e2e": 1e3 * statistics.median(times)}
+        if stats:
+            terms = 3 if prec == H.Precision.BF16X3 else 1
+            kp = (dim * terms + 63) // 64 * 64
+            score_ms = statistics.median(s_["score_ms"] for s_ in stats)
+            dev_ms = statistics.median(s_["prep_ms"] + s_["sample_ms"] + s_["score_ms"] + s_["rerank_ms"]
+                                       for s_ in stats)
+            executed = 2.0 * ((nq + 127) // 128 * 128) * ((nb + 255) // 256 * 256) * kp
+            useful = 2.0 * nq * nb * dim * terms
+            entry.update({
+                "qps_device": nq / (dev_ms / 1e3), "device_ms": dev_ms, "score_ms": score_ms,
+                "prep_ms": statistics.median(s_["prep_ms"] for s_ in stats),
+                "sample_ms": statistics.median(s_["sample_ms"] for s_ in stats),
+                "rerank_ms": statistics.median(s_["rerank_ms"] for s_ in stats),
+                "candidates_per_query": stats[-1]["candidates"] / max(stats[-1]["queries"], 1),
+                "tensor_tflops_executed": executed / (score_ms / 1e3) / 1e12,
+                "tensor_frac_of_burst": executed / (score_ms / 1e3) / 1e12 / peaks["bf16_tflops"],
+                "tensor_frac_of_sustained": executed / (score_ms / 1e3) / 1e12 / peaks["bf16_tflops_sustained"],
+                "useful_tflops": useful / (score_ms / 1e3) / 1e12,
+            })
+        out[prec.name] = entry
+        log(prec.name, entry)
+    # Identity with the exact FP32 path, and agreement with an FP64 oracle on a sample.
+    fp = results["FP32"]
+    same = {}
+    for name in ("BF16X3", "BF16"):
+        r = results[name]
+        same[name] = bool(np.array_equal(r[0], fp[0]) and np.array_equal(r[1].view(np.uint32), fp[1].view(np.uint32)))
+    sample = min(100, nq)
+    xs = base.astype(np.float64)
+    rows = (xs / np.sqrt((xs * xs).sum(1, keepdims=True))).astype(np.float32)
+    del xs
+    qs = queries[:sample].astype(np.float64)
+    qn = (qs / np.sqrt((qs * qs).sum(1, keepdims=True))).astype(np.float32)
+    t = time.time()
+    k64, d64 = O.brute_f64(2, rows, qn, k)
+    log(f"fp64 oracle on {sample} queries in {time.time() - t:.1f} s")
+    fp64 = {}
+    for name in ("BF16X3", "BF16", "FP32"):
+        r = results[name]
+        dis = 0
+        maxerr = 0.0
+        for i in range(sample):
+            ours = set(r[0][i, :k].tolist())
+            ref = k64[i].tolist()
+            dis += len(ours - set(ref))
+            pos = {key: j for j, key in enumerate(ref)}
+            for j in range(k):
+                key = int(r[0][i, j])
+                if key in pos:
+                    maxerr = max(maxerr, abs(float(r[1][i, j]) - float(d64[i, pos[key]])))
+        fp64[name] = {"top100_disagreement_per_query": dis / sample, "max_abs_distance_error": maxerr}
+    # CPU reference: the oracle's FP32 brute force on a sample of queries.
+    cores = os.cpu_count() or 1
+    cs = 160
+    t = time.perf_counter()
+    O.brute(2, rows, qn[:0] if False else queries[:cs] / np.linalg.norm(queries[:cs], axis=1, keepdims=True), k,
+            threads=cores)
+    cpu_qps = cs / (time.perf_counter() - t)
+    line = {
+        "metric": "brute-force QPS (1M x 768 cosine, k=100, BF16x3 + exact FP32 re-rank)",
+        "value": out["BF16X3"]["qps_device"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": 1, "higher_is_better": True, "dtype": "bf16x3", "data": "synthetic",
+        "config": {"workload": "brute-1Mx768-cosine", "n_base": nb, "n_queries": nq, "dim": dim, "k": k,
+                   "clusters": 4096, "sigma": 0.5, "seeds": [3, 4], "precisions": out,
+                   "identical_to_fp32": same, "fp64_sample": fp64},
+        "roofline": {"bound": "tensor", "achieved": out["BF16X3"]["tensor_tflops_executed"],
+                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": out["BF16X3"]["tensor_frac_of_burst"], "traffic": None, "peak_kind": "measured burst"},
+        "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"{cs} queries, oracle FP32 brute force"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,7 +516,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="plain-1Mx128", choices=["plain-1Mx128", "brute-1Mx768"])
+    ap.add_argument("--brute-n", type=int, default=1_000_000)
+    ap.add_argument("--brute-nq", type=int, default=10_000)
     args = ap.parse_args()
+    if args.workload == "brute-1Mx768":
+        return run_brute(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -129,6 +129,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// Metric distance of one accumulator value (approximate q.x).
+__device__ __forceinline__ float tile_distance(const TcScoreArgs& a, float s, float qn, uint32_t row) {
+    if (a.metric == 0) return qn + (row < a.n ? __ldg(a.xnorm2 + row) : 0.0f) - 2.0f * s;
+    if (a.metric == 1) return -s;
+    return 1.0f - s;
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -244,26 +251,58 @@ __global__ void __launch_bounds__(kThreads, 1)
             const bool qvalid = q < a.nq;
             const float thr = (qvalid && a.thr) ? a.thr[q] : 0.0f;
             const float qn = (qvalid && a.qnorm2) ? a.qnorm2[q] : 0.0f;
-            for (uint32_t c = 0; c < kTileN / 32; ++c) {
-                uint32_t v[32];
-                __syncwarp();
-                tmem_ld32(tmem_base + (lane_base << 16) + b * kTileN + c * 32, v);
-                const uint32_t row0 = nt * kTileN + c * 32;
+            const uint32_t acc_col = b * kTileN;
+            const uint32_t taddr = tmem_base + (lane_base << 16) + acc_col;
+            if (a.dense) {
+                for (uint32_t c = 0; c < kTileN / 32; ++c) {
+                    uint32_t v[32];
+                    __syncwarp();
+                    tmem_ld32(taddr + c * 32, v);
+                    const uint32_t row0 = nt * kTileN + c * 32;
 #pragma unroll
-                for (int j = 0; j < 32 && qvalid; ++j) {
-                    const uint32_t row = row0 + uint32_t(j);
-                    const float s = __uint_as_float(v[j]);
-                    float dist;
-                    if (a.metric == 0) dist = qn + (row < a.n ? a.xnorm2[row] : 0.0f) - 2.0f * s;
-                    else if (a.metric == 1) dist = -s;
-                    else dist = 1.0f - s;
-                    if (a.dense) {
-                        if (row >= a.row0 && row < a.row0 + a.ld) a.dense[size_t(q) * a.ld + (row - a.row0)] =
-                            row < a.n ? dist : __int_as_float(0x7f800000);
-                    } else if (row < a.n && dist <= thr) {
-                        const uint32_t slot = atomicAdd(a.cand_count + q, 1u);
-                        if (slot < a.cand_cap) {
-                            a.cand[size_t(q) * a.cand_cap + slot] = (uint64_t(__float_as_uint(dist)) << 32) | row;
+                    for (int j = 0; j < 32 && qvalid; ++j) {
+                        const uint32_t row = row0 + uint32_t(j);
+                        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+                        if (row >= a.row0 && row < a.row0 + a.ld)
+                            a.dense[size_t(q) * a.ld + (row - a.row0)] = row < a.n ? dist : __int_as_float(0x7f800000);
+                    }
+                }
+            } else {
+                // Pass 1: how many of this query's 256 rows pass the threshold.
+                uint32_t total_pass = 0;
+#pragma unroll 1
+                for (uint32_t c = 0; c < kTileN / 32; ++c) {
+                    uint32_t v[32];
+                    __syncwarp();
+                    tmem_ld32(taddr + c * 32, v);
+                    const uint32_t row0 = nt * kTileN + c * 32;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const uint32_t row = row0 + uint32_t(j);
+                        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+                        total_pass += (qvalid && row < a.n && dist <= thr) ? 1u : 0u;
+                    }
+                }
+                // One reservation per (query, tile); pass 2 writes the entries.
+                uint32_t slot = 0;
+                if (total_pass) slot = atomicAdd(a.cand_count + q, total_pass);
+                if (__any_sync(0xFFFFFFFFu, total_pass != 0)) {
+#pragma unroll 1
+                    for (uint32_t c = 0; c < kTileN / 32; ++c) {
+                        uint32_t v[32];
+                        __syncwarp();
+                        tmem_ld32(taddr + c * 32, v);
+                        const uint32_t row0 = nt * kTileN + c * 32;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const uint32_t row = row0 + uint32_t(j);
+                            const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+                            if (qvalid && row < a.n && dist <= thr) {
+                                if (slot < a.cand_cap)
+                                    a.cand[size_t(q) * a.cand_cap + slot] =
+                                        (uint64_t(__float_as_uint(dist)) << 32) | row;
+                                ++slot;
+                            }
                         }
                     }
                 }

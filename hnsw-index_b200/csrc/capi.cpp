@@ -238,12 +238,16 @@ struct hnsw_gpu_brute {
     uint32_t bop_kp[2] = {0, 0};
     DBuf aop, dense, thr1, thr2, margin, qnorm2, ccount, cand, err;
     uint64_t last_candidates = 0, last_queries = 0;
+    float last_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream = nullptr;
     ~hnsw_gpu_brute() {
         DeviceGuard g(device);
         for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &bop[0], &bop[1], &xnorm2,
                         &aop, &dense, &thr1, &thr2, &margin, &qnorm2, &ccount, &cand, &err})
             b->release();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -759,6 +763,8 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     a.metric = b->metric;
     a.nq = uint32_t(nq);
     a.k = k;
+    if (!b->ev[0])
+        for (cudaEvent_t& e : b->ev) CU(cudaEventCreate(&e), "cudaEventCreate");
     CU(b->q.ensure(nq * b->dim * 4), "cudaMalloc queries");
     CU(cudaMemcpyAsync(b->q.p, queries, nq * b->dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
     CU(b->qprep.ensure(size_t(qp) * b->dp * 4), "cudaMalloc qprep");
@@ -772,6 +778,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     a.out_dist = b->odist.as<float>();
     a.out_count = b->ocount.as<uint32_t>();
     a.out_status = b->ostatus.as<int32_t>();
+    CU(cudaEventRecord(b->ev[0], st), "event");
     CU(launch_brute_prep(a, st), "query prep");
     // Query norms (L2 epilogue and margins) and BF16 query operands.
     CU(b->qnorm2.ensure(size_t(qp) * 4), "cudaMalloc query norms");
@@ -788,6 +795,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     CU(b->err.ensure(16), "cudaMalloc error word");
     CU(cudaMemsetAsync(b->err.p, 0, 16, st), "memset error word");
     // Sample pass.
+    CU(cudaEventRecord(b->ev[1], st), "event");
     const uint32_t sample_rows = std::min<uint32_t>(np, 16384);
     CU(b->dense.ensure(size_t(qp) * sample_rows * 4), "cudaMalloc sample");
     CU(b->thr1.ensure(size_t(qp) * 4), "cudaMalloc thresholds");
@@ -821,13 +829,16 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     t.cand_count = b->ccount.as<uint32_t>();
     t.cand = b->cand.as<uint64_t>();
     t.cand_cap = cap;
+    CU(cudaEventRecord(b->ev[2], st), "event");
     CU(tc_score(b->aop.as<__nv_bfloat16>(), qp, b->bop[ti].as<__nv_bfloat16>(), np, kp, t, b->num_sms, st),
        "candidate pass");
+    CU(cudaEventRecord(b->ev[3], st), "event");
     CU(tc_kth_threshold(nullptr, 0, b->ccount.as<uint32_t>(), b->cand.as<uint64_t>(), cap, uint32_t(nq), kk,
                         b->margin.as<float>(), b->thr2.as<float>(), st),
        "candidate threshold");
     CU(launch_brute_rerank(a, b->cand.as<uint64_t>(), b->ccount.as<uint32_t>(), cap, b->thr2.as<float>(), st),
        "re-rank");
+    CU(cudaEventRecord(b->ev[4], st), "event");
     uint32_t err = 0;
     CU(cudaMemcpyAsync(&err, b->err.p, 4, cudaMemcpyDeviceToHost, st), "copy error word");
     CU(cudaMemcpyAsync(out_count, a.out_count, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
@@ -835,6 +846,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     CU(cudaMemcpyAsync(out_keys, a.out_keys, nq * size_t(k) * 8, cudaMemcpyDeviceToHost, st), "copy keys");
     CU(cudaMemcpyAsync(out_dist, a.out_dist, nq * size_t(k) * 4, cudaMemcpyDeviceToHost, st), "copy distances");
     CU(cudaStreamSynchronize(st), "tensor brute force");
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&b->last_ms[i], b->ev[i], b->ev[i + 1]);
     if (err) return set_error(HNSW_ERR_TIMEOUT, "tensor-core scoring: a bounded wait ran out");
     // Queries whose candidate list overflowed: exact FP32 kernels.
     std::vector<uint32_t> redo;
@@ -932,6 +944,10 @@ int hnsw_gpu_brute_stats(const hnsw_gpu_brute* b, hnsw_brute_stats* out) {
     if (!b || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
     out->candidates = b->last_candidates;
     out->queries = b->last_queries;
+    out->prep_ms = b->last_ms[0];
+    out->sample_ms = b->last_ms[1];
+    out->score_ms = b->last_ms[2];
+    out->rerank_ms = b->last_ms[3];
     return HNSW_OK;
 }
 

@@ -489,10 +489,36 @@ struct SplitMix64 {
 };
 }  // namespace
 
+namespace {
+constexpr uint64_t kGamma = 0x9E3779B97F4A7C15ULL;
+// Runs f(begin, end) over [0, n) on all cores (for independent chunks).
+template <class F>
+void parallel_chunks(size_t n, F&& f) {
+    const size_t threads = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), n / 4096 + 1));
+    if (threads == 1) {
+        f(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] { f(n * t / threads, n * (t + 1) / threads); });
+    for (auto& th : pool) th.join();
+}
+}  // namespace
+
+// SplitMix64 is counter based: output i of the stream seeded with s is
+// mix64(s + (i + 1) * gamma). Each chunk starts its own generator at its
+// offset, so the parallel fill is bit-identical to one sequential stream.
 void synthetic_gaussian(size_t nb, size_t nq, size_t dim, uint64_t seed, float* base, float* queries) {
-    SplitMix64 r{seed};
-    for (size_t i = 0; i < nb * dim; ++i) base[i] = float(r.gaussian());
-    for (size_t i = 0; i < nq * dim; ++i) queries[i] = float(r.gaussian());
+    const size_t total = (nb + nq) * dim;
+    parallel_chunks(total, [&](size_t b, size_t e) {
+        SplitMix64 r{seed + uint64_t(2 * b) * kGamma};
+        for (size_t i = b; i < e; ++i) {
+            const float v = float(r.gaussian());
+            if (i < nb * dim) base[i] = v;
+            else queries[i - nb * dim] = v;
+        }
+    });
 }
 
 void synthetic_mixture(size_t nb, size_t nq, size_t dim, size_t clusters, double sigma, uint64_t seed, float* base,
@@ -515,15 +541,19 @@ void synthetic_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, 
     SplitMix64 r{base_seed};
     std::vector<double> centers(clusters * dim);
     for (auto& c : centers) c = r.gaussian();
-    auto sample = [&](SplitMix64& g, size_t count, float* out) {
-        for (size_t p = 0; p < count; ++p) {
-            size_t c = size_t(g.below(clusters));
-            for (size_t j = 0; j < dim; ++j) out[p * dim + j] = float(centers[c * dim + j] + sigma * g.gaussian());
-        }
+    // Each point consumes 1 + 2 * dim outputs (next_below, then dim Gaussians).
+    const uint64_t per_point = 1 + 2 * uint64_t(dim);
+    auto sample = [&](uint64_t stream_start, size_t count, float* out) {
+        parallel_chunks(count, [&](size_t b, size_t e) {
+            SplitMix64 g{stream_start + uint64_t(b) * per_point * kGamma};
+            for (size_t p = b; p < e; ++p) {
+                size_t c = size_t(g.below(clusters));
+                for (size_t j = 0; j < dim; ++j) out[p * dim + j] = float(centers[c * dim + j] + sigma * g.gaussian());
+            }
+        });
     };
-    sample(r, nb, base);
-    SplitMix64 rq{query_seed};
-    sample(rq, nq, queries);
+    sample(r.s, nb, base);
+    sample(query_seed, nq, queries);
 }
 
 // ---------------------------------------------------------------------------

@@ -160,7 +160,8 @@ _lib.hnsw_gpu_brute_close.argtypes = [_vp]
 _lib.hnsw_gpu_brute_close.restype = None
 _lib.hnsw_gpu_brute_search_batch.argtypes = [_vp, _vp, _sz, _sz, C.c_uint32, C.c_int, _vp, _vp, _vp, _vp]
 class _BruteStats(C.Structure):
-    _fields_ = [("candidates", C.c_uint64), ("queries", C.c_uint64)]
+    _fields_ = [("candidates", C.c_uint64), ("queries", C.c_uint64), ("prep_ms", C.c_float),
+                ("sample_ms", C.c_float), ("score_ms", C.c_float), ("rerank_ms", C.c_float)]
 
 
 _lib.hnsw_gpu_brute_stats.argtypes = [_vp, C.POINTER(_BruteStats)]
@@ -552,6 +553,12 @@ class BruteForceIndex:
         if st != 0 and raise_on_error:
             _raise(st)
         return keys, dist, count, status
+
+    def last_stats(self) -> dict:
+        """Candidates and device stage times of the last tensor-core search."""
+        st = _BruteStats()
+        _check(_lib.hnsw_gpu_brute_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
 
     def last_candidates_per_query(self) -> float:
         """Mean candidates kept by the threshold in the last tensor-core search."""

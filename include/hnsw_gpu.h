@@ -177,6 +177,10 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* brute, const float* queries, siz
 typedef struct hnsw_brute_stats {
     uint64_t candidates;
     uint64_t queries;
+    float prep_ms;      /* query validation, norms, BF16 split */
+    float sample_ms;    /* dense scoring of the threshold sample + its select */
+    float score_ms;     /* candidate scoring over all rows (the GEMM) */
+    float rerank_ms;    /* candidate threshold + exact FP32 re-rank */
 } hnsw_brute_stats;
 int hnsw_gpu_brute_stats(const hnsw_gpu_brute* brute, hnsw_brute_stats* out);
 

@@ -32,6 +32,41 @@ def test_mixture_generator_matches_between_oracle_and_library():
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def test_split_mixture_streams_match_sequential_generators():
+    # Base (and centers) come from one SplitMix64 stream exactly as
+    # Dataset::clustered draws them (src/synthetic.rs:102-124); queries from
+    # their own stream. The library fills both in parallel chunks.
+    base, queries = H.mixture_split(5000, 3, 16, 7, 0.3, 1, 2)
+    ob, _ = O.clustered(5000, 0, 16, 7, 0.3, 1)
+    assert np.array_equal(base, ob)
+    centers, _ = O.gaussian(7, 0, 16, 1)  # the first 7*16 Gaussians of stream 1
+
+    mask = (1 << 64) - 1
+
+    def mix(z):
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        return z ^ (z >> 31)
+
+    state = 2
+    import math
+
+    def nxt():
+        nonlocal state
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        return mix(state)
+
+    for i in range(3):
+        c = (nxt() * 7) >> 64
+        for j in range(16):
+            u1 = 1.0 - (nxt() >> 11) * (1.0 / (1 << 53))
+            u2 = (nxt() >> 11) * (1.0 / (1 << 53))
+            g = math.sqrt(-2.0 * math.log(u1)) * math.cos(math.tau * u2)
+            # centers are float64 in the generator; the f32 copy from O.gaussian is only used
+            # to locate the cluster (tolerance covers the f32 rounding of the center).
+            assert abs(queries[i, j] - (float(centers[c, j]) + 0.3 * g)) < 1e-5
+
+
 @pytest.mark.parametrize("data,want", [(b"123456789", 0xCBF43926), (b"", 0),
                                        (b"The quick brown fox jumps over the lazy dog", 0x414FA339)])
 def test_crc32_check_values(data, want):
