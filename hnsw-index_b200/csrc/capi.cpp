@@ -20,20 +20,14 @@
 #include <string>
 #include <vector>
 
-#include "brute_tc.hpp"
-#include "device.hpp"
-#include "host_index.hpp"
+#include "capi_internal.hpp"
 
 using namespace hnswgpu;
 
+namespace hnswgpu {
+
 namespace {
-
 thread_local std::string g_last_error;
-
-int set_error(int status, const std::string& msg) {
-    g_last_error = msg;
-    return status;
-}
 
 std::string format_error_message(const Err& e) {
     char buf[256];
@@ -65,6 +59,15 @@ std::string format_error_message(const Err& e) {
     }
 }
 
+}  // namespace
+
+const char* last_error_text() { return g_last_error.c_str(); }
+
+int set_error(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
 int from_err(const Err& e) { return e ? set_error(e.status, format_error_message(e)) : HNSW_OK; }
 
 int cuda_fail(cudaError_t e, const char* where) {
@@ -73,96 +76,6 @@ int cuda_fail(cudaError_t e, const char* where) {
     return set_error(HNSW_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-#define CU(call, where)                             \
-    do {                                            \
-        cudaError_t _e = (call);                    \
-        if (_e != cudaSuccess) return cuda_fail(_e, where); \
-    } while (0)
-
-uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
-
-// Growable device buffer.
-struct DBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    cudaError_t ensure(size_t need) {
-        if (need <= bytes) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, need);
-        if (e == cudaSuccess) bytes = need;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
-
-// One concurrent call's stream and scratch.
-struct Slot {
-    cudaStream_t stream = nullptr;
-    DBuf q, ks, efs, fbits, fused, okeys, odist, ocount, ostatus, work, overflow, counters;
-    DBuf g_results, g_cands, g_visited;
-    uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
-    uint64_t g_words = 0;
-    DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
-    size_t last_nq = 0;
-    ~Slot() {
-        for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
-                        &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands})
-            b->release();
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-struct SlotPool {
-    std::mutex mu;
-    std::vector<std::unique_ptr<Slot>> free;
-    int device = 0;
-    int acquire(Slot** out) {
-        {
-            std::lock_guard<std::mutex> g(mu);
-            if (!free.empty()) {
-                *out = free.back().release();
-                free.pop_back();
-                return HNSW_OK;
-            }
-        }
-        auto* s = new (std::nothrow) Slot();
-        if (!s) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out of host memory");
-        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) {
-            delete s;
-            return cuda_fail(e, "cudaStreamCreate");
-        }
-        *out = s;
-        return HNSW_OK;
-    }
-    void release(Slot* s) {
-        std::lock_guard<std::mutex> g(mu);
-        free.emplace_back(s);
-    }
-};
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
-
-// Scratch geometry per (ef bound): results, candidates and the visited
-// hash sized so that a typical traversal at that ef stays in shared memory.
-// Queries whose ef exceeds the fast kernel's 1024 go to the retry pass.
 // Persistent warps spill to global memory instead of restarting, so their
 // visited hash is sized near the typical visit count (about 12 per unit of
 // ef on the 1M x 128 workload, p99 about 25); plain warps size it for the tail.
@@ -193,72 +106,92 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
     return g;
 }
 
-}  // namespace
+}  // namespace hnswgpu
 
-struct hnsw_gpu_index {
-    int device = 0;
-    int num_sms = 148;
-    hnsw_index_info info{};
-    DeviceIndexView view;
-    DBuf vec, codes, norms, offset, adj0, upoff, adjU, keys, dead;
-    SlotPool slots;
-    bool counters = false;
-    std::mutex counters_mu;
-    std::vector<uint32_t> last_counters;
-    // Scratch of the device-pointer entry point: one slot, ordered on the
-    // device (an event joins each call after the previous one).
-    std::mutex dev_mu;
-    std::unique_ptr<Slot> dev_slot;
-    cudaEvent_t dev_done = nullptr;
-    ~hnsw_gpu_index() {
-        DeviceGuard g(device);
-        if (dev_done) {
-            cudaEventSynchronize(dev_done);
-            cudaEventDestroy(dev_done);
+// Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
+static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
+    const uint32_t warps = uint32_t(gi->num_sms) * 4;
+    const uint32_t cand_cap = std::max<uint32_t>(1u << 14, 4 * ef_cap);
+    const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
+    CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
+    CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
+    CU(s->g_visited.ensure(size_t(warps) * words * 4), "cudaMalloc retry visited");
+    s->g_warps = warps;
+    s->g_ef_cap = ef_cap;
+    s->g_cand_cap = cand_cap;
+    s->g_words = words;
+    return HNSW_OK;
+}
+
+// Enqueues one search on `stream` with device pointers. ef_max bounds every
+// per-query max(ef, k) of the batch.
+int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
+                          const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
+                          uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
+                          uint32_t out_stride, cudaStream_t stream) {
+    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
+    CU(s->work.ensure(16), "cudaMalloc work counters");
+    CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
+    CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
+    int r = ensure_retry(gi, s, std::max(geo.ef_cap, round_up(ef_max, 32)));
+    if (r != HNSW_OK) return r;
+    SearchArgs a;
+    a.ix = gi->view;
+    a.queries = d_q;
+    a.nq = uint32_t(nq);
+    a.k = o.k;
+    a.ef = o.ef;
+    a.ks = d_ks;
+    a.efs = d_efs;
+    a.quantized = o.quantized;
+    a.filter_bits = d_fbits;
+    a.filter_nbits = o.filter_nbits;
+    a.filter_stride = o.filter_stride;
+    a.filter_used = d_fused;
+    a.out_keys = d_keys;
+    a.out_dist = d_dist;
+    a.out_count = d_count;
+    a.out_status = d_status;
+    a.out_stride = out_stride;
+    if (gi->counters) {
+        CU(s->counters.ensure(std::max<size_t>(nq, 1) * 16), "cudaMalloc counters");
+        a.counters = s->counters.as<uint32_t>();
+    }
+    a.work_next = s->work.as<uint32_t>();
+    a.overflow_count = s->work.as<uint32_t>() + 1;
+    a.overflow_list = s->overflow.as<uint32_t>();
+    a.persistent = o.mode == HNSW_MODE_PERSISTENT ? 1 : 0;
+    if (a.persistent) {
+        uint32_t warps = 0;
+        CU(persistent_warps(geo, gi->view.dp, gi->view.dc, gi->num_sms, &warps), "occupancy");
+        const uint32_t words = ((gi->view.n + 31) / 32 + 3) & ~3u;
+        const uint32_t cand_cap = std::max<uint32_t>(8192, 4 * geo.ef_cap);
+        const size_t bits_bytes = size_t(warps) * words * 4;
+        if (bits_bytes > s->spill_bits.bytes) {
+            CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
+            CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
         }
-        dev_slot.reset();
-        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead}) b->release();
-        std::lock_guard<std::mutex> l(slots.mu);
-        slots.free.clear();
+        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
+        a.spill_bits = s->spill_bits.as<uint32_t>();
+        a.spill_words = words;
+        a.spill_cands = s->spill_cands.as<uint64_t>();
+        a.spill_cand_cap = cand_cap;
+        a.spill_slots = warps;
     }
-};
-
-struct hnsw_gpu_brute {
-    int device = 0;
-    int num_sms = 148;
-    uint32_t n = 0, dim = 0, dp = 0;
-    int metric = 0;
-    float max_xnorm = 0.0f;  // largest row norm (error margins of the tensor-core path)
-    DBuf base, keys;
-    SlotPool slots;
-    std::mutex mu;
-    DBuf qprep, part, okeys, odist, ocount, ostatus, q;
-    // Tensor-core path: BF16 operand rows per term count (index 0: 1 term, 1: 3 terms).
-    DBuf bop[2], xnorm2;
-    uint32_t bop_kp[2] = {0, 0};
-    DBuf aop, dense, thr1, thr2, margin, qnorm2, ccount, cand, err;
-    uint64_t last_candidates = 0, last_queries = 0;
-    float last_ms[4] = {0, 0, 0, 0};
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t stream = nullptr;
-    ~hnsw_gpu_brute() {
-        DeviceGuard g(device);
-        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &bop[0], &bop[1], &xnorm2,
-                        &aop, &dense, &thr1, &thr2, &margin, &qnorm2, &ccount, &cand, &err})
-            b->release();
-        for (cudaEvent_t& e : ev)
-            if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-struct hnsw_builder {
-    std::unique_ptr<Builder> b;
-};
+    a.g_results = s->g_results.as<uint64_t>();
+    a.g_cands = s->g_cands.as<uint64_t>();
+    a.g_visited = s->g_visited.as<uint32_t>();
+    a.g_ef_cap = s->g_ef_cap;
+    a.g_cand_cap = s->g_cand_cap;
+    a.g_visited_words = s->g_words;
+    CU(launch_search(a, geo, gi->num_sms, stream), "search kernel");
+    CU(launch_search_retry(a, s->g_warps, stream), "search retry kernel");
+    return HNSW_OK;
+}
 
 extern "C" {
 
-const char* hnsw_last_error(void) { return g_last_error.c_str(); }
+const char* hnsw_last_error(void) { return hnswgpu::last_error_text(); }
 
 uint32_t hnsw_crc32(const uint8_t* bytes, size_t len) { return crc32(bytes, len); }
 
@@ -462,86 +395,6 @@ int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq)
     return HNSW_OK;
 }
 
-// Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
-static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
-    const uint32_t warps = uint32_t(gi->num_sms) * 4;
-    const uint32_t cand_cap = std::max<uint32_t>(1u << 14, 4 * ef_cap);
-    const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
-    CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
-    CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
-    CU(s->g_visited.ensure(size_t(warps) * words * 4), "cudaMalloc retry visited");
-    s->g_warps = warps;
-    s->g_ef_cap = ef_cap;
-    s->g_cand_cap = cand_cap;
-    s->g_words = words;
-    return HNSW_OK;
-}
-
-// Enqueues one search on `stream` with device pointers. ef_max bounds every
-// per-query max(ef, k) of the batch.
-static int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
-                          const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
-                          uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
-                          uint32_t out_stride, cudaStream_t stream) {
-    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
-    CU(s->work.ensure(16), "cudaMalloc work counters");
-    CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
-    CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
-    int r = ensure_retry(gi, s, std::max(geo.ef_cap, round_up(ef_max, 32)));
-    if (r != HNSW_OK) return r;
-    SearchArgs a;
-    a.ix = gi->view;
-    a.queries = d_q;
-    a.nq = uint32_t(nq);
-    a.k = o.k;
-    a.ef = o.ef;
-    a.ks = d_ks;
-    a.efs = d_efs;
-    a.quantized = o.quantized;
-    a.filter_bits = d_fbits;
-    a.filter_nbits = o.filter_nbits;
-    a.filter_stride = o.filter_stride;
-    a.filter_used = d_fused;
-    a.out_keys = d_keys;
-    a.out_dist = d_dist;
-    a.out_count = d_count;
-    a.out_status = d_status;
-    a.out_stride = out_stride;
-    if (gi->counters) {
-        CU(s->counters.ensure(std::max<size_t>(nq, 1) * 16), "cudaMalloc counters");
-        a.counters = s->counters.as<uint32_t>();
-    }
-    a.work_next = s->work.as<uint32_t>();
-    a.overflow_count = s->work.as<uint32_t>() + 1;
-    a.overflow_list = s->overflow.as<uint32_t>();
-    a.persistent = o.mode == HNSW_MODE_PERSISTENT ? 1 : 0;
-    if (a.persistent) {
-        uint32_t warps = 0;
-        CU(persistent_warps(geo, gi->view.dp, gi->view.dc, gi->num_sms, &warps), "occupancy");
-        const uint32_t words = ((gi->view.n + 31) / 32 + 3) & ~3u;
-        const uint32_t cand_cap = std::max<uint32_t>(8192, 4 * geo.ef_cap);
-        const size_t bits_bytes = size_t(warps) * words * 4;
-        if (bits_bytes > s->spill_bits.bytes) {
-            CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
-            CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
-        }
-        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
-        a.spill_bits = s->spill_bits.as<uint32_t>();
-        a.spill_words = words;
-        a.spill_cands = s->spill_cands.as<uint64_t>();
-        a.spill_cand_cap = cand_cap;
-        a.spill_slots = warps;
-    }
-    a.g_results = s->g_results.as<uint64_t>();
-    a.g_cands = s->g_cands.as<uint64_t>();
-    a.g_visited = s->g_visited.as<uint32_t>();
-    a.g_ef_cap = s->g_ef_cap;
-    a.g_cand_cap = s->g_cand_cap;
-    a.g_visited_words = s->g_words;
-    CU(launch_search(a, geo, gi->num_sms, stream), "search kernel");
-    CU(launch_search_retry(a, s->g_warps, stream), "search retry kernel");
-    return HNSW_OK;
-}
 
 int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim,
                           const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist, uint32_t* out_count,

@@ -1,0 +1,200 @@
+// Internals of the C ABI shared by capi.cpp and server.cpp: device buffers,
+// per-call scratch slots, the index and brute-force handles, and the launch
+// helper of one search.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "brute_tc.hpp"
+#include "device.hpp"
+#include "hnsw_gpu.h"
+#include "host_index.hpp"
+
+namespace hnswgpu {
+
+// Records the message of the last failure on this thread; returns status.
+int set_error(int status, const std::string& msg);
+const char* last_error_text();
+int from_err(const Err& e);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define CU(call, where)                                      \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) return ::hnswgpu::cuda_fail(_e, where); \
+    } while (0)
+
+inline uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+// Growable device buffer.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, need);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// One concurrent call's stream and scratch.
+struct Slot {
+    cudaStream_t stream = nullptr;
+    DBuf q, ks, efs, fbits, fused, okeys, odist, ocount, ostatus, work, overflow, counters;
+    DBuf g_results, g_cands, g_visited;
+    uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
+    uint64_t g_words = 0;
+    DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
+    size_t last_nq = 0;
+    ~Slot() {
+        for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
+                        &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands})
+            b->release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct SlotPool {
+    std::mutex mu;
+    std::vector<std::unique_ptr<Slot>> free;
+    int device = 0;
+    int acquire(Slot** out) {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            if (!free.empty()) {
+                *out = free.back().release();
+                free.pop_back();
+                return HNSW_OK;
+            }
+        }
+        auto* s = new (std::nothrow) Slot();
+        if (!s) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out of host memory");
+        cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete s;
+            return cuda_fail(e, "cudaStreamCreate");
+        }
+        *out = s;
+        return HNSW_OK;
+    }
+    void release(Slot* s) {
+        std::lock_guard<std::mutex> g(mu);
+        free.emplace_back(s);
+    }
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Scratch geometry per (ef bound): results, candidates and the visited
+// hash sized so that a typical traversal at that ef stays in shared memory.
+// Queries whose ef exceeds the fast kernel's 1024 go to the retry pass.
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent);
+
+}  // namespace hnswgpu
+
+// The handle types of the C ABI (opaque to callers).
+using hnswgpu::DBuf;
+using hnswgpu::DeviceGuard;
+using hnswgpu::DeviceIndexView;
+using hnswgpu::Slot;
+using hnswgpu::SlotPool;
+using hnswgpu::Builder;
+
+struct hnsw_gpu_index {
+    int device = 0;
+    int num_sms = 148;
+    hnsw_index_info info{};
+    DeviceIndexView view;
+    DBuf vec, codes, norms, offset, adj0, upoff, adjU, keys, dead;
+    SlotPool slots;
+    bool counters = false;
+    std::mutex counters_mu;
+    std::vector<uint32_t> last_counters;
+    // Scratch of the device-pointer entry point: one slot, ordered on the
+    // device (an event joins each call after the previous one).
+    std::mutex dev_mu;
+    std::unique_ptr<Slot> dev_slot;
+    cudaEvent_t dev_done = nullptr;
+    ~hnsw_gpu_index() {
+        DeviceGuard g(device);
+        if (dev_done) {
+            cudaEventSynchronize(dev_done);
+            cudaEventDestroy(dev_done);
+        }
+        dev_slot.reset();
+        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead}) b->release();
+        std::lock_guard<std::mutex> l(slots.mu);
+        slots.free.clear();
+    }
+};
+
+struct hnsw_gpu_brute {
+    int device = 0;
+    int num_sms = 148;
+    uint32_t n = 0, dim = 0, dp = 0;
+    int metric = 0;
+    float max_xnorm = 0.0f;  // largest row norm (error margins of the tensor-core path)
+    DBuf base, keys;
+    SlotPool slots;
+    std::mutex mu;
+    DBuf qprep, part, okeys, odist, ocount, ostatus, q;
+    // Tensor-core path: BF16 operand rows per term count (index 0: 1 term, 1: 3 terms).
+    DBuf bop[2], xnorm2;
+    uint32_t bop_kp[2] = {0, 0};
+    DBuf aop, dense, thr1, thr2, margin, qnorm2, ccount, cand, err;
+    uint64_t last_candidates = 0, last_queries = 0;
+    float last_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t stream = nullptr;
+    ~hnsw_gpu_brute() {
+        DeviceGuard g(device);
+        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &bop[0], &bop[1], &xnorm2,
+                        &aop, &dense, &thr1, &thr2, &margin, &qnorm2, &ccount, &cand, &err})
+            b->release();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct hnsw_builder {
+    std::unique_ptr<Builder> b;
+};
+
+namespace hnswgpu {
+// Enqueues one search on `stream` with device pointers. ef_max bounds every
+// per-query max(ef, k) of the batch.
+int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
+                   const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
+                   uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
+                   uint32_t out_stride, cudaStream_t stream);
+}  // namespace hnswgpu
