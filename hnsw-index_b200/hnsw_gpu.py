@@ -478,6 +478,92 @@ class HnswIndex:
                                                  d_dist, d_count, d_status, handle))
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
+                ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
+                ("filter_nbits", C.c_uint64), ("quantized", C.c_int32)]
+
+
+_lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
+_lib.hnsw_server_config_default.restype = None
+_lib.hnsw_gpu_server_start.argtypes = [_vp, C.POINTER(_ServerConfig), C.POINTER(_vp)]
+_lib.hnsw_gpu_server_stop.argtypes = [_vp]
+_lib.hnsw_gpu_server_stop.restype = None
+_lib.hnsw_gpu_submit.argtypes = [_vp, _vp, C.c_uint32, C.c_uint32, _vp, C.POINTER(C.c_uint64)]
+_lib.hnsw_gpu_poll.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_int)]
+_lib.hnsw_gpu_wait.argtypes = [_vp, C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_uint32),
+                               C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+_lib.hnsw_gpu_server_replay.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+_lib.hnsw_gpu_server_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+
+
+class Server:
+    """Request loop over a resident HnswIndex (continuous batching)."""
+
+    def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
+                 max_ef=512, linger_us=100, filter_nbits=0, quantized=False):
+        cfg = _ServerConfig()
+        _lib.hnsw_server_config_default(C.byref(cfg))
+        cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
+        cfg.max_k, cfg.max_ef, cfg.linger_us = max_k, max_ef, linger_us
+        cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
+        h = C.c_void_p()
+        _check(_lib.hnsw_gpu_server_start(index._h, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._index = index
+        self.max_k = max_k
+        self.words = (filter_nbits + 63) // 64
+
+    def submit(self, query, k: int, ef: int, filter_bits: Optional[np.ndarray] = None) -> int:
+        q = np.ascontiguousarray(query, np.float32)
+        fb = None if filter_bits is None else np.ascontiguousarray(filter_bits, np.uint64)
+        t = C.c_uint64()
+        _check(_lib.hnsw_gpu_submit(self._h, _ptr(q), k, ef, _ptr(fb), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000):
+        keys = np.zeros(self.max_k, np.uint64)
+        dist = np.zeros(self.max_k, np.float32)
+        cnt, st, lat = C.c_uint32(), C.c_int32(), C.c_double()
+        _check(_lib.hnsw_gpu_wait(self._h, ticket, timeout_ms, _ptr(keys), _ptr(dist), C.byref(cnt), C.byref(st),
+                                  C.byref(lat)))
+        c = cnt.value
+        return keys[:c], dist[:c], st.value, lat.value
+
+    def replay(self, queries, arrival_us, ks, efs, filtered=None, filter_bits=None):
+        q = np.ascontiguousarray(queries, np.float32)
+        n = q.shape[0]
+        arr = np.ascontiguousarray(arrival_us, np.float64)
+        ks_a = np.ascontiguousarray(ks, np.uint32)
+        efs_a = np.ascontiguousarray(efs, np.uint32)
+        fl = None if filtered is None else np.ascontiguousarray(filtered, np.uint8)
+        fb = None if filter_bits is None else np.ascontiguousarray(filter_bits, np.uint64)
+        keys = np.zeros((n, self.max_k), np.uint64)
+        dist = np.zeros((n, self.max_k), np.float32)
+        cnt = np.zeros(n, np.uint32)
+        st = np.zeros(n, np.int32)
+        lat = np.zeros(n, np.float64)
+        _check(_lib.hnsw_gpu_server_replay(self._h, _ptr(q), n, _ptr(arr), _ptr(ks_a), _ptr(efs_a), _ptr(fl),
+                                           _ptr(fb), _ptr(keys), _ptr(dist), _ptr(cnt), _ptr(st), _ptr(lat)))
+        return keys, dist, cnt, st, lat
+
+    def stats(self):
+        b, q = C.c_uint64(), C.c_uint64()
+        _check(_lib.hnsw_gpu_server_stats(self._h, C.byref(b), C.byref(q)))
+        return b.value, q.value
+
+    def stop(self):
+        if self._h:
+            _lib.hnsw_gpu_server_stop(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
 def validate_bytes(data: bytes, max_memory: Optional[int] = None) -> _Info:
     """Host-only validation with every check of HnswIndex::from_bytes."""
     buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)

@@ -147,6 +147,54 @@ int hnsw_gpu_set_counters(hnsw_gpu_index* index, int enabled);
 int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq);
 
 /* ------------------------------------------------------------------ */
+/* Request loop: continuous batching over a resident index             */
+/* ------------------------------------------------------------------ */
+/* No single counterpart in the reference: it serves search_with
+ * (src/hnsw/mod.rs:448-455) requests that arrive one at a time. A dispatcher
+ * thread batches pending requests and launches each batch on its own stream
+ * as soon as one of max_inflight device scratch slots is free, so requests
+ * arriving while earlier batches run join the next launch and overlap on the
+ * device. Each result equals the same search run alone. */
+
+typedef struct hnsw_gpu_server hnsw_gpu_server;
+
+typedef struct hnsw_server_config {
+    uint32_t max_batch;     /* queries per launch */
+    uint32_t max_inflight;  /* launches (device scratch slots) in flight */
+    uint32_t max_pending;   /* queued requests before submit is rejected */
+    uint32_t max_k, max_ef; /* admission bounds (scratch sizing) */
+    uint32_t linger_us;     /* how long a partial batch waits while others run */
+    uint64_t filter_nbits;  /* key-bitmap width of filtered requests; 0 = none */
+    int32_t quantized;      /* int8 traversal + exact re-rank */
+} hnsw_server_config;
+
+void hnsw_server_config_default(hnsw_server_config* cfg);
+int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg, hnsw_gpu_server** out);
+/* Finishes queued and in-flight requests, then frees the server. */
+void hnsw_gpu_server_stop(hnsw_gpu_server* server);
+/* Non-blocking: copies the query (and filter bitmap, filter_nbits bits) and
+ * returns a ticket, or HNSW_ERR_ADMISSION_REJECTED when the queue is full. */
+int hnsw_gpu_submit(hnsw_gpu_server* server, const float* query, uint32_t k, uint32_t ef,
+                    const uint64_t* filter_bits, uint64_t* ticket);
+int hnsw_gpu_poll(hnsw_gpu_server* server, uint64_t ticket, int* done);
+/* Waits up to timeout_ms; copies the results (keys/dist: k entries) and the
+ * request's latency (arrival to completion, microseconds), and frees the
+ * ticket. */
+int hnsw_gpu_wait(hnsw_gpu_server* server, uint64_t ticket, uint32_t timeout_ms, uint64_t* keys, float* dist,
+                  uint32_t* count, int32_t* status, double* latency_us);
+/* Open-loop load: request i is submitted at arrival_us[i] microseconds after
+ * the call starts (ascending); outputs as hnsw_gpu_wait, per request, with
+ * stride max_k for keys/dist (NULL to skip). Rejected requests get status
+ * HNSW_ERR_ADMISSION_REJECTED and latency -1. filter_bits holds one bitmap
+ * per request (stride ceil(filter_nbits / 64) words), used where filtered[i]. */
+int hnsw_gpu_server_replay(hnsw_gpu_server* server, const float* queries, size_t n, const double* arrival_us,
+                           const uint32_t* ks, const uint32_t* efs, const uint8_t* filtered,
+                           const uint64_t* filter_bits, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                           int32_t* out_status, double* out_latency_us);
+/* Launched batches and queries since start. */
+int hnsw_gpu_server_stats(const hnsw_gpu_server* server, uint64_t* batches, uint64_t* queries);
+
+/* ------------------------------------------------------------------ */
 /* Exact brute-force k-NN on the device                                */
 /* ------------------------------------------------------------------ */
 

@@ -1,0 +1,118 @@
+"""Request loop: continuous batching over a resident index.
+
+Each request submitted to the server must return exactly what the same
+search returns alone (search_with, src/hnsw/mod.rs:448-455): the batches mix
+k, ef and filters, run concurrently on several streams, and the kernel keeps
+every query's traversal independent.
+"""
+
+import numpy as np
+import pytest
+
+import hnsw_gpu as H
+import oracle as O
+from conftest import build_index
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def served():
+    base, queries = H.mixture(20000, 600, 32, 40, 0.4, 31)
+    data = build_index(base, metric=0, m=16, seed=3)
+    return base, queries, data
+
+
+def make_requests(queries, nbits, seed):
+    rng = np.random.default_rng(seed)
+    n = len(queries)
+    ks = rng.choice([10, 100], n).astype(np.uint32)
+    efs = np.exp(rng.uniform(np.log(32), np.log(512), n)).astype(np.uint32)
+    filtered = (rng.random(n) < 0.3).astype(np.uint8)
+    words = (nbits + 63) // 64
+    bits = np.zeros((n, words), np.uint64)
+    for i in range(n):
+        if filtered[i]:
+            sel = rng.random(nbits) < rng.uniform(0.05, 0.5)
+            bits[i] = H.key_bitmap(np.nonzero(sel)[0].astype(np.uint64), nbits)
+    return ks, efs, filtered, bits
+
+
+def alone(gi, oi, queries, ks, efs, filtered, bits, nbits):
+    """Each request searched alone (one query per call) on the GPU, and the oracle."""
+    out = []
+    for i in range(len(queries)):
+        fb = bits[i] if filtered[i] else None
+        g = gi.search_arrays(queries[i:i + 1], int(ks[i]), int(efs[i]), filter_bits=fb,
+                             filter_nbits=nbits if fb is not None else 0)
+        out.append(g)
+    words = bits.shape[1]
+    ref = oi.search(queries, 100, 16, ks=ks.astype(np.uint64), efs=efs.astype(np.uint64), filter_bits=bits,
+                    filter_nbits=nbits, filter_stride=words, filter_used=filtered)
+    return out, ref
+
+
+def test_submitted_requests_equal_alone_results(served):
+    base, queries, data = served
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    nbits = 20000
+    q = queries[:200]
+    ks, efs, filtered, bits = make_requests(q, nbits, 1)
+    srv = H.Server(gi, max_batch=64, max_inflight=3, filter_nbits=nbits)
+    tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), bits[i] if filtered[i] else None) for i in range(len(q))]
+    results = [srv.wait(t) for t in tickets]
+    batches, launched = srv.stats()
+    srv.stop()
+    assert launched == len(q) and batches >= 2
+    one, ref = alone(gi, oi, q, ks, efs, filtered, bits, nbits)
+    for i, (keys, dist, status, lat) in enumerate(results):
+        assert status == 0
+        c = int(ref[2][i])
+        np.testing.assert_array_equal(keys, ref[0][i, :c])
+        np.testing.assert_array_equal(dist.view(np.uint32), ref[1][i, :c].view(np.uint32))
+        np.testing.assert_array_equal(keys, one[i][0][0, :int(one[i][2][0])])
+        assert lat >= 0
+
+
+def test_open_loop_replay_mixes_requests_and_matches(served):
+    base, queries, data = served
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    nbits = 20000
+    ks, efs, filtered, bits = make_requests(queries, nbits, 2)
+    rng = np.random.default_rng(3)
+    arrivals = np.cumsum(rng.exponential(1e6 / 200000.0, len(queries)))  # 200k requests/s
+    srv = H.Server(gi, max_batch=128, max_inflight=4, filter_nbits=nbits, linger_us=50)
+    keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, filtered, bits)
+    batches, launched = srv.stats()
+    srv.stop()
+    assert (st == 0).all()
+    assert batches > 1
+    words = bits.shape[1]
+    ref = oi.search(queries, 100, 16, ks=ks.astype(np.uint64), efs=efs.astype(np.uint64), filter_bits=bits,
+                    filter_nbits=nbits, filter_stride=words, filter_used=filtered)
+    for i in range(len(queries)):
+        c = int(ref[2][i])
+        assert cnt[i] == c
+        np.testing.assert_array_equal(keys[i, :c], ref[0][i, :c])
+        np.testing.assert_array_equal(dist[i, :c].view(np.uint32), ref[1][i, :c].view(np.uint32))
+    assert (lat > 0).all()
+
+
+def test_admission_rejects_when_queue_is_full(served):
+    base, queries, data = served
+    gi = H.HnswIndex.from_bytes(data)
+    srv = H.Server(gi, max_batch=8, max_inflight=1, max_pending=16)
+    accepted, rejected = [], 0
+    for i in range(400):
+        try:
+            accepted.append(srv.submit(queries[i % len(queries)], 10, 512))
+        except H.Error as e:
+            assert e.status == H.Status.ADMISSION_REJECTED
+            rejected += 1
+    for t in accepted:
+        _, _, status, _ = srv.wait(t)
+        assert status == 0
+    srv.stop()
+    assert rejected > 0 and len(accepted) >= 16
