@@ -127,9 +127,11 @@ static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
 // per-query max(ef, k) of the batch.
 int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
                           const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
+                          const uint32_t* d_fids,
                           uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
                           uint32_t out_stride, cudaStream_t stream) {
-    SearchGeometry geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
+    SearchGeometry geo = gi->fixed.ef_cap ? gi->fixed
+                                          : pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
     CU(s->work.ensure(16), "cudaMalloc work counters");
     CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
     CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
@@ -148,6 +150,7 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.filter_nbits = o.filter_nbits;
     a.filter_stride = o.filter_stride;
     a.filter_used = d_fused;
+    a.filter_ids = d_fids;
     a.out_keys = d_keys;
     a.out_dist = d_dist;
     a.out_count = d_count;
@@ -381,6 +384,27 @@ int hnsw_gpu_set_tombstones(hnsw_gpu_index* index, const uint8_t* deleted, size_
     return HNSW_OK;
 }
 
+int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
+    if (!index) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null index");
+    if (!sc) {
+        index->fixed = SearchGeometry{0, 0, 0, 0, 0};
+        return HNSW_OK;
+    }
+    const bool pow2 = sc->hash_cap >= 64 && (sc->hash_cap & (sc->hash_cap - 1)) == 0;
+    if (sc->ef_cap < 32 || sc->ef_cap > 1024 || sc->ef_cap % 32 || sc->cand_cap < sc->ef_cap || !pow2 ||
+        sc->warps_per_block < 1 || sc->warps_per_block > 8)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule out of range");
+    SearchGeometry g;
+    g.ef_cap = sc->ef_cap;
+    g.cand_cap = sc->cand_cap;
+    g.hash_cap = sc->hash_cap;
+    g.warps_per_block = sc->warps_per_block;
+    if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
+    index->fixed = g;
+    return HNSW_OK;
+}
+
 int hnsw_gpu_set_counters(hnsw_gpu_index* index, int enabled) {
     if (!index) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null index");
     index->counters = enabled != 0;
@@ -443,9 +467,19 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
         CU(cudaMemcpyAsync(s->efs.p, o.efs, nq * 4, cudaMemcpyHostToDevice, st), "copy efs");
         d_efs = s->efs.as<uint32_t>();
     }
+    const uint32_t* d_fi = nullptr;
     if (o.filter_bits) {
         const uint64_t words = (o.filter_nbits + 63) / 64;
-        const uint64_t total = o.filter_stride ? o.filter_stride * (nq - 1) + words : words;
+        uint64_t bitmaps = nq;
+        if (o.filter_ids) {
+            uint32_t mx = 0;
+            for (size_t i = 0; i < nq; ++i) mx = std::max(mx, o.filter_ids[i]);
+            bitmaps = uint64_t(mx) + 1;
+            CU(s->fids.ensure(nq * 4), "cudaMalloc filter ids");
+            CU(cudaMemcpyAsync(s->fids.p, o.filter_ids, nq * 4, cudaMemcpyHostToDevice, st), "copy filter ids");
+            d_fi = s->fids.as<uint32_t>();
+        }
+        const uint64_t total = o.filter_stride ? o.filter_stride * (bitmaps - 1) + words : words;
         CU(s->fbits.ensure(total * 8), "cudaMalloc filter");
         CU(cudaMemcpyAsync(s->fbits.p, o.filter_bits, total * 8, cudaMemcpyHostToDevice, st), "copy filter");
         d_fb = s->fbits.as<uint64_t>();
@@ -459,7 +493,7 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
     CU(s->odist.ensure(nq * stride * 4), "cudaMalloc out dist");
     CU(s->ocount.ensure(nq * 4), "cudaMalloc out count");
     CU(s->ostatus.ensure(nq * 4), "cudaMalloc out status");
-    r = enqueue_search(gi, s, s->q.as<float>(), nq, o, d_ks, d_efs, d_fb, d_fu, s->okeys.as<uint64_t>(),
+    r = enqueue_search(gi, s, s->q.as<float>(), nq, o, d_ks, d_efs, d_fb, d_fu, d_fi, s->okeys.as<uint64_t>(),
                        s->odist.as<float>(), s->ocount.as<uint32_t>(), s->ostatus.as<int32_t>(), ef_bound, stride, st);
     if (r != HNSW_OK) return r;
     CU(cudaMemcpyAsync(out_count, s->ocount.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
@@ -508,10 +542,85 @@ int hnsw_gpu_search_batch_device(hnsw_gpu_index* gi, const float* d_queries, siz
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
     // The slot's buffers may still be in use by the previous call on another stream.
     CU(cudaStreamWaitEvent(st, gi->dev_done, 0), "cudaStreamWaitEvent");
-    int r = enqueue_search(gi, s, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used, d_keys, d_dist,
-                           d_count, d_status, ef_bound, stride, st);
+    int r = enqueue_search(gi, s, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used, o->filter_ids,
+                           d_keys, d_dist, d_count, d_status, ef_bound, stride, st);
     CU(cudaEventRecord(gi->dev_done, st), "cudaEventRecord");
     return r;
+}
+
+struct hnsw_gpu_graph {
+    hnsw_gpu_index* index = nullptr;
+    Slot* slot = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+// Captures memset + search + retry for a fixed batch (relaxed capture mode;
+// a warm-up enqueue first sizes every buffer, so the captured call allocates
+// nothing).
+int hnsw_gpu_graph_create(hnsw_gpu_index* gi, const float* d_queries, size_t nq, size_t dim,
+                          const hnsw_search_opts* o, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
+                          int32_t* d_status, hnsw_gpu_graph** out) {
+    if (!gi || !o || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (dim != gi->view.dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return set_error(HNSW_ERR_INVALID_ARGUMENT, "empty batch");
+    DeviceGuard dg(gi->device);
+    std::unique_ptr<hnsw_gpu_graph> g(new hnsw_gpu_graph());
+    g->index = gi;
+    int r = gi->slots.acquire(&g->slot);
+    if (r != HNSW_OK) return r;
+    cudaStream_t st = g->slot->stream;
+    const uint32_t ef_bound = std::max(o->k, o->ef);
+    const uint32_t stride = o->out_stride ? o->out_stride : std::max<uint32_t>(o->k, 1);
+    auto enqueue = [&]() {
+        return enqueue_search(gi, g->slot, d_queries, nq, *o, o->ks, o->efs, o->filter_bits, o->filter_used,
+                              o->filter_ids, d_keys, d_dist, d_count, d_status, ef_bound, stride, st);
+    };
+    r = enqueue();
+    if (r != HNSW_OK) {
+        gi->slots.release(g->slot);
+        return r;
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        gi->slots.release(g->slot);
+        return cuda_fail(e, "graph capture");
+    }
+    r = enqueue();
+    e = cudaStreamEndCapture(st, &g->graph);
+    if (r != HNSW_OK || e != cudaSuccess) {
+        if (g->graph) cudaGraphDestroy(g->graph);
+        gi->slots.release(g->slot);
+        return r != HNSW_OK ? r : cuda_fail(e, "graph capture");
+    }
+    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g->graph);
+        gi->slots.release(g->slot);
+        return cuda_fail(e, "graph instantiate");
+    }
+    *out = g.release();
+    return HNSW_OK;
+}
+
+int hnsw_gpu_graph_launch(hnsw_gpu_graph* g, void* stream) {
+    if (!g) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null graph");
+    DeviceGuard dg(g->index->device);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->slot->stream;
+    CU(cudaGraphLaunch(g->exec, st), "graph launch");
+    return HNSW_OK;
+}
+
+void hnsw_gpu_graph_destroy(hnsw_gpu_graph* g) {
+    if (!g) return;
+    DeviceGuard dg(g->index->device);
+    cudaStreamSynchronize(g->slot->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->index->slots.release(g->slot);
+    delete g;
 }
 
 // ------------------------------------------------------------------------

@@ -60,14 +60,14 @@ struct DBuf {
 // One concurrent call's stream and scratch.
 struct Slot {
     cudaStream_t stream = nullptr;
-    DBuf q, ks, efs, fbits, fused, okeys, odist, ocount, ostatus, work, overflow, counters;
+    DBuf q, ks, efs, fbits, fused, fids, okeys, odist, ocount, ostatus, work, overflow, counters;
     DBuf g_results, g_cands, g_visited;
     uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_words = 0;
     DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
     size_t last_nq = 0;
     ~Slot() {
-        for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
+        for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &fids, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
                         &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands})
             b->release();
         if (stream) cudaStreamDestroy(stream);
@@ -143,6 +143,8 @@ struct hnsw_gpu_index {
     // device (an event joins each call after the previous one).
     std::mutex dev_mu;
     std::unique_ptr<Slot> dev_slot;
+    // Fixed schedule (hnsw_gpu_set_schedule); ef_cap == 0 means automatic.
+    hnswgpu::SearchGeometry fixed{0, 0, 0, 0, 0};
     cudaEvent_t dev_done = nullptr;
     ~hnsw_gpu_index() {
         DeviceGuard g(device);
@@ -195,6 +197,6 @@ namespace hnswgpu {
 // per-query max(ef, k) of the batch.
 int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
                    const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
-                   uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
+                   const uint32_t* d_fids, uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
                    uint32_t out_stride, cudaStream_t stream);
 }  // namespace hnswgpu

@@ -55,6 +55,7 @@ struct SearchArgs {
     uint64_t filter_nbits = 0;
     uint64_t filter_stride = 0;
     const uint8_t* filter_used = nullptr;
+    const uint32_t* filter_ids = nullptr;  // optional bitmap index per query
     uint64_t* out_keys = nullptr;
     float* out_dist = nullptr;
     uint32_t* out_count = nullptr;

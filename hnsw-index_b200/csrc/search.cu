@@ -508,7 +508,8 @@ __device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
     c.s2 = __fmul_rn(ix.scale, ix.scale);
     c.qnorm = 0;
     c.use_filter = a.filter_bits != nullptr && (a.filter_used == nullptr || a.filter_used[qi] != 0);
-    c.fbits = a.filter_bits + (a.filter_stride ? size_t(qi) * a.filter_stride : 0);
+    const size_t fsel = a.filter_ids ? size_t(a.filter_ids[qi]) : size_t(qi);
+    c.fbits = a.filter_bits + (a.filter_stride ? fsel * a.filter_stride : 0);
     c.fnbits = a.filter_nbits;
     const uint32_t k = min(a.ks ? a.ks[qi] : a.k, a.out_stride);
     uint32_t ef = a.efs ? a.efs[qi] : a.ef;

@@ -34,7 +34,7 @@ enum class ReqState : uint8_t { Free, Pending, Inflight, Done };
 struct Request {
     ReqState state = ReqState::Free;
     uint32_t k = 0, ef = 0;
-    bool filtered = false;
+    int32_t filter_id = -1;
     int32_t status = 0;
     uint32_t count = 0;
     double t_arrival = 0, t_done = 0;
@@ -51,7 +51,7 @@ struct BatchSlot {
     uint32_t* h_ks = nullptr;
     uint32_t* h_efs = nullptr;
     uint8_t* h_fused = nullptr;
-    uint64_t* h_fbits = nullptr;
+    uint32_t* h_fids = nullptr;
     uint64_t* h_keys = nullptr;
     float* h_dist = nullptr;
     uint32_t* h_count = nullptr;
@@ -66,7 +66,7 @@ struct hnsw_gpu_server {
     uint32_t dim = 0, words = 0;
     std::vector<Request> req;
     std::vector<float> q;            // cap x dim
-    std::vector<uint64_t> fbits;     // cap x words
+    DBuf bank;                       // filter bank on the device
     std::vector<uint64_t> keys;      // cap x max_k
     std::vector<float> dist;         // cap x max_k
     uint64_t cap = 0;
@@ -94,12 +94,9 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
         std::memcpy(b.h_q + size_t(i) * dim, &s->q[(tickets[i] % s->cap) * dim], size_t(dim) * 4);
         b.h_ks[i] = r.k;
         b.h_efs[i] = r.ef;
-        b.h_fused[i] = r.filtered ? 1 : 0;
-        if (r.filtered) {
-            any_filter = true;
-            std::memcpy(b.h_fbits + size_t(i) * s->words, &s->fbits[(tickets[i] % s->cap) * s->words],
-                        size_t(s->words) * 8);
-        }
+        b.h_fused[i] = r.filter_id >= 0 ? 1 : 0;
+        b.h_fids[i] = r.filter_id >= 0 ? uint32_t(r.filter_id) : 0u;
+        any_filter |= r.filter_id >= 0;
     }
     Slot* sl = b.slot;
     cudaStream_t st = sl->stream;
@@ -115,14 +112,15 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     CU(cudaMemcpyAsync(sl->efs.p, b.h_efs, size_t(n) * 4, cudaMemcpyHostToDevice, st), "copy efs");
     const uint64_t* d_fb = nullptr;
     const uint8_t* d_fu = nullptr;
+    const uint32_t* d_fi = nullptr;
     if (any_filter && s->words) {
-        CU(sl->fbits.ensure(size_t(s->cfg.max_batch) * s->words * 8), "server filter bits");
         CU(sl->fused.ensure(size_t(s->cfg.max_batch)), "server filter flags");
-        CU(cudaMemcpyAsync(sl->fbits.p, b.h_fbits, size_t(n) * s->words * 8, cudaMemcpyHostToDevice, st),
-           "copy filter bits");
+        CU(sl->fids.ensure(size_t(s->cfg.max_batch) * 4), "server filter ids");
         CU(cudaMemcpyAsync(sl->fused.p, b.h_fused, n, cudaMemcpyHostToDevice, st), "copy filter flags");
-        d_fb = sl->fbits.as<uint64_t>();
+        CU(cudaMemcpyAsync(sl->fids.p, b.h_fids, size_t(n) * 4, cudaMemcpyHostToDevice, st), "copy filter ids");
+        d_fb = s->bank.as<uint64_t>();
         d_fu = sl->fused.as<uint8_t>();
+        d_fi = sl->fids.as<uint32_t>();
     }
     hnsw_search_opts o{};
     o.k = K;
@@ -133,7 +131,7 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     o.out_stride = K;
     o.mode = HNSW_MODE_PERSISTENT;
     int r = enqueue_search(s->index, sl, sl->q.as<float>(), n, o, sl->ks.as<uint32_t>(), sl->efs.as<uint32_t>(), d_fb,
-                           d_fu, sl->okeys.as<uint64_t>(), sl->odist.as<float>(), sl->ocount.as<uint32_t>(),
+                           d_fu, d_fi, sl->okeys.as<uint64_t>(), sl->odist.as<float>(), sl->ocount.as<uint32_t>(),
                            sl->ostatus.as<int32_t>(), std::max(K, s->cfg.max_ef), K, st);
     if (r != HNSW_OK) return r;
     CU(cudaMemcpyAsync(b.h_count, sl->ocount.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st), "copy counts");
@@ -247,6 +245,8 @@ void hnsw_server_config_default(hnsw_server_config* c) {
     c->linger_us = 100;
     c->filter_nbits = 0;
     c->quantized = 0;
+    c->filter_bank = nullptr;
+    c->filter_count = 0;
 }
 
 int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_in, hnsw_gpu_server** out) {
@@ -267,9 +267,16 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
     s->dim = index->view.dim;
     s->words = uint32_t((cfg.filter_nbits + 63) / 64);
     s->cap = uint64_t(cfg.max_pending) + uint64_t(cfg.max_inflight) * cfg.max_batch;
+    if ((cfg.filter_count > 0) != (cfg.filter_bank != nullptr) || (cfg.filter_count && !s->words))
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "filter bank needs filter_nbits, bitmaps and their count");
     s->req.resize(s->cap);
     s->q.resize(s->cap * s->dim);
-    s->fbits.resize(s->cap * std::max<uint32_t>(s->words, 1));
+    if (cfg.filter_count) {
+        const size_t bytes = size_t(cfg.filter_count) * s->words * 8;
+        CU(s->bank.ensure(bytes), "cudaMalloc filter bank");
+        CU(cudaMemcpy(s->bank.p, cfg.filter_bank, bytes, cudaMemcpyHostToDevice), "copy filter bank");
+    }
+    s->cfg.filter_bank = nullptr;
     s->keys.resize(s->cap * cfg.max_k);
     s->dist.resize(s->cap * cfg.max_k);
     s->batches.resize(cfg.max_inflight);
@@ -282,7 +289,7 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
         CU(cudaMallocHost(&b.h_ks, B * 4), "pinned ks");
         CU(cudaMallocHost(&b.h_efs, B * 4), "pinned efs");
         CU(cudaMallocHost(&b.h_fused, B), "pinned filter flags");
-        CU(cudaMallocHost(&b.h_fbits, B * std::max<uint32_t>(s->words, 1) * 8), "pinned filter bits");
+        CU(cudaMallocHost(&b.h_fids, B * 4), "pinned filter ids");
         CU(cudaMallocHost(&b.h_keys, B * cfg.max_k * 8), "pinned keys");
         CU(cudaMallocHost(&b.h_dist, B * cfg.max_k * 4), "pinned dist");
         CU(cudaMallocHost(&b.h_count, B * 4), "pinned counts");
@@ -305,22 +312,23 @@ void hnsw_gpu_server_stop(hnsw_gpu_server* s) {
     DeviceGuard dg(s->index->device);
     for (BatchSlot& b : s->batches) {
         if (b.done) cudaEventDestroy(b.done);
-        for (void* p : {(void*)b.h_q, (void*)b.h_ks, (void*)b.h_efs, (void*)b.h_fused, (void*)b.h_fbits,
+        for (void* p : {(void*)b.h_q, (void*)b.h_ks, (void*)b.h_efs, (void*)b.h_fused, (void*)b.h_fids,
                         (void*)b.h_keys, (void*)b.h_dist, (void*)b.h_count, (void*)b.h_status})
             if (p) cudaFreeHost(p);
         if (b.slot) s->index->slots.release(b.slot);
     }
+    s->bank.release();
     delete s;
 }
 
 // Admits requests whose arrival time (microseconds on the server clock, or
 // now when arrival_us < 0) is given; the caller holds no lock.
-static int submit_locked(hnsw_gpu_server* s, const float* query, uint32_t k, uint32_t ef, const uint64_t* filter_bits,
+static int submit_locked(hnsw_gpu_server* s, const float* query, uint32_t k, uint32_t ef, int32_t filter_id,
                          double arrival_us, uint64_t* ticket) {
     if (k == 0 || k > s->cfg.max_k || ef > s->cfg.max_ef)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "k or ef outside the server's bounds");
-    if (filter_bits && s->words == 0)
-        return set_error(HNSW_ERR_INVALID_ARGUMENT, "server started without filter support");
+    if (filter_id >= 0 && uint32_t(filter_id) >= s->cfg.filter_count)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "filter id outside the server's filter bank");
     if (s->pending.size() >= s->cfg.max_pending)
         return set_error(HNSW_ERR_ADMISSION_REJECTED, "request queue full");
     const uint64_t t = s->next_ticket;
@@ -331,25 +339,24 @@ static int submit_locked(hnsw_gpu_server* s, const float* query, uint32_t k, uin
     r.ticket = t;
     r.k = k;
     r.ef = ef;
-    r.filtered = filter_bits != nullptr;
+    r.filter_id = filter_id;
     r.status = 0;
     r.count = 0;
     r.t_arrival = arrival_us >= 0 ? arrival_us : now_us();
     std::memcpy(&s->q[(t % s->cap) * s->dim], query, size_t(s->dim) * 4);
-    if (filter_bits) std::memcpy(&s->fbits[(t % s->cap) * s->words], filter_bits, size_t(s->words) * 8);
     s->pending.push_back(t);
     *ticket = t;
     return HNSW_OK;
 }
 
-int hnsw_gpu_submit(hnsw_gpu_server* s, const float* query, uint32_t k, uint32_t ef, const uint64_t* filter_bits,
+int hnsw_gpu_submit(hnsw_gpu_server* s, const float* query, uint32_t k, uint32_t ef, int32_t filter_id,
                     uint64_t* ticket) {
     if (!s || !query || !ticket) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
     int r;
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (s->stop) return set_error(HNSW_ERR_INVALID_ARGUMENT, "server stopped");
-        r = submit_locked(s, query, k, ef, filter_bits, -1.0, ticket);
+        r = submit_locked(s, query, k, ef, filter_id, -1.0, ticket);
     }
     if (r == HNSW_OK) s->cv_work.notify_one();
     return r;
@@ -386,9 +393,8 @@ int hnsw_gpu_wait(hnsw_gpu_server* s, uint64_t ticket, uint32_t timeout_ms, uint
 }
 
 int hnsw_gpu_server_replay(hnsw_gpu_server* s, const float* queries, size_t n, const double* arrival_us,
-                           const uint32_t* ks, const uint32_t* efs, const uint8_t* filtered, const uint64_t* filter_bits,
-                           uint64_t* out_keys, float* out_dist, uint32_t* out_count, int32_t* out_status,
-                           double* out_latency_us) {
+                           const uint32_t* ks, const uint32_t* efs, const int32_t* filter_ids, uint64_t* out_keys,
+                           float* out_dist, uint32_t* out_count, int32_t* out_status, double* out_latency_us) {
     if (!s || (n && (!queries || !arrival_us || !ks || !efs || !out_count || !out_status || !out_latency_us)))
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
     const uint32_t dim = s->dim, K = s->cfg.max_k;
@@ -409,9 +415,9 @@ int hnsw_gpu_server_replay(hnsw_gpu_server* s, const float* queries, size_t n, c
             {
                 std::lock_guard<std::mutex> g(s->mu);
                 while (i < n && arrival_us[i] <= now_us() - t0) {
-                    const uint64_t* fb = (filtered && filtered[i] && filter_bits) ? filter_bits + i * s->words : nullptr;
+                    const int32_t fid = filter_ids ? filter_ids[i] : -1;
                     uint64_t t = 0;
-                    if (submit_locked(s, queries + i * dim, ks[i], efs[i], fb, t0 + arrival_us[i], &t) == HNSW_OK) {
+                    if (submit_locked(s, queries + i * dim, ks[i], efs[i], fid, t0 + arrival_us[i], &t) == HNSW_OK) {
                         tickets[i] = t;
                         admitted[i] = 1;
                     }

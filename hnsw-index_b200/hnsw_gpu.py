@@ -130,7 +130,7 @@ class _Opts(C.Structure):
         ("k", C.c_uint32), ("ef", C.c_uint32), ("ks", C.c_void_p), ("efs", C.c_void_p),
         ("quantized", C.c_int32), ("filter_bits", C.c_void_p), ("filter_nbits", C.c_uint64),
         ("filter_stride", C.c_uint64), ("filter_used", C.c_void_p), ("out_stride", C.c_uint32),
-        ("mode", C.c_int32),
+        ("mode", C.c_int32), ("filter_ids", C.c_void_p),
     ]
 
 
@@ -154,6 +154,18 @@ _lib.hnsw_gpu_set_tombstones.argtypes = [_vp, _vp, _sz]
 _lib.hnsw_gpu_search_batch.argtypes = [_vp, _vp, _sz, _sz, C.POINTER(_Opts), _vp, _vp, _vp, _vp]
 _lib.hnsw_gpu_search_batch_device.argtypes = [_vp, _vp, _sz, _sz, C.POINTER(_Opts), _vp, _vp, _vp, _vp, _vp]
 _lib.hnsw_gpu_set_counters.argtypes = [_vp, C.c_int]
+
+
+class _Schedule(C.Structure):
+    _fields_ = [("ef_cap", C.c_uint32), ("cand_cap", C.c_uint32), ("hash_cap", C.c_uint32),
+                ("warps_per_block", C.c_uint32)]
+
+
+_lib.hnsw_gpu_set_schedule.argtypes = [_vp, C.POINTER(_Schedule)]
+_lib.hnsw_gpu_graph_create.argtypes = [_vp, _vp, _sz, _sz, C.POINTER(_Opts), _vp, _vp, _vp, _vp, C.POINTER(_vp)]
+_lib.hnsw_gpu_graph_launch.argtypes = [_vp, _vp]
+_lib.hnsw_gpu_graph_destroy.argtypes = [_vp]
+_lib.hnsw_gpu_graph_destroy.restype = None
 _lib.hnsw_gpu_read_counters.argtypes = [_vp, _vp, _sz]
 _lib.hnsw_gpu_brute_open.argtypes = [_vp, _vp, _sz, _sz, C.c_int, C.c_int, C.POINTER(_vp)]
 _lib.hnsw_gpu_brute_close.argtypes = [_vp]
@@ -379,7 +391,7 @@ class HnswIndex:
                       filter_bits: Optional[np.ndarray] = None, filter_nbits: int = 0,
                       filter_stride: int = 0, filter_used: Optional[np.ndarray] = None,
                       ks: Optional[np.ndarray] = None, efs: Optional[np.ndarray] = None,
-                      mode: int = 0, raise_on_error: bool = True):
+                      mode: int = 0, raise_on_error: bool = True, filter_ids: Optional[np.ndarray] = None):
         """Batched search returning arrays (keys, dist, count, status)."""
         q = np.ascontiguousarray(queries, dtype=np.float32)
         if q.ndim == 1:
@@ -406,6 +418,8 @@ class HnswIndex:
         o.filter_nbits = filter_nbits if fb is not None else 0
         o.filter_stride = filter_stride
         o.filter_used = _ptr(fu)
+        fi = None if filter_ids is None else np.ascontiguousarray(filter_ids, dtype=np.uint32)
+        o.filter_ids = _ptr(fi)
         o.out_stride = stride
         o.mode = mode
         st = _lib.hnsw_gpu_search_batch(self._h, _ptr(q), nq, dim, C.byref(o), _ptr(keys), _ptr(dist),
@@ -455,6 +469,14 @@ class HnswIndex:
         _check(_lib.hnsw_gpu_index_info(self._h, C.byref(info)))
         self._info = info
 
+    def set_schedule(self, ef_cap=None, cand_cap=None, hash_cap=None, warps_per_block=None):
+        """Fixes the traversal scratch geometry; no arguments restores the automatic choice."""
+        if ef_cap is None:
+            _check(_lib.hnsw_gpu_set_schedule(self._h, None))
+            return
+        sc = _Schedule(ef_cap, cand_cap or 2 * ef_cap + 32, hash_cap, warps_per_block)
+        _check(_lib.hnsw_gpu_set_schedule(self._h, C.byref(sc)))
+
     def set_counters(self, enabled: bool):
         _check(_lib.hnsw_gpu_set_counters(self._h, int(enabled)))
 
@@ -462,6 +484,19 @@ class HnswIndex:
         out = np.zeros((nq, 4), dtype=np.uint32)
         _check(_lib.hnsw_gpu_read_counters(self._h, _ptr(out), nq))
         return out
+
+    def graph(self, d_queries: int, nq: int, k: int, ef: int, d_keys: int, d_dist: int, d_count: int,
+              d_status: int, mode: int = 1, quantized: bool = False):
+        """Captures the launch sequence of one device-pointer search (CUDA graph)."""
+        o = _Opts()
+        o.k, o.ef = k, ef
+        o.quantized = int(quantized)
+        o.out_stride = k
+        o.mode = mode
+        g = C.c_void_p()
+        _check(_lib.hnsw_gpu_graph_create(self._h, d_queries, nq, self.dim(), C.byref(o), d_keys, d_dist, d_count,
+                                          d_status, C.byref(g)))
+        return SearchGraph(g)
 
     def search_device(self, d_queries: int, nq: int, k: int, ef: int, d_keys: int, d_dist: int,
                       d_count: int, d_status: int, stream: Optional[int] = None, quantized: bool = False,
@@ -481,7 +516,8 @@ class HnswIndex:
 class _ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
                 ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
-                ("filter_nbits", C.c_uint64), ("quantized", C.c_int32)]
+                ("filter_nbits", C.c_uint64), ("quantized", C.c_int32), ("filter_bank", C.c_void_p),
+                ("filter_count", C.c_uint32)]
 
 
 _lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
@@ -489,11 +525,11 @@ _lib.hnsw_server_config_default.restype = None
 _lib.hnsw_gpu_server_start.argtypes = [_vp, C.POINTER(_ServerConfig), C.POINTER(_vp)]
 _lib.hnsw_gpu_server_stop.argtypes = [_vp]
 _lib.hnsw_gpu_server_stop.restype = None
-_lib.hnsw_gpu_submit.argtypes = [_vp, _vp, C.c_uint32, C.c_uint32, _vp, C.POINTER(C.c_uint64)]
+_lib.hnsw_gpu_submit.argtypes = [_vp, _vp, C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_uint64)]
 _lib.hnsw_gpu_poll.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_int)]
 _lib.hnsw_gpu_wait.argtypes = [_vp, C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_uint32),
                                C.POINTER(C.c_int32), C.POINTER(C.c_double)]
-_lib.hnsw_gpu_server_replay.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+_lib.hnsw_gpu_server_replay.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
 _lib.hnsw_gpu_server_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
 
 
@@ -501,12 +537,17 @@ class Server:
     """Request loop over a resident HnswIndex (continuous batching)."""
 
     def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
-                 max_ef=512, linger_us=100, filter_nbits=0, quantized=False):
+                 max_ef=512, linger_us=100, filter_nbits=0, filter_bank: Optional[np.ndarray] = None,
+                 quantized=False):
         cfg = _ServerConfig()
         _lib.hnsw_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
         cfg.max_k, cfg.max_ef, cfg.linger_us = max_k, max_ef, linger_us
         cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
+        bank = None if filter_bank is None else np.ascontiguousarray(filter_bank, np.uint64)
+        if bank is not None:
+            cfg.filter_bank = _ptr(bank)
+            cfg.filter_count = bank.shape[0]
         h = C.c_void_p()
         _check(_lib.hnsw_gpu_server_start(index._h, C.byref(cfg), C.byref(h)))
         self._h = h
@@ -514,11 +555,10 @@ class Server:
         self.max_k = max_k
         self.words = (filter_nbits + 63) // 64
 
-    def submit(self, query, k: int, ef: int, filter_bits: Optional[np.ndarray] = None) -> int:
+    def submit(self, query, k: int, ef: int, filter_id: int = -1) -> int:
         q = np.ascontiguousarray(query, np.float32)
-        fb = None if filter_bits is None else np.ascontiguousarray(filter_bits, np.uint64)
         t = C.c_uint64()
-        _check(_lib.hnsw_gpu_submit(self._h, _ptr(q), k, ef, _ptr(fb), C.byref(t)))
+        _check(_lib.hnsw_gpu_submit(self._h, _ptr(q), k, ef, filter_id, C.byref(t)))
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 60000):
@@ -530,21 +570,20 @@ class Server:
         c = cnt.value
         return keys[:c], dist[:c], st.value, lat.value
 
-    def replay(self, queries, arrival_us, ks, efs, filtered=None, filter_bits=None):
+    def replay(self, queries, arrival_us, ks, efs, filter_ids=None):
         q = np.ascontiguousarray(queries, np.float32)
         n = q.shape[0]
         arr = np.ascontiguousarray(arrival_us, np.float64)
         ks_a = np.ascontiguousarray(ks, np.uint32)
         efs_a = np.ascontiguousarray(efs, np.uint32)
-        fl = None if filtered is None else np.ascontiguousarray(filtered, np.uint8)
-        fb = None if filter_bits is None else np.ascontiguousarray(filter_bits, np.uint64)
+        fi = None if filter_ids is None else np.ascontiguousarray(filter_ids, np.int32)
         keys = np.zeros((n, self.max_k), np.uint64)
         dist = np.zeros((n, self.max_k), np.float32)
         cnt = np.zeros(n, np.uint32)
         st = np.zeros(n, np.int32)
         lat = np.zeros(n, np.float64)
-        _check(_lib.hnsw_gpu_server_replay(self._h, _ptr(q), n, _ptr(arr), _ptr(ks_a), _ptr(efs_a), _ptr(fl),
-                                           _ptr(fb), _ptr(keys), _ptr(dist), _ptr(cnt), _ptr(st), _ptr(lat)))
+        _check(_lib.hnsw_gpu_server_replay(self._h, _ptr(q), n, _ptr(arr), _ptr(ks_a), _ptr(efs_a), _ptr(fi),
+                                           _ptr(keys), _ptr(dist), _ptr(cnt), _ptr(st), _ptr(lat)))
         return keys, dist, cnt, st, lat
 
     def stats(self):
@@ -560,6 +599,28 @@ class Server:
     def __del__(self):
         try:
             self.stop()
+        except Exception:
+            pass
+
+
+class SearchGraph:
+    """A captured search launch sequence (hnsw_gpu_graph_*)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def launch(self, stream: Optional[int] = None):
+        handle = None if stream is None else (stream if stream != 0 else 1)
+        _check(_lib.hnsw_gpu_graph_launch(self._h, handle))
+
+    def close(self):
+        if self._h:
+            _lib.hnsw_gpu_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -112,6 +112,8 @@ typedef struct hnsw_search_opts {
     const uint8_t* filter_used; /* optional per-query flag: 0 = no filter for that query */
     uint32_t out_stride;        /* entries per query row of the outputs; 0 = max k */
     int32_t mode;               /* HNSW_MODE_* */
+    const uint32_t* filter_ids; /* optional: query i uses bitmap filter_ids[i] (stride filter_stride)
+                                   instead of bitmap i, so many queries can share a few filters */
 } hnsw_search_opts;
 
 enum {
@@ -139,6 +141,30 @@ int hnsw_gpu_search_batch_device(hnsw_gpu_index* index, const float* d_queries, 
                                  const hnsw_search_opts* d_opts, uint64_t* d_keys, float* d_dist,
                                  uint32_t* d_count, int32_t* d_status, void* stream);
 
+/* A captured launch sequence (CUDA graph) of one device-pointer search:
+ * the batch shape, options and buffers are fixed at capture; the caller
+ * rewrites the query buffer in place and relaunches. For small batches this
+ * replaces the memset and two kernel launches with one graph launch. */
+typedef struct hnsw_gpu_graph hnsw_gpu_graph;
+int hnsw_gpu_graph_create(hnsw_gpu_index* index, const float* d_queries, size_t nq, size_t dim,
+                          const hnsw_search_opts* d_opts, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
+                          int32_t* d_status, hnsw_gpu_graph** out);
+int hnsw_gpu_graph_launch(hnsw_gpu_graph* graph, void* stream);
+void hnsw_gpu_graph_destroy(hnsw_gpu_graph* graph);
+
+/* Scratch geometry of the traversal kernel ("schedule"). By default the
+ * library picks it per call from the batch's largest ef and the index's
+ * dimension (results capacity, candidate capacity, visited-hash size, warps
+ * per block chosen for the most resident warps). A fixed schedule overrides
+ * that; NULL restores the automatic choice. Results do not depend on it. */
+typedef struct hnsw_schedule {
+    uint32_t ef_cap;          /* >= every max(ef, k) of a batch; multiple of 32, <= 1024 */
+    uint32_t cand_cap;        /* candidate array entries */
+    uint32_t hash_cap;        /* visited-hash entries, power of two */
+    uint32_t warps_per_block; /* 1..8 */
+} hnsw_schedule;
+int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
+
 /* Per-query traversal counters of the last search on this thread's slot
  * (device pointer, nq x 4 u32: layer-0 distances, layer-0 expansions,
  * upper-layer distances, upper-layer list reads). Enabled by
@@ -164,18 +190,22 @@ typedef struct hnsw_server_config {
     uint32_t max_pending;   /* queued requests before submit is rejected */
     uint32_t max_k, max_ef; /* admission bounds (scratch sizing) */
     uint32_t linger_us;     /* how long a partial batch waits while others run */
-    uint64_t filter_nbits;  /* key-bitmap width of filtered requests; 0 = none */
+    uint64_t filter_nbits;  /* key-bitmap width of the filter bank; 0 = no filters */
     int32_t quantized;      /* int8 traversal + exact re-rank */
+    const uint64_t* filter_bank; /* host: filter_count bitmaps of ceil(filter_nbits / 64) words,
+                                    copied to the device at start */
+    uint32_t filter_count;
 } hnsw_server_config;
 
 void hnsw_server_config_default(hnsw_server_config* cfg);
 int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg, hnsw_gpu_server** out);
 /* Finishes queued and in-flight requests, then frees the server. */
 void hnsw_gpu_server_stop(hnsw_gpu_server* server);
-/* Non-blocking: copies the query (and filter bitmap, filter_nbits bits) and
- * returns a ticket, or HNSW_ERR_ADMISSION_REJECTED when the queue is full. */
-int hnsw_gpu_submit(hnsw_gpu_server* server, const float* query, uint32_t k, uint32_t ef,
-                    const uint64_t* filter_bits, uint64_t* ticket);
+/* Non-blocking: copies the query and returns a ticket, or
+ * HNSW_ERR_ADMISSION_REJECTED when the queue is full. filter_id selects a
+ * bitmap of the server's filter bank (-1 = no filter). */
+int hnsw_gpu_submit(hnsw_gpu_server* server, const float* query, uint32_t k, uint32_t ef, int32_t filter_id,
+                    uint64_t* ticket);
 int hnsw_gpu_poll(hnsw_gpu_server* server, uint64_t ticket, int* done);
 /* Waits up to timeout_ms; copies the results (keys/dist: k entries) and the
  * request's latency (arrival to completion, microseconds), and frees the
@@ -185,12 +215,11 @@ int hnsw_gpu_wait(hnsw_gpu_server* server, uint64_t ticket, uint32_t timeout_ms,
 /* Open-loop load: request i is submitted at arrival_us[i] microseconds after
  * the call starts (ascending); outputs as hnsw_gpu_wait, per request, with
  * stride max_k for keys/dist (NULL to skip). Rejected requests get status
- * HNSW_ERR_ADMISSION_REJECTED and latency -1. filter_bits holds one bitmap
- * per request (stride ceil(filter_nbits / 64) words), used where filtered[i]. */
+ * HNSW_ERR_ADMISSION_REJECTED and latency -1. filter_ids (NULL = none) gives
+ * each request's filter-bank entry or -1. */
 int hnsw_gpu_server_replay(hnsw_gpu_server* server, const float* queries, size_t n, const double* arrival_us,
-                           const uint32_t* ks, const uint32_t* efs, const uint8_t* filtered,
-                           const uint64_t* filter_bits, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
-                           int32_t* out_status, double* out_latency_us);
+                           const uint32_t* ks, const uint32_t* efs, const int32_t* filter_ids, uint64_t* out_keys,
+                           float* out_dist, uint32_t* out_count, int32_t* out_status, double* out_latency_us);
 /* Launched batches and queries since start. */
 int hnsw_gpu_server_stats(const hnsw_gpu_server* server, uint64_t* batches, uint64_t* queries);
 

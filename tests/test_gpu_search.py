@@ -334,3 +334,54 @@ def test_modes_on_quantized_filtered_tombstoned_mixture(mode):
     ref = oi.search(queries, 100, 16, quantized=True, filter_bits=bits, filter_nbits=6000,
                     filter_stride=words, ks=ks, efs=efs)
     assert_same(got, ref, f"config-4-like mode={mode}")
+
+
+def test_shared_filter_bitmaps_by_id():
+    base, queries = H.gaussian(3000, 64, 16, 12)
+    data = build_index(base, metric=0, m=12, seed=2)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    rng = np.random.default_rng(9)
+    words = (3000 + 63) // 64
+    bank = np.zeros((5, words), np.uint64)
+    for j in range(5):
+        bank[j] = H.key_bitmap(np.nonzero(rng.random(3000) < 0.1 * (j + 1))[0].astype(np.uint64), 3000)
+    ids = rng.integers(0, 5, 64).astype(np.uint32)
+    got = gi.search_arrays(queries, 10, 48, filter_bits=bank, filter_nbits=3000, filter_stride=words, filter_ids=ids)
+    ref = oi.search(queries, 10, 48, filter_bits=bank[ids], filter_nbits=3000, filter_stride=words)
+    assert_same(got, ref, "filter ids")
+
+
+def test_fixed_schedule_gives_identical_results(gaussian_10k):
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    want = gi.search_arrays(queries[:200], 10, 64, mode=1)
+    for ef_cap, hash_cap, wpb in [(512, 32768, 1), (64, 1024, 4), (128, 4096, 2)]:
+        gi.set_schedule(ef_cap=ef_cap, hash_cap=hash_cap, warps_per_block=wpb)
+        for mode in (0, 1):
+            assert_same(gi.search_arrays(queries[:200], 10, 64, mode=mode), want, f"schedule {ef_cap}/{hash_cap}")
+    gi.set_schedule()
+
+
+def test_cuda_graph_replays_the_search(gaussian_10k):
+    import torch
+
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    want = gi.search_arrays(queries[:256], 10, 64)
+    dev = torch.device("cuda", 0)
+    q = torch.zeros((256, 128), dtype=torch.float32, device=dev)
+    keys = torch.zeros((256, 10), dtype=torch.int64, device=dev)
+    dist = torch.zeros((256, 10), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(256, dtype=torch.int32, device=dev)
+    st = torch.zeros(256, dtype=torch.int32, device=dev)
+    g = gi.graph(q.data_ptr(), 256, 10, 64, keys.data_ptr(), dist.data_ptr(), cnt.data_ptr(), st.data_ptr())
+    for _ in range(2):
+        q.copy_(torch.from_numpy(queries[:256]))
+        torch.cuda.synchronize()
+        g.launch()
+        torch.cuda.synchronize()
+        got = (keys.cpu().numpy().view(np.uint64), dist.cpu().numpy(), cnt.cpu().numpy().view(np.uint32),
+               st.cpu().numpy())
+        assert_same(got, want, "graph")
+    g.close()

@@ -23,33 +23,40 @@ def served():
     return base, queries, data
 
 
-def make_requests(queries, nbits, seed):
+def make_requests(queries, nbits, seed, bank_size=8):
+    """Per request k in {10, 100}, ef log-uniform in [32, 512], 30% filtered by
+    one of `bank_size` key bitmaps of selectivity 5%-50%."""
     rng = np.random.default_rng(seed)
     n = len(queries)
     ks = rng.choice([10, 100], n).astype(np.uint32)
     efs = np.exp(rng.uniform(np.log(32), np.log(512), n)).astype(np.uint32)
-    filtered = (rng.random(n) < 0.3).astype(np.uint8)
     words = (nbits + 63) // 64
-    bits = np.zeros((n, words), np.uint64)
-    for i in range(n):
-        if filtered[i]:
-            sel = rng.random(nbits) < rng.uniform(0.05, 0.5)
-            bits[i] = H.key_bitmap(np.nonzero(sel)[0].astype(np.uint64), nbits)
-    return ks, efs, filtered, bits
+    bank = np.zeros((bank_size, words), np.uint64)
+    for j in range(bank_size):
+        sel = rng.random(nbits) < rng.uniform(0.05, 0.5)
+        bank[j] = H.key_bitmap(np.nonzero(sel)[0].astype(np.uint64), nbits)
+    fids = np.where(rng.random(n) < 0.3, rng.integers(0, bank_size, n), -1).astype(np.int32)
+    return ks, efs, fids, bank
 
 
-def alone(gi, oi, queries, ks, efs, filtered, bits, nbits):
-    """Each request searched alone (one query per call) on the GPU, and the oracle."""
+def oracle_results(oi, queries, ks, efs, fids, bank, nbits):
+    words = bank.shape[1]
+    bits = np.zeros((len(queries), words), np.uint64)
+    bits[fids >= 0] = bank[fids[fids >= 0]]
+    used = (fids >= 0).astype(np.uint8)
+    return oi.search(queries, 100, 16, ks=ks.astype(np.uint64), efs=efs.astype(np.uint64), filter_bits=bits,
+                     filter_nbits=nbits, filter_stride=words, filter_used=used)
+
+
+def alone(gi, queries, ks, efs, fids, bank, nbits):
+    """Each request searched alone (one query per call) on the GPU."""
     out = []
     for i in range(len(queries)):
-        fb = bits[i] if filtered[i] else None
+        fb = bank[fids[i]] if fids[i] >= 0 else None
         g = gi.search_arrays(queries[i:i + 1], int(ks[i]), int(efs[i]), filter_bits=fb,
                              filter_nbits=nbits if fb is not None else 0)
         out.append(g)
-    words = bits.shape[1]
-    ref = oi.search(queries, 100, 16, ks=ks.astype(np.uint64), efs=efs.astype(np.uint64), filter_bits=bits,
-                    filter_nbits=nbits, filter_stride=words, filter_used=filtered)
-    return out, ref
+    return out
 
 
 def test_submitted_requests_equal_alone_results(served):
@@ -58,14 +65,15 @@ def test_submitted_requests_equal_alone_results(served):
     oi = O.Index(data)
     nbits = 20000
     q = queries[:200]
-    ks, efs, filtered, bits = make_requests(q, nbits, 1)
-    srv = H.Server(gi, max_batch=64, max_inflight=3, filter_nbits=nbits)
-    tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), bits[i] if filtered[i] else None) for i in range(len(q))]
+    ks, efs, fids, bank = make_requests(q, nbits, 1)
+    srv = H.Server(gi, max_batch=64, max_inflight=3, filter_nbits=nbits, filter_bank=bank)
+    tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), int(fids[i])) for i in range(len(q))]
     results = [srv.wait(t) for t in tickets]
     batches, launched = srv.stats()
     srv.stop()
     assert launched == len(q) and batches >= 2
-    one, ref = alone(gi, oi, q, ks, efs, filtered, bits, nbits)
+    one = alone(gi, q, ks, efs, fids, bank, nbits)
+    ref = oracle_results(oi, q, ks, efs, fids, bank, nbits)
     for i, (keys, dist, status, lat) in enumerate(results):
         assert status == 0
         c = int(ref[2][i])
@@ -80,18 +88,16 @@ def test_open_loop_replay_mixes_requests_and_matches(served):
     gi = H.HnswIndex.from_bytes(data)
     oi = O.Index(data)
     nbits = 20000
-    ks, efs, filtered, bits = make_requests(queries, nbits, 2)
+    ks, efs, fids, bank = make_requests(queries, nbits, 2)
     rng = np.random.default_rng(3)
     arrivals = np.cumsum(rng.exponential(1e6 / 200000.0, len(queries)))  # 200k requests/s
-    srv = H.Server(gi, max_batch=128, max_inflight=4, filter_nbits=nbits, linger_us=50)
-    keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, filtered, bits)
+    srv = H.Server(gi, max_batch=128, max_inflight=4, filter_nbits=nbits, filter_bank=bank, linger_us=50)
+    keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, fids)
     batches, launched = srv.stats()
     srv.stop()
     assert (st == 0).all()
     assert batches > 1
-    words = bits.shape[1]
-    ref = oi.search(queries, 100, 16, ks=ks.astype(np.uint64), efs=efs.astype(np.uint64), filter_bits=bits,
-                    filter_nbits=nbits, filter_stride=words, filter_used=filtered)
+    ref = oracle_results(oi, queries, ks, efs, fids, bank, nbits)
     for i in range(len(queries)):
         c = int(ref[2][i])
         assert cnt[i] == c
