@@ -509,6 +509,228 @@ def run_brute(args):
     return 0
 
 
+def cached_index(tag, build):
+    """Builds an index file once per box and caches it under CACHE."""
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"index-{hashlib.sha1(tag.encode()).hexdigest()[:12]}.hnsw")
+    build_s = None
+    if not os.path.exists(path):
+        t = time.time()
+        data = build()
+        build_s = time.time() - t
+        tmp = path + f".tmp{os.getpid()}"
+        with open(tmp, "wb") as f:
+            f.write(data)
+        os.replace(tmp, path)
+        log(f"built {tag} in {build_s:.1f} s ({len(data) / 1e9:.2f} GB)")
+    with open(path, "rb") as f:
+        return f.read(), build_s
+
+
+def random_bitmaps(rng, nb, selectivities):
+    """One key bitmap (uint64 words) per selectivity, each key kept with that probability."""
+    words = (nb + 63) // 64
+    bank = np.zeros((len(selectivities), words), np.uint64)
+    for j, p in enumerate(selectivities):
+        packed = np.packbits(rng.random(nb) < p, bitorder="little")
+        row = np.zeros(words * 8, np.uint8)
+        row[:packed.size] = packed
+        bank[j] = row.view(np.uint64)
+    return bank
+
+
+def timed_search(index, queries, k, ef, steps, **kw):
+    index.search_arrays(queries, k, ef, **kw)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        res = index.search_arrays(queries, k, ef, **kw)
+        times.append(time.perf_counter() - t)
+    return len(queries) / statistics.median(times), res
+
+
+# ---------------------------------------------------------------------------
+# Batching workload (config 4): 5M x 96 inner product, int8 traversal +
+# exact re-rank, 5% tombstones, per-query filters, uneven k and ef.
+# ---------------------------------------------------------------------------
+def run_batch(args):
+    import hnsw_gpu as H
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nb, nq, dim = args.batch_n, args.batch_nq, 96
+    t = time.time()
+    base, queries = H.mixture_split(nb, nq, dim, 2000, 0.4, 5, 6)
+    log(f"data in {time.time() - t:.1f} s")
+    rng = np.random.default_rng(7)
+    dead = np.sort(rng.choice(nb, nb // 20, replace=False)).astype(np.uint64)
+
+    def build():
+        b = H.IndexBuilder(dim, H.Metric.InnerProduct, H.HnswParams(m=24, ef_construction=200, seed=0))
+        b.insert_batch(np.arange(nb, dtype=np.uint64), base)
+        for key in dead.tolist():
+            b.remove(int(key))
+        b.enable_quantization()
+        return b.to_bytes()
+
+    data, build_s = cached_index(f"batch-{nb}-{dim}-5-6-m24-dead7-q", build)
+    index = H.HnswIndex.from_bytes(data)
+    rq = np.random.default_rng(8)
+    ks = rq.choice([1, 10, 100], nq).astype(np.uint32)
+    efs = rq.choice([16, 32, 64, 128, 256, 512], nq).astype(np.uint32)
+    nbank, words = 256, (nb + 63) // 64
+    bank = random_bitmaps(rq, nb, np.exp(rq.uniform(np.log(0.01), np.log(0.9), nbank)))
+    fids = rq.integers(0, nbank, nq).astype(np.uint32)
+    common = dict(quantized=True, ks=ks, efs=efs, filter_bits=bank, filter_nbits=nb, filter_stride=words,
+                  filter_ids=fids)
+    out = {}
+    out["persistent_heuristic_qps"], res = timed_search(index, queries, 100, 16, args.steps, mode=1, **common)
+    out["plain_heuristic_qps"], _ = timed_search(index, queries, 100, 16, args.steps, mode=0, **common)
+    # Autotune on a sample of the same request mix, then time the tuned schedule.
+    ns = min(nq, 8000)
+    t = time.time()
+    best, trials = index.autotune(queries[:ns], 100, 16, reps=2, quantized=True, ks=ks[:ns], efs=efs[:ns],
+                                  filter_bits=bank, filter_nbits=nb, filter_stride=words, filter_ids=fids[:ns])
+    out["autotune_s"] = time.time() - t
+    out["autotune_best"] = best
+    out["autotune_trials"] = len(trials)
+    qps, tuned_res = timed_search(index, queries, 100, 16, args.steps, mode=2, **common)
+    out["autotuned_qps"] = qps
+    out["tuned_equals_heuristic"] = bool(np.array_equal(tuned_res[0], res[0]) and np.array_equal(tuned_res[2], res[2]))
+    index.set_schedule(ef_cap=512, hash_cap=32768, warps_per_block=1)
+    out["fixed_schedule_qps"], fixed_res = timed_search(index, queries, 100, 16, args.steps, mode=1, **common)
+    index.set_schedule()
+    out["fixed_equals_heuristic"] = bool(np.array_equal(fixed_res[0], res[0]))
+    # One query per call (the reference's search_with called per query).
+    npc = 500
+    t = time.perf_counter()
+    for i in range(npc):
+        index.search_arrays(queries[i:i + 1], int(ks[i]), int(efs[i]), quantized=True, filter_bits=bank[fids[i]],
+                            filter_nbits=nb)
+    out["per_call_qps"] = npc / (time.perf_counter() - t)
+    # Recall@10 on a sample against exact filtered search (float64 scores).
+    samp = 100
+    alive = np.ones(nb, bool)
+    alive[dead.astype(np.int64)] = False
+    hits = tot = 0
+    for i in range(samp):
+        allowed = np.unpackbits(bank[fids[i]].view(np.uint8), bitorder="little")[:nb].astype(bool)
+        mask = allowed & alive
+        idx = np.nonzero(mask)[0]
+        sc = base[idx].astype(np.float64) @ queries[i].astype(np.float64)
+        kk = min(10, int(ks[i]), idx.size)
+        truth = idx[np.argsort(-sc, kind="stable")[:kk]]
+        got = res[0][i, :min(kk, int(res[2][i]))]
+        hits += np.isin(got, truth.astype(np.uint64)).sum()
+        tot += kk
+    out["recall_at_10_sample"] = hits / max(tot, 1)
+    # CPU baseline: the oracle with quantized traversal and the same filters.
+    oi = O.Index(data)
+    cs = 1000
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    ok_, od_, oc_, os_ = oi.search(queries[:cs], 100, 16, quantized=True, ks=ks[:cs].astype(np.uint64),
+                                   efs=efs[:cs].astype(np.uint64), filter_bits=bank[fids[:cs]], filter_nbits=nb,
+                                   filter_stride=words, threads=cores)
+    cpu_qps = cs / (time.perf_counter() - t)
+    same = 0
+    for i in range(cs):
+        c = int(oc_[i])
+        same += int(c == int(res[2][i]) and np.array_equal(ok_[i, :c], res[0][i, :c])
+                    and np.array_equal(od_[i, :c].view(np.uint32), res[1][i, :c].view(np.uint32)))
+    out["identical_to_oracle"] = f"{same}/{cs}"
+    line = {
+        "metric": "QPS, batched persistent search (5M x 96 IP, int8 + re-rank, filters, tombstones, uneven k/ef)",
+        "value": out["autotuned_qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "higher_is_better": True, "dtype": "int8+f32", "data": "synthetic",
+        "config": {"workload": "batch-5Mx96-ip", "n_base": nb, "n_queries": nq, "tombstoned": int(dead.size),
+                   "filters": nbank, "index_build_s": build_s, **out},
+        "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"{cs} queries, oracle search_with(quantized, filter)"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Serving workload (config 5): 10M x 128 L2, open-loop Poisson arrivals.
+# ---------------------------------------------------------------------------
+def run_serve(args):
+    import hnsw_gpu as H
+
+    nb, dim, pool = args.serve_n, 128, 200_000
+    t = time.time()
+    base, queries = H.mixture_split(nb, pool, dim, 10000, 0.3, 9, 10)
+    log(f"data in {time.time() - t:.1f} s")
+
+    def build():
+        b = H.IndexBuilder(dim, H.Metric.L2, H.HnswParams(m=16, ef_construction=200, seed=0))
+        b.insert_batch(np.arange(nb, dtype=np.uint64), base)
+        b.enable_quantization()
+        return b.to_bytes()
+
+    data, build_s = cached_index(f"serve-{nb}-{dim}-9-10-m16-q", build)
+    del base
+    index = H.HnswIndex.from_bytes(data)
+    del data
+    rq = np.random.default_rng(11)
+    ks = rq.choice([10, 100], pool).astype(np.uint32)
+    efs = np.exp(rq.uniform(np.log(32), np.log(512), pool)).astype(np.uint32)
+    nbank, words = 64, (nb + 63) // 64
+    bank = random_bitmaps(rq, nb, rq.uniform(0.05, 0.5, nbank))
+    fids = np.where(rq.random(pool) < 0.3, rq.integers(0, nbank, pool), -1).astype(np.int32)
+    # The plain batched GPU path on the same requests (reference results).
+    used = (fids >= 0).astype(np.uint8)
+    ids = np.where(fids >= 0, fids, 0).astype(np.uint32)
+    t = time.perf_counter()
+    ref = index.search_arrays(queries, 100, 16, ks=ks, efs=efs, filter_bits=bank, filter_nbits=nb,
+                              filter_stride=words, filter_used=used, filter_ids=ids, mode=1, quantized=True)
+    batched_qps = pool / (time.perf_counter() - t)
+    # Tune the schedule for the request mix (batches of max_batch requests).
+    nt = min(pool, args.serve_batch)
+    tuned, _ = index.autotune(queries[:nt], 100, 16, reps=3, ks=ks[:nt], efs=efs[:nt], filter_bits=bank,
+                              filter_nbits=nb, filter_stride=words, filter_used=used[:nt], filter_ids=ids[:nt],
+                              quantized=True)
+    log(f"tuned: {tuned}")
+    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=4, max_pending=1 << 17, max_k=100, max_ef=512,
+                   linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
+    sweep = []
+    for rate in (10_000, 30_000, 100_000, 300_000, 1_000_000):
+        n = int(min(pool, max(5000, rate * 1.0)))
+        arr = np.cumsum(rq.exponential(1e6 / rate, n))
+        t = time.perf_counter()
+        keys, dist, cnt, st, lat = srv.replay(queries[:n], arr, ks[:n], efs[:n], fids[:n])
+        wall = time.perf_counter() - t
+        ok = st == 0
+        lat_ok = lat[ok]
+        same = 0
+        for i in np.nonzero(ok)[0]:
+            c = int(cnt[i])
+            same += int(c == int(ref[2][i]) and np.array_equal(keys[i, :c], ref[0][i, :c]))
+        sweep.append({"offered_qps": rate, "requests": n, "completed": int(ok.sum()),
+                      "rejected": int((st == H.Status.ADMISSION_REJECTED).sum()),
+                      "achieved_qps": float(ok.sum() / wall), "p50_ms": float(np.percentile(lat_ok, 50) / 1e3),
+                      "p99_ms": float(np.percentile(lat_ok, 99) / 1e3),
+                      "identical_to_batched": same / max(int(ok.sum()), 1)})
+        log(sweep[-1])
+    batches, launched = srv.stats()
+    srv.stop()
+    best = max((s_ for s_ in sweep if s_["p99_ms"] <= 2.0), key=lambda s_: s_["achieved_qps"], default=None)
+    line = {
+        "metric": "served QPS with p99 <= 2 ms (10M x 128 L2, open-loop Poisson)",
+        "value": best["achieved_qps"] if best else 0.0, "unit": "queries/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s,
+                   "batched_qps_same_requests": batched_qps, "max_batch": args.serve_batch,
+                   "linger_us": args.serve_linger, "launched_batches": batches, "launched_queries": launched,
+                   "tuned_schedule": tuned,
+                   "sweep": sweep},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -516,12 +738,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="plain-1Mx128", choices=["plain-1Mx128", "brute-1Mx768"])
+    ap.add_argument("--workload", default="plain-1Mx128",
+                    choices=["plain-1Mx128", "brute-1Mx768", "batch-5Mx96", "serve-10Mx128"])
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
+    ap.add_argument("--batch-n", type=int, default=5_000_000)
+    ap.add_argument("--batch-nq", type=int, default=50_000)
+    ap.add_argument("--serve-n", type=int, default=10_000_000)
+    ap.add_argument("--serve-batch", type=int, default=1024)
+    ap.add_argument("--serve-linger", type=int, default=100)
     args = ap.parse_args()
     if args.workload == "brute-1Mx768":
         return run_brute(args)
+    if args.workload == "batch-5Mx96":
+        return run_batch(args)
+    if args.workload == "serve-10Mx128":
+        return run_serve(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

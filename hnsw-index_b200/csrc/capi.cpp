@@ -111,7 +111,7 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
 // Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
 static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
     const uint32_t warps = uint32_t(gi->num_sms) * 4;
-    const uint32_t cand_cap = std::max<uint32_t>(1u << 14, 4 * ef_cap);
+    const uint32_t cand_cap = std::max<uint32_t>(4096, 2 * ef_cap + 32);
     const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
     CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
     CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
@@ -125,16 +125,36 @@ static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
 
 // Enqueues one search on `stream` with device pointers. ef_max bounds every
 // per-query max(ef, k) of the batch.
-int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
+// The schedule comes from, in order: `force` (the autotuner's trials), the
+// fixed schedule, the tuning table, the occupancy heuristic. HNSW_MODE_AUTO
+// resolves to the tuned mode of the bucket, else persistent.
+int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o_in,
                           const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
                           const uint32_t* d_fids,
                           uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
-                          uint32_t out_stride, cudaStream_t stream) {
-    SearchGeometry geo = gi->fixed.ef_cap ? gi->fixed
-                                          : pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
-    CU(s->work.ensure(16), "cudaMalloc work counters");
+                          uint32_t out_stride, cudaStream_t stream, const SearchGeometry* force) {
+    hnsw_search_opts o = o_in;
+    if (o.mode != HNSW_MODE_PLAIN && o.mode != HNSW_MODE_PERSISTENT && o.mode != HNSW_MODE_AUTO)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown search mode");
+    SearchGeometry geo{0, 0, 0, 0, 0};
+    if (force) {
+        geo = *force;
+    } else if (gi->fixed.ef_cap) {
+        geo = gi->fixed;
+    } else {
+        std::lock_guard<std::mutex> l(gi->tune_mu);
+        const hnsw_gpu_index::Tuned& t = gi->tuned[tune_bucket(ef_max)];
+        if (o.mode == HNSW_MODE_AUTO) o.mode = t.mode >= 0 ? t.mode : HNSW_MODE_PERSISTENT;
+        if (t.geo[o.mode].ef_cap) geo = t.geo[o.mode];
+    }
+    if (o.mode == HNSW_MODE_AUTO) o.mode = HNSW_MODE_PERSISTENT;
+    if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
+    // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
+    // out by the fast and retry kernels, [4] last-resort count.
+    CU(s->work.ensure(32), "cudaMalloc work counters");
     CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
-    CU(cudaMemsetAsync(s->work.p, 0, 16, stream), "memset work counters");
+    CU(s->overflow2.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
+    CU(cudaMemsetAsync(s->work.p, 0, 32, stream), "memset work counters");
     int r = ensure_retry(gi, s, std::max(geo.ef_cap, round_up(ef_max, 32)));
     if (r != HNSW_OK) return r;
     SearchArgs a;
@@ -151,6 +171,7 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.filter_stride = o.filter_stride;
     a.filter_used = d_fused;
     a.filter_ids = d_fids;
+    a.filter_by_node = o.filter_by_node;
     a.out_keys = d_keys;
     a.out_dist = d_dist;
     a.out_count = d_count;
@@ -168,18 +189,33 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
         uint32_t warps = 0;
         CU(persistent_warps(geo, gi->view.dp, gi->view.dc, gi->num_sms, &warps), "occupancy");
         const uint32_t words = ((gi->view.n + 31) / 32 + 3) & ~3u;
-        const uint32_t cand_cap = std::max<uint32_t>(8192, 4 * geo.ef_cap);
         const size_t bits_bytes = size_t(warps) * words * 4;
         if (bits_bytes > s->spill_bits.bytes) {
             CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
             CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
         }
-        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
         a.spill_bits = s->spill_bits.as<uint32_t>();
         a.spill_words = words;
-        a.spill_cands = s->spill_cands.as<uint64_t>();
-        a.spill_cand_cap = cand_cap;
         a.spill_slots = warps;
+    }
+    // Cold candidate lists: a pool of 8 entries per node or 8 chunks per
+    // warp, whichever is more (1 GiB at most), shared by the persistent warps,
+    // then reused whole by the retry warps; a list never holds more entries
+    // than there are nodes.
+    const uint32_t tab_cap = (gi->view.n + kColdChunk - 1) / kColdChunk + 2;
+    {
+        const uint32_t slots = std::max(a.spill_slots, s->g_warps);
+        const uint64_t want = std::max<uint64_t>((uint64_t(gi->view.n) * 8 + kColdChunk - 1) / kColdChunk,
+                                                 uint64_t(slots) * 8);
+        const uint32_t chunks = geo.cold_chunks ? geo.cold_chunks : uint32_t(std::min<uint64_t>(want, 1u << 17));
+        CU(s->cold_pool.ensure(size_t(chunks) * kColdChunk * 8), "cudaMalloc cold candidate pool");
+        CU(s->cold_tab.ensure(size_t(slots) * tab_cap * 4), "cudaMalloc cold chunk tables");
+        a.cold_pool = s->cold_pool.as<uint64_t>();
+        a.cold_chunks = chunks;
+        a.cold_next = s->work.as<uint32_t>() + 2;
+        a.cold_tab = s->cold_tab.as<uint32_t>();
+        a.cold_tab_cap = tab_cap;
+        a.cold_slots = slots;
     }
     a.g_results = s->g_results.as<uint64_t>();
     a.g_cands = s->g_cands.as<uint64_t>();
@@ -187,8 +223,32 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.g_ef_cap = s->g_ef_cap;
     a.g_cand_cap = s->g_cand_cap;
     a.g_visited_words = s->g_words;
+    // Last-resort regions: kLastResortWarps rows of tab_cap chunks each,
+    // chunk table rows preassigned once.
+    if (s->last_tab.bytes < size_t(kLastResortWarps) * tab_cap * 4) {
+        CU(s->last_pool.ensure(size_t(kLastResortWarps) * tab_cap * kColdChunk * 8), "cudaMalloc last-resort pool");
+        CU(s->last_tab.ensure(size_t(kLastResortWarps) * tab_cap * 4), "cudaMalloc last-resort table");
+        std::vector<uint32_t> ids(size_t(kLastResortWarps) * tab_cap);
+        for (size_t i = 0; i < ids.size(); ++i) ids[i] = uint32_t(i);
+        CU(cudaMemcpy(s->last_tab.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice), "copy last-resort table");
+    }
+    a.overflow_list2 = s->overflow2.as<uint32_t>();
+    a.overflow_count2 = s->work.as<uint32_t>() + 4;
     CU(launch_search(a, geo, gi->num_sms, stream), "search kernel");
     CU(launch_search_retry(a, s->g_warps, stream), "search retry kernel");
+    SearchArgs last = a;
+    last.overflow_list = a.overflow_list2;
+    last.overflow_count = a.overflow_count2;
+    last.overflow_list2 = nullptr;
+    last.overflow_count2 = nullptr;
+    last.cold_pool = s->last_pool.as<uint64_t>();
+    last.cold_chunks = kLastResortWarps * tab_cap;
+    last.cold_next = nullptr;
+    last.cold_tab = s->last_tab.as<uint32_t>();
+    last.cold_tab_cap = tab_cap;
+    last.cold_slots = kLastResortWarps;
+    last.cold_private = 1;
+    CU(launch_search_retry(last, kLastResortWarps, stream), "search last-resort kernel");
     return HNSW_OK;
 }
 
@@ -399,6 +459,7 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     g.cand_cap = sc->cand_cap;
     g.hash_cap = sc->hash_cap;
     g.warps_per_block = sc->warps_per_block;
+    g.cold_chunks = sc->cold_chunks;
     if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
     index->fixed = g;
@@ -420,19 +481,14 @@ int hnsw_gpu_read_counters(hnsw_gpu_index* index, uint32_t* host_out, size_t nq)
 }
 
 
-int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim,
-                          const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
-                          int32_t* out_status) {
-    if (!gi || !opts) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+// Validates a host-buffer batch: the bound on max(ef, k) and the row stride.
+static int check_batch(hnsw_gpu_index* gi, size_t nq, size_t dim, const hnsw_search_opts& o, uint32_t* ef_bound,
+                       uint32_t* stride) {
     if (dim != gi->view.dim) {
         return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch: expected " + std::to_string(gi->view.dim) +
                                                           ", got " + std::to_string(dim));
     }
-    if (nq == 0) return HNSW_OK;
-    if (!queries || !out_keys || !out_dist || !out_count || !out_status)
-        return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
     if (nq > 0x7FFFFFFFu) return set_error(HNSW_ERR_INVALID_ARGUMENT, "batch too large");
-    const hnsw_search_opts& o = *opts;
     uint32_t kmax = o.k, efmax = o.ef;
     if (o.ks)
         for (size_t i = 0; i < nq; ++i) kmax = std::max(kmax, o.ks[i]);
@@ -440,16 +496,27 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
         kmax = o.k;
     if (o.efs)
         for (size_t i = 0; i < nq; ++i) efmax = std::max(efmax, o.efs[i]);
-    uint32_t ef_bound = std::max(kmax, efmax);
-    if (ef_bound > 65536) return set_error(HNSW_ERR_INVALID_ARGUMENT, "ef and k above 65536 are not supported on the device");
-    const uint32_t stride = o.out_stride ? o.out_stride : std::max<uint32_t>(kmax, 1);
-    if (stride < kmax) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out_stride below k");
+    *ef_bound = std::max(kmax, efmax);
+    if (*ef_bound > 65536) return set_error(HNSW_ERR_INVALID_ARGUMENT, "ef and k above 65536 are not supported on the device");
+    *stride = o.out_stride ? o.out_stride : std::max<uint32_t>(kmax, 1);
+    if (*stride < kmax) return set_error(HNSW_ERR_INVALID_ARGUMENT, "out_stride below k");
     if (o.filter_bits && o.filter_nbits == 0) return set_error(HNSW_ERR_INVALID_ARGUMENT, "filter bitmap has no bits");
-    DeviceGuard dg(gi->device);
-    Slot* s = nullptr;
-    int r = gi->slots.acquire(&s);
-    if (r != HNSW_OK) return r;
-    std::unique_ptr<Slot, std::function<void(Slot*)>> hold(s, [gi](Slot* p) { gi->slots.release(p); });
+    if (o.mode != HNSW_MODE_PLAIN && o.mode != HNSW_MODE_PERSISTENT && o.mode != HNSW_MODE_AUTO)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown search mode");
+    return HNSW_OK;
+}
+
+// Device copies of a host batch's inputs, staged on the slot's stream.
+struct StagedBatch {
+    const uint32_t* ks = nullptr;
+    const uint32_t* efs = nullptr;
+    const uint64_t* fbits = nullptr;
+    const uint8_t* fused = nullptr;
+    const uint32_t* fids = nullptr;
+};
+
+static int stage_batch(Slot* s, const float* queries, size_t nq, size_t dim, const hnsw_search_opts& o,
+                       uint32_t stride, StagedBatch* out) {
     cudaStream_t st = s->stream;
     CU(s->q.ensure(nq * dim * 4), "cudaMalloc queries");
     CU(cudaMemcpyAsync(s->q.p, queries, nq * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
@@ -493,8 +560,37 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
     CU(s->odist.ensure(nq * stride * 4), "cudaMalloc out dist");
     CU(s->ocount.ensure(nq * 4), "cudaMalloc out count");
     CU(s->ostatus.ensure(nq * 4), "cudaMalloc out status");
-    r = enqueue_search(gi, s, s->q.as<float>(), nq, o, d_ks, d_efs, d_fb, d_fu, d_fi, s->okeys.as<uint64_t>(),
-                       s->odist.as<float>(), s->ocount.as<uint32_t>(), s->ostatus.as<int32_t>(), ef_bound, stride, st);
+    out->ks = d_ks;
+    out->efs = d_efs;
+    out->fbits = d_fb;
+    out->fused = d_fu;
+    out->fids = d_fi;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim,
+                          const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                          int32_t* out_status) {
+    if (!gi || !opts) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    const hnsw_search_opts& o = *opts;
+    uint32_t ef_bound = 0, stride = 0;
+    int r = check_batch(gi, nq, dim, o, &ef_bound, &stride);
+    if (r != HNSW_OK) return r;
+    if (nq == 0) return HNSW_OK;
+    if (!queries || !out_keys || !out_dist || !out_count || !out_status)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    DeviceGuard dg(gi->device);
+    Slot* s = nullptr;
+    r = gi->slots.acquire(&s);
+    if (r != HNSW_OK) return r;
+    std::unique_ptr<Slot, std::function<void(Slot*)>> hold(s, [gi](Slot* p) { gi->slots.release(p); });
+    cudaStream_t st = s->stream;
+    StagedBatch sb;
+    r = stage_batch(s, queries, nq, dim, o, stride, &sb);
+    if (r != HNSW_OK) return r;
+    r = enqueue_search(gi, s, s->q.as<float>(), nq, o, sb.ks, sb.efs, sb.fbits, sb.fused, sb.fids,
+                       s->okeys.as<uint64_t>(), s->odist.as<float>(), s->ocount.as<uint32_t>(),
+                       s->ostatus.as<int32_t>(), ef_bound, stride, st);
     if (r != HNSW_OK) return r;
     CU(cudaMemcpyAsync(out_count, s->ocount.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
     CU(cudaMemcpyAsync(out_status, s->ostatus.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
@@ -517,6 +613,127 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
                                                                   : "query failed";
             return set_error(code, msg);
         }
+    return HNSW_OK;
+}
+
+int hnsw_gpu_clear_tuning(hnsw_gpu_index* gi) {
+    if (!gi) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null index");
+    std::lock_guard<std::mutex> l(gi->tune_mu);
+    for (auto& t : gi->tuned) t = hnsw_gpu_index::Tuned();
+    return HNSW_OK;
+}
+
+int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim, const hnsw_search_opts* opts,
+                      uint32_t reps, hnsw_tune_entry* entries, size_t cap, size_t* written, hnsw_tune_entry* best) {
+    if (written) *written = 0;
+    if (!gi || !opts) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    const hnsw_search_opts& o = *opts;
+    uint32_t ef_bound = 0, stride = 0;
+    int r = check_batch(gi, nq, dim, o, &ef_bound, &stride);
+    if (r != HNSW_OK) return r;
+    if (nq == 0 || !queries) return set_error(HNSW_ERR_INVALID_ARGUMENT, "the autotuner needs a sample batch");
+    if (reps == 0) reps = 3;
+    if (reps > 50) return set_error(HNSW_ERR_INVALID_ARGUMENT, "at most 50 timed runs per schedule");
+    DeviceGuard dg(gi->device);
+    Slot* s = nullptr;
+    r = gi->slots.acquire(&s);
+    if (r != HNSW_OK) return r;
+    std::unique_ptr<Slot, std::function<void(Slot*)>> hold(s, [gi](Slot* p) { gi->slots.release(p); });
+    cudaStream_t st = s->stream;
+    StagedBatch sb;
+    r = stage_batch(s, queries, nq, dim, o, stride, &sb);
+    if (r != HNSW_OK) return r;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    CU(cudaEventCreate(&ev[0]), "cudaEventCreate");
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return cuda_fail(cudaGetLastError(), "cudaEventCreate");
+    }
+    std::unique_ptr<cudaEvent_t, void (*)(cudaEvent_t*)> evs(ev, [](cudaEvent_t* e) {
+        cudaEventDestroy(e[0]);
+        cudaEventDestroy(e[1]);
+    });
+    // The grid: both modes; warps per block 1..8; visited hash 16/32/64
+    // entries per result slot (powers of two within 1024..32768); the
+    // heuristic's own choice first. ef_cap is the bucket's bound.
+    const uint32_t ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_bound, 32)));
+    struct Trial {
+        SearchGeometry g;
+        int32_t mode;
+        int32_t heuristic;
+        float ms;
+    };
+    std::vector<Trial> trials;
+    for (int32_t mode : {HNSW_MODE_PLAIN, HNSW_MODE_PERSISTENT}) {
+        SearchGeometry h = pick_geometry(ef_bound, gi->view.dp, gi->view.dc, mode == HNSW_MODE_PERSISTENT);
+        trials.push_back({h, mode, 1, 0.0f});
+        for (uint32_t per : {16u, 32u, 64u}) {
+            uint32_t hc = 1024;
+            while (hc < ef_cap * per && hc < 32768) hc <<= 1;
+            for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
+                SearchGeometry g;
+                g.ef_cap = ef_cap;
+                g.cand_cap = 2 * ef_cap + 32;
+                g.hash_cap = hc;
+                g.warps_per_block = wpb;
+                if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * wpb > 220 * 1024) continue;
+                if (g.hash_cap == h.hash_cap && g.cand_cap == h.cand_cap && wpb == h.warps_per_block &&
+                    g.ef_cap == h.ef_cap)
+                    continue;
+                trials.push_back({g, mode, 0, 0.0f});
+            }
+        }
+    }
+    std::vector<float> times(reps);
+    for (Trial& t : trials) {
+        hnsw_search_opts ot = o;
+        ot.mode = t.mode;
+        auto run = [&]() {
+            return enqueue_search(gi, s, s->q.as<float>(), nq, ot, sb.ks, sb.efs, sb.fbits, sb.fused, sb.fids,
+                                  s->okeys.as<uint64_t>(), s->odist.as<float>(), s->ocount.as<uint32_t>(),
+                                  s->ostatus.as<int32_t>(), ef_bound, stride, st, &t.g);
+        };
+        r = run();  // warm-up; sizes every buffer
+        if (r != HNSW_OK) return r;
+        for (uint32_t i = 0; i < reps; ++i) {
+            CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
+            r = run();
+            if (r != HNSW_OK) return r;
+            CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
+            CU(cudaEventSynchronize(ev[1]), "autotune run");
+            CU(cudaEventElapsedTime(&times[i], ev[0], ev[1]), "cudaEventElapsedTime");
+        }
+        std::vector<float> sorted = times;
+        std::sort(sorted.begin(), sorted.end());
+        t.ms = sorted[reps / 2];
+    }
+    const Trial* win[2] = {nullptr, nullptr};
+    for (const Trial& t : trials)
+        if (!win[t.mode] || t.ms < win[t.mode]->ms) win[t.mode] = &t;
+    const Trial* top = win[0]->ms <= win[1]->ms ? win[0] : win[1];
+    {
+        std::lock_guard<std::mutex> l(gi->tune_mu);
+        hnsw_gpu_index::Tuned& slot = gi->tuned[tune_bucket(ef_bound)];
+        slot.geo[0] = win[0]->g;
+        slot.geo[1] = win[1]->g;
+        slot.mode = top->mode;
+    }
+    auto fill = [](const Trial& t, hnsw_tune_entry* e) {
+        e->schedule.ef_cap = t.g.ef_cap;
+        e->schedule.cand_cap = t.g.cand_cap;
+        e->schedule.hash_cap = t.g.hash_cap;
+        e->schedule.warps_per_block = t.g.warps_per_block;
+        e->schedule.cold_chunks = t.g.cold_chunks;
+        e->mode = t.mode;
+        e->heuristic = t.heuristic;
+        e->ms = t.ms;
+    };
+    if (entries) {
+        const size_t n = std::min(cap, trials.size());
+        for (size_t i = 0; i < n; ++i) fill(trials[i], &entries[i]);
+        if (written) *written = n;
+    }
+    if (best) fill(*top, best);
     return HNSW_OK;
 }
 

@@ -41,6 +41,7 @@ struct SearchGeometry {
     uint32_t hash_cap = 4096; // visited hash entries (power of two)
     uint32_t warps_per_block = 4;
     uint32_t bytes_per_warp = 0;
+    uint32_t cold_chunks = 0;  // cold-list pool size in chunks; 0 = automatic
 };
 
 struct SearchArgs {
@@ -56,6 +57,7 @@ struct SearchArgs {
     uint64_t filter_stride = 0;
     const uint8_t* filter_used = nullptr;
     const uint32_t* filter_ids = nullptr;  // optional bitmap index per query
+    int filter_by_node = 0;                // bitmaps indexed by node id instead of key
     uint64_t* out_keys = nullptr;
     float* out_dist = nullptr;
     uint32_t* out_count = nullptr;
@@ -74,13 +76,34 @@ struct SearchArgs {
     uint32_t* g_visited = nullptr;  // bitmap, ceil(n/32) words per warp
     uint32_t g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_visited_words = 0;
-    // Per-warp spill areas of the persistent kernel (slot = global warp index).
+    // Per-warp spill bitmaps of the persistent kernel (slot = global warp index).
     uint32_t* spill_bits = nullptr;   // spill_slots * spill_words (multiple of 4 words)
     uint32_t spill_words = 0;
-    uint64_t* spill_cands = nullptr;  // spill_slots * (spill_cand_cap + 1)
-    uint32_t spill_cand_cap = 0;
     uint32_t spill_slots = 0;
+    // Cold candidate lists: chunks of kColdChunk entries drawn from a pool by
+    // the persistent warps (slot < cold_slots) and the retry warps. Each warp
+    // records the chunks it owns in its row of `cold_tab` (cold_tab_cap ids).
+    // cold_next[0] counts the chunks handed out by the fast kernel,
+    // cold_next[1] those of the retry kernel (which reuses the whole pool).
+    uint64_t* cold_pool = nullptr;
+    uint32_t cold_chunks = 0;
+    uint32_t* cold_next = nullptr;
+    uint32_t* cold_tab = nullptr;
+    uint32_t cold_tab_cap = 0;
+    uint32_t cold_slots = 0;
+    // Last-resort pass: the retry kernel lists the queries that still did not
+    // fit (pool exhausted) here; a final launch of a few warps, each owning a
+    // private region of every chunk a list can need (cold_private: the chunk
+    // table rows are preassigned), runs them.
+    uint32_t* overflow_list2 = nullptr;
+    uint32_t* overflow_count2 = nullptr;
+    int cold_private = 0;
 };
+
+constexpr uint32_t kLastResortWarps = 4;
+
+constexpr uint32_t kColdChunkShift = 10;
+constexpr uint32_t kColdChunk = 1u << kColdChunkShift;  // entries per cold chunk (8 KB)
 
 // Launches the fast search (plain or persistent) followed by the retry pass
 // for queries that overflowed. All on `stream`.

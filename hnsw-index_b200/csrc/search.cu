@@ -46,18 +46,25 @@ struct Ws {
     uint32_t ef_cap, cand_cap, hash_cap;
     bool bitmap_mode;  // H is a bitmap over node ids (retry kernel, or after a spill)
     uint32_t bitmap_words;
-    // Persistent warps own spill areas in global memory: when the shared
-    // visited hash or candidate array fills, the query continues there
-    // instead of restarting. Null in the plain and retry kernels.
+    // Persistent warps own a spill bitmap in global memory: when the shared
+    // visited hash fills, the query continues there instead of restarting.
+    // Null in the plain and retry kernels.
     uint32_t* spill_bits;   // bitmap over node ids (spill_words words, zero between queries)
     uint32_t spill_words;
-    uint64_t* spill_cands;  // spill_cand_cap + 1 entries
-    uint32_t spill_cand_cap;
-    // The shared-memory arrays, restored after a spilled query.
-    uint32_t* H0;
-    uint64_t* C0;
-    uint32_t cand_cap0;
-    bool spilled_bits, spilled_cands;
+    uint32_t* H0;           // the shared-memory hash, restored after a spilled query
+    bool spilled_bits;
+    // Cold part of the candidate queue (persistent and retry warps; null
+    // pool in the plain kernel): an unsorted list in chunks drawn from a
+    // pool. Every entry of C is below b_min, the smallest cold entry, so C's
+    // head is always the best candidate; C is refilled from the cold list
+    // when it runs empty, and its upper half moves there when it fills.
+    uint64_t* pool;
+    uint32_t* pool_next;
+    uint32_t pool_chunks;
+    uint32_t* tab;          // chunk ids owned by this warp (kept across its queries)
+    uint32_t tab_cap;
+    uint32_t b_chunks, b_count;
+    uint64_t b_min, b_max;
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -117,6 +124,7 @@ struct QueryCtx {
     float s2;
     int qnorm;  // squared norm of the query code (L2 on codes)
     bool use_filter;
+    bool by_node;
     const uint64_t* fbits;
     uint64_t fnbits;
     Counters cnt;
@@ -126,7 +134,7 @@ __device__ __forceinline__ bool admit(const QueryCtx& c, uint32_t id) {
     const DeviceIndexView& ix = c.a->ix;
     if (ix.has_dead && ((__ldg(ix.dead + (id >> 5)) >> (id & 31)) & 1u)) return false;
     if (!c.use_filter) return true;
-    uint64_t key = ix.keys_are_ids ? uint64_t(id) : __ldg(ix.keys + id);
+    uint64_t key = (ix.keys_are_ids || c.by_node) ? uint64_t(id) : __ldg(ix.keys + id);
     return key < c.fnbits && ((__ldg(c.fbits + (key >> 6)) >> (key & 63)) & 1ull);
 }
 
@@ -264,9 +272,69 @@ __device__ __forceinline__ void batch_merge(uint64_t* A, uint32_t lo, uint32_t h
     __syncwarp();
 }
 
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const uint64_t o = __shfl_xor_sync(kFull, v, off);
+        v = o < v ? o : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const uint64_t o = __shfl_xor_sync(kFull, v, off);
+        v = o > v ? o : v;
+    }
+    return v;
+}
+
+// Lane of the r-th (from 0) set bit of m; m has more than r bits set.
+__device__ __forceinline__ int nth_set(uint32_t m, int r) {
+    for (int i = 0; i < r; ++i) m &= m - 1u;
+    return __ffs(int(m)) - 1;
+}
+
+__device__ __forceinline__ uint64_t* cold_slot(const Ws& w, uint32_t pos) {
+    return w.pool + (size_t(w.tab[pos >> kColdChunkShift]) << kColdChunkShift) + (pos & (kColdChunk - 1));
+}
+
+__device__ __forceinline__ void cold_reset(Ws& w) {
+    w.b_count = 0;
+    w.b_min = ~0ull;
+    w.b_max = 0;
+}
+
+// Appends the entries x of the lanes in S to the cold list. Returns false
+// when the pool has no chunk left. All lanes call.
+__device__ bool cold_append(Ws& w, uint32_t S, uint64_t x) {
+    const int lane = lane_id();
+    const uint32_t n = __popc(S);
+    if (n == 0) return true;
+    if (w.b_count + n > (w.b_chunks << kColdChunkShift)) {
+        if (w.b_chunks >= w.tab_cap) return false;
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(w.pool_next, 1u);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= w.pool_chunks) return false;
+        if (lane == 0) w.tab[w.b_chunks] = c;
+        ++w.b_chunks;
+        __syncwarp();
+    }
+    const bool in = (S >> lane) & 1u;
+    if (in) *cold_slot(w, w.b_count + __popc(S & ((1u << lane) - 1u))) = x;
+    w.b_count += n;
+    w.b_min = min(w.b_min, warp_min_u64(in ? x : ~0ull));
+    w.b_max = max(w.b_max, warp_max_u64(in ? x : 0ull));
+    __syncwarp();
+    return true;
+}
+
 // Makes room for `need` more candidates: compacts the queue to the front,
 // then drops candidates worse than the worst of ef results (they can never be
-// expanded). Returns false if the queue is still too small.
+// expanded), then moves the upper part of the array to the cold list.
+// Returns false if the queue is still too small.
 __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail, uint32_t need, uint32_t rs,
                                           uint32_t ef) {
     if (tail + need <= w.cand_cap) return true;
@@ -293,21 +361,144 @@ __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail,
         }
         tail = keep;
     }
-    if (tail + need > w.cand_cap && w.spill_cands && !w.spilled_cands && w.spill_cand_cap > w.cand_cap) {
-        // Move the queue to the warp's global spill array.
-        const uint32_t n = tail - head;
-        for (uint32_t b = 0; b < n; b += 32) {
+    if (tail + need > w.cand_cap && w.pool && need <= w.cand_cap) {
+        // Keep the lower half (or less, to fit `need`); the rest is larger
+        // than everything kept, so the cold list's minimum stays above C.
+        const uint32_t keep = min((tail - head) >> 1, w.cand_cap - need);
+        for (uint32_t b = head + keep; b < tail; b += 32) {
             const uint32_t j = b + lane;
-            if (j < n) w.spill_cands[j] = w.C[head + j];
+            const bool in = j < tail;
+            const uint64_t v = in ? w.C[j] : 0;
+            if (!cold_append(w, __ballot_sync(kFull, in), v)) return false;
         }
-        __syncwarp();
-        w.C = w.spill_cands;
-        w.cand_cap = w.spill_cand_cap;
-        w.spilled_cands = true;
-        head = 0;
-        tail = n;
+        tail = head + keep;
     }
     return tail + need <= w.cand_cap;
+}
+
+// Refills the empty candidate array from the cold list with its smallest
+// entries, in order (at least one, at most half the array). When ef results
+// exist (`full`), cold entries worse than the worst result are dropped
+// first: they can never be expanded. The 64 words at w.fr serve as the
+// histogram of a radix selection of the cut.
+__device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, float worst) {
+    const int lane = lane_id();
+    const uint32_t lt = (1u << lane) - 1u;
+    head = tail = 0;
+    if (full) {
+        uint32_t keep = 0;
+        uint64_t mn = ~0ull, mx = 0;
+        for (uint32_t b = 0; b < w.b_count; b += 32) {
+            const uint32_t j = b + lane;
+            const uint64_t v = j < w.b_count ? *cold_slot(w, j) : 0;
+            const bool ok = j < w.b_count && !(pdist(v) > worst);
+            const uint32_t K = __ballot_sync(kFull, ok);
+            __syncwarp();
+            if (ok) {
+                *cold_slot(w, keep + __popc(K & lt)) = v;
+                mn = min(mn, v);
+                mx = max(mx, v);
+            }
+            keep += __popc(K);
+        }
+        __syncwarp();
+        w.b_count = keep;
+        w.b_min = warp_min_u64(mn);
+        w.b_max = warp_max_u64(mx);
+        if (keep == 0) return;
+    }
+    const uint32_t target = max(1u, min(w.b_count, w.cand_cap >> 1));
+    // Take every cold entry below `bound`. Entries are distinct, and b_max
+    // is below ~0 (ids are below the sentinel), so bound = b_max + 1 takes all.
+    uint64_t bound = w.b_max + 1;
+    if (w.b_count > target) {
+        // Window [lo, lo + 2^wbits) holding the undecided entries, split into
+        // 64 bins of 2^s keys; `known` entries lie below the window.
+        const int p = 63 - __clzll(static_cast<long long>(w.b_min ^ w.b_max));
+        int wbits = p + 1;
+        int s = max(wbits - 6, 0);
+        uint64_t lo = wbits >= 64 ? 0ull : (w.b_min & ~((1ull << wbits) - 1ull));
+        uint32_t known = 0;
+        uint32_t* hist = w.fr;
+        for (int pass = 0; pass < 12; ++pass) {
+            hist[lane] = 0;
+            hist[lane + 32] = 0;
+            __syncwarp();
+            for (uint32_t b = 0; b < w.b_count; b += 32) {
+                const uint32_t j = b + lane;
+                if (j < w.b_count) {
+                    const uint64_t v = *cold_slot(w, j);
+                    const uint64_t off = v - lo;
+                    if (v >= lo && (wbits >= 64 || (off >> wbits) == 0)) atomicAdd(&hist[uint32_t(off >> s)], 1u);
+                }
+            }
+            __syncwarp();
+            const uint32_t c0 = hist[2 * lane], c1 = hist[2 * lane + 1];
+            uint32_t incl = c0 + c1;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t o = __shfl_up_sync(kFull, incl, off);
+                if (lane >= off) incl += o;
+            }
+            const uint32_t excl = incl - c0 - c1;
+            // Largest bin count j with known + (entries in bins below j) <= target.
+            const bool q1 = known + excl + c0 <= target, q2 = known + incl <= target;
+            const uint32_t jstar = __reduce_add_sync(kFull, uint32_t(q1) + uint32_t(q2));
+            const uint32_t taken =
+                known + __reduce_max_sync(kFull, q2 ? incl : (q1 ? excl + c0 : 0u));
+            __syncwarp();
+            bound = lo + (uint64_t(jstar) << s);
+            if ((taken >= 1 && 2 * taken >= target) || s == 0) break;
+            known = taken;
+            lo += uint64_t(jstar) << s;
+            wbits = s;
+            s = max(s - 6, 0);
+        }
+    }
+    // Move the entries below `bound` into C through a 32-entry stage held one
+    // per lane; compact the others in place.
+    uint64_t stage = 0, mn = ~0ull, mx = 0;
+    uint32_t sn = 0, keep = 0;
+    for (uint32_t b = 0; b < w.b_count; b += 32) {
+        const uint32_t j = b + lane;
+        const bool valid = j < w.b_count;
+        const uint64_t v = valid ? *cold_slot(w, j) : 0;
+        const bool sel = valid && v < bound, kp = valid && !sel;
+        const uint32_t S = __ballot_sync(kFull, sel), K = __ballot_sync(kFull, kp);
+        __syncwarp();
+        if (kp) {
+            *cold_slot(w, keep + __popc(K & lt)) = v;
+            mn = min(mn, v);
+            mx = max(mx, v);
+        }
+        keep += __popc(K);
+        const uint32_t ns = __popc(S);
+        if (ns) {
+            // Lanes sn.. receive the selected entries in lane order.
+            const int r = lane - int(sn);
+            const bool take = r >= 0 && r < int(ns);
+            const uint64_t got = __shfl_sync(kFull, v, take ? nth_set(S, r) : 0);
+            if (take) stage = got;
+            const uint32_t fit = min(ns, 32u - sn);
+            sn += fit;
+            if (sn == 32) {
+                batch_merge(w.C, 0, tail, kFull, stage, w.cand_cap);
+                tail += 32;
+                const uint32_t r2 = uint32_t(lane) + fit;
+                const uint64_t rest = __shfl_sync(kFull, v, r2 < ns ? nth_set(S, int(r2)) : 0);
+                if (r2 < ns) stage = rest;
+                sn = ns - fit;
+            }
+        }
+    }
+    if (sn) {
+        batch_merge(w.C, 0, tail, (sn == 32 ? kFull : ((1u << sn) - 1u)), stage, w.cand_cap);
+        tail += sn;
+    }
+    __syncwarp();
+    w.b_count = keep;
+    w.b_min = warp_min_u64(mn);
+    w.b_max = warp_max_u64(mx);
 }
 
 // search_layer on layer 0 (src/hnsw/search.rs:81-142). Returns the number of
@@ -326,6 +517,7 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const uint32_t hash_limit = (w.hash_cap >> 2) * 3;
     uint32_t visited = 0;
     uint32_t rs = 0, head = 0, tail = 0;
+    cold_reset(w);
     if (lane == 0) visit(w, pid(ep));
     visited = 1;
     if (lane == 0) w.C[0] = ep;
@@ -335,7 +527,12 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
         rs = 1;
     }
     __syncwarp();
-    while (head < tail) {
+    for (;;) {
+        if (head == tail) {
+            if (w.b_count == 0) break;
+            cold_refill(w, head, tail, rs >= ef, rs > 0 ? pdist(w.R[rs - 1]) : 0.0f);
+            if (head == tail) break;
+        }
         const uint64_t cur = w.C[head];
         ++head;
         const float worst0 = rs > 0 ? pdist(w.R[rs - 1]) : 0.0f;
@@ -416,9 +613,25 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                         rs = min(rs + uint32_t(__popc(IR)), ef);
                     }
                     if (I) {
-                        if (!make_room(w, head, tail, uint32_t(__popc(I)), rs, ef)) return -1;
-                        batch_merge(w.C, head, tail, I, my_x, w.cand_cap);
-                        tail += uint32_t(__popc(I));
+                        // Entries above the cold minimum join the cold list.
+                        uint32_t IA = I, IB = 0;
+                        if (w.b_count) {
+                            IB = I & __ballot_sync(kFull, my_x > w.b_min);
+                            IA &= ~IB;
+                        }
+                        if (IA) {
+                            if (!make_room(w, head, tail, uint32_t(__popc(IA)), rs, ef)) return -1;
+                            if (w.b_count) {
+                                const uint32_t mv = IA & __ballot_sync(kFull, my_x > w.b_min);
+                                IA &= ~mv;
+                                IB |= mv;
+                            }
+                            if (IA) {
+                                batch_merge(w.C, head, tail, IA, my_x, w.cand_cap);
+                                tail += uint32_t(__popc(IA));
+                            }
+                        }
+                        if (IB && !cold_append(w, IB, my_x)) return -1;
                     }
                 } else {
                     while (P) {
@@ -429,9 +642,17 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                         const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
                         if (!improves) continue;
                         const uint64_t x = pack(d, nid);
-                        if (!make_room(w, head, tail, 1, rs, ef)) return -1;
-                        sorted_insert(w.C, head, tail, x);
-                        ++tail;
+                        bool cold = w.b_count != 0 && x > w.b_min;
+                        if (!cold) {
+                            if (!make_room(w, head, tail, 1, rs, ef)) return -1;
+                            cold = w.b_count != 0 && x > w.b_min;
+                        }
+                        if (cold) {
+                            if (!cold_append(w, 1u, x)) return -1;
+                        } else {
+                            sorted_insert(w.C, head, tail, x);
+                            ++tail;
+                        }
                         if ((A >> i) & 1u) {
                             sorted_insert(w.R, 0, rs, x);
                             ++rs;
@@ -511,6 +732,7 @@ __device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
     const size_t fsel = a.filter_ids ? size_t(a.filter_ids[qi]) : size_t(qi);
     c.fbits = a.filter_bits + (a.filter_stride ? fsel * a.filter_stride : 0);
     c.fnbits = a.filter_nbits;
+    c.by_node = a.filter_by_node != 0;
     const uint32_t k = min(a.ks ? a.ks[qi] : a.k, a.out_stride);
     uint32_t ef = a.efs ? a.efs[qi] : a.ef;
     uint32_t count = 0;
@@ -604,12 +826,26 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_
     w.bitmap_words = 0;
     w.spill_bits = nullptr;
     w.spill_words = 0;
-    w.spill_cands = nullptr;
-    w.spill_cand_cap = 0;
     w.H0 = w.H;
-    w.C0 = w.C;
-    w.cand_cap0 = cand_cap;
-    w.spilled_bits = w.spilled_cands = false;
+    w.spilled_bits = false;
+    w.pool = nullptr;
+    w.pool_next = nullptr;
+    w.pool_chunks = 0;
+    w.tab = nullptr;
+    w.tab_cap = 0;
+    w.b_chunks = 0;
+    cold_reset(w);
+}
+
+// Gives the warp its cold-list row of the pool (`slot` < cold_slots).
+__device__ void attach_cold(Ws& w, const SearchArgs& a, uint32_t slot, uint32_t* next) {
+    if (!a.cold_pool || slot >= a.cold_slots) return;
+    w.pool = a.cold_pool;
+    w.pool_next = next;
+    w.pool_chunks = a.cold_chunks;
+    w.tab = a.cold_tab + size_t(slot) * a.cold_tab_cap;
+    w.tab_cap = a.cold_tab_cap;
+    if (a.cold_private) w.b_chunks = w.tab_cap;
 }
 
 // Clears a spill bitmap and points the workspace back at shared memory.
@@ -625,11 +861,6 @@ __device__ void end_spill(Ws& w) {
         w.bitmap_words = 0;
         w.spilled_bits = false;
     }
-    if (w.spilled_cands) {
-        w.C = w.C0;
-        w.cand_cap = w.cand_cap0;
-        w.spilled_cands = false;
-    }
 }
 
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
@@ -643,9 +874,8 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
         if (a.spill_bits && slot < a.spill_slots) {
             w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;
             w.spill_words = a.spill_words;
-            w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
-            w.spill_cand_cap = a.spill_cand_cap;
         }
+        attach_cold(w, a, slot, a.cold_next);
         for (;;) {
             uint32_t qi = 0;
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
@@ -695,16 +925,23 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.bitmap_words = uint32_t(a.g_visited_words);
     w.spill_bits = nullptr;
     w.spill_words = 0;
-    w.spill_cands = nullptr;
-    w.spill_cand_cap = 0;
     w.H0 = w.H;
-    w.C0 = w.C;
-    w.cand_cap0 = w.cand_cap;
-    w.spilled_bits = w.spilled_cands = false;
+    w.spilled_bits = false;
+    w.pool = nullptr;
+    w.pool_next = nullptr;
+    w.pool_chunks = 0;
+    w.tab = nullptr;
+    w.tab_cap = 0;
+    w.b_chunks = 0;
+    cold_reset(w);
+    attach_cold(w, a, gw, a.cold_next ? a.cold_next + 1 : nullptr);
     const uint32_t total = *a.overflow_count;
     for (uint32_t t = gw; t < total; t += nwarps) {
         const uint32_t qi = a.overflow_list[t];
-        run_query(a, w, qi);  // writes ST_OVERFLOW again if even this scratch is too small
+        // Writes ST_OVERFLOW again if even this scratch is too small; the
+        // last-resort pass then takes the query.
+        if (run_query(a, w, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)
+            a.overflow_list2[atomicAdd(a.overflow_count2, 1u)] = qi;
     }
 }
 

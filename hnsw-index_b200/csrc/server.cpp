@@ -127,9 +127,10 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     o.ef = s->cfg.max_ef;
     o.quantized = s->cfg.quantized;
     o.filter_nbits = s->cfg.filter_nbits;
+    o.filter_by_node = s->cfg.filter_by_node;
     o.filter_stride = s->words;
     o.out_stride = K;
-    o.mode = HNSW_MODE_PERSISTENT;
+    o.mode = HNSW_MODE_AUTO;
     int r = enqueue_search(s->index, sl, sl->q.as<float>(), n, o, sl->ks.as<uint32_t>(), sl->efs.as<uint32_t>(), d_fb,
                            d_fu, d_fi, sl->okeys.as<uint64_t>(), sl->odist.as<float>(), sl->ocount.as<uint32_t>(),
                            sl->ostatus.as<int32_t>(), std::max(K, s->cfg.max_ef), K, st);

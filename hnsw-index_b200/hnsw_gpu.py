@@ -130,7 +130,7 @@ class _Opts(C.Structure):
         ("k", C.c_uint32), ("ef", C.c_uint32), ("ks", C.c_void_p), ("efs", C.c_void_p),
         ("quantized", C.c_int32), ("filter_bits", C.c_void_p), ("filter_nbits", C.c_uint64),
         ("filter_stride", C.c_uint64), ("filter_used", C.c_void_p), ("out_stride", C.c_uint32),
-        ("mode", C.c_int32), ("filter_ids", C.c_void_p),
+        ("mode", C.c_int32), ("filter_ids", C.c_void_p), ("filter_by_node", C.c_int32),
     ]
 
 
@@ -158,10 +158,21 @@ _lib.hnsw_gpu_set_counters.argtypes = [_vp, C.c_int]
 
 class _Schedule(C.Structure):
     _fields_ = [("ef_cap", C.c_uint32), ("cand_cap", C.c_uint32), ("hash_cap", C.c_uint32),
-                ("warps_per_block", C.c_uint32)]
+                ("warps_per_block", C.c_uint32), ("cold_chunks", C.c_uint32)]
 
 
 _lib.hnsw_gpu_set_schedule.argtypes = [_vp, C.POINTER(_Schedule)]
+
+
+class _TuneEntry(C.Structure):
+    _fields_ = [("schedule", _Schedule), ("mode", C.c_int32), ("heuristic", C.c_int32), ("ms", C.c_float)]
+
+
+_lib.hnsw_gpu_autotune.argtypes = [_vp, _vp, _sz, _sz, C.POINTER(_Opts), C.c_uint32, C.POINTER(_TuneEntry), _sz,
+                                   C.POINTER(_sz), C.POINTER(_TuneEntry)]
+_lib.hnsw_gpu_clear_tuning.argtypes = [_vp]
+
+MODE_PLAIN, MODE_PERSISTENT, MODE_AUTO = 0, 1, 2
 _lib.hnsw_gpu_graph_create.argtypes = [_vp, _vp, _sz, _sz, C.POINTER(_Opts), _vp, _vp, _vp, _vp, C.POINTER(_vp)]
 _lib.hnsw_gpu_graph_launch.argtypes = [_vp, _vp]
 _lib.hnsw_gpu_graph_destroy.argtypes = [_vp]
@@ -206,7 +217,8 @@ EXPORTED_SYMBOLS = (
     "hnsw_params_default", "hnsw_builder_new", "hnsw_builder_free", "hnsw_builder_insert",
     "hnsw_builder_insert_batch", "hnsw_builder_remove", "hnsw_builder_enable_quantization",
     "hnsw_builder_to_bytes", "hnsw_bytes_free", "hnsw_synthetic_gaussian",
-    "hnsw_synthetic_mixture", "hnsw_synthetic_mixture_split", "hnsw_crc32",
+    "hnsw_synthetic_mixture", "hnsw_synthetic_mixture_split", "hnsw_crc32", "hnsw_gpu_autotune",
+    "hnsw_gpu_clear_tuning", "hnsw_gpu_set_schedule",
 )
 
 LIBRARY_PATH = _LIB_PATH
@@ -378,36 +390,25 @@ class HnswIndex:
     # -- search --
     def _filter_bits(self, f):
         if f is None:
-            return None, 0
+            return None, 0, False
         if callable(f):
-            live = self._keys[self._deleted == 0]
-            accepted = np.fromiter((k for k in live.tolist() if f(k)), dtype=np.uint64)
-            nbits = int(self._keys.max()) + 1 if self._keys.size else 1
-            return key_bitmap(accepted, nbits), nbits
+            # The closure runs once per live node on the calling thread; the
+            # bitmap is indexed by node id, so any u64 key set works.
+            live = np.nonzero(self._deleted == 0)[0]
+            keys = self._keys[live].tolist()
+            accepted = np.fromiter((i for i, k in zip(live.tolist(), keys) if f(k)), dtype=np.uint64)
+            nbits = max(int(self._keys.size), 1)
+            return key_bitmap(accepted, nbits), nbits, True
         bits = np.ascontiguousarray(f, dtype=np.uint64)
-        return bits, bits.size * 64
+        return bits, bits.size * 64, False
 
-    def search_arrays(self, queries: np.ndarray, k: int, ef: int, *, quantized: bool = False,
-                      filter_bits: Optional[np.ndarray] = None, filter_nbits: int = 0,
-                      filter_stride: int = 0, filter_used: Optional[np.ndarray] = None,
-                      ks: Optional[np.ndarray] = None, efs: Optional[np.ndarray] = None,
-                      mode: int = 0, raise_on_error: bool = True, filter_ids: Optional[np.ndarray] = None):
-        """Batched search returning arrays (keys, dist, count, status)."""
-        q = np.ascontiguousarray(queries, dtype=np.float32)
-        if q.ndim == 1:
-            if q.size % max(self.dim(), 1):
-                raise Error(Status.DIMENSION_MISMATCH,
-                            f"dimension mismatch: expected {self.dim()}, got {q.size}")
-            q = q.reshape(-1, self.dim())
-        nq, dim = q.shape
+    @staticmethod
+    def _opts(nq, k, ef, quantized=False, filter_bits=None, filter_nbits=0, filter_stride=0, filter_used=None,
+              ks=None, efs=None, mode=0, filter_ids=None, filter_by_node=False):
+        """hnsw_search_opts for a batch, and the arrays it points into (keep them alive)."""
         ks_a = None if ks is None else np.ascontiguousarray(ks, dtype=np.uint32)
         efs_a = None if efs is None else np.ascontiguousarray(efs, dtype=np.uint32)
         kmax = int(ks_a.max()) if ks_a is not None and ks_a.size else k
-        stride = max(kmax, 1)
-        keys = np.zeros((nq, stride), dtype=np.uint64)
-        dist = np.zeros((nq, stride), dtype=np.float32)
-        count = np.zeros(nq, dtype=np.uint32)
-        status = np.zeros(nq, dtype=np.int32)
         o = _Opts()
         o.k, o.ef = k, ef
         o.ks, o.efs = _ptr(ks_a), _ptr(efs_a)
@@ -420,8 +421,33 @@ class HnswIndex:
         o.filter_used = _ptr(fu)
         fi = None if filter_ids is None else np.ascontiguousarray(filter_ids, dtype=np.uint32)
         o.filter_ids = _ptr(fi)
-        o.out_stride = stride
+        o.filter_by_node = int(filter_by_node)
+        o.out_stride = max(kmax, 1)
         o.mode = mode
+        return o, (ks_a, efs_a, fb, fu, fi)
+
+    def search_arrays(self, queries: np.ndarray, k: int, ef: int, *, quantized: bool = False,
+                      filter_bits: Optional[np.ndarray] = None, filter_nbits: int = 0,
+                      filter_stride: int = 0, filter_used: Optional[np.ndarray] = None,
+                      ks: Optional[np.ndarray] = None, efs: Optional[np.ndarray] = None,
+                      mode: int = 0, raise_on_error: bool = True, filter_ids: Optional[np.ndarray] = None,
+                      filter_by_node: bool = False):
+        """Batched search returning arrays (keys, dist, count, status)."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        if q.ndim == 1:
+            if q.size % max(self.dim(), 1):
+                raise Error(Status.DIMENSION_MISMATCH,
+                            f"dimension mismatch: expected {self.dim()}, got {q.size}")
+            q = q.reshape(-1, self.dim())
+        nq, dim = q.shape
+        o, keep = self._opts(nq, k, ef, quantized=quantized, filter_bits=filter_bits, filter_nbits=filter_nbits,
+                             filter_stride=filter_stride, filter_used=filter_used, ks=ks, efs=efs, mode=mode,
+                             filter_ids=filter_ids, filter_by_node=filter_by_node)
+        stride = o.out_stride
+        keys = np.zeros((nq, stride), dtype=np.uint64)
+        dist = np.zeros((nq, stride), dtype=np.float32)
+        count = np.zeros(nq, dtype=np.uint32)
+        status = np.zeros(nq, dtype=np.int32)
         st = _lib.hnsw_gpu_search_batch(self._h, _ptr(q), nq, dim, C.byref(o), _ptr(keys), _ptr(dist),
                                         _ptr(count), _ptr(status))
         if st != 0 and raise_on_error:
@@ -446,10 +472,10 @@ class HnswIndex:
         if q.size != self.dim():
             raise Error(Status.DIMENSION_MISMATCH,
                         f"dimension mismatch: expected {self.dim()}, got {q.size}")
-        bits, nbits = self._filter_bits(options._filter)
+        bits, nbits, by_node = self._filter_bits(options._filter)
         keys, dist, count, _ = self.search_arrays(q.reshape(1, -1), k, options.ef(),
                                                   quantized=options._quantized,
-                                                  filter_bits=bits, filter_nbits=nbits)
+                                                  filter_bits=bits, filter_nbits=nbits, filter_by_node=by_node)
         return self._to_lists(keys, dist, count)[0]
 
     def search_batch(self, queries, k: int, ef: int):
@@ -469,13 +495,37 @@ class HnswIndex:
         _check(_lib.hnsw_gpu_index_info(self._h, C.byref(info)))
         self._info = info
 
-    def set_schedule(self, ef_cap=None, cand_cap=None, hash_cap=None, warps_per_block=None):
+    def set_schedule(self, ef_cap=None, cand_cap=None, hash_cap=None, warps_per_block=None, cold_chunks=0):
         """Fixes the traversal scratch geometry; no arguments restores the automatic choice."""
         if ef_cap is None:
             _check(_lib.hnsw_gpu_set_schedule(self._h, None))
             return
-        sc = _Schedule(ef_cap, cand_cap or 2 * ef_cap + 32, hash_cap, warps_per_block)
+        sc = _Schedule(ef_cap, cand_cap or 2 * ef_cap + 32, hash_cap, warps_per_block, cold_chunks)
         _check(_lib.hnsw_gpu_set_schedule(self._h, C.byref(sc)))
+
+    def autotune(self, queries, k: int, ef: int, reps: int = 3, **search_kw):
+        """Times the sample batch under every schedule of the tuner's grid and
+        installs the fastest per mode for this ef bucket (hnsw_gpu_autotune).
+        Returns (best, trials), each trial a dict of schedule, mode, ms."""
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, self.dim())
+        o, keep = self._opts(q.shape[0], k, ef, **search_kw)
+        entries = (_TuneEntry * 128)()
+        n = C.c_size_t()
+        best = _TuneEntry()
+        _check(_lib.hnsw_gpu_autotune(self._h, _ptr(q), q.shape[0], q.shape[1], C.byref(o), reps, entries, 128,
+                                      C.byref(n), C.byref(best)))
+        del keep
+
+        def d(e):
+            s = e.schedule
+            return {"ef_cap": s.ef_cap, "cand_cap": s.cand_cap, "hash_cap": s.hash_cap,
+                    "warps_per_block": s.warps_per_block, "mode": e.mode, "heuristic": bool(e.heuristic),
+                    "ms": e.ms}
+
+        return d(best), [d(entries[i]) for i in range(n.value)]
+
+    def clear_tuning(self):
+        _check(_lib.hnsw_gpu_clear_tuning(self._h))
 
     def set_counters(self, enabled: bool):
         _check(_lib.hnsw_gpu_set_counters(self._h, int(enabled)))
@@ -517,7 +567,7 @@ class _ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
                 ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
                 ("filter_nbits", C.c_uint64), ("quantized", C.c_int32), ("filter_bank", C.c_void_p),
-                ("filter_count", C.c_uint32)]
+                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32)]
 
 
 _lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
@@ -538,12 +588,13 @@ class Server:
 
     def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
                  max_ef=512, linger_us=100, filter_nbits=0, filter_bank: Optional[np.ndarray] = None,
-                 quantized=False):
+                 quantized=False, filter_by_node=False):
         cfg = _ServerConfig()
         _lib.hnsw_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
         cfg.max_k, cfg.max_ef, cfg.linger_us = max_k, max_ef, linger_us
         cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
+        cfg.filter_by_node = int(filter_by_node)
         bank = None if filter_bank is None else np.ascontiguousarray(filter_bank, np.uint64)
         if bank is not None:
             cfg.filter_bank = _ptr(bank)

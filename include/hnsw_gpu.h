@@ -114,11 +114,15 @@ typedef struct hnsw_search_opts {
     int32_t mode;               /* HNSW_MODE_* */
     const uint32_t* filter_ids; /* optional: query i uses bitmap filter_ids[i] (stride filter_stride)
                                    instead of bitmap i, so many queries can share a few filters */
+    int32_t filter_by_node;     /* 0: bit = key (keys below filter_nbits); 1: bit = node id, i.e.
+                                   position in the file's node order, for indexes whose keys are
+                                   sparse u64 values (a closure filter evaluated once per node) */
 } hnsw_search_opts;
 
 enum {
     HNSW_MODE_PLAIN = 0,      /* one warp per query, one launch per call */
-    HNSW_MODE_PERSISTENT = 1  /* persistent CTAs draining a device work queue */
+    HNSW_MODE_PERSISTENT = 1, /* persistent CTAs draining a device work queue */
+    HNSW_MODE_AUTO = 2        /* the mode hnsw_gpu_autotune found faster for this ef (else persistent) */
 };
 
 /* Batched search: HnswIndex::search_batch / search_with / search_filtered
@@ -162,8 +166,35 @@ typedef struct hnsw_schedule {
     uint32_t cand_cap;        /* candidate array entries */
     uint32_t hash_cap;        /* visited-hash entries, power of two */
     uint32_t warps_per_block; /* 1..8 */
+    uint32_t cold_chunks;     /* pool of the queues' cold lists, in chunks of 1024 candidates;
+                                 0 = automatic (8 per node or 8 per warp). A smaller pool sends
+                                 more queries to the retry and last-resort passes; results
+                                 never change */
 } hnsw_schedule;
 int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
+
+/* Autotuner (no reference counterpart; the crate has no device schedule).
+ * Times the search of a sample batch (host buffers, same options as
+ * hnsw_gpu_search_batch) under every feasible schedule of the grid
+ * mode x warps per block {1, 2, 4, 8} x visited-hash size {16, 32, 64} x
+ * ef_cap (rounded up to a power of two, 1024..32768 entries), plus the
+ * heuristic's own choice, `reps` timed runs each after one warm-up (median,
+ * CUDA events). The fastest schedule of each mode is stored in the index's
+ * tuning table for the ef bucket of the sample's max(ef, k) (buckets of 32),
+ * used from then on by searches in that bucket unless a fixed schedule is
+ * set; HNSW_MODE_AUTO picks the faster mode. Results never depend on the
+ * schedule. `entries` (optional, `cap` entries) receives every trial. */
+typedef struct hnsw_tune_entry {
+    hnsw_schedule schedule;
+    int32_t mode;  /* HNSW_MODE_PLAIN or HNSW_MODE_PERSISTENT */
+    int32_t heuristic; /* 1 for the occupancy heuristic's own choice */
+    float ms;      /* median time of the sample batch */
+} hnsw_tune_entry;
+int hnsw_gpu_autotune(hnsw_gpu_index* index, const float* queries, size_t nq, size_t dim,
+                      const hnsw_search_opts* opts, uint32_t reps, hnsw_tune_entry* entries, size_t cap,
+                      size_t* written, hnsw_tune_entry* best);
+/* Forgets every autotuned schedule of the index. */
+int hnsw_gpu_clear_tuning(hnsw_gpu_index* index);
 
 /* Per-query traversal counters of the last search on this thread's slot
  * (device pointer, nq x 4 u32: layer-0 distances, layer-0 expansions,
@@ -195,6 +226,7 @@ typedef struct hnsw_server_config {
     const uint64_t* filter_bank; /* host: filter_count bitmaps of ceil(filter_nbits / 64) words,
                                     copied to the device at start */
     uint32_t filter_count;
+    int32_t filter_by_node; /* the bank's bitmaps are indexed by node id, not key */
 } hnsw_server_config;
 
 void hnsw_server_config_default(hnsw_server_config* cfg);

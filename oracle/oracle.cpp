@@ -349,8 +349,11 @@ struct Scratch {
 
 struct Filter {
     // Key bitmap: key admitted iff key < nbits and bit set. nullptr = no filter.
+    // With by_node the bitmap is indexed by node id instead (the same closure
+    // evaluated once per node, for indexes whose keys are sparse u64 values).
     const uint64_t* bits = nullptr;
     uint64_t nbits = 0;
+    bool by_node = false;
     bool accept(uint64_t key) const {
         if (!bits) return true;
         return key < nbits && ((bits[key >> 6] >> (key & 63)) & 1);
@@ -464,7 +467,9 @@ int32_t search_one(const Index& ix, Scratch& sc, const float* query, size_t k, s
     if (quantized && !ix.quantized) return QUANTIZATION_DISABLED;
     if (k == 0 || ix.live == 0) return OK;
     ef = std::max(ef, k);
-    auto admit = [&](uint32_t id) { return !ix.deleted[id] && filter.accept(ix.keys[id]); };
+    auto admit = [&](uint32_t id) {
+        return !ix.deleted[id] && filter.accept(filter.by_node ? uint64_t(id) : ix.keys[id]);
+    };
     auto exact = [&](uint32_t id) { return metric_distance(ix.metric, q.data(), ix.vec(id), ix.dim); };
     std::vector<Cand> found;
     if (ix.entry == 0xFFFFFFFFu) return OK;
@@ -647,7 +652,7 @@ void orc_search_batch(void* handle, const float* queries, size_t nq, size_t k, c
                       size_t ef, const size_t* efs, int quantized, const uint64_t* filter_bits,
                       uint64_t filter_nbits, size_t filter_stride, const uint8_t* use_filter,
                       uint64_t* out_keys, float* out_dist, uint32_t* counts, int32_t* status,
-                      uint64_t* stats, int threads, size_t out_stride) {
+                      uint64_t* stats, int threads, size_t out_stride, int filter_by_node) {
     const Index& ix = *static_cast<Index*>(handle);
     int nt = threads <= 0 ? int(std::max(1u, std::thread::hardware_concurrency())) : threads;
     std::vector<Scratch> scratch(static_cast<size_t>(nt));
@@ -657,6 +662,7 @@ void orc_search_batch(void* handle, const float* queries, size_t nq, size_t k, c
         if (filter_bits && (!use_filter || use_filter[i])) {
             f.bits = filter_bits + (filter_stride ? i * filter_stride : 0);
             f.nbits = filter_nbits;
+            f.by_node = filter_by_node != 0;
         }
         std::vector<Hit> hits;
         Stats st;

@@ -51,7 +51,7 @@ for name, res, args in [
     ("orc_index_dim", C.c_uint32, [_vp]),
     ("orc_index_metric", C.c_int, [_vp]),
     ("orc_search_batch", None, [_vp, _vp, _sz, _sz, _vp, _sz, _vp, C.c_int, _vp, C.c_uint64, _sz, _vp,
-                                _vp, _vp, _vp, _vp, _vp, C.c_int, _sz]),
+                                _vp, _vp, _vp, _vp, _vp, C.c_int, _sz, C.c_int]),
     ("orc_brute_batch", None, [C.c_int, _vp, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _vp, _vp, _vp, C.c_int]),
     ("orc_brute_f64", None, [C.c_int, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _vp, C.c_int]),
     ("orc_recall_at_k", C.c_double, [_vp, _vp, _sz, _vp, _vp, _sz, _sz, _sz]),
@@ -172,7 +172,7 @@ class Index:
             self._h = None
 
     def search(self, queries, k: int, ef: int, *, quantized=False, filter_bits=None, filter_nbits=0,
-               filter_stride=0, filter_used=None, ks=None, efs=None, threads=0, stats=False):
+               filter_stride=0, filter_used=None, ks=None, efs=None, threads=0, stats=False, filter_by_node=False):
         """HnswIndex::search_batch / search_with (src/hnsw/mod.rs:412-536): arrays out."""
         q = _f32(queries).reshape(-1, self.dim)
         nq = q.shape[0]
@@ -188,7 +188,7 @@ class Index:
         fu = None if filter_used is None else np.ascontiguousarray(filter_used, np.uint8)
         _lib.orc_search_batch(self._h, _p(q), nq, k, _p(ks_a), ef, _p(efs_a), int(quantized), _p(fb),
                               filter_nbits, filter_stride, _p(fu), _p(keys), _p(dist), _p(counts),
-                              _p(status), _p(st), threads, stride)
+                              _p(status), _p(st), threads, stride, int(filter_by_node))
         if stats:
             return keys, dist, counts, status, st
         return keys, dist, counts, status

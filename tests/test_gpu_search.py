@@ -352,6 +352,77 @@ def test_shared_filter_bitmaps_by_id():
     assert_same(got, ref, "filter ids")
 
 
+def test_node_bitmaps_for_sparse_u64_keys():
+    """Closure filters on keys far above the node count (src/hnsw/mod.rs:432-440):
+    the bitmap is indexed by node id, so its size is the node count."""
+    base, queries = H.gaussian(2500, 40, 24, 14)
+    rng = np.random.default_rng(15)
+    keys = np.unique(rng.integers(1 << 40, 1 << 63, 2600, dtype=np.uint64))[:2500]
+    rng.shuffle(keys)
+    data = build_index(base, metric=0, m=12, seed=3, keys=keys, deleted_keys=keys[:40:3])
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    for pred, k, ef in [(lambda key: key % 7 == 1, 10, 64), (lambda key: key >= (1 << 62), 5, 32),
+                        (lambda key: False, 3, 10)]:
+        for i in range(0, 40, 13):
+            got = gi.search_filtered(queries[i], k, ef, pred)
+            ref = oi.search(queries[i:i + 1], k, ef, filter_bits=gi._filter_bits(pred)[0], filter_nbits=2500,
+                            filter_by_node=True)
+            c = int(ref[2][0])
+            assert [n.key for n in got] == ref[0][0, :c].tolist()
+            assert all(pred(n.key) for n in got)
+    # Per-query node bitmaps through the batched entry point.
+    words = (2500 + 63) // 64
+    bank = np.zeros((40, words), np.uint64)
+    for j in range(40):
+        bank[j] = H.key_bitmap(np.nonzero(rng.random(2500) < 0.2)[0].astype(np.uint64), 2500)
+    got = gi.search_arrays(queries, 10, 48, filter_bits=bank, filter_nbits=2500, filter_stride=words,
+                           filter_by_node=True, mode=1)
+    ref = oi.search(queries, 10, 48, filter_bits=bank, filter_nbits=2500, filter_stride=words, filter_by_node=True)
+    assert_same(got, ref, "node bitmaps")
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_cold_candidate_list_under_selective_filters(mode):
+    """Filters so selective that ef results never fill: the beam explores
+    most of the graph and the candidate queue grows towards the node count
+    (the reference's heap is unbounded). The queue's cold list, its refills
+    and the evictions of the array's upper half must not change a result."""
+    base, queries = H.mixture(20000, 48, 16, 40, 0.4, 31)
+    data = build_index(base, metric=0, m=8, seed=5, deleted_keys=range(0, 20000, 97))
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    rng = np.random.default_rng(32)
+    nbits, words = 20000, (20000 + 63) // 64
+    sels = [0.0003, 0.002, 0.01, 0.05, 0.3]
+    bank = np.zeros((len(sels), words), np.uint64)
+    for j, p in enumerate(sels):
+        bank[j] = H.key_bitmap(np.nonzero(rng.random(nbits) < p)[0].astype(np.uint64), nbits)
+    ids = rng.integers(0, len(sels), 48).astype(np.uint32)
+    ks = rng.choice([1, 10, 100], 48).astype(np.uint32)
+    efs = rng.choice([16, 64, 256, 512], 48).astype(np.uint32)
+    ref = oi.search(queries, 100, 16, filter_bits=bank[ids], filter_nbits=nbits, filter_stride=words, ks=ks, efs=efs)
+    # cold_chunks=1: the shared pools run dry at once, so the queries end in
+    # the last-resort pass (private regions).
+    for sched in [None, dict(ef_cap=512, cand_cap=512, hash_cap=4096, warps_per_block=2),
+                  dict(ef_cap=512, cand_cap=1056, hash_cap=8192, warps_per_block=1, cold_chunks=1)]:
+        if sched:
+            gi.set_schedule(**sched)
+        got = gi.search_arrays(queries, 100, 16, filter_bits=bank, filter_nbits=nbits, filter_stride=words,
+                               filter_ids=ids, ks=ks, efs=efs, mode=mode)
+        assert_same(got, ref, f"schedule {sched}")
+    # The smallest arrays: every few insertions move half the queue to the cold list.
+    gi.set_schedule(ef_cap=64, cand_cap=64, hash_cap=1024, warps_per_block=4)
+    small = np.minimum(efs, 64).astype(np.uint32)
+    ks_small = np.minimum(ks, 10).astype(np.uint32)
+    got = gi.search_arrays(queries, 10, 16, filter_bits=bank, filter_nbits=nbits, filter_stride=words,
+                           filter_ids=ids, ks=ks_small, efs=small, mode=mode)
+    ref = oi.search(queries, 10, 16, filter_bits=bank[ids], filter_nbits=nbits, filter_stride=words, ks=ks_small,
+                    efs=small)
+    assert_same(got, ref, "cand_cap 64")
+    gi.set_schedule()
+
+
 def test_fixed_schedule_gives_identical_results(gaussian_10k):
     _, queries, data = gaussian_10k
     gi = H.HnswIndex.from_bytes(data)
@@ -361,6 +432,31 @@ def test_fixed_schedule_gives_identical_results(gaussian_10k):
         for mode in (0, 1):
             assert_same(gi.search_arrays(queries[:200], 10, 64, mode=mode), want, f"schedule {ef_cap}/{hash_cap}")
     gi.set_schedule()
+
+
+def test_autotune_installs_schedules_without_changing_results(gaussian_10k):
+    _, queries, data = gaussian_10k
+    gi = H.HnswIndex.from_bytes(data)
+    sample = queries[:300]
+    want = gi.search_arrays(sample, 10, 64, mode=1)
+    best, trials = gi.autotune(sample, 10, 64, reps=2)
+    assert len(trials) > 8
+    assert {t["mode"] for t in trials} == {0, 1}
+    assert sum(t["heuristic"] for t in trials) == 2
+    assert all(t["ms"] > 0 for t in trials)
+    assert best["ms"] == min(t["ms"] for t in trials)
+    for mode in (H.MODE_PLAIN, H.MODE_PERSISTENT, H.MODE_AUTO):
+        assert_same(gi.search_arrays(sample, 10, 64, mode=mode), want, f"tuned, mode {mode}")
+    # A filtered batch with per-query k and ef, tuned in its own bucket.
+    rng = np.random.default_rng(4)
+    bits = H.key_bitmap(np.nonzero(rng.random(10_000) < 0.2)[0].astype(np.uint64), 10_000)
+    efs = rng.choice([32, 100, 200], 300).astype(np.uint32)
+    kw = dict(filter_bits=bits, filter_nbits=10_000, efs=efs)
+    want_f = gi.search_arrays(sample, 10, 16, mode=0, **kw)
+    gi.autotune(sample, 10, 16, reps=1, **kw)
+    assert_same(gi.search_arrays(sample, 10, 16, mode=H.MODE_AUTO, **kw), want_f, "tuned filtered")
+    gi.clear_tuning()
+    assert_same(gi.search_arrays(sample, 10, 64, mode=H.MODE_AUTO), want, "after clear")
 
 
 def test_cuda_graph_replays_the_search(gaussian_10k):
