@@ -346,6 +346,43 @@ def run_gpu(args):
     h2d = N_QUERY * DIM * 4
     d2h = N_QUERY * K * 12 + N_QUERY * 8
 
+    # One search call per query (the per-call API path), on a sample.
+    npc = 2000
+    t = time.perf_counter()
+    for i in range(npc):
+        index.search_arrays(queries[i:i + 1], K, ef)
+    per_call_qps = world * npc / (time.perf_counter() - t)
+
+    # Served load: open-loop Poisson arrivals through the request loop
+    # (continuous batching; each request completes when its own query does).
+    served = []
+    if world == 1 and not args.no_serve:
+        srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 18, max_k=K, max_ef=ef,
+                       linger_us=args.serve_linger)
+        ref_keys = kk
+        rng = np.random.default_rng(21)
+        reps = 20
+        pool_q = np.tile(queries, (reps, 1))
+        # Warm-up replay: the first launches size every device buffer.
+        srv.replay(pool_q[:20_000], np.cumsum(rng.exponential(1e6 / 300_000, 20_000)), np.full(20_000, K, np.uint32),
+                   np.full(20_000, ef, np.uint32))
+        for rate in (100_000, 300_000, 1_000_000, 2_000_000):
+            n = int(min(len(pool_q), max(20_000, rate // 2)))
+            arr = np.cumsum(rng.exponential(1e6 / rate, n))
+            t = time.perf_counter()
+            skeys, _, scnt, sst, lat = srv.replay(pool_q[:n], arr, np.full(n, K, np.uint32),
+                                                  np.full(n, ef, np.uint32))
+            wall = time.perf_counter() - t
+            ok = sst == 0
+            same = bool(np.array_equal(skeys[ok][:, :K], ref_keys[np.nonzero(ok)[0] % N_QUERY]))
+            served.append({"offered_qps": rate, "requests": n, "completed": int(ok.sum()),
+                           "rejected": int((sst == H.Status.ADMISSION_REJECTED).sum()),
+                           "achieved_qps": float(ok.sum() / wall),
+                           "p50_ms": float(np.percentile(lat[ok], 50) / 1e3),
+                           "p99_ms": float(np.percentile(lat[ok], 99) / 1e3), "identical_to_batched": same})
+            log(served[-1])
+        srv.stop()
+
     mean_s = statistics.mean(step_ms) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / mean_s / 1e9
@@ -381,13 +418,15 @@ def run_gpu(args):
                 "clusters": CLUSTERS, "sigma": SIGMA, "M": M, "M0": 2 * M, "ef_construction": EF_CONSTRUCTION,
                 "k": K, "ef": ef, "recall_at_10": recalls[ef], "sweep_recall": recalls, "sweep_qps": sweep_qps,
                 "plain_qps": plain_qps, "persistent_over_plain": value / world / plain_qps,
+                "per_call_qps": per_call_qps, "persistent_over_per_call": value / per_call_qps,
+                "served": served,
                 "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
                 "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush",
                 "parallelism": f"replicas x{world}", "index_build_s": build_s,
                 "layer0_distances_per_query": visit_stats,
             },
             "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 3 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
@@ -693,8 +732,9 @@ def run_serve(args):
                               filter_nbits=nb, filter_stride=words, filter_used=used[:nt], filter_ids=ids[:nt],
                               quantized=True)
     log(f"tuned: {tuned}")
-    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=4, max_pending=1 << 17, max_k=100, max_ef=512,
+    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 17, max_k=100, max_ef=512,
                    linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
+    srv.replay(queries[:5000], np.cumsum(rq.exponential(1e6 / 30_000, 5000)), ks[:5000], efs[:5000], fids[:5000])
     sweep = []
     for rate in (10_000, 30_000, 100_000, 300_000, 1_000_000):
         n = int(min(pool, max(5000, rate * 1.0)))
@@ -747,6 +787,7 @@ def main():
     ap.add_argument("--serve-n", type=int, default=10_000_000)
     ap.add_argument("--serve-batch", type=int, default=1024)
     ap.add_argument("--serve-linger", type=int, default=100)
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     if args.workload == "brute-1Mx768":
         return run_brute(args)

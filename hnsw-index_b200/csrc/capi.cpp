@@ -111,7 +111,7 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
 // Ensures the retry workspaces of a slot (visited bitmap over all nodes, heaps).
 static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
     const uint32_t warps = uint32_t(gi->num_sms) * 4;
-    const uint32_t cand_cap = std::max<uint32_t>(4096, 2 * ef_cap + 32);
+    const uint32_t cand_cap = std::max<uint32_t>(1u << 14, 4 * ef_cap);
     const uint64_t words = (uint64_t(gi->view.n) + 31) / 32 + 1;
     CU(s->g_results.ensure(size_t(warps) * (ef_cap + 1) * 8), "cudaMalloc retry results");
     CU(s->g_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc retry candidates");
@@ -132,7 +132,7 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
                           const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
                           const uint32_t* d_fids,
                           uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
-                          uint32_t out_stride, cudaStream_t stream, const SearchGeometry* force) {
+                          uint32_t out_stride, cudaStream_t stream, const SearchGeometry* force, bool publish) {
     hnsw_search_opts o = o_in;
     if (o.mode != HNSW_MODE_PLAIN && o.mode != HNSW_MODE_PERSISTENT && o.mode != HNSW_MODE_AUTO)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown search mode");
@@ -149,8 +149,13 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     }
     if (o.mode == HNSW_MODE_AUTO) o.mode = HNSW_MODE_PERSISTENT;
     if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
-    // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
-    // out by the fast and retry kernels, [4] last-resort count.
+    geo.stage_row_bytes =
+        geo.stage_rows ? ((o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4) : 0;
+    // A schedule tuned on int8 rows may not fit f32 rows.
+    if (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024)
+        geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
+    // work: [0] next query, [1] overflow count, [2] unused, [3] cold chunks
+    // handed out by the retry kernel, [4] last-resort count.
     CU(s->work.ensure(32), "cudaMalloc work counters");
     CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
     CU(s->overflow2.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
@@ -177,6 +182,7 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.out_count = d_count;
     a.out_status = d_status;
     a.out_stride = out_stride;
+    a.publish = publish ? 1 : 0;
     if (gi->counters) {
         CU(s->counters.ensure(std::max<size_t>(nq, 1) * 16), "cudaMalloc counters");
         a.counters = s->counters.as<uint32_t>();
@@ -189,22 +195,25 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
         uint32_t warps = 0;
         CU(persistent_warps(geo, gi->view.dp, gi->view.dc, gi->num_sms, &warps), "occupancy");
         const uint32_t words = ((gi->view.n + 31) / 32 + 3) & ~3u;
+        const uint32_t cand_cap = std::max<uint32_t>(8192, 4 * geo.ef_cap);
         const size_t bits_bytes = size_t(warps) * words * 4;
         if (bits_bytes > s->spill_bits.bytes) {
             CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
             CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
         }
+        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
         a.spill_bits = s->spill_bits.as<uint32_t>();
         a.spill_words = words;
+        a.spill_cands = s->spill_cands.as<uint64_t>();
+        a.spill_cand_cap = cand_cap;
         a.spill_slots = warps;
     }
-    // Cold candidate lists: a pool of 8 entries per node or 8 chunks per
-    // warp, whichever is more (1 GiB at most), shared by the persistent warps,
-    // then reused whole by the retry warps; a list never holds more entries
-    // than there are nodes.
+    // Cold candidate lists of the retry warps: a pool of 8 entries per node
+    // or 8 chunks per warp, whichever is more (1 GiB at most); a list never
+    // holds more entries than there are nodes.
     const uint32_t tab_cap = (gi->view.n + kColdChunk - 1) / kColdChunk + 2;
     {
-        const uint32_t slots = std::max(a.spill_slots, s->g_warps);
+        const uint32_t slots = s->g_warps;
         const uint64_t want = std::max<uint64_t>((uint64_t(gi->view.n) * 8 + kColdChunk - 1) / kColdChunk,
                                                  uint64_t(slots) * 8);
         const uint32_t chunks = geo.cold_chunks ? geo.cold_chunks : uint32_t(std::min<uint64_t>(want, 1u << 17));
@@ -452,7 +461,7 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     }
     const bool pow2 = sc->hash_cap >= 64 && (sc->hash_cap & (sc->hash_cap - 1)) == 0;
     if (sc->ef_cap < 32 || sc->ef_cap > 1024 || sc->ef_cap % 32 || sc->cand_cap < sc->ef_cap || !pow2 ||
-        sc->warps_per_block < 1 || sc->warps_per_block > 8)
+        sc->warps_per_block < 1 || sc->warps_per_block > 8 || sc->stage_rows > 32)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule out of range");
     SearchGeometry g;
     g.ef_cap = sc->ef_cap;
@@ -460,6 +469,7 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     g.hash_cap = sc->hash_cap;
     g.warps_per_block = sc->warps_per_block;
     g.cold_chunks = sc->cold_chunks;
+    g.stage_rows = sc->stage_rows;
     if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
     index->fixed = g;
@@ -657,6 +667,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     // entries per result slot (powers of two within 1024..32768); the
     // heuristic's own choice first. ef_cap is the bucket's bound.
     const uint32_t ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_bound, 32)));
+    const uint32_t row_bytes = (o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4;
     struct Trial {
         SearchGeometry g;
         int32_t mode;
@@ -670,18 +681,21 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         for (uint32_t per : {16u, 32u, 64u}) {
             uint32_t hc = 1024;
             while (hc < ef_cap * per && hc < 32768) hc <<= 1;
-            for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
-                SearchGeometry g;
-                g.ef_cap = ef_cap;
-                g.cand_cap = 2 * ef_cap + 32;
-                g.hash_cap = hc;
-                g.warps_per_block = wpb;
-                if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * wpb > 220 * 1024) continue;
-                if (g.hash_cap == h.hash_cap && g.cand_cap == h.cand_cap && wpb == h.warps_per_block &&
-                    g.ef_cap == h.ef_cap)
-                    continue;
-                trials.push_back({g, mode, 0, 0.0f});
-            }
+            for (uint32_t wpb : {1u, 2u, 4u, 8u})
+                for (uint32_t stage : {0u, 16u, 32u}) {
+                    SearchGeometry g;
+                    g.ef_cap = ef_cap;
+                    g.cand_cap = 2 * ef_cap + 32;
+                    g.hash_cap = hc;
+                    g.warps_per_block = wpb;
+                    g.stage_rows = stage;
+                    g.stage_row_bytes = stage ? row_bytes : 0;
+                    if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * wpb > 220 * 1024) continue;
+                    if (g.hash_cap == h.hash_cap && g.cand_cap == h.cand_cap && wpb == h.warps_per_block &&
+                        g.ef_cap == h.ef_cap && stage == h.stage_rows)
+                        continue;
+                    trials.push_back({g, mode, 0, 0.0f});
+                }
         }
     }
     std::vector<float> times(reps);
@@ -724,6 +738,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         e->schedule.hash_cap = t.g.hash_cap;
         e->schedule.warps_per_block = t.g.warps_per_block;
         e->schedule.cold_chunks = t.g.cold_chunks;
+        e->schedule.stage_rows = t.g.stage_rows;
         e->mode = t.mode;
         e->heuristic = t.heuristic;
         e->ms = t.ms;

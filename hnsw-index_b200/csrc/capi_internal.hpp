@@ -64,13 +64,13 @@ struct Slot {
     DBuf g_results, g_cands, g_visited;
     uint32_t g_warps = 0, g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_words = 0;
-    DBuf spill_bits;          // persistent-mode spill bitmaps (kept zero between queries)
+    DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
     DBuf cold_pool, cold_tab; // cold candidate lists (persistent and retry warps)
     DBuf last_pool, last_tab, overflow2;  // last-resort pass (private cold regions)
     size_t last_nq = 0;
     ~Slot() {
         for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &fids, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
-                        &g_results, &g_cands, &g_visited, &spill_bits, &cold_pool, &cold_tab, &last_pool,
+                        &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands, &cold_pool, &cold_tab, &last_pool,
                         &last_tab, &overflow2})
             b->release();
         if (stream) cudaStreamDestroy(stream);
@@ -211,7 +211,8 @@ namespace hnswgpu {
 int enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o,
                    const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
                    const uint32_t* d_fids, uint64_t* d_keys, float* d_dist, uint32_t* d_count, int32_t* d_status, uint32_t ef_max,
-                   uint32_t out_stride, cudaStream_t stream, const SearchGeometry* force = nullptr);
+                   uint32_t out_stride, cudaStream_t stream, const SearchGeometry* force = nullptr,
+                   bool publish = false);
 // The ef bucket of the tuning table for a batch whose max(ef, k) is ef_max.
 inline uint32_t tune_bucket(uint32_t ef_max) {
     return ef_max > 1024 ? 32u : std::max<uint32_t>(1, (ef_max + 31) / 32);

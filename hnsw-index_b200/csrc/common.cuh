@@ -36,6 +36,38 @@ __device__ __forceinline__ uint32_t pid(uint64_t p) { return uint32_t(p); }
 
 __device__ __forceinline__ float4 ldg_f4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
+// Row loads: read-only global path, or shared memory (rows staged by cp.async).
+template <bool SMEM>
+__device__ __forceinline__ float4 row_f4(const float* p) {
+    if (SMEM) return *reinterpret_cast<const float4*>(p);
+    return ldg_f4(p);
+}
+template <bool SMEM>
+__device__ __forceinline__ float row_f1(const float* p) {
+    if (SMEM) return *p;
+    return __ldg(p);
+}
+template <bool SMEM>
+__device__ __forceinline__ int4 row_i4(const int8_t* p) {
+    if (SMEM) return *reinterpret_cast<const int4*>(p);
+    return __ldg(reinterpret_cast<const int4*>(p));
+}
+
+// Asynchronous 16-byte (and 4-byte) copies global -> shared, completed by
+// cp_async_wait_all (a hardware wait, no spin).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Asks the memory system to bring `bytes` (multiple of 16, 16-byte aligned
 // source) into L2 without occupying registers or shared memory.
 __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
@@ -78,7 +110,7 @@ __device__ __forceinline__ float reduce_avx2_order(const float (&a)[4]) {
 // aligned, padded to a multiple of 32 floats) for this lane's group of
 // eight. Valid in lane g8 == 0 of the group. All 32 lanes must call with the
 // same `dim`.
-template <bool L2>
+template <bool L2, bool SMEM = false>
 __device__ __forceinline__ float group_sum(const float* __restrict__ row, const float* __restrict__ q, int dim,
                                            int g8) {
     float a[4] = {0.f, 0.f, 0.f, 0.f};
@@ -86,20 +118,22 @@ __device__ __forceinline__ float group_sum(const float* __restrict__ row, const 
     const float* r = row + 4 * g8;
     const float* qq = q + 4 * g8;
 #pragma unroll 4
-    for (int k = 0; k < nfull; ++k) acc4<L2>(ldg_f4(r + 32 * k), *reinterpret_cast<const float4*>(qq + 32 * k), a);
+    for (int k = 0; k < nfull; ++k)
+        acc4<L2>(row_f4<SMEM>(r + 32 * k), *reinterpret_cast<const float4*>(qq + 32 * k), a);
     // 8-wide remainder blocks go into chain 0 (lanes g8 = 0, 1).
     const int rem8 = (dim & 31) >> 3;
     if (g8 < 2)
         for (int s = 0; s < rem8; ++s)
-            acc4<L2>(ldg_f4(r + 32 * nfull + 8 * s), *reinterpret_cast<const float4*>(qq + 32 * nfull + 8 * s), a);
+            acc4<L2>(row_f4<SMEM>(r + 32 * nfull + 8 * s), *reinterpret_cast<const float4*>(qq + 32 * nfull + 8 * s),
+                     a);
     float sum = reduce_avx2_order(a);
     if (g8 == 0)
         for (int i = (nfull << 5) + (rem8 << 3); i < dim; ++i) {
             if (L2) {
-                float d = __fsub_rn(q[i], __ldg(row + i));
+                float d = __fsub_rn(q[i], row_f1<SMEM>(row + i));
                 sum = __fadd_rn(sum, __fmul_rn(d, d));
             } else {
-                sum = __fadd_rn(sum, __fmul_rn(q[i], __ldg(row + i)));
+                sum = __fadd_rn(sum, __fmul_rn(q[i], row_f1<SMEM>(row + i)));
             }
         }
     return sum;
@@ -113,12 +147,13 @@ __device__ __forceinline__ float metric_from_sum(int metric, float s) {
 // Integer dot product of an int8 code row with the query code for the
 // group of eight lanes (dc bytes, multiple of 16). Exact; valid in all lanes
 // of the group.
+template <bool SMEM = false>
 __device__ __forceinline__ int group_i8dot(const int8_t* __restrict__ row, const int8_t* __restrict__ qc, int dc,
                                            int g8) {
     int acc = 0;
     const int n16 = dc >> 4;
     for (int p = g8; p < n16; p += 8) {
-        int4 x = __ldg(reinterpret_cast<const int4*>(row) + p);
+        int4 x = row_i4<SMEM>(row + 16 * p);
         int4 y = *(reinterpret_cast<const int4*>(qc) + p);
         acc = __dp4a(x.x, y.x, acc);
         acc = __dp4a(x.y, y.y, acc);

@@ -42,6 +42,11 @@ struct SearchGeometry {
     uint32_t warps_per_block = 4;
     uint32_t bytes_per_warp = 0;
     uint32_t cold_chunks = 0;  // cold-list pool size in chunks; 0 = automatic
+    // Staged gathers: up to stage_rows fresh neighbor rows per round are
+    // copied into shared memory with cp.async before their distances are
+    // computed (0 = rows are read from global memory group by group).
+    uint32_t stage_rows = 0;
+    uint32_t stage_row_bytes = 0;  // set per launch: dc (int8 traversal) or dp * 4
 };
 
 struct SearchArgs {
@@ -76,15 +81,16 @@ struct SearchArgs {
     uint32_t* g_visited = nullptr;  // bitmap, ceil(n/32) words per warp
     uint32_t g_ef_cap = 0, g_cand_cap = 0;
     uint64_t g_visited_words = 0;
-    // Per-warp spill bitmaps of the persistent kernel (slot = global warp index).
+    // Per-warp spill areas of the persistent kernel (slot = global warp index).
     uint32_t* spill_bits = nullptr;   // spill_slots * spill_words (multiple of 4 words)
     uint32_t spill_words = 0;
+    uint64_t* spill_cands = nullptr;  // spill_slots * (spill_cand_cap + 1)
+    uint32_t spill_cand_cap = 0;
     uint32_t spill_slots = 0;
-    // Cold candidate lists: chunks of kColdChunk entries drawn from a pool by
-    // the persistent warps (slot < cold_slots) and the retry warps. Each warp
-    // records the chunks it owns in its row of `cold_tab` (cold_tab_cap ids).
-    // cold_next[0] counts the chunks handed out by the fast kernel,
-    // cold_next[1] those of the retry kernel (which reuses the whole pool).
+    // Cold candidate lists of the retry warps: chunks of kColdChunk entries
+    // drawn from a pool (warp slot < cold_slots). Each warp records the
+    // chunks it owns in its row of `cold_tab` (cold_tab_cap ids).
+    // cold_next[1] counts the chunks handed out (cold_next[0] is unused).
     uint64_t* cold_pool = nullptr;
     uint32_t cold_chunks = 0;
     uint32_t* cold_next = nullptr;
@@ -98,6 +104,10 @@ struct SearchArgs {
     uint32_t* overflow_list2 = nullptr;
     uint32_t* overflow_count2 = nullptr;
     int cold_private = 0;
+    // Outputs live in mapped host memory and each query's status is its
+    // completion flag: the status is written last, after a system-scope
+    // fence, so a host thread that sees it can read the query's results.
+    int publish = 0;
 };
 
 constexpr uint32_t kLastResortWarps = 4;

@@ -43,18 +43,29 @@ struct Ws {
     uint32_t* H;       // hash_cap entries, or a bitmap when bitmap_mode
     uint32_t* fr;      // 32: fresh neighbor positions
     float* fd;         // 32: distances of fresh neighbors
+    // Staged gathers (null stage: off): stage_rows rows of stage_row_bytes,
+    // the fresh ids in rank order, and their code norms.
+    uint8_t* stage;
+    uint32_t stage_rows, stage_row_bytes;
+    uint32_t* fi;
+    int32_t* fnorm;
     uint32_t ef_cap, cand_cap, hash_cap;
     bool bitmap_mode;  // H is a bitmap over node ids (retry kernel, or after a spill)
     uint32_t bitmap_words;
-    // Persistent warps own a spill bitmap in global memory: when the shared
-    // visited hash fills, the query continues there instead of restarting.
-    // Null in the plain and retry kernels.
+    // Persistent warps own spill areas in global memory: when the shared
+    // visited hash or candidate array fills, the query continues there
+    // instead of restarting. Null in the plain and retry kernels.
     uint32_t* spill_bits;   // bitmap over node ids (spill_words words, zero between queries)
     uint32_t spill_words;
-    uint32_t* H0;           // the shared-memory hash, restored after a spilled query
-    bool spilled_bits;
-    // Cold part of the candidate queue (persistent and retry warps; null
-    // pool in the plain kernel): an unsorted list in chunks drawn from a
+    uint64_t* spill_cands;  // spill_cand_cap + 1 entries
+    uint32_t spill_cand_cap;
+    // The shared-memory arrays, restored after a spilled query.
+    uint32_t* H0;
+    uint64_t* C0;
+    uint32_t cand_cap0;
+    bool spilled_bits, spilled_cands;
+    // Cold part of the candidate queue (retry and last-resort warps; null
+    // pool in the fast kernel): an unsorted list in chunks drawn from a
     // pool. Every entry of C is below b_min, the smallest cold entry, so C's
     // head is always the best candidate; C is refilled from the cold list
     // when it runs empty, and its upper half moves there when it fills.
@@ -155,6 +166,22 @@ __device__ __forceinline__ float group_distance(const QueryCtx& c, uint32_t id, 
     return metric_from_sum(c.metric, s);
 }
 
+// group_distance for a row staged in shared memory (`norm`: its code norm).
+__device__ __forceinline__ float staged_distance(const QueryCtx& c, const uint8_t* row, int32_t norm, int g8) {
+    const DeviceIndexView& ix = c.a->ix;
+    if (c.quant) {
+        int dot = group_i8dot<true>(reinterpret_cast<const int8_t*>(row), c.w->qc, int(ix.dc), g8);
+        long long l2 = 0;
+        if (c.metric == 0) l2 = (long long)c.qnorm + (long long)norm - 2ll * (long long)dot;
+        return sq_distance(c.metric, dot, l2, c.s2);
+    }
+    const float* r = reinterpret_cast<const float*>(row);
+    float s = c.metric == 0 ? group_sum<true, true>(r, c.w->qf, int(ix.dim), g8)
+                            : group_sum<false, true>(r, c.w->qf, int(ix.dim), g8);
+    s = __shfl_sync(kFull, s, (lane_id() & ~7));
+    return metric_from_sum(c.metric, s);
+}
+
 // Exact f32 distance (for the re-rank), valid in every lane of the group.
 __device__ __forceinline__ float group_exact(const QueryCtx& c, uint32_t id, int g8) {
     const DeviceIndexView& ix = c.a->ix;
@@ -172,9 +199,41 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
     const int lane = lane_id();
     const int g = lane >> 3, g8 = lane & 7;
     // Ranks of fresh lanes -> compact list of positions.
-    if ((F >> lane) & 1u) w.fr[__popc(F & ((1u << lane) - 1u))] = uint32_t(lane);
+    if ((F >> lane) & 1u) {
+        const uint32_t rk = __popc(F & ((1u << lane) - 1u));
+        w.fr[rk] = uint32_t(lane);
+        if (w.stage) w.fi[rk] = my_id;
+    }
     __syncwarp();
     const uint32_t nf = __popc(F);
+    if (w.stage) {
+        // All rows of a round in flight at once, one wait, then the
+        // distances from shared memory.
+        const DeviceIndexView& ix = c.a->ix;
+        const uint32_t rb = w.stage_row_bytes, cpr = rb >> 4;
+        const char* src = c.quant ? reinterpret_cast<const char*>(ix.codes) : reinterpret_cast<const char*>(ix.vec);
+        const size_t stride = c.quant ? size_t(ix.dc) : size_t(ix.dp) * 4;
+        const bool norms = c.quant && c.metric == 0;
+        for (uint32_t r0 = 0; r0 < nf; r0 += w.stage_rows) {
+            const uint32_t nr = min(w.stage_rows, nf - r0);
+            for (uint32_t t = lane; t < nr * cpr; t += 32) {
+                const uint32_t slot = t / cpr, part = t - slot * cpr;
+                cp_async16(w.stage + slot * rb + part * 16, src + size_t(w.fi[r0 + slot]) * stride + part * 16);
+            }
+            if (norms && uint32_t(lane) < nr) cp_async4(w.fnorm + lane, ix.code_norm + w.fi[r0 + lane]);
+            cp_async_wait_all();
+            __syncwarp();
+            for (uint32_t s0 = 0; s0 < nr; s0 += 4) {
+                const uint32_t slot = s0 + uint32_t(g);
+                const bool active = slot < nr;
+                const uint32_t sl = active ? slot : 0u;
+                const float d = staged_distance(c, w.stage + sl * rb, norms ? w.fnorm[sl] : 0, g8);
+                if (active && g8 == 0) w.fd[w.fr[r0 + slot]] = d;
+            }
+            __syncwarp();
+        }
+        return;
+    }
     for (uint32_t r = 0; r < nf; r += 4) {
         uint32_t slot = r + uint32_t(g);
         bool active = slot < nf;
@@ -360,6 +419,20 @@ __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail,
             keep += __popc(__ballot_sync(kFull, ok));
         }
         tail = keep;
+    }
+    if (tail + need > w.cand_cap && w.spill_cands && !w.spilled_cands && w.spill_cand_cap > w.cand_cap) {
+        // Move the queue to the warp's larger global array.
+        const uint32_t n = tail - head;
+        for (uint32_t b = 0; b < n; b += 32) {
+            const uint32_t j = b + lane;
+            if (j < n) w.spill_cands[j] = w.C[head + j];
+        }
+        __syncwarp();
+        w.C = w.spill_cands;
+        w.cand_cap = w.spill_cand_cap;
+        w.spilled_cands = true;
+        head = 0;
+        tail = n;
     }
     if (tail + need > w.cand_cap && w.pool && need <= w.cand_cap) {
         // Keep the lower half (or less, to fit `need`); the rest is larger
@@ -560,7 +633,7 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                 w.spilled_bits = true;
             }
             const bool fresh = valid && visit(w, id);
-            if (fresh) {
+            if (fresh && !w.stage) {
                 if (c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
                 else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
             }
@@ -788,8 +861,13 @@ __device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
         }
         __syncwarp();
     }
+    if (a.publish) {
+        __threadfence_system();
+        __syncwarp();
+    }
     if (lane == 0) {
         a.out_count[qi] = st == ST_OK ? count : 0u;
+        if (a.publish) __threadfence_system();
         a.out_status[qi] = st;
         if (a.counters) {
             a.counters[4 * size_t(qi) + 0] = c.cnt.dist0;
@@ -803,8 +881,8 @@ __device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
 
 __device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
 
-__device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_cap, uint32_t cand_cap,
-                      uint32_t hash_cap) {
+__device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const SearchGeometry& g) {
+    const uint32_t ef_cap = g.ef_cap, cand_cap = g.cand_cap, hash_cap = g.hash_cap;
     size_t off = 0;
     w.qf = reinterpret_cast<float*>(base + off);
     off = align_up(off + size_t(ix.dp) * 4, 16);
@@ -818,6 +896,21 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_
     off += 32 * 4;
     w.fd = reinterpret_cast<float*>(base + off);
     off += 32 * 4;
+    w.stage = nullptr;
+    w.stage_rows = 0;
+    w.stage_row_bytes = 0;
+    w.fi = nullptr;
+    w.fnorm = nullptr;
+    if (g.stage_rows) {
+        w.fi = reinterpret_cast<uint32_t*>(base + off);
+        off += 32 * 4;
+        w.fnorm = reinterpret_cast<int32_t*>(base + off);
+        off += 32 * 4;
+        w.stage = reinterpret_cast<uint8_t*>(base + off);
+        w.stage_rows = g.stage_rows;
+        w.stage_row_bytes = g.stage_row_bytes;
+        off = align_up(off + size_t(g.stage_rows) * g.stage_row_bytes, 16);
+    }
     w.H = reinterpret_cast<uint32_t*>(base + off);
     w.ef_cap = ef_cap;
     w.cand_cap = cand_cap;
@@ -826,8 +919,12 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, uint32_t ef_
     w.bitmap_words = 0;
     w.spill_bits = nullptr;
     w.spill_words = 0;
+    w.spill_cands = nullptr;
+    w.spill_cand_cap = 0;
     w.H0 = w.H;
-    w.spilled_bits = false;
+    w.C0 = w.C;
+    w.cand_cap0 = cand_cap;
+    w.spilled_bits = w.spilled_cands = false;
     w.pool = nullptr;
     w.pool_next = nullptr;
     w.pool_chunks = 0;
@@ -861,21 +958,30 @@ __device__ void end_spill(Ws& w) {
         w.bitmap_words = 0;
         w.spilled_bits = false;
     }
+    if (w.spilled_cands) {
+        w.C = w.C0;
+        w.cand_cap = w.cand_cap0;
+        w.spilled_cands = false;
+    }
 }
 
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
     Ws w;
-    carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g.ef_cap, g.cand_cap, g.hash_cap);
+    carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g);
     const int lane = lane_id();
     if (a.persistent) {
         const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
         if (a.spill_bits && slot < a.spill_slots) {
             w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;
             w.spill_words = a.spill_words;
+            w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
+            w.spill_cand_cap = a.spill_cand_cap;
         }
-        attach_cold(w, a, slot, a.cold_next);
+        // No cold list here: without it the compiler drops that code from
+        // this path (fewer live registers, measurably faster). A queue that
+        // outgrows the spill array goes to the retry pass.
         for (;;) {
             uint32_t qi = 0;
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
@@ -915,6 +1021,11 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.qc = reinterpret_cast<int8_t*>(base + align_up(size_t(ix.dp) * 4, 16));
     w.fr = reinterpret_cast<uint32_t*>(base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16));
     w.fd = reinterpret_cast<float*>(w.fr + 32);
+    w.stage = nullptr;
+    w.stage_rows = 0;
+    w.stage_row_bytes = 0;
+    w.fi = nullptr;
+    w.fnorm = nullptr;
     w.R = a.g_results + size_t(gw) * (a.g_ef_cap + 1);
     w.C = a.g_cands + size_t(gw) * (a.g_cand_cap + 1);
     w.H = a.g_visited + size_t(gw) * a.g_visited_words;
@@ -925,8 +1036,12 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.bitmap_words = uint32_t(a.g_visited_words);
     w.spill_bits = nullptr;
     w.spill_words = 0;
+    w.spill_cands = nullptr;
+    w.spill_cand_cap = 0;
     w.H0 = w.H;
-    w.spilled_bits = false;
+    w.C0 = w.C;
+    w.cand_cap0 = w.cand_cap;
+    w.spilled_bits = w.spilled_cands = false;
     w.pool = nullptr;
     w.pool_next = nullptr;
     w.pool_chunks = 0;
@@ -969,6 +1084,10 @@ uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t 
     auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
     size_t b = al(size_t(dp) * 4) + al(dc) + al(size_t(g.ef_cap + 1) * 8) + al(size_t(g.cand_cap + 1) * 8) + 256 +
                size_t(g.hash_cap) * 4;
+    if (g.stage_rows) {
+        const size_t rb = g.stage_row_bytes ? g.stage_row_bytes : size_t(dp) * 4;
+        b += 256 + al(size_t(g.stage_rows) * rb);
+    }
     return uint32_t(al(b));
 }
 

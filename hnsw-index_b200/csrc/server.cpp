@@ -9,7 +9,9 @@
 // device. When every slot is busy, requests wait on the host; when the
 // pending queue is full, submission is rejected (ADMISSION_REJECTED). A batch
 // runs the persistent search kernel with per-query k, ef and filters, so each
-// result equals the result of the same search run alone.
+// result equals the result of the same search run alone. The kernel writes
+// each query's results into mapped host memory and publishes its status last,
+// so a request completes when its own query does, not when its batch does.
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -52,11 +54,23 @@ struct BatchSlot {
     uint32_t* h_efs = nullptr;
     uint8_t* h_fused = nullptr;
     uint32_t* h_fids = nullptr;
+    // Outputs, mapped into the device address space (the kernel writes them).
     uint64_t* h_keys = nullptr;
     float* h_dist = nullptr;
     uint32_t* h_count = nullptr;
     int32_t* h_status = nullptr;
+    uint64_t* d_keys = nullptr;
+    float* d_dist = nullptr;
+    uint32_t* d_count = nullptr;
+    int32_t* d_status = nullptr;
+    std::vector<uint8_t> finished;  // per batch entry: request already completed
+    uint32_t remaining = 0;
 };
+
+// Status value of an entry whose query has not published yet.
+constexpr int32_t kUnpublished = -1;
+// Status the fast kernels write before the retry passes take a query over.
+constexpr int32_t kRetrying = HNSW_ERR_SCRATCH_OVERFLOW;
 
 }  // namespace
 
@@ -89,11 +103,14 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     const uint32_t n = uint32_t(tickets.size());
     const uint32_t dim = s->dim, K = s->cfg.max_k;
     bool any_filter = false;
+    uint32_t ef_max = 1;
     for (uint32_t i = 0; i < n; ++i) {
         Request& r = s->at(tickets[i]);
         std::memcpy(b.h_q + size_t(i) * dim, &s->q[(tickets[i] % s->cap) * dim], size_t(dim) * 4);
         b.h_ks[i] = r.k;
         b.h_efs[i] = r.ef;
+        b.h_status[i] = kUnpublished;
+        ef_max = std::max(ef_max, std::max(r.k, r.ef));
         b.h_fused[i] = r.filter_id >= 0 ? 1 : 0;
         b.h_fids[i] = r.filter_id >= 0 ? uint32_t(r.filter_id) : 0u;
         any_filter |= r.filter_id >= 0;
@@ -103,10 +120,6 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     CU(sl->q.ensure(size_t(s->cfg.max_batch) * dim * 4), "server queries");
     CU(sl->ks.ensure(size_t(s->cfg.max_batch) * 4), "server ks");
     CU(sl->efs.ensure(size_t(s->cfg.max_batch) * 4), "server efs");
-    CU(sl->okeys.ensure(size_t(s->cfg.max_batch) * K * 8), "server keys");
-    CU(sl->odist.ensure(size_t(s->cfg.max_batch) * K * 4), "server dist");
-    CU(sl->ocount.ensure(size_t(s->cfg.max_batch) * 4), "server count");
-    CU(sl->ostatus.ensure(size_t(s->cfg.max_batch) * 4), "server status");
     CU(cudaMemcpyAsync(sl->q.p, b.h_q, size_t(n) * dim * 4, cudaMemcpyHostToDevice, st), "copy queries");
     CU(cudaMemcpyAsync(sl->ks.p, b.h_ks, size_t(n) * 4, cudaMemcpyHostToDevice, st), "copy ks");
     CU(cudaMemcpyAsync(sl->efs.p, b.h_efs, size_t(n) * 4, cudaMemcpyHostToDevice, st), "copy efs");
@@ -131,34 +144,49 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     o.filter_stride = s->words;
     o.out_stride = K;
     o.mode = HNSW_MODE_AUTO;
+    b.finished.assign(n, 0);
+    b.remaining = n;
+    // Scratch sized for the batch's own largest max(ef, k).
     int r = enqueue_search(s->index, sl, sl->q.as<float>(), n, o, sl->ks.as<uint32_t>(), sl->efs.as<uint32_t>(), d_fb,
-                           d_fu, d_fi, sl->okeys.as<uint64_t>(), sl->odist.as<float>(), sl->ocount.as<uint32_t>(),
-                           sl->ostatus.as<int32_t>(), std::max(K, s->cfg.max_ef), K, st);
+                           d_fu, d_fi, b.d_keys, b.d_dist, b.d_count, b.d_status, ef_max, K, st, nullptr, true);
     if (r != HNSW_OK) return r;
-    CU(cudaMemcpyAsync(b.h_count, sl->ocount.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st), "copy counts");
-    CU(cudaMemcpyAsync(b.h_status, sl->ostatus.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
-    CU(cudaMemcpyAsync(b.h_keys, sl->okeys.p, size_t(n) * K * 8, cudaMemcpyDeviceToHost, st), "copy keys");
-    CU(cudaMemcpyAsync(b.h_dist, sl->odist.p, size_t(n) * K * 4, cudaMemcpyDeviceToHost, st), "copy distances");
     CU(cudaEventRecord(b.done, st), "record batch event");
     return HNSW_OK;
 }
 
-// Copies a finished batch's results into the request table (caller holds mu).
-void complete(hnsw_gpu_server* s, BatchSlot& b) {
-    const double t = now_us();
+// Moves entry i of a batch into the request table (caller holds mu).
+void complete_one(hnsw_gpu_server* s, BatchSlot& b, size_t i, int32_t status, double t) {
     const uint32_t K = s->cfg.max_k;
-    for (size_t i = 0; i < b.tickets.size(); ++i) {
-        Request& r = s->at(b.tickets[i]);
-        const uint64_t row = b.tickets[i] % s->cap;
-        r.status = b.h_status[i];
-        r.count = r.status == 0 ? std::min(b.h_count[i], r.k) : 0;
-        std::memcpy(&s->keys[row * K], b.h_keys + i * K, size_t(r.count) * 8);
-        std::memcpy(&s->dist[row * K], b.h_dist + i * K, size_t(r.count) * 4);
-        r.t_done = t;
-        r.state = ReqState::Done;
+    Request& r = s->at(b.tickets[i]);
+    const uint64_t row = b.tickets[i] % s->cap;
+    r.status = status;
+    r.count = status == 0 ? std::min(b.h_count[i], r.k) : 0;
+    std::memcpy(&s->keys[row * K], b.h_keys + i * K, size_t(r.count) * 8);
+    std::memcpy(&s->dist[row * K], b.h_dist + i * K, size_t(r.count) * 4);
+    r.t_done = t;
+    r.state = ReqState::Done;
+    b.finished[i] = 1;
+    --b.remaining;
+}
+
+// Completes the entries whose queries have published; with `all` (the
+// batch's event has fired) every entry. Returns whether any completed.
+bool harvest(hnsw_gpu_server* s, BatchSlot& b, bool all) {
+    const double t = now_us();
+    bool any = false;
+    for (size_t i = 0; i < b.tickets.size() && b.remaining; ++i) {
+        if (b.finished[i]) continue;
+        const int32_t st = reinterpret_cast<volatile int32_t*>(b.h_status)[i];
+        if (!all && (st == kUnpublished || st == kRetrying)) continue;
+        std::atomic_thread_fence(std::memory_order_acquire);
+        complete_one(s, b, i, st, t);
+        any = true;
     }
-    b.tickets.clear();
-    b.busy = false;
+    if (all) {
+        b.tickets.clear();
+        b.busy = false;
+    }
+    return any;
 }
 
 void dispatch_loop(hnsw_gpu_server* s) {
@@ -172,9 +200,10 @@ void dispatch_loop(hnsw_gpu_server* s) {
         for (BatchSlot& b : s->batches) {
             if (!b.busy) continue;
             if (cudaEventQuery(b.done) == cudaSuccess) {
-                complete(s, b);
+                harvest(s, b, true);
                 retired = true;
             } else {
+                retired |= harvest(s, b, false);
                 ++inflight;
             }
         }
@@ -291,10 +320,14 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
         CU(cudaMallocHost(&b.h_efs, B * 4), "pinned efs");
         CU(cudaMallocHost(&b.h_fused, B), "pinned filter flags");
         CU(cudaMallocHost(&b.h_fids, B * 4), "pinned filter ids");
-        CU(cudaMallocHost(&b.h_keys, B * cfg.max_k * 8), "pinned keys");
-        CU(cudaMallocHost(&b.h_dist, B * cfg.max_k * 4), "pinned dist");
-        CU(cudaMallocHost(&b.h_count, B * 4), "pinned counts");
-        CU(cudaMallocHost(&b.h_status, B * 4), "pinned statuses");
+        CU(cudaHostAlloc(&b.h_keys, B * cfg.max_k * 8, cudaHostAllocMapped), "mapped keys");
+        CU(cudaHostAlloc(&b.h_dist, B * cfg.max_k * 4, cudaHostAllocMapped), "mapped dist");
+        CU(cudaHostAlloc(&b.h_count, B * 4, cudaHostAllocMapped), "mapped counts");
+        CU(cudaHostAlloc(&b.h_status, B * 4, cudaHostAllocMapped), "mapped statuses");
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_keys), b.h_keys, 0), "mapped keys");
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_dist), b.h_dist, 0), "mapped dist");
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_count), b.h_count, 0), "mapped counts");
+        CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_status), b.h_status, 0), "mapped statuses");
     }
     hnsw_gpu_server* raw = s.get();
     raw->dispatcher = std::thread(dispatch_loop, raw);

@@ -170,6 +170,8 @@ typedef struct hnsw_schedule {
                                  0 = automatic (8 per node or 8 per warp). A smaller pool sends
                                  more queries to the retry and last-resort passes; results
                                  never change */
+    uint32_t stage_rows;      /* 0..32: neighbor rows gathered into shared memory per round with
+                                 cp.async before their distances (0 = read in place) */
 } hnsw_schedule;
 int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
 

@@ -427,10 +427,32 @@ def test_fixed_schedule_gives_identical_results(gaussian_10k):
     _, queries, data = gaussian_10k
     gi = H.HnswIndex.from_bytes(data)
     want = gi.search_arrays(queries[:200], 10, 64, mode=1)
-    for ef_cap, hash_cap, wpb in [(512, 32768, 1), (64, 1024, 4), (128, 4096, 2)]:
-        gi.set_schedule(ef_cap=ef_cap, hash_cap=hash_cap, warps_per_block=wpb)
+    for ef_cap, hash_cap, wpb, stage in [(512, 32768, 1, 0), (64, 1024, 4, 0), (128, 4096, 2, 0), (64, 2048, 4, 16),
+                                         (128, 4096, 2, 32), (64, 2048, 1, 5)]:
+        gi.set_schedule(ef_cap=ef_cap, hash_cap=hash_cap, warps_per_block=wpb, stage_rows=stage)
         for mode in (0, 1):
             assert_same(gi.search_arrays(queries[:200], 10, 64, mode=mode), want, f"schedule {ef_cap}/{hash_cap}")
+    gi.set_schedule()
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("dim", [7, 33, 96])
+def test_staged_gathers_match_oracle(metric, dim):
+    """Rows gathered into shared memory by cp.async: f32 and int8 traversal,
+    upper layers and layer 0, every metric, dims with scalar tails."""
+    base, queries = H.mixture(3000, 40, dim, 30, 0.5, 200 + dim)
+    if metric == 2:
+        base[:, 0] += np.where(base[:, 0] >= 0, 1.0, -1.0)
+        queries[:, 0] += 1.0
+    data = build_index(base, metric=metric, m=12, seed=3, quantize=True)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    for stage, wpb in [(32, 2), (8, 4), (3, 1)]:
+        gi.set_schedule(ef_cap=128, hash_cap=4096, warps_per_block=wpb, stage_rows=stage)
+        for quant in (False, True):
+            for mode in (0, 1):
+                got = gi.search_arrays(queries, 10, 100, quantized=quant, mode=mode)
+                assert_same(got, oi.search(queries, 10, 100, quantized=quant), f"stage {stage} quant {quant}")
     gi.set_schedule()
 
 
