@@ -7,7 +7,9 @@ from the same mixture (seed 2); L2, M=16, M0=32, efConstruction=200; k=10;
 ef swept over {16, 32, 64, 128, 256}. The headline ef is the smallest whose
 recall@10 (against exact brute force on the GPU) is >= 0.95.
 
-A step is one search_batch of the 10,000 queries. `value` is QPS with the
+A step is one search_batch of the 10,000 queries under the schedule the
+library's autotuner picked for that ef (hnsw_gpu_autotune on the first 5,000
+queries, then HNSW_MODE_AUTO). `value` is QPS with the
 queries already resident in HBM (CUDA events on the launching stream); `e2e`
 is QPS through the public host-buffer entry point (hnsw_gpu_search_batch),
 host<->device copies included. Inputs (index and vectors, ~650 MB) are far
@@ -310,17 +312,21 @@ def run_gpu(args):
             barrier()
         return [s.elapsed_time(e) for s, e in zip(starts, ends)]
 
-    # Plain (one launch per call, warp per query) vs persistent work queue.
-    sweep_qps = {}
-    for e in EF_SWEEP:
-        ms = timed(e, 1, 3, 1)
-        sweep_qps[e] = N_QUERY / (statistics.median(ms) / 1e3)
+    # Heuristic schedules: plain (warp per query, one launch) and persistent
+    # (device work queue); then the autotuned schedule per ef (AUTO mode).
     plain_ms = timed(ef, 0, max(3, args.steps // 2), 1)
     plain_qps = N_QUERY / (statistics.median(plain_ms) / 1e3)
+    pers_ms = timed(ef, 1, max(3, args.steps // 2), 1)
+    pers_qps = N_QUERY / (statistics.median(pers_ms) / 1e3)
+    sweep_qps, tuned = {}, {}
+    for e in EF_SWEEP:
+        tuned[e], _ = index.autotune(queries[:5000], K, e, reps=3)
+        ms = timed(e, 2, 3, 1)
+        sweep_qps[e] = N_QUERY / (statistics.median(ms) / 1e3)
 
     clock_path = f"/tmp/hnsw_bench_clocks_{rank}.csv"
     sampler = start_clock_sampler(local, clock_path)
-    step_ms = timed(ef, 1, args.steps, args.warmup)
+    step_ms = timed(ef, 2, args.steps, args.warmup)
     clocks = stop_clock_sampler(sampler, clock_path)
     total_ms = sum(step_ms)
     if world > 1:
@@ -334,7 +340,7 @@ def run_gpu(args):
     e2e_times = []
     for i in range(args.warmup + args.steps):
         t = time.perf_counter()
-        kk, dd, cc, ss = index.search_arrays(q_pin.numpy(), K, ef, mode=1)
+        kk, dd, cc, ss = index.search_arrays(q_pin.numpy(), K, ef, mode=2)
         if i >= args.warmup:
             e2e_times.append(time.perf_counter() - t)
     e2e_total = sum(e2e_times)
@@ -417,8 +423,9 @@ def run_gpu(args):
                 "workload": "plain-1Mx128-clustered", "n_base": N_BASE, "n_queries_per_gpu": N_QUERY, "dim": DIM,
                 "clusters": CLUSTERS, "sigma": SIGMA, "M": M, "M0": 2 * M, "ef_construction": EF_CONSTRUCTION,
                 "k": K, "ef": ef, "recall_at_10": recalls[ef], "sweep_recall": recalls, "sweep_qps": sweep_qps,
-                "plain_qps": plain_qps, "persistent_over_plain": value / world / plain_qps,
-                "per_call_qps": per_call_qps, "persistent_over_per_call": value / per_call_qps,
+                "schedule": tuned[ef], "plain_heuristic_qps": plain_qps, "persistent_heuristic_qps": pers_qps,
+                "tuned_over_plain": value / world / plain_qps,
+                "per_call_qps": per_call_qps, "tuned_over_per_call": value / per_call_qps,
                 "served": served,
                 "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
                 "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush",
@@ -637,7 +644,7 @@ def run_batch(args):
     qps, tuned_res = timed_search(index, queries, 100, 16, args.steps, mode=2, **common)
     out["autotuned_qps"] = qps
     out["tuned_equals_heuristic"] = bool(np.array_equal(tuned_res[0], res[0]) and np.array_equal(tuned_res[2], res[2]))
-    index.set_schedule(ef_cap=512, hash_cap=32768, warps_per_block=1)
+    index.set_schedule(ef_cap=512, hash_cap=16384, warps_per_block=1, cold=1)
     out["fixed_schedule_qps"], fixed_res = timed_search(index, queries, 100, 16, args.steps, mode=1, **common)
     index.set_schedule()
     out["fixed_equals_heuristic"] = bool(np.array_equal(fixed_res[0], res[0]))
@@ -646,7 +653,7 @@ def run_batch(args):
     t = time.perf_counter()
     for i in range(npc):
         index.search_arrays(queries[i:i + 1], int(ks[i]), int(efs[i]), quantized=True, filter_bits=bank[fids[i]],
-                            filter_nbits=nb)
+                            filter_nbits=nb, mode=2)
     out["per_call_qps"] = npc / (time.perf_counter() - t)
     # Recall@10 on a sample against exact filtered search (float64 scores).
     samp = 100

@@ -79,7 +79,7 @@ int cuda_fail(cudaError_t e, const char* where) {
 // Persistent warps spill to global memory instead of restarting, so their
 // visited hash is sized near the typical visit count (about 12 per unit of
 // ef on the 1M x 128 workload, p99 about 25); plain warps size it for the tail.
-SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent) {
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent, bool filtered) {
     constexpr uint32_t kSmemBudget = 220 * 1024;
     SearchGeometry g;
     g.ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_max, 32)));
@@ -103,6 +103,9 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
         }
     }
     g.warps_per_block = best_wpb;
+    // Filtered batches: admitted results fill slowly, so queues grow long;
+    // the cold-list variant keeps them in the fast kernel.
+    g.cold = persistent && filtered ? 1 : 0;
     return g;
 }
 
@@ -148,14 +151,16 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
         if (t.geo[o.mode].ef_cap) geo = t.geo[o.mode];
     }
     if (o.mode == HNSW_MODE_AUTO) o.mode = HNSW_MODE_PERSISTENT;
-    if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
+    const bool persistent = o.mode == HNSW_MODE_PERSISTENT, filtered = d_fbits != nullptr;
+    if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
     geo.stage_row_bytes =
         geo.stage_rows ? ((o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4) : 0;
     // A schedule tuned on int8 rows may not fit f32 rows.
     if (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024)
-        geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, o.mode == HNSW_MODE_PERSISTENT);
-    // work: [0] next query, [1] overflow count, [2] unused, [3] cold chunks
-    // handed out by the retry kernel, [4] last-resort count.
+        geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
+    if (!persistent) geo.cold = 0;  // cold lists need the persistent warps' chunk tables
+    // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
+    // out by the fast (cold variant) and retry kernels, [4] last-resort count.
     CU(s->work.ensure(32), "cudaMalloc work counters");
     CU(s->overflow.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
     CU(s->overflow2.ensure(std::max<size_t>(nq, 1) * 4), "cudaMalloc overflow list");
@@ -201,19 +206,22 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
             CU(s->spill_bits.ensure(bits_bytes), "cudaMalloc spill bitmaps");
             CU(cudaMemsetAsync(s->spill_bits.p, 0, s->spill_bits.bytes, stream), "memset spill bitmaps");
         }
-        CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
+        if (!geo.cold) {
+            CU(s->spill_cands.ensure(size_t(warps) * (cand_cap + 1) * 8), "cudaMalloc spill candidates");
+            a.spill_cands = s->spill_cands.as<uint64_t>();
+            a.spill_cand_cap = cand_cap;
+        }
         a.spill_bits = s->spill_bits.as<uint32_t>();
         a.spill_words = words;
-        a.spill_cands = s->spill_cands.as<uint64_t>();
-        a.spill_cand_cap = cand_cap;
         a.spill_slots = warps;
     }
-    // Cold candidate lists of the retry warps: a pool of 8 entries per node
-    // or 8 chunks per warp, whichever is more (1 GiB at most); a list never
-    // holds more entries than there are nodes.
+    // Cold candidate lists (the cold variant's persistent warps, then the
+    // retry warps, which reuse the whole pool): 8 entries per node or 8
+    // chunks per warp, whichever is more (1 GiB at most); a list never holds
+    // more entries than there are nodes.
     const uint32_t tab_cap = (gi->view.n + kColdChunk - 1) / kColdChunk + 2;
     {
-        const uint32_t slots = s->g_warps;
+        const uint32_t slots = geo.cold ? std::max(a.spill_slots, s->g_warps) : s->g_warps;
         const uint64_t want = std::max<uint64_t>((uint64_t(gi->view.n) * 8 + kColdChunk - 1) / kColdChunk,
                                                  uint64_t(slots) * 8);
         const uint32_t chunks = geo.cold_chunks ? geo.cold_chunks : uint32_t(std::min<uint64_t>(want, 1u << 17));
@@ -470,6 +478,7 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     g.warps_per_block = sc->warps_per_block;
     g.cold_chunks = sc->cold_chunks;
     g.stage_rows = sc->stage_rows;
+    g.cold = sc->cold ? 1 : 0;
     if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
     index->fixed = g;
@@ -663,11 +672,14 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         cudaEventDestroy(e[0]);
         cudaEventDestroy(e[1]);
     });
-    // The grid: both modes; warps per block 1..8; visited hash 16/32/64
-    // entries per result slot (powers of two within 1024..32768); the
-    // heuristic's own choice first. ef_cap is the bucket's bound.
+    // Coordinate descent per mode from the heuristic's choice: the
+    // cold-list variant (persistent), warps per block {1,2,4,8}, visited hash
+    // {16,32,64} entries per result slot (powers of two within 1024..32768),
+    // staged rows {0,16,32}, then warps per block again; a change is kept
+    // when it is faster. ef_cap is the bucket's bound.
     const uint32_t ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_bound, 32)));
     const uint32_t row_bytes = (o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4;
+    const bool filtered = o.filter_bits != nullptr;
     struct Trial {
         SearchGeometry g;
         int32_t mode;
@@ -675,51 +687,88 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         float ms;
     };
     std::vector<Trial> trials;
-    for (int32_t mode : {HNSW_MODE_PLAIN, HNSW_MODE_PERSISTENT}) {
-        SearchGeometry h = pick_geometry(ef_bound, gi->view.dp, gi->view.dc, mode == HNSW_MODE_PERSISTENT);
-        trials.push_back({h, mode, 1, 0.0f});
-        for (uint32_t per : {16u, 32u, 64u}) {
-            uint32_t hc = 1024;
-            while (hc < ef_cap * per && hc < 32768) hc <<= 1;
-            for (uint32_t wpb : {1u, 2u, 4u, 8u})
-                for (uint32_t stage : {0u, 16u, 32u}) {
-                    SearchGeometry g;
-                    g.ef_cap = ef_cap;
-                    g.cand_cap = 2 * ef_cap + 32;
-                    g.hash_cap = hc;
-                    g.warps_per_block = wpb;
-                    g.stage_rows = stage;
-                    g.stage_row_bytes = stage ? row_bytes : 0;
-                    if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * wpb > 220 * 1024) continue;
-                    if (g.hash_cap == h.hash_cap && g.cand_cap == h.cand_cap && wpb == h.warps_per_block &&
-                        g.ef_cap == h.ef_cap && stage == h.stage_rows)
-                        continue;
-                    trials.push_back({g, mode, 0, 0.0f});
-                }
-        }
-    }
     std::vector<float> times(reps);
-    for (Trial& t : trials) {
+    auto same = [](const SearchGeometry& x, const SearchGeometry& y) {
+        return x.ef_cap == y.ef_cap && x.cand_cap == y.cand_cap && x.hash_cap == y.hash_cap &&
+               x.warps_per_block == y.warps_per_block && x.stage_rows == y.stage_rows && x.cold == y.cold;
+    };
+    // Times one schedule; returns false on an error (status in r).
+    auto timed = [&](const SearchGeometry& g, int32_t mode, int32_t heuristic, float* ms) {
         hnsw_search_opts ot = o;
-        ot.mode = t.mode;
+        ot.mode = mode;
         auto run = [&]() {
             return enqueue_search(gi, s, s->q.as<float>(), nq, ot, sb.ks, sb.efs, sb.fbits, sb.fused, sb.fids,
                                   s->okeys.as<uint64_t>(), s->odist.as<float>(), s->ocount.as<uint32_t>(),
-                                  s->ostatus.as<int32_t>(), ef_bound, stride, st, &t.g);
+                                  s->ostatus.as<int32_t>(), ef_bound, stride, st, &g);
         };
         r = run();  // warm-up; sizes every buffer
-        if (r != HNSW_OK) return r;
+        if (r != HNSW_OK) return false;
         for (uint32_t i = 0; i < reps; ++i) {
-            CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
-            r = run();
-            if (r != HNSW_OK) return r;
-            CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
-            CU(cudaEventSynchronize(ev[1]), "autotune run");
-            CU(cudaEventElapsedTime(&times[i], ev[0], ev[1]), "cudaEventElapsedTime");
+            cudaError_t e = cudaEventRecord(ev[0], st);
+            if (e == cudaSuccess) {
+                r = run();
+                if (r != HNSW_OK) return false;
+                e = cudaEventRecord(ev[1], st);
+            }
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&times[i], ev[0], ev[1]);
+            if (e != cudaSuccess) {
+                r = cuda_fail(e, "autotune run");
+                return false;
+            }
         }
         std::vector<float> sorted = times;
         std::sort(sorted.begin(), sorted.end());
-        t.ms = sorted[reps / 2];
+        *ms = sorted[reps / 2];
+        trials.push_back({g, mode, heuristic, *ms});
+        return true;
+    };
+    for (int32_t mode : {HNSW_MODE_PLAIN, HNSW_MODE_PERSISTENT}) {
+        const bool pers = mode == HNSW_MODE_PERSISTENT;
+        SearchGeometry cur = pick_geometry(ef_bound, gi->view.dp, gi->view.dc, pers, filtered);
+        cur.stage_row_bytes = cur.stage_rows ? row_bytes : 0;
+        float best_ms = 0.0f;
+        if (!timed(cur, mode, 1, &best_ms)) return r;
+        auto consider = [&](SearchGeometry g) {
+            g.stage_row_bytes = g.stage_rows ? row_bytes : 0;
+            if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * g.warps_per_block > 220 * 1024)
+                return true;
+            for (const Trial& t : trials)
+                if (t.mode == mode && same(t.g, g)) return true;
+            float ms = 0.0f;
+            if (!timed(g, mode, 0, &ms)) return false;
+            if (ms < best_ms) {
+                best_ms = ms;
+                cur = g;
+            }
+            return true;
+        };
+        if (pers) {
+            SearchGeometry g = cur;
+            g.cold ^= 1u;
+            if (!consider(g)) return r;
+        }
+        for (int pass = 0; pass < 2; ++pass) {
+            for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
+                SearchGeometry g = cur;
+                g.warps_per_block = wpb;
+                if (!consider(g)) return r;
+            }
+            if (pass == 1) break;
+            for (uint32_t per : {16u, 32u, 64u}) {
+                uint32_t hc = 1024;
+                while (hc < ef_cap * per && hc < 32768) hc <<= 1;
+                SearchGeometry g = cur;
+                g.ef_cap = ef_cap;
+                g.hash_cap = hc;
+                if (!consider(g)) return r;
+            }
+            for (uint32_t stage : {0u, 16u, 32u}) {
+                SearchGeometry g = cur;
+                g.stage_rows = stage;
+                if (!consider(g)) return r;
+            }
+        }
     }
     const Trial* win[2] = {nullptr, nullptr};
     for (const Trial& t : trials)
@@ -739,6 +788,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         e->schedule.warps_per_block = t.g.warps_per_block;
         e->schedule.cold_chunks = t.g.cold_chunks;
         e->schedule.stage_rows = t.g.stage_rows;
+        e->schedule.cold = t.g.cold;
         e->mode = t.mode;
         e->heuristic = t.heuristic;
         e->ms = t.ms;

@@ -139,6 +139,46 @@ __device__ __forceinline__ float group_sum(const float* __restrict__ row, const 
     return sum;
 }
 
+// group_sum of two rows at once (the loads of both rows issued together, so
+// one memory round trip serves eight rows per warp). Results valid in lane
+// g8 == 0 of the group, each bit-identical to group_sum on its row.
+template <bool L2>
+__device__ __forceinline__ void group_sum2(const float* __restrict__ row0, const float* __restrict__ row1,
+                                           const float* __restrict__ q, int dim, int g8, float& s0, float& s1) {
+    float a[4] = {0.f, 0.f, 0.f, 0.f}, b[4] = {0.f, 0.f, 0.f, 0.f};
+    const int nfull = dim >> 5;
+    const float* r0 = row0 + 4 * g8;
+    const float* r1 = row1 + 4 * g8;
+    const float* qq = q + 4 * g8;
+#pragma unroll 4
+    for (int k = 0; k < nfull; ++k) {
+        const float4 x0 = ldg_f4(r0 + 32 * k), x1 = ldg_f4(r1 + 32 * k);
+        const float4 y = *reinterpret_cast<const float4*>(qq + 32 * k);
+        acc4<L2>(x0, y, a);
+        acc4<L2>(x1, y, b);
+    }
+    const int rem8 = (dim & 31) >> 3;
+    if (g8 < 2)
+        for (int s = 0; s < rem8; ++s) {
+            const float4 y = *reinterpret_cast<const float4*>(qq + 32 * nfull + 8 * s);
+            acc4<L2>(ldg_f4(r0 + 32 * nfull + 8 * s), y, a);
+            acc4<L2>(ldg_f4(r1 + 32 * nfull + 8 * s), y, b);
+        }
+    s0 = reduce_avx2_order(a);
+    s1 = reduce_avx2_order(b);
+    if (g8 == 0)
+        for (int i = (nfull << 5) + (rem8 << 3); i < dim; ++i) {
+            if (L2) {
+                const float d0 = __fsub_rn(q[i], __ldg(row0 + i)), d1 = __fsub_rn(q[i], __ldg(row1 + i));
+                s0 = __fadd_rn(s0, __fmul_rn(d0, d0));
+                s1 = __fadd_rn(s1, __fmul_rn(d1, d1));
+            } else {
+                s0 = __fadd_rn(s0, __fmul_rn(q[i], __ldg(row0 + i)));
+                s1 = __fadd_rn(s1, __fmul_rn(q[i], __ldg(row1 + i)));
+            }
+        }
+}
+
 // Metric::distance (src/metric.rs:35-41) from a raw sum.
 __device__ __forceinline__ float metric_from_sum(int metric, float s) {
     return metric == 0 ? s : (metric == 1 ? -s : __fsub_rn(1.0f, s));

@@ -47,6 +47,9 @@ struct SearchGeometry {
     // computed (0 = rows are read from global memory group by group).
     uint32_t stage_rows = 0;
     uint32_t stage_row_bytes = 0;  // set per launch: dc (int8 traversal) or dp * 4
+    // Fast-kernel variant with the cold candidate list (persistent warps
+    // move queue overflow there directly instead of to a global array).
+    uint32_t cold = 0;
 };
 
 struct SearchArgs {
@@ -87,10 +90,12 @@ struct SearchArgs {
     uint64_t* spill_cands = nullptr;  // spill_slots * (spill_cand_cap + 1)
     uint32_t spill_cand_cap = 0;
     uint32_t spill_slots = 0;
-    // Cold candidate lists of the retry warps: chunks of kColdChunk entries
-    // drawn from a pool (warp slot < cold_slots). Each warp records the
-    // chunks it owns in its row of `cold_tab` (cold_tab_cap ids).
-    // cold_next[1] counts the chunks handed out (cold_next[0] is unused).
+    // Cold candidate lists: chunks of kColdChunk entries drawn from a pool by
+    // the persistent warps of the cold variant (slot < cold_slots) and by the
+    // retry warps. Each warp records the chunks it owns in its row of
+    // `cold_tab` (cold_tab_cap ids). cold_next[0] counts the chunks handed
+    // out by the fast kernel, cold_next[1] those of the retry kernel (which
+    // reuses the whole pool).
     uint64_t* cold_pool = nullptr;
     uint32_t cold_chunks = 0;
     uint32_t* cold_next = nullptr;

@@ -234,6 +234,38 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
         }
         return;
     }
+    if (!c.quant) {
+        // f32 rows: two rows per group while at least five remain.
+        const DeviceIndexView& ix = c.a->ix;
+        uint32_t r = 0;
+        for (; r + 4 < nf; r += 8) {
+            const uint32_t sa = r + uint32_t(g), sb = r + 4 + uint32_t(g);
+            const bool aa = sa < nf, ab = sb < nf;
+            const uint32_t pa = aa ? w.fr[sa] : w.fr[0], pb = ab ? w.fr[sb] : w.fr[0];
+            const uint32_t ida = __shfl_sync(kFull, my_id, int(pa)), idb = __shfl_sync(kFull, my_id, int(pb));
+            float s0, s1;
+            if (c.metric == 0)
+                group_sum2<true>(ix.vec + size_t(ida) * ix.dp, ix.vec + size_t(idb) * ix.dp, w.qf, int(ix.dim), g8, s0,
+                                 s1);
+            else
+                group_sum2<false>(ix.vec + size_t(ida) * ix.dp, ix.vec + size_t(idb) * ix.dp, w.qf, int(ix.dim), g8,
+                                  s0, s1);
+            s0 = __shfl_sync(kFull, s0, (lane & ~7));
+            s1 = __shfl_sync(kFull, s1, (lane & ~7));
+            if (aa && g8 == 0) w.fd[pa] = metric_from_sum(c.metric, s0);
+            if (ab && g8 == 0) w.fd[pb] = metric_from_sum(c.metric, s1);
+        }
+        if (r < nf) {
+            const uint32_t slot = r + uint32_t(g);
+            const bool active = slot < nf;
+            const uint32_t pos = active ? w.fr[slot] : w.fr[0];
+            const uint32_t id = __shfl_sync(kFull, my_id, int(pos));
+            const float d = group_distance(c, id, g8);
+            if (active && g8 == 0) w.fd[pos] = d;
+        }
+        __syncwarp();
+        return;
+    }
     for (uint32_t r = 0; r < nf; r += 4) {
         uint32_t slot = r + uint32_t(g);
         bool active = slot < nf;
@@ -394,6 +426,7 @@ __device__ bool cold_append(Ws& w, uint32_t S, uint64_t x) {
 // then drops candidates worse than the worst of ef results (they can never be
 // expanded), then moves the upper part of the array to the cold list.
 // Returns false if the queue is still too small.
+template <bool COLD>
 __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail, uint32_t need, uint32_t rs,
                                           uint32_t ef) {
     if (tail + need <= w.cand_cap) return true;
@@ -434,7 +467,7 @@ __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail,
         head = 0;
         tail = n;
     }
-    if (tail + need > w.cand_cap && w.pool && need <= w.cand_cap) {
+    if (COLD && tail + need > w.cand_cap && w.pool && need <= w.cand_cap) {
         // Keep the lower half (or less, to fit `need`); the rest is larger
         // than everything kept, so the cold list's minimum stays above C.
         const uint32_t keep = min((tail - head) >> 1, w.cand_cap - need);
@@ -576,7 +609,11 @@ __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, fl
 
 // search_layer on layer 0 (src/hnsw/search.rs:81-142). Returns the number of
 // results in w.R (sorted ascending), or -1 on scratch overflow.
-__device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
+// COLD: the cold list is compiled in (retry kernels, and the fast kernel's
+// variant for batches whose queues outgrow shared memory, e.g. selective
+// filters); without it the hot loop keeps fewer registers live.
+template <bool COLD>
+__device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
     const int lane = lane_id();
@@ -602,7 +639,7 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     __syncwarp();
     for (;;) {
         if (head == tail) {
-            if (w.b_count == 0) break;
+            if (!COLD || w.b_count == 0) break;
             cold_refill(w, head, tail, rs >= ef, rs > 0 ? pdist(w.R[rs - 1]) : 0.0f);
             if (head == tail) break;
         }
@@ -688,13 +725,13 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                     if (I) {
                         // Entries above the cold minimum join the cold list.
                         uint32_t IA = I, IB = 0;
-                        if (w.b_count) {
+                        if (COLD && w.b_count) {
                             IB = I & __ballot_sync(kFull, my_x > w.b_min);
                             IA &= ~IB;
                         }
                         if (IA) {
-                            if (!make_room(w, head, tail, uint32_t(__popc(IA)), rs, ef)) return -1;
-                            if (w.b_count) {
+                            if (!make_room<COLD>(w, head, tail, uint32_t(__popc(IA)), rs, ef)) return -1;
+                            if (COLD && w.b_count) {
                                 const uint32_t mv = IA & __ballot_sync(kFull, my_x > w.b_min);
                                 IA &= ~mv;
                                 IB |= mv;
@@ -704,7 +741,7 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                                 tail += uint32_t(__popc(IA));
                             }
                         }
-                        if (IB && !cold_append(w, IB, my_x)) return -1;
+                        if (COLD && IB && !cold_append(w, IB, my_x)) return -1;
                     }
                 } else {
                     while (P) {
@@ -715,12 +752,12 @@ __device__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                         const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
                         if (!improves) continue;
                         const uint64_t x = pack(d, nid);
-                        bool cold = w.b_count != 0 && x > w.b_min;
+                        bool cold = COLD && w.b_count != 0 && x > w.b_min;
                         if (!cold) {
-                            if (!make_room(w, head, tail, 1, rs, ef)) return -1;
-                            cold = w.b_count != 0 && x > w.b_min;
+                            if (!make_room<COLD>(w, head, tail, 1, rs, ef)) return -1;
+                            cold = COLD && w.b_count != 0 && x > w.b_min;
                         }
-                        if (cold) {
+                        if (COLD && cold) {
                             if (!cold_append(w, 1u, x)) return -1;
                         } else {
                             sorted_insert(w.C, head, tail, x);
@@ -788,7 +825,8 @@ __device__ int32_t prepare(QueryCtx& c, const float* q) {
 }
 
 // One query, start to finish. Returns the status written.
-__device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
+template <bool COLD>
+__device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
     const DeviceIndexView& ix = a.ix;
     const int lane = lane_id();
     QueryCtx c;
@@ -823,7 +861,7 @@ __device__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
         c.cnt.dist_up++;
         uint64_t ep = pack(d0, ix.entry);
         for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
-        int rs = layer0(c, ep, ef);
+        int rs = layer0<COLD>(c, ep, ef);
         if (rs < 0) return ST_OVERFLOW;
         // Quantized: exact distances for the survivors (src/hnsw/mod.rs:494-498).
         if (c.quant) {
@@ -965,6 +1003,10 @@ __device__ void end_spill(Ws& w) {
     }
 }
 
+// The fast kernel. COLD = false: candidate queues spill to a per-warp global
+// array and, beyond it, to the retry pass. COLD = true: the shared array's
+// upper half moves to the cold list directly.
+template <bool COLD>
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -976,18 +1018,18 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
         if (a.spill_bits && slot < a.spill_slots) {
             w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;
             w.spill_words = a.spill_words;
-            w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
-            w.spill_cand_cap = a.spill_cand_cap;
+            if (!COLD && a.spill_cands) {
+                w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
+                w.spill_cand_cap = a.spill_cand_cap;
+            }
         }
-        // No cold list here: without it the compiler drops that code from
-        // this path (fewer live registers, measurably faster). A queue that
-        // outgrows the spill array goes to the retry pass.
+        if (COLD) attach_cold(w, a, slot, a.cold_next);
         for (;;) {
             uint32_t qi = 0;
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
             qi = __shfl_sync(kFull, qi, 0);
             if (qi >= a.nq) break;
-            const int32_t st = run_query(a, w, qi);
+            const int32_t st = run_query<COLD>(a, w, qi);
             end_spill(w);
             if (st == ST_OVERFLOW && lane == 0) {
                 a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
@@ -997,7 +1039,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     } else {
         const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
         if (qi >= a.nq) return;
-        if (run_query(a, w, qi) == ST_OVERFLOW && lane == 0) {
+        if (run_query<COLD>(a, w, qi) == ST_OVERFLOW && lane == 0) {
             a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
             a.out_status[qi] = ST_OVERFLOW;
         }
@@ -1055,7 +1097,7 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
         const uint32_t qi = a.overflow_list[t];
         // Writes ST_OVERFLOW again if even this scratch is too small; the
         // last-resort pass then takes the query.
-        if (run_query(a, w, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)
+        if (run_query<true>(a, w, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)
             a.overflow_list2[atomicAdd(a.overflow_count2, 1u)] = qi;
     }
 }
@@ -1095,13 +1137,14 @@ cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, 
     SearchGeometry geo = geo_in;
     geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
     const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
-    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    auto kern = geo.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     dim3 block(32 * geo.warps_per_block);
     dim3 grid;
     if (args.persistent) {
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::search_kernel, int(block.x), smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(block.x), smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         grid = dim3(uint32_t(num_sms * per_sm));
@@ -1111,7 +1154,7 @@ cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, 
         grid = dim3((args.nq + geo.warps_per_block - 1) / geo.warps_per_block);
     }
     if (grid.x == 0) return cudaSuccess;
-    dev::search_kernel<<<grid, block, smem, stream>>>(args, geo);
+    kern<<<grid, block, smem, stream>>>(args, geo);
     return cudaGetLastError();
 }
 
@@ -1119,10 +1162,11 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     SearchGeometry g = g_in;
     g.bytes_per_warp = geometry_bytes_per_warp(g, dp, dc);
     const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
-    cudaError_t e = cudaFuncSetAttribute(dev::search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    auto kern = g.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::search_kernel, int(32 * g.warps_per_block), smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(32 * g.warps_per_block), smem);
     if (e != cudaSuccess) return e;
     *warps = uint32_t(std::max(per_sm, 1)) * g.warps_per_block * uint32_t(num_sms);
     return cudaSuccess;

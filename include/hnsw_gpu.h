@@ -172,6 +172,9 @@ typedef struct hnsw_schedule {
                                  never change */
     uint32_t stage_rows;      /* 0..32: neighbor rows gathered into shared memory per round with
                                  cp.async before their distances (0 = read in place) */
+    uint32_t cold;            /* 1: the fast kernel's variant that keeps candidate queues of any
+                                 length (cold list), for selective filters; 0: leaner variant,
+                                 overflow goes to the retry pass */
 } hnsw_schedule;
 int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
 

@@ -405,21 +405,24 @@ def test_cold_candidate_list_under_selective_filters(mode):
     # cold_chunks=1: the shared pools run dry at once, so the queries end in
     # the last-resort pass (private regions).
     for sched in [None, dict(ef_cap=512, cand_cap=512, hash_cap=4096, warps_per_block=2),
-                  dict(ef_cap=512, cand_cap=1056, hash_cap=8192, warps_per_block=1, cold_chunks=1)]:
+                  dict(ef_cap=512, cand_cap=512, hash_cap=4096, warps_per_block=2, cold=1),
+                  dict(ef_cap=512, cand_cap=1056, hash_cap=8192, warps_per_block=1, cold_chunks=1),
+                  dict(ef_cap=512, cand_cap=1056, hash_cap=8192, warps_per_block=1, cold_chunks=1, cold=1)]:
         if sched:
             gi.set_schedule(**sched)
         got = gi.search_arrays(queries, 100, 16, filter_bits=bank, filter_nbits=nbits, filter_stride=words,
                                filter_ids=ids, ks=ks, efs=efs, mode=mode)
         assert_same(got, ref, f"schedule {sched}")
     # The smallest arrays: every few insertions move half the queue to the cold list.
-    gi.set_schedule(ef_cap=64, cand_cap=64, hash_cap=1024, warps_per_block=4)
     small = np.minimum(efs, 64).astype(np.uint32)
     ks_small = np.minimum(ks, 10).astype(np.uint32)
-    got = gi.search_arrays(queries, 10, 16, filter_bits=bank, filter_nbits=nbits, filter_stride=words,
-                           filter_ids=ids, ks=ks_small, efs=small, mode=mode)
     ref = oi.search(queries, 10, 16, filter_bits=bank[ids], filter_nbits=nbits, filter_stride=words, ks=ks_small,
                     efs=small)
-    assert_same(got, ref, "cand_cap 64")
+    for cold in (0, 1):
+        gi.set_schedule(ef_cap=64, cand_cap=64, hash_cap=1024, warps_per_block=4, cold=cold)
+        got = gi.search_arrays(queries, 10, 16, filter_bits=bank, filter_nbits=nbits, filter_stride=words,
+                               filter_ids=ids, ks=ks_small, efs=small, mode=mode)
+        assert_same(got, ref, f"cand_cap 64, cold {cold}")
     gi.set_schedule()
 
 
