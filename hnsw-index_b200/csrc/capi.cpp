@@ -216,15 +216,16 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
         a.spill_slots = warps;
     }
     // Cold candidate lists (the cold variant's persistent warps, then the
-    // retry warps, which reuse the whole pool): 8 entries per node or 8
-    // chunks per warp, whichever is more (1 GiB at most); a list never holds
-    // more entries than there are nodes.
+    // retry warps, which reuse the whole pool): 8 entries per node or 32
+    // chunks (32768 candidates) per warp, whichever is more, 2 GiB at most. A
+    // list never holds more entries than there are nodes; a query whose warp
+    // finds the pool empty moves on to the next pass.
     const uint32_t tab_cap = (gi->view.n + kColdChunk - 1) / kColdChunk + 2;
     {
         const uint32_t slots = geo.cold ? std::max(a.spill_slots, s->g_warps) : s->g_warps;
         const uint64_t want = std::max<uint64_t>((uint64_t(gi->view.n) * 8 + kColdChunk - 1) / kColdChunk,
-                                                 uint64_t(slots) * 8);
-        const uint32_t chunks = geo.cold_chunks ? geo.cold_chunks : uint32_t(std::min<uint64_t>(want, 1u << 17));
+                                                 uint64_t(slots) * 32);
+        const uint32_t chunks = geo.cold_chunks ? geo.cold_chunks : uint32_t(std::min<uint64_t>(want, 1u << 18));
         CU(s->cold_pool.ensure(size_t(chunks) * kColdChunk * 8), "cudaMalloc cold candidate pool");
         CU(s->cold_tab.ensure(size_t(slots) * tab_cap * 4), "cudaMalloc cold chunk tables");
         a.cold_pool = s->cold_pool.as<uint64_t>();

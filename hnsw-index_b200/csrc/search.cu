@@ -482,6 +482,19 @@ __device__ __forceinline__ bool make_room(Ws& w, uint32_t& head, uint32_t& tail,
     return tail + need <= w.cand_cap;
 }
 
+// Loads cold entries b + lane + 32k, k = 0..3 (b a multiple of 128, so the
+// four lie in one chunk): four independent loads in flight per lane.
+__device__ __forceinline__ void cold_load4(const Ws& w, uint32_t b, uint64_t (&v)[4], bool (&ok)[4]) {
+    const int lane = lane_id();
+    const uint64_t* base =
+        w.pool + (size_t(w.tab[b >> kColdChunkShift]) << kColdChunkShift) + (b & (kColdChunk - 1));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        ok[k] = b + uint32_t(lane + 32 * k) < w.b_count;
+        v[k] = ok[k] ? base[lane + 32 * k] : 0ull;
+    }
+}
+
 // Refills the empty candidate array from the cold list with its smallest
 // entries, in order (at least one, at most half the array). When ef results
 // exist (`full`), cold entries worse than the worst result are dropped
@@ -494,20 +507,24 @@ __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, fl
     if (full) {
         uint32_t keep = 0;
         uint64_t mn = ~0ull, mx = 0;
-        for (uint32_t b = 0; b < w.b_count; b += 32) {
-            const uint32_t j = b + lane;
-            const uint64_t v = j < w.b_count ? *cold_slot(w, j) : 0;
-            const bool ok = j < w.b_count && !(pdist(v) > worst);
-            const uint32_t K = __ballot_sync(kFull, ok);
+        for (uint32_t b = 0; b < w.b_count; b += 128) {
+            uint64_t v[4];
+            bool ok[4];
+            cold_load4(w, b, v, ok);
             __syncwarp();
-            if (ok) {
-                *cold_slot(w, keep + __popc(K & lt)) = v;
-                mn = min(mn, v);
-                mx = max(mx, v);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const bool kp = ok[k] && !(pdist(v[k]) > worst);
+                const uint32_t K = __ballot_sync(kFull, kp);
+                if (kp) {
+                    *cold_slot(w, keep + __popc(K & lt)) = v[k];
+                    mn = min(mn, v[k]);
+                    mx = max(mx, v[k]);
+                }
+                keep += __popc(K);
             }
-            keep += __popc(K);
+            __syncwarp();
         }
-        __syncwarp();
         w.b_count = keep;
         w.b_min = warp_min_u64(mn);
         w.b_max = warp_max_u64(mx);
@@ -530,12 +547,15 @@ __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, fl
             hist[lane] = 0;
             hist[lane + 32] = 0;
             __syncwarp();
-            for (uint32_t b = 0; b < w.b_count; b += 32) {
-                const uint32_t j = b + lane;
-                if (j < w.b_count) {
-                    const uint64_t v = *cold_slot(w, j);
-                    const uint64_t off = v - lo;
-                    if (v >= lo && (wbits >= 64 || (off >> wbits) == 0)) atomicAdd(&hist[uint32_t(off >> s)], 1u);
+            for (uint32_t b = 0; b < w.b_count; b += 128) {
+                uint64_t v[4];
+                bool ok[4];
+                cold_load4(w, b, v, ok);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const uint64_t off = v[k] - lo;
+                    if (ok[k] && v[k] >= lo && (wbits >= 64 || (off >> wbits) == 0))
+                        atomicAdd(&hist[uint32_t(off >> s)], 1u);
                 }
             }
             __syncwarp();
@@ -565,37 +585,43 @@ __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, fl
     // per lane; compact the others in place.
     uint64_t stage = 0, mn = ~0ull, mx = 0;
     uint32_t sn = 0, keep = 0;
-    for (uint32_t b = 0; b < w.b_count; b += 32) {
-        const uint32_t j = b + lane;
-        const bool valid = j < w.b_count;
-        const uint64_t v = valid ? *cold_slot(w, j) : 0;
-        const bool sel = valid && v < bound, kp = valid && !sel;
-        const uint32_t S = __ballot_sync(kFull, sel), K = __ballot_sync(kFull, kp);
+    for (uint32_t b = 0; b < w.b_count; b += 128) {
+        uint64_t vv[4];
+        bool okv[4];
+        cold_load4(w, b, vv, okv);
         __syncwarp();
-        if (kp) {
-            *cold_slot(w, keep + __popc(K & lt)) = v;
-            mn = min(mn, v);
-            mx = max(mx, v);
-        }
-        keep += __popc(K);
-        const uint32_t ns = __popc(S);
-        if (ns) {
-            // Lanes sn.. receive the selected entries in lane order.
-            const int r = lane - int(sn);
-            const bool take = r >= 0 && r < int(ns);
-            const uint64_t got = __shfl_sync(kFull, v, take ? nth_set(S, r) : 0);
-            if (take) stage = got;
-            const uint32_t fit = min(ns, 32u - sn);
-            sn += fit;
-            if (sn == 32) {
-                batch_merge(w.C, 0, tail, kFull, stage, w.cand_cap);
-                tail += 32;
-                const uint32_t r2 = uint32_t(lane) + fit;
-                const uint64_t rest = __shfl_sync(kFull, v, r2 < ns ? nth_set(S, int(r2)) : 0);
-                if (r2 < ns) stage = rest;
-                sn = ns - fit;
+#pragma unroll 1
+        for (int k = 0; k < 4; ++k) {
+            const uint64_t v = vv[k];
+            const bool valid = okv[k];
+            const bool sel = valid && v < bound, kp = valid && !sel;
+            const uint32_t S = __ballot_sync(kFull, sel), K = __ballot_sync(kFull, kp);
+            if (kp) {
+                *cold_slot(w, keep + __popc(K & lt)) = v;
+                mn = min(mn, v);
+                mx = max(mx, v);
+            }
+            keep += __popc(K);
+            const uint32_t ns = __popc(S);
+            if (ns) {
+                // Lanes sn.. receive the selected entries in lane order.
+                const int r = lane - int(sn);
+                const bool take = r >= 0 && r < int(ns);
+                const uint64_t got = __shfl_sync(kFull, v, take ? nth_set(S, r) : 0);
+                if (take) stage = got;
+                const uint32_t fit = min(ns, 32u - sn);
+                sn += fit;
+                if (sn == 32) {
+                    batch_merge(w.C, 0, tail, kFull, stage, w.cand_cap);
+                    tail += 32;
+                    const uint32_t r2 = uint32_t(lane) + fit;
+                    const uint64_t rest = __shfl_sync(kFull, v, r2 < ns ? nth_set(S, int(r2)) : 0);
+                    if (r2 < ns) stage = rest;
+                    sn = ns - fit;
+                }
             }
         }
+        __syncwarp();
     }
     if (sn) {
         batch_merge(w.C, 0, tail, (sn == 32 ? kFull : ((1u << sn) - 1u)), stage, w.cand_cap);
@@ -917,7 +943,18 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
     return st;
 }
 
-__device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
+__host__ __device__ __forceinline__ size_t align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
+
+// The retry kernel keeps its heaps in shared memory up to this ef capacity
+// (results + candidates: about 25 KB per warp at 1024).
+__host__ __device__ __forceinline__ bool retry_shared_heaps(uint32_t ef_cap) { return ef_cap <= 1024; }
+
+__host__ __device__ __forceinline__ size_t retry_bytes_per_warp(uint32_t dp, uint32_t dc, uint32_t ef_cap) {
+    size_t b = align_up(size_t(dp) * 4, 16) + align_up(size_t(dc), 16) + 256;
+    if (retry_shared_heaps(ef_cap))
+        b += align_up(size_t(ef_cap + 1) * 8, 16) + align_up(size_t(2 * ef_cap + 32 + 1) * 8, 16);
+    return b;
+}
 
 __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const SearchGeometry& g) {
     const uint32_t ef_cap = g.ef_cap, cand_cap = g.cand_cap, hash_cap = g.hash_cap;
@@ -1046,8 +1083,10 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     }
 }
 
-// Retry pass: each warp owns a global-memory workspace with a visited bitmap
-// over all nodes and large heaps; it takes overflowed queries in turn.
+// Retry pass: each warp owns a visited bitmap over all nodes and a cold
+// candidate list; its results and candidate arrays sit in shared memory when
+// ef fits (retry_shared_heaps) and in global memory otherwise. It takes
+// overflowed queries in turn.
 __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1055,9 +1094,10 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     const DeviceIndexView& ix = a.ix;
     Ws w;
-    // Query vectors and small buffers in shared memory; heaps and visited
-    // set in global memory.
-    size_t per = align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256;
+    // Query vectors and small buffers in shared memory, then the heaps when
+    // they fit; the visited set in global memory.
+    const bool sh = retry_shared_heaps(a.g_ef_cap);
+    const size_t per = retry_bytes_per_warp(ix.dp, ix.dc, a.g_ef_cap);
     char* base = smem + size_t(warp) * per;
     w.qf = reinterpret_cast<float*>(base);
     w.qc = reinterpret_cast<int8_t*>(base + align_up(size_t(ix.dp) * 4, 16));
@@ -1068,11 +1108,18 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.stage_row_bytes = 0;
     w.fi = nullptr;
     w.fnorm = nullptr;
-    w.R = a.g_results + size_t(gw) * (a.g_ef_cap + 1);
-    w.C = a.g_cands + size_t(gw) * (a.g_cand_cap + 1);
+    if (sh) {
+        char* heaps = base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256;
+        w.R = reinterpret_cast<uint64_t*>(heaps);
+        w.C = reinterpret_cast<uint64_t*>(heaps + align_up(size_t(a.g_ef_cap + 1) * 8, 16));
+        w.cand_cap = 2 * a.g_ef_cap + 32;
+    } else {
+        w.R = a.g_results + size_t(gw) * (a.g_ef_cap + 1);
+        w.C = a.g_cands + size_t(gw) * (a.g_cand_cap + 1);
+        w.cand_cap = a.g_cand_cap;
+    }
     w.H = a.g_visited + size_t(gw) * a.g_visited_words;
     w.ef_cap = a.g_ef_cap;
-    w.cand_cap = a.g_cand_cap;
     w.hash_cap = 0;
     w.bitmap_mode = true;
     w.bitmap_words = uint32_t(a.g_visited_words);
@@ -1174,9 +1221,7 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
 
 cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream) {
     const uint32_t wpb = 4;
-    auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
-    size_t per = al(size_t(args.ix.dp) * 4) + al(args.ix.dc) + 256;
-    size_t smem = per * wpb;
+    const size_t smem = dev::retry_bytes_per_warp(args.ix.dp, args.ix.dc, args.g_ef_cap) * wpb;
     cudaError_t e = cudaFuncSetAttribute(dev::search_retry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     dev::search_retry_kernel<<<(warps + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(args);

@@ -167,7 +167,7 @@ typedef struct hnsw_schedule {
     uint32_t hash_cap;        /* visited-hash entries, power of two */
     uint32_t warps_per_block; /* 1..8 */
     uint32_t cold_chunks;     /* pool of the queues' cold lists, in chunks of 1024 candidates;
-                                 0 = automatic (8 per node or 8 per warp). A smaller pool sends
+                                 0 = automatic (8 per node or 32 per warp). A smaller pool sends
                                  more queries to the retry and last-resort passes; results
                                  never change */
     uint32_t stage_rows;      /* 0..32: neighbor rows gathered into shared memory per round with
