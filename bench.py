@@ -763,9 +763,11 @@ def run_serve(args):
         log(sweep[-1])
     batches, launched = srv.stats()
     srv.stop()
-    best = max((s_ for s_ in sweep if s_["p99_ms"] <= 2.0), key=lambda s_: s_["achieved_qps"], default=None)
+    # Headline: the highest served rate with every request admitted; p50/p99
+    # per offered load are in config.sweep.
+    best = max((s_ for s_ in sweep if s_["rejected"] == 0), key=lambda s_: s_["achieved_qps"], default=None)
     line = {
-        "metric": "served QPS with p99 <= 2 ms (10M x 128 L2, open-loop Poisson)",
+        "metric": "served QPS with no rejections (10M x 128 L2, open-loop Poisson; p50/p99 per load in config)",
         "value": best["achieved_qps"] if best else 0.0, "unit": "queries/s", "n_gpus": 1,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s,
@@ -778,6 +780,80 @@ def run_serve(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Small single-kernel cases, sized for ncu captures (a few GB on the device at
+# most, inputs larger than L2, three launches of the kernel of interest).
+# ---------------------------------------------------------------------------
+def run_case(args):
+    import hnsw_gpu as H
+
+    rng = np.random.default_rng(3)
+    times = []
+
+    def timed_call(fn):
+        t = time.perf_counter()
+        r = fn()
+        times.append((time.perf_counter() - t) * 1e3)
+        return r
+
+    if args.workload == "case-search-1Mx128":
+        # search_kernel<0>: config 2's index and queries, ef=64.
+        base, queries = load_data()
+        data, _ = index_file(base, 0, lambda: None)
+        index = H.HnswIndex.from_bytes(data)
+        for _ in range(3):
+            r = timed_call(lambda: index.search_arrays(queries, K, 64, mode=args.case_mode))
+    elif args.workload == "case-cold-500kx96":
+        # search_kernel<1>: 500k x 96 inner product, int8 traversal, per-query
+        # filters (1-90%), uneven k/ef, persistent mode.
+        nb, nq = 500_000, 5000
+        base, queries = H.mixture_split(nb, nq, 96, 2000, 0.4, 5, 6)
+
+        def build():
+            b = H.IndexBuilder(96, H.Metric.InnerProduct, H.HnswParams(m=24, ef_construction=100, seed=0))
+            b.insert_batch(np.arange(nb, dtype=np.uint64), base)
+            b.enable_quantization()
+            return b.to_bytes()
+
+        data, _ = cached_index(f"case-cold-{nb}", build)
+        index = H.HnswIndex.from_bytes(data)
+        ks = rng.choice([1, 10, 100], nq).astype(np.uint32)
+        efs = rng.choice([16, 32, 64, 128, 256, 512], nq).astype(np.uint32)
+        words = (nb + 63) // 64
+        bank = random_bitmaps(rng, nb, np.exp(rng.uniform(np.log(0.01), np.log(0.9), 64)))
+        fids = rng.integers(0, 64, nq).astype(np.uint32)
+        for _ in range(3):
+            r = timed_call(lambda: index.search_arrays(queries, 100, 16, quantized=True, ks=ks, efs=efs,
+                                                       filter_bits=bank, filter_nbits=nb, filter_stride=words,
+                                                       filter_ids=fids, mode=1))
+    elif args.workload == "case-retry-200kx64":
+        # search_retry_kernel: a 1% filter at ef=256 in plain mode, so most
+        # queries outgrow the shared scratch and finish in the retry pass.
+        nb = 200_000
+        base, queries = H.mixture_split(nb, 2000, 64, 500, 0.4, 11, 12)
+
+        def build():
+            b = H.IndexBuilder(64, H.Metric.L2, H.HnswParams(m=16, ef_construction=100, seed=0))
+            b.insert_batch(np.arange(nb, dtype=np.uint64), base)
+            return b.to_bytes()
+
+        data, _ = cached_index(f"case-retry-{nb}", build)
+        index = H.HnswIndex.from_bytes(data)
+        bits = random_bitmaps(rng, nb, [0.01])[0]
+        for _ in range(3):
+            r = timed_call(lambda: index.search_arrays(queries, 10, 256, filter_bits=bits, filter_nbits=nb, mode=0))
+    else:  # case-brute-200kx768
+        # Brute-force kernels: 200k x 768 cosine, 1000 queries, k=100; FP32
+        # twice, then BF16x3 twice.
+        base, queries = H.mixture_split(200_000, 1000, 768, 4096, 0.5, 3, 4)
+        bf = H.BruteForceIndex(768, H.Metric.Cosine)
+        bf.insert_batch(np.arange(200_000, dtype=np.uint64), base)
+        for prec in (H.Precision.FP32, H.Precision.FP32, H.Precision.BF16X3, H.Precision.BF16X3):
+            r = timed_call(lambda: bf.search_arrays(queries, 100, prec))
+    print(json.dumps({"workload": args.workload, "host_ms_per_call": times, "results": int(r[2].sum())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -786,7 +862,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="plain-1Mx128",
-                    choices=["plain-1Mx128", "brute-1Mx768", "batch-5Mx96", "serve-10Mx128"])
+                    choices=["plain-1Mx128", "brute-1Mx768", "batch-5Mx96", "serve-10Mx128", "case-search-1Mx128",
+                             "case-cold-500kx96", "case-retry-200kx64", "case-brute-200kx768"])
+    ap.add_argument("--case-mode", type=int, default=1)
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
     ap.add_argument("--batch-n", type=int, default=5_000_000)
@@ -802,6 +880,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve-10Mx128":
         return run_serve(args)
+    if args.workload.startswith("case-"):
+        return run_case(args)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

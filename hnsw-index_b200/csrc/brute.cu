@@ -111,6 +111,15 @@ __device__ __forceinline__ int pair_of_lane(int L) {
     return (((L >> 3) & 1) << 4) | (((L >> 4) & 1) << 3) | (((L >> 2) & 1) << 2) | ((L & 1) << 1) | ((L >> 1) & 1);
 }
 
+// Whether query q admits row r under the optional filter.
+__device__ __forceinline__ bool brute_admits(const BruteArgs& a, uint32_t q, uint32_t r) {
+    if (!a.filter_bits || (a.filter_used && !a.filter_used[q])) return true;
+    const size_t sel = a.filter_ids ? size_t(a.filter_ids[q]) : size_t(q);
+    const uint64_t* bits = a.filter_bits + (a.filter_stride ? sel * a.filter_stride : 0);
+    const uint64_t bit = a.filter_by_row ? uint64_t(r) : __ldg(a.keys + r);
+    return bit < a.filter_nbits && ((__ldg(bits + (bit >> 6)) >> (bit & 63)) & 1ull);
+}
+
 template <bool L2>
 __global__ void __launch_bounds__(128) brute_score_kernel(BruteArgs a, uint32_t kk) {
     extern __shared__ __align__(16) char smem[];
@@ -197,7 +206,7 @@ __global__ void __launch_bounds__(128) brute_score_kernel(BruteArgs a, uint32_t 
         const float dist = metric_from_sum(a.metric, s);
         const uint32_t row = t0 + uint32_t(my_r);
         const uint32_t qg = q0 + uint32_t(warp * 4 + my_q);
-        const bool valid = row < r_end && qg < a.nq;
+        const bool valid = row < r_end && qg < a.nq && brute_admits(a, qg, row);
         const uint64_t cand = (uint64_t(fkey(dist)) << 32) | row;
         // Per-query top-k update (rare after warm-up).
 #pragma unroll
@@ -357,7 +366,7 @@ cudaError_t launch_brute_rerank(const BruteArgs& a, const uint64_t* cand, const 
     const uint32_t kk = std::max<uint32_t>(1, std::min<uint32_t>(a.k, a.n ? a.n : 1));
     const uint32_t wpb = 4;
     const size_t smem = size_t(wpb) * (kk + 1) * 8 + size_t(wpb) * 32 * 4;
-    cudaError_t e = cudaFuncSetAttribute(dev::brute_rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dev::brute_rerank_kernel));
     if (e != cudaSuccess) return e;
     dev::brute_rerank_kernel<<<(a.nq + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(a, cand, cand_count, cand_cap, thr2, kk);
     return cudaGetLastError();
@@ -377,11 +386,11 @@ cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream) {
     const size_t smem = (size_t(dev::kQB) + dev::kRT) * a.dp * 4 + size_t(dev::kQB) * (kk + 1) * 8;
     dim3 grid((a.nq + dev::kQB - 1) / dev::kQB, nslices);
     if (a.metric == 0) {
-        e = cudaFuncSetAttribute(dev::brute_score_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        e = raise_smem_limit(reinterpret_cast<const void*>(dev::brute_score_kernel<true>));
         if (e != cudaSuccess) return e;
         dev::brute_score_kernel<true><<<grid, 128, smem, stream>>>(a, kk);
     } else {
-        e = cudaFuncSetAttribute(dev::brute_score_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        e = raise_smem_limit(reinterpret_cast<const void*>(dev::brute_score_kernel<false>));
         if (e != cudaSuccess) return e;
         dev::brute_score_kernel<false><<<grid, 128, smem, stream>>>(a, kk);
     }

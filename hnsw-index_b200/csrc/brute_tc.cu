@@ -486,7 +486,7 @@ cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B
     a.q_tiles = qp / tc::kTileM;
     a.k_chunks = kp / tc::kTileK;
     const size_t smem = 1024 + size_t(tc::kStages) * tc::kStageBytes + 256;
-    cudaError_t e = cudaFuncSetAttribute(tc::score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(tc::score_kernel));
     if (e != cudaSuccess) return e;
     const uint32_t total = a.q_tiles * (a.n_tile_end - a.n_tile_begin);
     if (total == 0) return cudaSuccess;

@@ -89,6 +89,11 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
     while (h < want && h < 32768) h <<= 1;
     g.hash_cap = h;
     while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget && g.hash_cap > 1024) g.hash_cap >>= 1;
+    // Keep at least four warps per SM: a query that outgrows a smaller hash
+    // continues in its spill bitmap (persistent) or the retry pass (plain),
+    // which costs less than idle SMs (measured: a 64 KB hash at ef = 512 left
+    // two warps per SM).
+    while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget / 4 && g.hash_cap > 4096) g.hash_cap >>= 1;
     // Warps per block that maximise resident warps per SM.
     uint32_t best_warps = 0, best_wpb = 1;
     for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
@@ -1132,17 +1137,10 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     return HNSW_OK;
 }
 
-int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
-                                int precision, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
-                                int32_t* out_status) {
-    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
-    if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
-    if (nq == 0) return HNSW_OK;
-    if (precision < HNSW_PRECISION_FP32 || precision > HNSW_PRECISION_BF16X3)
-        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown precision");
-    if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
-    if (precision != HNSW_PRECISION_FP32 && b->n > 0 && k > 0)
-        return brute_search_tensor(b, queries, nq, k, precision, out_keys, out_dist, out_count, out_status);
+// Exact FP32 brute force (reference kernel order), optionally filtered.
+static int brute_search_fp32(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
+                             const hnsw_brute_filter* f, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                             int32_t* out_status) {
     std::lock_guard<std::mutex> lock(b->mu);
     DeviceGuard dg(b->device);
     cudaStream_t st = b->stream;
@@ -1172,6 +1170,30 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t 
     a.out_dist = b->odist.as<float>();
     a.out_count = b->ocount.as<uint32_t>();
     a.out_status = b->ostatus.as<int32_t>();
+    if (f && f->bits) {
+        const uint64_t words = (f->nbits + 63) / 64;
+        uint64_t bitmaps = f->stride ? nq : 1;
+        if (f->ids) {
+            uint32_t mx = 0;
+            for (size_t i = 0; i < nq; ++i) mx = std::max(mx, f->ids[i]);
+            bitmaps = uint64_t(mx) + 1;
+            CU(b->fids.ensure(nq * 4), "cudaMalloc filter ids");
+            CU(cudaMemcpyAsync(b->fids.p, f->ids, nq * 4, cudaMemcpyHostToDevice, st), "copy filter ids");
+            a.filter_ids = b->fids.as<uint32_t>();
+        }
+        const uint64_t total = f->stride ? f->stride * (bitmaps - 1) + words : words;
+        CU(b->fbits.ensure(total * 8), "cudaMalloc filter");
+        CU(cudaMemcpyAsync(b->fbits.p, f->bits, total * 8, cudaMemcpyHostToDevice, st), "copy filter");
+        a.filter_bits = b->fbits.as<uint64_t>();
+        a.filter_nbits = f->nbits;
+        a.filter_stride = f->stride;
+        a.filter_by_row = f->by_row;
+        if (f->used) {
+            CU(b->fused.ensure(nq), "cudaMalloc filter flags");
+            CU(cudaMemcpyAsync(b->fused.p, f->used, nq, cudaMemcpyHostToDevice, st), "copy filter flags");
+            a.filter_used = b->fused.as<uint8_t>();
+        }
+    }
     CU(launch_brute_fp32(a, st), "brute kernel");
     CU(cudaMemcpyAsync(out_count, b->ocount.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy counts");
     CU(cudaMemcpyAsync(out_status, b->ostatus.p, nq * 4, cudaMemcpyDeviceToHost, st), "copy statuses");
@@ -1183,6 +1205,34 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t 
     for (size_t i = 0; i < nq; ++i)
         if (out_status[i] != HNSW_OK) return set_error(out_status[i], "query failed validation");
     return HNSW_OK;
+}
+
+int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
+                                int precision, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
+                                int32_t* out_status) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return HNSW_OK;
+    if (precision < HNSW_PRECISION_FP32 || precision > HNSW_PRECISION_BF16X3)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
+    if (precision != HNSW_PRECISION_FP32 && b->n > 0 && k > 0)
+        return brute_search_tensor(b, queries, nq, k, precision, out_keys, out_dist, out_count, out_status);
+    return brute_search_fp32(b, queries, nq, dim, k, nullptr, out_keys, out_dist, out_count, out_status);
+}
+
+int hnsw_gpu_brute_search_filtered(hnsw_gpu_brute* b, const float* queries, size_t nq, size_t dim, uint32_t k,
+                                   const hnsw_brute_filter* filter, uint64_t* out_keys, float* out_dist,
+                                   uint32_t* out_count, int32_t* out_status) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    if (dim != b->dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    if (nq == 0) return HNSW_OK;
+    if (k > 1024) return set_error(HNSW_ERR_INVALID_ARGUMENT, "k above 1024 is not supported on the device");
+    if (filter && filter->bits && filter->nbits == 0)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "filter bitmap has no bits");
+    if (!queries || (k && (!out_keys || !out_dist)) || !out_count || !out_status)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
+    return brute_search_fp32(b, queries, nq, dim, k, filter, out_keys, out_dist, out_count, out_status);
 }
 
 int hnsw_gpu_brute_stats(const hnsw_gpu_brute* b, hnsw_brute_stats* out) {

@@ -182,6 +182,7 @@ struct hnsw_gpu_brute {
     SlotPool slots;
     std::mutex mu;
     DBuf qprep, part, okeys, odist, ocount, ostatus, q;
+    DBuf fbits, fused, fids;  // filter bitmaps, flags and bitmap ids of a filtered search
     // Tensor-core path: BF16 operand rows per term count (index 0: 1 term, 1: 3 terms).
     DBuf bop[2], xnorm2;
     uint32_t bop_kp[2] = {0, 0};
@@ -192,7 +193,8 @@ struct hnsw_gpu_brute {
     cudaStream_t stream = nullptr;
     ~hnsw_gpu_brute() {
         DeviceGuard g(device);
-        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &bop[0], &bop[1], &xnorm2,
+        for (DBuf* b : {&base, &keys, &qprep, &part, &okeys, &odist, &ocount, &ostatus, &q, &fbits, &fused, &fids,
+                        &bop[0], &bop[1], &xnorm2,
                         &aop, &dense, &thr1, &thr2, &margin, &qnorm2, &ccount, &cand, &err})
             b->release();
         for (cudaEvent_t& e : ev)

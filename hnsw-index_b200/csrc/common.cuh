@@ -9,7 +9,34 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace hnswgpu {
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum, once per (kernel, device). The limit is process-wide state, so
+// setting it to each launch's size would race with host threads launching the
+// same kernel with other sizes (a launch above the current limit fails).
+inline cudaError_t raise_smem_limit(const void* func) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({func, dev})) return cudaSuccess;
+    int optin = 0;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, func);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(fa.sharedSizeBytes));
+    if (e == cudaSuccess) done.insert({func, dev});
+    return e;
+}
 namespace dev {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;

@@ -153,6 +153,16 @@ struct BruteArgs {
     float* qprep = nullptr;         // nq * dp
     uint64_t* part = nullptr;       // nq * tiles * k partial top-k (packed dist key, row)
     uint32_t tiles = 0;
+    // Optional filter (BruteForceIndex::search_filtered): a row is scored
+    // only when its bit is set; bit = key, or row index with filter_by_row.
+    // Query q uses bitmap filter_ids[q] (or q) at filter_stride words each
+    // (stride 0: one shared bitmap), unless filter_used[q] == 0.
+    const uint64_t* filter_bits = nullptr;
+    uint64_t filter_nbits = 0;
+    uint64_t filter_stride = 0;
+    const uint8_t* filter_used = nullptr;
+    const uint32_t* filter_ids = nullptr;
+    int filter_by_row = 0;
 };
 cudaError_t launch_brute_fp32(const BruteArgs& a, cudaStream_t stream);
 // Query preparation only (vector::check, cosine normalisation) into a.qprep.

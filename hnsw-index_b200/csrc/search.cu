@@ -1185,7 +1185,7 @@ cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, 
     geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
     const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
     auto kern = geo.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
     dim3 block(32 * geo.warps_per_block);
     dim3 grid;
@@ -1210,7 +1210,7 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     g.bytes_per_warp = geometry_bytes_per_warp(g, dp, dc);
     const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
     auto kern = g.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(32 * g.warps_per_block), smem);
@@ -1222,7 +1222,7 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
 cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream) {
     const uint32_t wpb = 4;
     const size_t smem = dev::retry_bytes_per_warp(args.ix.dp, args.ix.dc, args.g_ef_cap) * wpb;
-    cudaError_t e = cudaFuncSetAttribute(dev::search_retry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dev::search_retry_kernel));
     if (e != cudaSuccess) return e;
     dev::search_retry_kernel<<<(warps + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(args);
     return cudaGetLastError();

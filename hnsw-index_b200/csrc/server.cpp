@@ -143,7 +143,7 @@ int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& ti
     o.filter_by_node = s->cfg.filter_by_node;
     o.filter_stride = s->words;
     o.out_stride = K;
-    o.mode = HNSW_MODE_AUTO;
+    o.mode = s->cfg.mode;
     b.finished.assign(n, 0);
     b.remaining = n;
     // Scratch sized for the batch's own largest max(ef, k).
@@ -277,6 +277,7 @@ void hnsw_server_config_default(hnsw_server_config* c) {
     c->quantized = 0;
     c->filter_bank = nullptr;
     c->filter_count = 0;
+    c->mode = HNSW_MODE_PERSISTENT;
 }
 
 int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_in, hnsw_gpu_server** out) {
@@ -286,7 +287,8 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
     if (cfg_in) cfg = *cfg_in;
     else hnsw_server_config_default(&cfg);
     if (cfg.max_batch == 0 || cfg.max_inflight == 0 || cfg.max_pending == 0 || cfg.max_k == 0 || cfg.max_ef == 0 ||
-        cfg.max_batch > (1u << 20) || cfg.max_inflight > 64 || cfg.max_k > 1024 || cfg.max_ef > 65536)
+        cfg.max_batch > (1u << 20) || cfg.max_inflight > 64 || cfg.max_k > 1024 || cfg.max_ef > 65536 ||
+        (cfg.mode != HNSW_MODE_PLAIN && cfg.mode != HNSW_MODE_PERSISTENT && cfg.mode != HNSW_MODE_AUTO))
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "server configuration out of range");
     if (cfg.quantized && !index->view.quantized)
         return set_error(HNSW_ERR_QUANTIZATION_DISABLED, "quantized search requested but quantization is not enabled");

@@ -189,6 +189,15 @@ class _BruteStats(C.Structure):
 
 
 _lib.hnsw_gpu_brute_stats.argtypes = [_vp, C.POINTER(_BruteStats)]
+
+
+class _BruteFilter(C.Structure):
+    _fields_ = [("bits", C.c_void_p), ("nbits", C.c_uint64), ("stride", C.c_uint64), ("used", C.c_void_p),
+                ("ids", C.c_void_p), ("by_row", C.c_int32)]
+
+
+_lib.hnsw_gpu_brute_search_filtered.argtypes = [_vp, _vp, _sz, _sz, C.c_uint32, C.POINTER(_BruteFilter), _vp, _vp,
+                                                _vp, _vp]
 _lib.hnsw_params_default.argtypes = [C.c_uint32, C.POINTER(_Params)]
 _lib.hnsw_params_default.restype = None
 _lib.hnsw_builder_new.argtypes = [_sz, C.c_int, C.POINTER(_Params), C.POINTER(_vp)]
@@ -219,7 +228,7 @@ EXPORTED_SYMBOLS = (
     "hnsw_builder_insert_batch", "hnsw_builder_remove", "hnsw_builder_enable_quantization",
     "hnsw_builder_to_bytes", "hnsw_bytes_free", "hnsw_synthetic_gaussian",
     "hnsw_synthetic_mixture", "hnsw_synthetic_mixture_split", "hnsw_crc32", "hnsw_gpu_autotune",
-    "hnsw_gpu_clear_tuning", "hnsw_gpu_set_schedule",
+    "hnsw_gpu_clear_tuning", "hnsw_gpu_set_schedule", "hnsw_gpu_brute_search_filtered",
 )
 
 LIBRARY_PATH = _LIB_PATH
@@ -572,7 +581,7 @@ class _ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
                 ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
                 ("filter_nbits", C.c_uint64), ("quantized", C.c_int32), ("filter_bank", C.c_void_p),
-                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32)]
+                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32), ("mode", C.c_int32)]
 
 
 _lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
@@ -593,13 +602,14 @@ class Server:
 
     def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
                  max_ef=512, linger_us=100, filter_nbits=0, filter_bank: Optional[np.ndarray] = None,
-                 quantized=False, filter_by_node=False):
+                 quantized=False, filter_by_node=False, mode=1):
         cfg = _ServerConfig()
         _lib.hnsw_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
         cfg.max_k, cfg.max_ef, cfg.linger_us = max_k, max_ef, linger_us
         cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
         cfg.filter_by_node = int(filter_by_node)
+        cfg.mode = int(mode)
         bank = None if filter_bank is None else np.ascontiguousarray(filter_bank, np.uint64)
         if bank is not None:
             cfg.filter_bank = _ptr(bank)
@@ -739,7 +749,12 @@ class BruteForceIndex:
     def len(self):
         return int(self._keys.size)
 
-    def search_arrays(self, queries, k: int, precision: Precision = Precision.FP32, raise_on_error=True):
+    def search_arrays(self, queries, k: int, precision: Precision = Precision.FP32, raise_on_error=True, *,
+                      filter_bits=None, filter_nbits: int = 0, filter_stride: int = 0, filter_used=None,
+                      filter_ids=None, filter_by_row: bool = False):
+        """Batched exact search returning arrays (keys, dist, count, status).
+        With filter_bits, hnsw_gpu_brute_search_filtered (FP32, any precision
+        argument notwithstanding)."""
         q = np.ascontiguousarray(queries, dtype=np.float32)
         if q.ndim == 1:
             q = q.reshape(-1, self._dim)
@@ -751,11 +766,34 @@ class BruteForceIndex:
         status = np.zeros(nq, np.int32)
         if self._h is None:
             self.insert_batch(np.zeros(0, np.uint64), np.zeros((0, self._dim), np.float32))
-        st = _lib.hnsw_gpu_brute_search_batch(self._h, _ptr(q), nq, q.shape[1], int(k), int(precision),
-                                              _ptr(keys), _ptr(dist), _ptr(count), _ptr(status))
+        if filter_bits is not None:
+            fb = np.ascontiguousarray(filter_bits, np.uint64)
+            fu = None if filter_used is None else np.ascontiguousarray(filter_used, np.uint8)
+            fi = None if filter_ids is None else np.ascontiguousarray(filter_ids, np.uint32)
+            f = _BruteFilter(_ptr(fb), filter_nbits, filter_stride, _ptr(fu), _ptr(fi), int(filter_by_row))
+            st = _lib.hnsw_gpu_brute_search_filtered(self._h, _ptr(q), nq, q.shape[1], int(k), C.byref(f), _ptr(keys),
+                                                     _ptr(dist), _ptr(count), _ptr(status))
+        else:
+            st = _lib.hnsw_gpu_brute_search_batch(self._h, _ptr(q), nq, q.shape[1], int(k), int(precision),
+                                                  _ptr(keys), _ptr(dist), _ptr(count), _ptr(status))
         if st != 0 and raise_on_error:
             _raise(st)
         return keys, dist, count, status
+
+    def search_filtered(self, query, k: int, filter):
+        """BruteForceIndex::search_filtered (src/brute.rs:131-160). `filter` is a
+        closure over keys (run once per row on the calling thread) or a key
+        bitmap (uint64 words)."""
+        if callable(filter):
+            accepted = np.fromiter((i for i, key in enumerate(self._keys.tolist()) if filter(key)), dtype=np.uint64)
+            nbits = max(int(self._keys.size), 1)
+            bits, by_row = key_bitmap(accepted, nbits), True
+        else:
+            bits = np.ascontiguousarray(filter, np.uint64)
+            nbits, by_row = bits.size * 64, False
+        keys, dist, count, _ = self.search_arrays(np.asarray(query, np.float32).reshape(1, -1), k,
+                                                  filter_bits=bits, filter_nbits=nbits, filter_by_row=by_row)
+        return [Neighbor(int(keys[0, j]), float(dist[0, j])) for j in range(int(count[0]))]
 
     def last_stats(self) -> dict:
         """Candidates and device stage times of the last tensor-core search."""

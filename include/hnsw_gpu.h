@@ -232,6 +232,8 @@ typedef struct hnsw_server_config {
                                     copied to the device at start */
     uint32_t filter_count;
     int32_t filter_by_node; /* the bank's bitmaps are indexed by node id, not key */
+    int32_t mode;           /* HNSW_MODE_* of the batches; default PERSISTENT (the device work queue
+                               spreads a small batch's queries over every SM); AUTO uses the tuned mode */
 } hnsw_server_config;
 
 void hnsw_server_config_default(hnsw_server_config* cfg);
@@ -288,6 +290,26 @@ int hnsw_gpu_brute_search_batch(hnsw_gpu_brute* brute, const float* queries, siz
 
 /* Counters of the last tensor-core search on this handle: candidates kept
  * by the scoring threshold, summed over the batch's queries. */
+/* BruteForceIndex::search_filtered (src/brute.rs:131-160): the exact top-k
+ * among the rows a filter admits, computed in FP32 in the reference kernel
+ * order (bit-identical to the reference). A row is admitted when its bit is
+ * set: bit = key (keys below nbits), or the row's index in insertion order
+ * with by_row (any u64 key set). One shared bitmap (stride 0), one per query
+ * (stride words apart), or a bank selected per query by ids; used[q] == 0
+ * turns the filter off for query q. k is capped at the index size, as in the
+ * reference, and a query returns fewer results when fewer rows pass. */
+typedef struct hnsw_brute_filter {
+    const uint64_t* bits;
+    uint64_t nbits;
+    uint64_t stride;
+    const uint8_t* used;
+    const uint32_t* ids;
+    int32_t by_row;
+} hnsw_brute_filter;
+int hnsw_gpu_brute_search_filtered(hnsw_gpu_brute* brute, const float* queries, size_t nq, size_t dim, uint32_t k,
+                                   const hnsw_brute_filter* filter, uint64_t* out_keys, float* out_dist,
+                                   uint32_t* out_count, int32_t* out_status);
+
 typedef struct hnsw_brute_stats {
     uint64_t candidates;
     uint64_t queries;

@@ -685,19 +685,30 @@ void orc_search_batch(void* handle, const float* queries, size_t nq, size_t k, c
 // BruteForceIndex::search_filtered / search_batch (src/brute.rs:122-180) over
 // rows already prepared (unit length for cosine, src/vector.rs:50-66): a
 // bounded max-heap of (total_cmp distance, key), into_sorted_vec ascending.
-void orc_brute_batch(int metric, const float* base, const uint64_t* keys, size_t nb, size_t dim,
-                     const float* queries, size_t nq, size_t k, uint64_t* out_keys, float* out_dist,
-                     uint32_t* counts, int32_t* status, int threads) {
+// With `filter_bits`, a row is scored only when its bit is set (bit = key, or
+// row index with by_row): query i uses filter_bits + i * filter_stride words
+// (stride 0: one shared bitmap), as search_filtered's closure does.
+void orc_brute_filtered(int metric, const float* base, const uint64_t* keys, size_t nb, size_t dim,
+                        const float* queries, size_t nq, size_t k, const uint64_t* filter_bits, uint64_t filter_nbits,
+                        size_t filter_stride, int by_row, uint64_t* out_keys, float* out_dist, uint32_t* counts,
+                        int32_t* status, int threads) {
     parallel_for(nq, threads, [&](int, size_t i) {
         std::vector<float> q(dim);
         status[i] = prepare_query(metric, queries + i * dim, dim, q.data());
         counts[i] = 0;
         if (status[i] != OK || k == 0) return;
+        // At most `len` results, whatever k asks for (src/brute.rs:141-142).
         size_t kk = std::min(k, nb);
         auto less = [](const Hit& a, const Hit& b) { return hit_less(a, b); };
         std::priority_queue<Hit, std::vector<Hit>, decltype(less)> heap(less);
+        const uint64_t* fb = filter_bits ? filter_bits + i * filter_stride : nullptr;
         for (size_t r = 0; r < nb; ++r) {
-            Hit h{keys ? keys[r] : uint64_t(r), metric_distance(metric, q.data(), base + r * dim, dim)};
+            const uint64_t key = keys ? keys[r] : uint64_t(r);
+            if (fb) {
+                const uint64_t bit = by_row ? uint64_t(r) : key;
+                if (bit >= filter_nbits || !((fb[bit >> 6] >> (bit & 63)) & 1)) continue;
+            }
+            Hit h{key, metric_distance(metric, q.data(), base + r * dim, dim)};
             if (heap.size() < kk) heap.push(h);
             else if (hit_less(h, heap.top())) {
                 heap.pop();
@@ -712,6 +723,13 @@ void orc_brute_batch(int metric, const float* base, const uint64_t* keys, size_t
             heap.pop();
         }
     });
+}
+
+void orc_brute_batch(int metric, const float* base, const uint64_t* keys, size_t nb, size_t dim,
+                     const float* queries, size_t nq, size_t k, uint64_t* out_keys, float* out_dist,
+                     uint32_t* counts, int32_t* status, int threads) {
+    orc_brute_filtered(metric, base, keys, nb, dim, queries, nq, k, nullptr, 0, 0, 0, out_keys, out_dist, counts,
+                       status, threads);
 }
 
 // Double-precision scoring for the precision study of brute force: exact

@@ -53,6 +53,8 @@ for name, res, args in [
     ("orc_search_batch", None, [_vp, _vp, _sz, _sz, _vp, _sz, _vp, C.c_int, _vp, C.c_uint64, _sz, _vp,
                                 _vp, _vp, _vp, _vp, _vp, C.c_int, _sz, C.c_int]),
     ("orc_brute_batch", None, [C.c_int, _vp, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _vp, _vp, _vp, C.c_int]),
+    ("orc_brute_filtered", None, [C.c_int, _vp, _vp, _sz, _sz, _vp, _sz, _sz, _vp, C.c_uint64, _sz, C.c_int, _vp,
+                                  _vp, _vp, _vp, C.c_int]),
     ("orc_brute_f64", None, [C.c_int, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _vp, C.c_int]),
     ("orc_recall_at_k", C.c_double, [_vp, _vp, _sz, _vp, _vp, _sz, _sz, _sz]),
 ]:
@@ -208,6 +210,25 @@ def brute(metric: int, base, queries, k: int, keys=None, threads=0):
     ka = None if keys is None else np.ascontiguousarray(keys, np.uint64)
     _lib.orc_brute_batch(int(metric), _p(base), _p(ka), nb, dim, _p(q), nq, k, _p(ok), _p(od), _p(oc), _p(os_),
                          threads)
+    return ok, od, oc, os_
+
+
+def brute_filtered(metric: int, base, queries, k: int, filter_bits, filter_nbits: int, filter_stride: int = 0,
+                   by_row: bool = False, keys=None, threads=0):
+    """BruteForceIndex::search_filtered (src/brute.rs:131-160) with a bitmap for the closure."""
+    base = _f32(base)
+    q = _f32(queries)
+    nb, dim = base.shape
+    nq = q.shape[0]
+    kk = max(k, 1)
+    ok = np.zeros((nq, kk), np.uint64)
+    od = np.zeros((nq, kk), np.float32)
+    oc = np.zeros(nq, np.uint32)
+    os_ = np.zeros(nq, np.int32)
+    ka = None if keys is None else np.ascontiguousarray(keys, np.uint64)
+    fb = np.ascontiguousarray(filter_bits, np.uint64)
+    _lib.orc_brute_filtered(int(metric), _p(base), _p(ka), nb, dim, _p(q), nq, k, _p(fb), filter_nbits, filter_stride,
+                            int(by_row), _p(ok), _p(od), _p(oc), _p(os_), threads)
     return ok, od, oc, os_
 
 
