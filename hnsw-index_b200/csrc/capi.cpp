@@ -257,6 +257,12 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     }
     a.overflow_list2 = s->overflow2.as<uint32_t>();
     a.overflow_count2 = s->work.as<uint32_t>() + 4;
+    if (o.exact_below > 0.0f && d_fbits) {
+        CU(s->planned.ensure(std::max<size_t>(nq, 1)), "cudaMalloc planner flags");
+        a.plan_max = uint32_t(std::max(1.0, std::floor(double(o.exact_below) * double(gi->view.live))));
+        CU(launch_plan(a, s->planned.as<uint8_t>(), stream), "planner kernel");
+        a.planned = s->planned.as<uint8_t>();
+    }
     CU(launch_search(a, geo, gi->num_sms, stream), "search kernel");
     CU(launch_search_retry(a, s->g_warps, stream), "search retry kernel");
     SearchArgs last = a;

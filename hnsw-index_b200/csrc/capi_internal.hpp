@@ -67,11 +67,12 @@ struct Slot {
     DBuf spill_bits, spill_cands;  // persistent-mode spill areas (bitmaps kept zero)
     DBuf cold_pool, cold_tab; // cold candidate lists (persistent and retry warps)
     DBuf last_pool, last_tab, overflow2;  // last-resort pass (private cold regions)
+    DBuf planned;                         // selectivity planner flags
     size_t last_nq = 0;
     ~Slot() {
         for (DBuf* b : {&q, &ks, &efs, &fbits, &fused, &fids, &okeys, &odist, &ocount, &ostatus, &work, &overflow, &counters,
                         &g_results, &g_cands, &g_visited, &spill_bits, &spill_cands, &cold_pool, &cold_tab, &last_pool,
-                        &last_tab, &overflow2})
+                        &last_tab, &overflow2, &planned})
             b->release();
         if (stream) cudaStreamDestroy(stream);
     }

@@ -109,6 +109,10 @@ struct SearchArgs {
     uint32_t* overflow_list2 = nullptr;
     uint32_t* overflow_count2 = nullptr;
     int cold_private = 0;
+    // Selectivity planner: planned[q] != 0 sends query q to the exact scan
+    // of its admitted nodes; plan_max is the admitted-count bound.
+    const uint8_t* planned = nullptr;
+    uint32_t plan_max = 0;
     // Outputs live in mapped host memory and each query's status is its
     // completion flag: the status is written last, after a system-scope
     // fence, so a host thread that sees it can read the query's results.
@@ -123,6 +127,9 @@ constexpr uint32_t kColdChunk = 1u << kColdChunkShift;  // entries per cold chun
 // Launches the fast search (plain or persistent) followed by the retry pass
 // for queries that overflowed. All on `stream`.
 cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo, int num_sms, cudaStream_t stream);
+// Selectivity planner: sets planned[q] when query q's filter admits at most
+// args.plan_max nodes (counting stops early past the bound).
+cudaError_t launch_plan(const SearchArgs& args, uint8_t* planned, cudaStream_t stream);
 // Retry pass only (global-memory scratch); `warps` warps.
 cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStream_t stream);
 // Scratch bytes per warp of a geometry for dimension dp (floats) / dc (bytes).

@@ -803,6 +803,50 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     return int(rs);
 }
 
+// Exact scan of the nodes a selective filter admits (the planner's route,
+// advised by src/hnsw/mod.rs:421-425): every admitted live node gets its f32
+// distance in the reference kernel order, and the best ef by (distance, id)
+// stay in w.R; the caller sorts them by (distance, key). Returns the count.
+__device__ int exact_scan(QueryCtx& c, uint32_t ef) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    c.quant = false;             // exact rows, not codes
+    uint8_t* stage = w.stage;    // staged gathers are sized for the request's rows
+    w.stage = nullptr;
+    uint32_t rs = 0;
+    const uint64_t nb = min(c.fnbits, uint64_t(ix.n));
+    const uint32_t nwords = uint32_t((nb + 63) / 64);
+    for (uint32_t w0 = 0; w0 < nwords; w0 += 32) {
+        const uint32_t wi = w0 + uint32_t(lane);
+        uint64_t word = wi < nwords ? __ldg(c.fbits + wi) : 0ull;
+        if (wi + 1 == nwords && (nb & 63)) word &= (1ull << (nb & 63)) - 1ull;
+        while (__any_sync(kFull, word != 0)) {
+            bool has = word != 0;
+            uint32_t id = 0;
+            if (has) {
+                id = wi * 64u + uint32_t(__ffsll(static_cast<long long>(word)) - 1);
+                word &= word - 1ull;
+            }
+            has = has && !(ix.has_dead && ((__ldg(ix.dead + (id >> 5)) >> (id & 31)) & 1u));
+            const uint32_t F = __ballot_sync(kFull, has);
+            if (F == 0) continue;
+            chunk_distances(c, id, F);
+            c.cnt.dist0 += __popc(F);
+            const float my_d = has ? w.fd[lane] : 0.0f;
+            const uint64_t my_x = pack(my_d, id);
+            const uint64_t worst = rs >= ef ? w.R[rs - 1] : ~0ull;
+            const uint32_t P = __ballot_sync(kFull, has && my_x < worst);
+            if (P) {
+                batch_merge(w.R, 0, rs, P, my_x, ef);
+                rs = min(rs + uint32_t(__popc(P)), ef);
+            }
+        }
+    }
+    w.stage = stage;
+    return int(rs);
+}
+
 // Prepares the query (vector::check + normalisation, src/vector.rs:22-45,
 // 90-104; and the int8 code, src/quantization.rs:73-81) into the workspace.
 // Returns a status.
@@ -878,17 +922,22 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
     if (st == ST_OK && k != 0 && ix.live != 0 && ix.entry != kEmpty) {
         ef = max(ef, k);
         if (ef > w.ef_cap) return ST_OVERFLOW;
-        // search_graph (src/hnsw/search.rs:146-161)
-        float d0;
-        {
-            const int g8 = lane & 7;
-            d0 = group_distance(c, ix.entry, g8);
+        int rs;
+        if (a.planned && a.planned[qi]) {
+            rs = exact_scan(c, ef);
+        } else {
+            // search_graph (src/hnsw/search.rs:146-161)
+            float d0;
+            {
+                const int g8 = lane & 7;
+                d0 = group_distance(c, ix.entry, g8);
+            }
+            c.cnt.dist_up++;
+            uint64_t ep = pack(d0, ix.entry);
+            for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
+            rs = layer0<COLD>(c, ep, ef);
+            if (rs < 0) return ST_OVERFLOW;
         }
-        c.cnt.dist_up++;
-        uint64_t ep = pack(d0, ix.entry);
-        for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
-        int rs = layer0<COLD>(c, ep, ef);
-        if (rs < 0) return ST_OVERFLOW;
         // Quantized: exact distances for the survivors (src/hnsw/mod.rs:494-498).
         if (c.quant) {
             const int g = lane >> 3, g8 = lane & 7;
@@ -1149,6 +1198,33 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     }
 }
 
+// One warp per query: whether its filter admits at most a.plan_max nodes.
+__global__ void plan_kernel(SearchArgs a, uint8_t* planned) {
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const DeviceIndexView& ix = a.ix;
+    for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < a.nq; qi += warps) {
+        const bool use = a.filter_bits != nullptr && (a.filter_used == nullptr || a.filter_used[qi] != 0) &&
+                         (ix.keys_are_ids || a.filter_by_node);
+        bool plan = false;
+        if (use) {
+            const size_t fsel = a.filter_ids ? size_t(a.filter_ids[qi]) : size_t(qi);
+            const uint64_t* bits = a.filter_bits + (a.filter_stride ? fsel * a.filter_stride : 0);
+            const uint64_t nb = min(a.filter_nbits, uint64_t(ix.n));
+            const uint32_t nwords = uint32_t((nb + 63) / 64);
+            uint32_t count = 0;
+            for (uint32_t w0 = 0; w0 < nwords && count <= a.plan_max; w0 += 32) {
+                const uint32_t wi = w0 + uint32_t(lane);
+                uint64_t word = wi < nwords ? __ldg(bits + wi) : 0ull;
+                if (wi + 1 == nwords && (nb & 63)) word &= (1ull << (nb & 63)) - 1ull;
+                count += __reduce_add_sync(kFull, uint32_t(__popcll(static_cast<long long>(word))));
+            }
+            plan = count <= a.plan_max;
+        }
+        if (lane == 0) planned[qi] = plan ? 1 : 0;
+    }
+}
+
 __global__ void encode_codes_kernel(const float* __restrict__ vec, uint32_t n, uint32_t dim, uint32_t dp,
                                     uint32_t dc, const float* __restrict__ offset, float scale,
                                     int8_t* __restrict__ codes, int32_t* __restrict__ norms) {
@@ -1225,6 +1301,13 @@ cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStre
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dev::search_retry_kernel));
     if (e != cudaSuccess) return e;
     dev::search_retry_kernel<<<(warps + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plan(const SearchArgs& args, uint8_t* planned, cudaStream_t stream) {
+    if (args.nq == 0) return cudaSuccess;
+    const uint32_t blocks = std::min<uint32_t>(148u * 8u, (args.nq * 32u + 255u) / 256u);
+    dev::plan_kernel<<<blocks, 256, 0, stream>>>(args, planned);
     return cudaGetLastError();
 }
 

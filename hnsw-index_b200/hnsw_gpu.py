@@ -131,6 +131,7 @@ class _Opts(C.Structure):
         ("quantized", C.c_int32), ("filter_bits", C.c_void_p), ("filter_nbits", C.c_uint64),
         ("filter_stride", C.c_uint64), ("filter_used", C.c_void_p), ("out_stride", C.c_uint32),
         ("mode", C.c_int32), ("filter_ids", C.c_void_p), ("filter_by_node", C.c_int32),
+        ("exact_below", C.c_float),
     ]
 
 
@@ -414,7 +415,7 @@ class HnswIndex:
 
     @staticmethod
     def _opts(nq, k, ef, quantized=False, filter_bits=None, filter_nbits=0, filter_stride=0, filter_used=None,
-              ks=None, efs=None, mode=0, filter_ids=None, filter_by_node=False):
+              ks=None, efs=None, mode=0, filter_ids=None, filter_by_node=False, exact_below=0.0):
         """hnsw_search_opts for a batch, and the arrays it points into (keep them alive)."""
         ks_a = None if ks is None else np.ascontiguousarray(ks, dtype=np.uint32)
         efs_a = None if efs is None else np.ascontiguousarray(efs, dtype=np.uint32)
@@ -432,6 +433,7 @@ class HnswIndex:
         fi = None if filter_ids is None else np.ascontiguousarray(filter_ids, dtype=np.uint32)
         o.filter_ids = _ptr(fi)
         o.filter_by_node = int(filter_by_node)
+        o.exact_below = float(exact_below)
         o.out_stride = max(kmax, 1)
         o.mode = mode
         return o, (ks_a, efs_a, fb, fu, fi)
@@ -441,8 +443,9 @@ class HnswIndex:
                       filter_stride: int = 0, filter_used: Optional[np.ndarray] = None,
                       ks: Optional[np.ndarray] = None, efs: Optional[np.ndarray] = None,
                       mode: int = 0, raise_on_error: bool = True, filter_ids: Optional[np.ndarray] = None,
-                      filter_by_node: bool = False):
-        """Batched search returning arrays (keys, dist, count, status)."""
+                      filter_by_node: bool = False, exact_below: float = 0.0):
+        """Batched search returning arrays (keys, dist, count, status).
+        exact_below > 0 turns on the selectivity planner (hnsw_search_opts)."""
         q = np.ascontiguousarray(queries, dtype=np.float32)
         if q.ndim == 1:
             if q.size % max(self.dim(), 1):
@@ -452,7 +455,7 @@ class HnswIndex:
         nq, dim = q.shape
         o, keep = self._opts(nq, k, ef, quantized=quantized, filter_bits=filter_bits, filter_nbits=filter_nbits,
                              filter_stride=filter_stride, filter_used=filter_used, ks=ks, efs=efs, mode=mode,
-                             filter_ids=filter_ids, filter_by_node=filter_by_node)
+                             filter_ids=filter_ids, filter_by_node=filter_by_node, exact_below=exact_below)
         stride = o.out_stride
         keys = np.zeros((nq, stride), dtype=np.uint64)
         dist = np.zeros((nq, stride), dtype=np.float32)

@@ -117,6 +117,13 @@ typedef struct hnsw_search_opts {
     int32_t filter_by_node;     /* 0: bit = key (keys below filter_nbits); 1: bit = node id, i.e.
                                    position in the file's node order, for indexes whose keys are
                                    sparse u64 values (a closure filter evaluated once per node) */
+    float exact_below;          /* selectivity planner (off at 0): a filtered query whose bitmap
+                                   admits at most this fraction of the live nodes is answered by an
+                                   exact scan of the admitted nodes (f32, the reference's distance
+                                   order, ties by key) instead of the graph walk, as the crate's
+                                   documentation advises for very selective filters
+                                   (src/hnsw/mod.rs:421-425). Needs node bitmaps, or keys equal to
+                                   node ids; other queries are unaffected */
 } hnsw_search_opts;
 
 enum {

@@ -506,3 +506,47 @@ def test_cuda_graph_replays_the_search(gaussian_10k):
                st.cpu().numpy())
         assert_same(got, want, "graph")
     g.close()
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("quant", [False, True])
+def test_planner_exact_scan_for_selective_filters(metric, quant):
+    """Queries whose filter admits few nodes get the exact top-k among the
+    admitted live nodes (BruteForceIndex::search_filtered on the index's own
+    rows); the others keep the graph walk's results."""
+    base, queries = H.mixture(6000, 48, 20, 30, 0.5, 300 + metric)
+    if metric == 2:
+        base[:, 0] += np.where(base[:, 0] >= 0, 1.0, -1.0)
+        queries[:, 0] += 1.0
+    dead = list(range(0, 6000, 37))
+    data = build_index(base, metric=metric, m=10, seed=4, deleted_keys=dead, quantize=True)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    rng = np.random.default_rng(metric)
+    words = (6000 + 63) // 64
+    sels = [0.002, 0.01, 0.03, 0.5]
+    bank = np.zeros((len(sels), words), np.uint64)
+    for j, p in enumerate(sels):
+        bank[j] = H.key_bitmap(np.nonzero(rng.random(6000) < p)[0].astype(np.uint64), 6000)
+    ids = rng.integers(0, len(sels), 48).astype(np.uint32)
+    kw = dict(filter_bits=bank, filter_nbits=6000, filter_stride=words, filter_ids=ids, quantized=quant)
+    got = gi.search_arrays(queries, 10, 40, exact_below=0.05, mode=1, **kw)
+    graph = oi.search(queries, 10, 40, filter_bits=bank[ids], filter_nbits=6000, filter_stride=words, quantized=quant)
+    alive = np.ones(6000, bool)
+    alive[dead] = False
+    rows = base if metric != 2 else O.normalize_rows(base)
+    live_bank = bank.copy()
+    for j in range(len(sels)):
+        live_bank[j] = H.key_bitmap(np.nonzero(np.unpackbits(bank[j].view(np.uint8), bitorder="little")[:6000]
+                                               .astype(bool) & alive)[0].astype(np.uint64), 6000)
+    exact = O.brute_filtered(metric, rows, queries, 10, live_bank[ids], 6000, words)
+    planned = 0
+    for i in range(48):
+        admitted = int(np.unpackbits(bank[ids[i]].view(np.uint8), bitorder="little")[:6000].sum())
+        ref = exact if admitted <= int(0.05 * len(alive[alive])) else graph
+        planned += ref is exact
+        c = int(ref[2][i])
+        assert int(got[2][i]) == c
+        np.testing.assert_array_equal(got[0][i, :c], ref[0][i, :c])
+        np.testing.assert_array_equal(got[1][i, :c].view(np.uint32), ref[1][i, :c].view(np.uint32))
+    assert 0 < planned < 48
