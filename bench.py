@@ -727,7 +727,15 @@ def run_serve(args):
 
     data, build_s = cached_index(f"serve-{nb}-{dim}-9-10-m16-q", build)
     del base
+    # Open time: device ingest (hnsw_gpu_index_open) against the host
+    # loader's checks alone (hnsw_validate_bytes).
+    t = time.perf_counter()
     index = H.HnswIndex.from_bytes(data)
+    open_s = time.perf_counter() - t
+    t = time.perf_counter()
+    H.validate_bytes(data)
+    host_validate_s = time.perf_counter() - t
+    file_gb = len(data) / 1e9
     del data
     rq = np.random.default_rng(11)
     ks = rq.choice([10, 100], pool).astype(np.uint32)
@@ -779,7 +787,8 @@ def run_serve(args):
         "metric": "served QPS with no rejections (10M x 128 L2, open-loop Poisson; p50/p99 per load in config)",
         "value": best["achieved_qps"] if best else 0.0, "unit": "queries/s", "n_gpus": 1,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s,
+        "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s, "file_gb": file_gb,
+                   "open_s": open_s, "host_validate_s": host_validate_s,
                    "batched_qps_same_requests": batched_qps, "max_batch": args.serve_batch,
                    "linger_us": args.serve_linger, "launched_batches": batches, "launched_queries": launched,
                    "tuned_schedule": tuned,

@@ -315,108 +315,164 @@ int hnsw_validate_bytes(const uint8_t* bytes, size_t len, uint64_t max_memory, h
     return HNSW_OK;
 }
 
-// Flattens a loaded index into the device layout (see device.hpp).
-static int upload(hnsw_gpu_index* gi, const HostIndex& ix) {
-    DeviceIndexView& v = gi->view;
-    const uint32_t n = uint32_t(ix.node_count());
-    v.n = n;
-    v.dim = ix.dim;
-    v.dp = round_up(ix.dim, 32);
-    v.dc = round_up(ix.dim, 16);
-    v.m = ix.params.m;
-    v.m0 = ix.params.m0;
-    v.mp = round_up(ix.params.m, 32);
-    v.m0p = round_up(ix.params.m0, 32);
-    v.metric = ix.metric;
-    v.quantized = ix.quantized ? 1 : 0;
-    v.scale = ix.q_scale;
-    v.live = uint32_t(ix.key_to_id.size());
-    v.entry = ix.has_entry() ? ix.entry_id() : kSentinel;
-    v.top = ix.has_entry() ? ix.top_level() : 0;
-    const size_t nn = std::max<size_t>(n, 1);
+// Device ingest (ingest.cu): every check of io::read in the reference's
+// order, the per-byte and per-node ones on the device, building the device
+// layout from one copy of the file. Temporaries are freed on every path.
+static int ingest_open(hnsw_gpu_index* gi, const uint8_t* bytes, size_t len, uint64_t max_memory) {
+    size_t body_len = 0;
+    uint32_t stored = 0;
+    Err e = check_envelope(bytes, len, &body_len, &stored);
+    if (e) return from_err(e);
+    struct Tmp {
+        DBuf file, part, pow8, word, words, noff, upoff_tmp, table, flags;
+        ~Tmp() {
+            for (DBuf* b : {&file, &part, &pow8, &word, &words, &noff, &upoff_tmp, &table, &flags}) b->release();
+        }
+    } t;
     cudaStream_t st = nullptr;
-
+    // 1. The file on the device; CRC-32 of the body (verify_envelope).
+    CU(t.file.ensure(std::max<size_t>(len, 16)), "cudaMalloc file");
+    CU(cudaMemcpy(t.file.p, bytes, len, cudaMemcpyHostToDevice), "copy file");
+    const uint8_t* df = t.file.as<uint8_t>();
+    const size_t nchunks = std::max<size_t>(1, (body_len + kIngestCrcChunk - 1) / kIngestCrcChunk);
+    CU(t.part.ensure(nchunks * 4), "cudaMalloc crc chunks");
+    CU(t.pow8.ensure(64 * 4), "cudaMalloc crc powers");
+    CU(t.word.ensure(64), "cudaMalloc crc word");
+    uint32_t computed = 0;
+    CU(ingest_crc(df, body_len, t.part.as<uint32_t>(), t.pow8.as<uint32_t>(), t.word.as<uint32_t>(), &computed, st),
+       "crc kernel");
+    if (computed != stored) return from_err(checksum_error(stored, computed));
+    // 2. Header, columns, list counts, memory limit (host).
+    FileLayout L;
+    e = scan_layout(bytes, body_len, max_memory, &L);
+    if (e) return from_err(e);
+    const uint32_t n = L.n;
+    const size_t nn = std::max<size_t>(n, 1);
+    DeviceIndexView& v = gi->view;
+    v.n = n;
+    v.dim = L.dim;
+    v.dp = round_up(L.dim, 32);
+    v.dc = round_up(L.dim, 16);
+    v.m = L.params.m;
+    v.m0 = L.params.m0;
+    v.mp = round_up(L.params.m, 32);
+    v.m0p = round_up(L.params.m0, 32);
+    v.metric = L.metric;
+    v.quantized = L.quantized ? 1 : 0;
+    // 3. Vectors into padded rows, then read_nodes' checks (device).
+    CU(t.flags.ensure(64), "cudaMalloc flags");
+    unsigned long long* first = t.flags.as<unsigned long long>();
+    CU(cudaMemset(t.flags.p, 0xFF, 8), "memset flags");
     CU(gi->vec.ensure(nn * v.dp * 4), "cudaMalloc vectors");
-    if (v.dp == v.dim) {
-        CU(cudaMemcpy(gi->vec.p, ix.vectors.data(), size_t(n) * v.dim * 4, cudaMemcpyHostToDevice), "copy vectors");
-    } else {
-        CU(cudaMemset(gi->vec.p, 0, nn * v.dp * 4), "memset vectors");
-        if (n)
-            CU(cudaMemcpy2D(gi->vec.p, size_t(v.dp) * 4, ix.vectors.data(), size_t(v.dim) * 4, size_t(v.dim) * 4, n,
-                            cudaMemcpyHostToDevice),
-               "copy vectors");
-    }
+    if (v.dp != v.dim) CU(cudaMemset(gi->vec.p, 0, nn * v.dp * 4), "memset vectors");
+    if (n)
+        CU(cudaMemcpy2D(gi->vec.p, size_t(v.dp) * 4, df + (L.vectors - bytes), size_t(v.dim) * 4, size_t(v.dim) * 4, n,
+                        cudaMemcpyDeviceToDevice),
+           "copy vectors");
     v.vec = gi->vec.as<float>();
-
-    // Layer-0 rows: ids then sentinel.
-    {
-        std::vector<uint32_t> rows(nn * v.m0p, kSentinel);
-        for (uint32_t id = 0; id < n; ++id) {
-            const uint32_t* blk = ix.block(id, 0);
-            std::copy(blk + 1, blk + 1 + blk[0], rows.begin() + size_t(id) * v.m0p);
-        }
-        CU(gi->adj0.ensure(rows.size() * 4), "cudaMalloc adj0");
-        CU(cudaMemcpy(gi->adj0.p, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice), "copy adj0");
-        v.adj0 = gi->adj0.as<uint32_t>();
+    CU(ingest_check_vectors(v.vec, n, v.dim, v.dp, L.metric == HNSW_METRIC_COSINE, first, st), "vector checks");
+    unsigned long long bad = 0;
+    CU(cudaMemcpy(&bad, first, 8, cudaMemcpyDeviceToHost), "vector checks");
+    if (bad != ~0ull)
+        return from_err(invalid_field((bad & 1ull) ? "cosine vector is not unit length" : "vector out of range"));
+    // 4. read_links' checks and the CSR (device).
+    std::vector<uint32_t> off(nn, 0);
+    size_t blocks = 0;
+    for (uint32_t id = 0; id < n; ++id) {
+        off[id] = uint32_t(blocks);
+        blocks += L.levels[id];
     }
-    // Upper layers: one block of mp ids per (node, layer >= 1).
-    {
-        std::vector<uint32_t> off(nn, 0);
-        size_t blocks = 0;
-        for (uint32_t id = 0; id < n; ++id) {
-            off[id] = uint32_t(blocks);
-            blocks += ix.levels[id];
-        }
-        std::vector<uint32_t> adj(std::max<size_t>(blocks, 1) * v.mp, kSentinel);
-        for (uint32_t id = 0; id < n; ++id)
-            for (unsigned layer = 1; layer <= ix.levels[id]; ++layer) {
-                const uint32_t* blk = ix.block(id, layer);
-                std::copy(blk + 1, blk + 1 + blk[0], adj.begin() + size_t(off[id] + layer - 1) * v.mp);
-            }
-        CU(gi->upoff.ensure(off.size() * 4), "cudaMalloc up_off");
-        CU(cudaMemcpy(gi->upoff.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice), "copy up_off");
-        CU(gi->adjU.ensure(adj.size() * 4), "cudaMalloc adjU");
-        CU(cudaMemcpy(gi->adjU.p, adj.data(), adj.size() * 4, cudaMemcpyHostToDevice), "copy adjU");
-        v.up_off = gi->upoff.as<uint32_t>();
-        v.adjU = gi->adjU.as<uint32_t>();
-    }
-    // Keys and tombstones.
-    {
-        CU(gi->keys.ensure(nn * 8), "cudaMalloc keys");
-        if (n) CU(cudaMemcpy(gi->keys.p, ix.keys.data(), size_t(n) * 8, cudaMemcpyHostToDevice), "copy keys");
-        v.keys = gi->keys.as<uint64_t>();
-        bool ids = true;
-        for (uint32_t id = 0; id < n && ids; ++id) ids = ix.keys[id] == id;
-        v.keys_are_ids = ids ? 1 : 0;
-        std::vector<uint32_t> dead((nn + 31) / 32, 0);
-        v.has_dead = 0;
-        for (uint32_t id = 0; id < n; ++id)
-            if (ix.deleted[id]) {
-                dead[id >> 5] |= 1u << (id & 31);
-                v.has_dead = 1;
-            }
-        CU(gi->dead.ensure(dead.size() * 4), "cudaMalloc dead");
-        CU(cudaMemcpy(gi->dead.p, dead.data(), dead.size() * 4, cudaMemcpyHostToDevice), "copy dead");
-        v.dead = gi->dead.as<uint32_t>();
-    }
-    // Quantizer: offsets, then codes derived on the device.
-    if (ix.quantized) {
-        std::vector<float> off(v.dp, 0.0f);
-        std::copy(ix.q_offset.begin(), ix.q_offset.end(), off.begin());
-        CU(gi->offset.ensure(off.size() * 4), "cudaMalloc offsets");
-        CU(cudaMemcpy(gi->offset.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice), "copy offsets");
+    CU(gi->adj0.ensure(nn * v.m0p * 4), "cudaMalloc adj0");
+    CU(cudaMemset(gi->adj0.p, 0xFF, nn * v.m0p * 4), "memset adj0");
+    CU(gi->upoff.ensure(nn * 4), "cudaMalloc up_off");
+    CU(cudaMemcpy(gi->upoff.p, off.data(), nn * 4, cudaMemcpyHostToDevice), "copy up_off");
+    CU(gi->adjU.ensure(std::max<size_t>(blocks, 1) * v.mp * 4), "cudaMalloc adjU");
+    CU(cudaMemset(gi->adjU.p, 0xFF, std::max<size_t>(blocks, 1) * v.mp * 4), "memset adjU");
+    v.adj0 = gi->adj0.as<uint32_t>();
+    v.up_off = gi->upoff.as<uint32_t>();
+    v.adjU = gi->adjU.as<uint32_t>();
+    const size_t link_bytes = L.links_end - L.links_begin;
+    CU(t.words.ensure(std::max<size_t>(link_bytes, 16)), "cudaMalloc lists");
+    if (link_bytes) CU(cudaMemcpy(t.words.p, df + L.links_begin, link_bytes, cudaMemcpyDeviceToDevice), "copy lists");
+    CU(t.noff.ensure(nn * 8), "cudaMalloc list offsets");
+    if (n) CU(cudaMemcpy(t.noff.p, L.node_off.data(), size_t(n) * 8, cudaMemcpyHostToDevice), "copy list offsets");
+    CU(cudaMemset(t.flags.p, 0xFF, 8), "memset flags");
+    CU(ingest_links(t.words.as<uint32_t>(), t.noff.as<uint64_t>(), L.links_begin, df + (L.levels - bytes), n, v.m0p,
+                    v.mp, gi->upoff.as<uint32_t>(), gi->adj0.as<uint32_t>(), gi->adjU.as<uint32_t>(), first, st),
+       "list checks");
+    CU(cudaMemcpy(&bad, first, 8, cudaMemcpyDeviceToHost), "list checks");
+    if (bad != ~0ull) return from_err(invalid_field((bad & 1ull) ? "duplicate neighbor id" : "neighbor id"));
+    // 5. Quantizer section and trailing bytes (host).
+    std::vector<float> q_offset;
+    float q_scale = 0.0f;
+    e = scan_tail(bytes, L, &q_offset, &q_scale);
+    if (e) return from_err(e);
+    v.scale = q_scale;
+    // 6. Keys: distinct among live nodes (device), then the entry point.
+    CU(gi->keys.ensure(nn * 8), "cudaMalloc keys");
+    if (n) CU(cudaMemcpy(gi->keys.p, df + (L.keys - bytes), size_t(n) * 8, cudaMemcpyDeviceToDevice), "copy keys");
+    v.keys = gi->keys.as<uint64_t>();
+    uint64_t cap = 2;
+    while (cap < 2 * uint64_t(nn)) cap <<= 1;
+    CU(t.table.ensure(cap * 8), "cudaMalloc key set");
+    CU(cudaMemset(t.table.p, 0xFF, cap * 8), "memset key set");
+    unsigned int* kflags = reinterpret_cast<unsigned int*>(t.flags.as<uint8_t>() + 16);
+    CU(cudaMemset(kflags, 0, 12), "memset key flags");
+    CU(ingest_live_keys(v.keys, df + (L.dead - bytes), n, t.table.as<unsigned long long>(), cap, kflags, st),
+       "key checks");
+    unsigned int kf[3] = {0, 0, 0};
+    CU(cudaMemcpy(kf, kflags, 12, cudaMemcpyDeviceToHost), "key checks");
+    if (kf[1]) return from_err(invalid_field("duplicate live key"));
+    v.keys_are_ids = kf[2] ? 0 : 1;
+    uint64_t entry_word = 0;
+    e = check_entry(L, &entry_word);
+    if (e) return from_err(e);
+    v.entry = n ? uint32_t(entry_word) : kSentinel;
+    v.top = n ? uint32_t(entry_word >> 32) : 0;
+    // 7. Tombstones.
+    CU(gi->dead.ensure(((nn + 31) / 32) * 4), "cudaMalloc dead");
+    CU(cudaMemset(gi->dead.p, 0, ((nn + 31) / 32) * 4), "memset dead");
+    unsigned long long* dead_count = first;
+    CU(cudaMemset(dead_count, 0, 8), "memset dead count");
+    CU(ingest_dead(df + (L.dead - bytes), n, gi->dead.as<uint32_t>(), dead_count, st), "tombstones");
+    unsigned long long ndead = 0;
+    CU(cudaMemcpy(&ndead, dead_count, 8, cudaMemcpyDeviceToHost), "tombstones");
+    v.dead = gi->dead.as<uint32_t>();
+    v.has_dead = ndead ? 1 : 0;
+    v.live = uint32_t(n - ndead);
+    // 8. Quantizer: offsets, then codes derived on the device.
+    if (L.quantized) {
+        std::vector<float> offp(v.dp, 0.0f);
+        std::copy(q_offset.begin(), q_offset.end(), offp.begin());
+        CU(gi->offset.ensure(offp.size() * 4), "cudaMalloc offsets");
+        CU(cudaMemcpy(gi->offset.p, offp.data(), offp.size() * 4, cudaMemcpyHostToDevice), "copy offsets");
         CU(gi->codes.ensure(nn * v.dc), "cudaMalloc codes");
         CU(gi->norms.ensure(nn * 4), "cudaMalloc code norms");
         CU(launch_encode_codes(v.vec, n, v.dim, v.dp, v.dc, gi->offset.as<float>(), v.scale, gi->codes.as<int8_t>(),
                                gi->norms.as<int32_t>(), st),
            "encode codes");
-        CU(cudaDeviceSynchronize(), "encode codes");
         v.q_offset = gi->offset.as<float>();
         v.codes = gi->codes.as<int8_t>();
         v.code_norm = gi->norms.as<int32_t>();
     }
-    gi->info.device_bytes = gi->vec.bytes + gi->adj0.bytes + gi->upoff.bytes + gi->adjU.bytes + gi->keys.bytes +
-                            gi->dead.bytes + gi->offset.bytes + gi->codes.bytes + gi->norms.bytes;
+    CU(cudaDeviceSynchronize(), "ingest");
+    hnsw_index_info& info = gi->info;
+    std::memset(&info, 0, sizeof info);
+    info.dim = L.dim;
+    info.metric = L.metric;
+    info.m = L.params.m;
+    info.m0 = L.params.m0;
+    info.ef_construction = L.params.ef_construction;
+    info.quantized = L.quantized ? 1 : 0;
+    info.nodes = n;
+    info.live = v.live;
+    info.top_level = v.top;
+    info.entry = v.entry;
+    info.seed = L.params.seed;
+    info.level_multiplier = L.params.level_multiplier;
+    info.required_memory = L.required;
+    info.device_bytes = gi->vec.bytes + gi->adj0.bytes + gi->upoff.bytes + gi->adjU.bytes + gi->keys.bytes +
+                        gi->dead.bytes + gi->offset.bytes + gi->codes.bytes + gi->norms.bytes;
     return HNSW_OK;
 }
 
@@ -425,24 +481,19 @@ int hnsw_gpu_index_open(const uint8_t* bytes, size_t len, uint64_t max_memory, i
     *out = nullptr;
     if (!bytes && len) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
     static const uint8_t empty = 0;
-    HostIndex ix;
-    uint64_t required = 0;
-    Err e = load_index(bytes ? bytes : &empty, len, max_memory, &ix, &required);
-    if (e) return from_err(e);
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0)
         return set_error(HNSW_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
     if (device < 0 || device >= ndev) return set_error(HNSW_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    if (ix.dim > 8192) return set_error(HNSW_ERR_INVALID_ARGUMENT, "dimension above the device path's limit of 8192");
     DeviceGuard dg(device);
     std::unique_ptr<hnsw_gpu_index> gi(new hnsw_gpu_index());
     gi->device = device;
     gi->slots.device = device;
     cudaDeviceGetAttribute(&gi->num_sms, cudaDevAttrMultiProcessorCount, device);
-    fill_info(ix, required, &gi->info);
-    int s = upload(gi.get(), ix);
+    int s = ingest_open(gi.get(), bytes ? bytes : &empty, len, max_memory);
     if (s != HNSW_OK) return s;
+    if (gi->view.dim > 8192) return set_error(HNSW_ERR_INVALID_ARGUMENT, "dimension above the device path's limit of 8192");
     *out = gi.release();
     return HNSW_OK;
 }

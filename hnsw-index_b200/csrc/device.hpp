@@ -137,6 +137,28 @@ uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t 
 // Resident warps of the persistent kernel for a geometry (spill slots needed).
 cudaError_t persistent_warps(const SearchGeometry& g, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps);
 
+// Device ingest of a format-v1 file (ingest.cu).
+constexpr size_t kIngestCrcChunk = 4096;  // bytes per CRC chunk (multiple of 16)
+// CRC-32 of data[0, len) (the file buffer, 256-byte aligned) into *crc
+// (host), synchronising the stream. Device scratch: part holds one word per
+// chunk, pow8 64 words, out one word.
+cudaError_t ingest_crc(const uint8_t* data, size_t len, uint32_t* part, uint32_t* pow8, uint32_t* out,
+                       uint32_t* crc, cudaStream_t stream);
+// Vector checks over the padded rows; *first = min(node * 2 + kind).
+cudaError_t ingest_check_vectors(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, bool cosine,
+                                 unsigned long long* first, cudaStream_t stream);
+// List checks and CSR write; words = the lists section copied to an aligned
+// buffer (word 0 at byte links_begin); *first = min(list byte * 2 + kind).
+cudaError_t ingest_links(const uint32_t* words, const uint64_t* node_off, uint64_t links_begin, const uint8_t* levels,
+                         uint32_t n, uint32_t m0p, uint32_t mp, const uint32_t* up_off, uint32_t* adj0,
+                         uint32_t* adjU, unsigned long long* first, cudaStream_t stream);
+cudaError_t ingest_dead(const uint8_t* flags, uint32_t n, uint32_t* dead, unsigned long long* dead_count,
+                        cudaStream_t stream);
+// flags_out[0] counts live keys equal to ~0, [1] is set on a repeated live
+// key, [2] when some key differs from its node id.
+cudaError_t ingest_live_keys(const uint64_t* keys, const uint8_t* flags, uint32_t n, unsigned long long* table,
+                             uint64_t cap, unsigned int* flags_out, cudaStream_t stream);
+
 // Derives int8 codes and their squared norms from offsets and scale
 // (ScalarQuantizer::encode_into, src/quantization.rs:73-81).
 cudaError_t launch_encode_codes(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, uint32_t dc,

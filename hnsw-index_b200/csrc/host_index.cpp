@@ -245,9 +245,9 @@ uint64_t sat_mul(uint64_t a, uint64_t b) {
 
 }  // namespace
 
-Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex* out, uint64_t* required_out) {
-    if (max_memory == 0) max_memory = std::max<uint64_t>(sat_mul(len, 64), uint64_t(64) << 20);
-    // verify_envelope (io.rs:278-305)
+// verify_envelope without the checksum (io.rs:278-305): magic, version,
+// minimum length. *body_len is the length the CRC covers, *stored the CRC.
+Err check_envelope(const uint8_t* bytes, size_t len, size_t* body_len, uint32_t* stored) {
     if (len < 12) {
         size_t pl = std::min<size_t>(len, 8);
         return fail(std::memcmp(bytes, kMagic, pl) == 0 ? HNSW_ERR_FORMAT_TRUNCATED : HNSW_ERR_FORMAT_BAD_MAGIC);
@@ -261,18 +261,30 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
         return e;
     }
     if (len < kHeaderLen + kTrailerLen) return fail(HNSW_ERR_FORMAT_TRUNCATED);
-    size_t body_len = len - kTrailerLen;
-    uint32_t stored;
-    std::memcpy(&stored, bytes + body_len, 4);
-    uint32_t computed = crc32(bytes, body_len);
-    if (stored != computed) {
-        Err e = fail(HNSW_ERR_FORMAT_CHECKSUM);
-        e.a = stored;
-        e.b = computed;
-        return e;
-    }
+    *body_len = len - kTrailerLen;
+    std::memcpy(stored, bytes + *body_len, 4);
+    return Err();
+}
+
+Err invalid_field(const char* what) { return invalid(what); }
+
+Err checksum_error(uint32_t stored, uint32_t computed) {
+    Err e = fail(HNSW_ERR_FORMAT_CHECKSUM);
+    e.a = stored;
+    e.b = computed;
+    return e;
+}
+
+// read_header, read_columns, scan_links and required_memory (io.rs:317-445)
+// on a body whose checksum is verified: every check that needs no vector or
+// list contents, in the reference's order, recording where each part lies.
+Err scan_layout(const uint8_t* bytes, size_t body_len, uint64_t max_memory, FileLayout* out) {
+    if (max_memory == 0) max_memory = std::max<uint64_t>(sat_mul(body_len + kTrailerLen, 64), uint64_t(64) << 20);
     Reader r{bytes, body_len, 12};
     const Err truncated = fail(HNSW_ERR_FORMAT_TRUNCATED);
+    FileLayout& L = *out;
+    L = FileLayout();
+    L.body_len = body_len;
 
     // read_header (io.rs:317-361)
     uint8_t metric, sel, flags, qflag;
@@ -303,6 +315,12 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
     if (!r.get(&n)) return truncated;
     if (uint64_t(n) > kMaxNodes) return invalid("node count");
     if (!r.get(&entry_id)) return truncated;
+    L.metric = metric;
+    L.quantized = qflag != 0;
+    L.params = p;
+    L.dim = dim;
+    L.n = n;
+    L.entry_id = entry_id;
 
     // read_columns (io.rs:375-402)
     const uint8_t *kcol, *lcol, *fcol, *vcol;
@@ -317,11 +335,20 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
     for (uint32_t i = 0; i < n; ++i) level_sum += lcol[i];
     double expected = double(n) / std::expm1(1.0 / ml);
     if (double(level_sum) > 2.0 * expected + 1024.0) return invalid("implausible level distribution");
+    L.keys = kcol;
+    L.levels = lcol;
+    L.dead = fcol;
+    L.vectors = vcol;
+    L.level_sum = level_sum;
+    L.links_begin = r.pos;
 
-    // scan_links (io.rs:407-419): walk without allocating.
+    // scan_links (io.rs:407-419): walk without allocating (beyond one offset
+    // per node, where the node's first list starts).
     {
         Reader s = r;
-        for (uint32_t i = 0; i < n; ++i)
+        L.node_off.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            L.node_off[i] = s.pos;
             for (unsigned layer = 0; layer <= lcol[i]; ++layer) {
                 uint32_t count;
                 if (!s.get(&count)) return truncated;
@@ -330,6 +357,8 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
                 const uint8_t* skip;
                 if (!s.take(size_t(count) * 4, &skip)) return truncated;
             }
+        }
+        L.links_end = s.pos;
     }
     // required_memory (io.rs:424-445); Mutex<()> is 1 byte, Box<[AtomicU32]> 16.
     uint64_t code = qflag ? dim : 0;
@@ -338,13 +367,67 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
     uint64_t required = sat_add(sat_add(sat_add(sat_mul(n, per_node), sat_mul(level_sum, (uint64_t(m) + 1) * 4)),
                                         key_map_heap_bytes(n)),
                                 quantizer);
-    if (required_out) *required_out = required;
+    L.required = required;
     if (required > max_memory) {
         Err e = fail(HNSW_ERR_MEMORY_LIMIT_EXCEEDED);
         e.a = required;
         e.b = max_memory;
         return e;
     }
+    return Err();
+}
+
+// The quantizer section and the trailing-bytes check (io.rs:487-515, after
+// the lists), then the entry point (io.rs:517-540).
+Err scan_tail(const uint8_t* bytes, const FileLayout& L, std::vector<float>* q_offset, float* q_scale) {
+    Reader r{bytes, L.body_len, L.links_end};
+    const Err truncated = fail(HNSW_ERR_FORMAT_TRUNCATED);
+    if (L.quantized) {
+        q_offset->resize(L.dim);
+        const uint8_t* ob;
+        if (!r.take(size_t(L.dim) * 4, &ob)) return truncated;
+        std::memcpy(q_offset->data(), ob, size_t(L.dim) * 4);
+        for (float o : *q_offset)
+            if (!std::isfinite(o)) return invalid("quantizer offset");
+        float scale;
+        if (!r.get(&scale)) return truncated;
+        if (!(std::isfinite(scale) && scale > 0.0f)) return invalid("quantizer");
+        *q_scale = scale;
+    }
+    if (r.pos != r.len) return fail(HNSW_ERR_FORMAT_TRAILING_BYTES);
+    return Err();
+}
+
+// The entry point check of finish (io.rs:517-540), after the key checks.
+Err check_entry(const FileLayout& L, uint64_t* entry_word) {
+    if (L.n == 0) {
+        if (L.entry_id != kNoEntry) return invalid("entry point of an empty index");
+        *entry_word = ~0ull;
+        return Err();
+    }
+    const uint8_t top = *std::max_element(L.levels, L.levels + L.n);
+    if (L.entry_id >= L.n || L.levels[L.entry_id] != top) return invalid("entry point");
+    *entry_word = (uint64_t(top) << 32) | L.entry_id;
+    return Err();
+}
+
+Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex* out, uint64_t* required_out) {
+    size_t body_len = 0;
+    uint32_t stored = 0;
+    Err e = check_envelope(bytes, len, &body_len, &stored);
+    if (e) return e;
+    const uint32_t computed = crc32(bytes, body_len);
+    if (stored != computed) return checksum_error(stored, computed);
+    FileLayout L;
+    e = scan_layout(bytes, body_len, max_memory, &L);
+    if (required_out) *required_out = L.required;
+    if (e) return e;
+    Reader r{bytes, body_len, L.links_begin};
+    const Err truncated = fail(HNSW_ERR_FORMAT_TRUNCATED);
+    const uint32_t n = L.n, dim = L.dim, m0 = L.params.m0, m = L.params.m;
+    const uint8_t *kcol = L.keys, *lcol = L.levels, *fcol = L.dead, *vcol = L.vectors;
+    const uint8_t metric = L.metric;
+    const Params p = L.params;
 
     // read_nodes (io.rs:448-485)
     HostIndex& ix = *out;
@@ -391,34 +474,15 @@ Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex*
             blk[0] = count;
             std::copy(nbrs.begin(), nbrs.end(), blk + 1);
         }
-    if (qflag) {
-        ix.q_offset.resize(dim);
-        const uint8_t* ob;
-        if (!r.take(size_t(dim) * 4, &ob)) return truncated;
-        std::memcpy(ix.q_offset.data(), ob, size_t(dim) * 4);
-        for (float o : ix.q_offset)
-            if (!std::isfinite(o)) return invalid("quantizer offset");
-        float scale;
-        if (!r.get(&scale)) return truncated;
-        if (!(std::isfinite(scale) && scale > 0.0f)) return invalid("quantizer");
-        ix.quantized = true;
-        ix.q_scale = scale;
-    }
-    if (r.pos != r.len) return fail(HNSW_ERR_FORMAT_TRAILING_BYTES);
+    e = scan_tail(bytes, L, &ix.q_offset, &ix.q_scale);
+    if (e) return e;
+    ix.quantized = L.quantized;
 
     // finish (io.rs:517-540)
     ix.key_to_id.reserve(n);
     for (uint32_t id = 0; id < n; ++id)
         if (!ix.deleted[id] && !ix.key_to_id.emplace(ix.keys[id], id).second) return invalid("duplicate live key");
-    if (n == 0) {
-        if (entry_id != kNoEntry) return invalid("entry point of an empty index");
-        ix.entry_word = ~0ull;
-    } else {
-        uint8_t top = *std::max_element(ix.levels.begin(), ix.levels.end());
-        if (entry_id >= n || ix.levels[entry_id] != top) return invalid("entry point");
-        ix.entry_word = (uint64_t(top) << 32) | entry_id;
-    }
-    return Err();
+    return check_entry(L, &ix.entry_word);
 }
 
 // ---------------------------------------------------------------------------

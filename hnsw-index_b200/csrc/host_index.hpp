@@ -82,6 +82,32 @@ uint32_t crc32(const uint8_t* p, size_t n);
 // max_memory == 0 selects default_memory_limit (io.rs:271-275).
 Err load_index(const uint8_t* bytes, size_t len, uint64_t max_memory, HostIndex* out,
                uint64_t* required_memory);
+
+// The stages of load_index, for a loader that verifies the checksum, the
+// vectors and the neighbor lists elsewhere (the device ingest) while keeping
+// the reference's order of checks and its messages.
+struct FileLayout {
+    uint8_t metric = 0;
+    bool quantized = false;
+    Params params;
+    uint32_t dim = 0, n = 0, entry_id = 0;
+    size_t body_len = 0;
+    const uint8_t *keys = nullptr, *levels = nullptr, *dead = nullptr, *vectors = nullptr;
+    size_t links_begin = 0, links_end = 0;  // byte range of the neighbor lists
+    std::vector<uint64_t> node_off;         // byte offset of each node's first list
+    uint64_t level_sum = 0, required = 0;
+};
+// Magic, version and minimum length; *body_len bytes are covered by *stored.
+Err check_envelope(const uint8_t* bytes, size_t len, size_t* body_len, uint32_t* stored);
+Err checksum_error(uint32_t stored, uint32_t computed);
+// Header, columns, list counts and the memory limit, on a verified body.
+Err scan_layout(const uint8_t* bytes, size_t body_len, uint64_t max_memory, FileLayout* out);
+// Quantizer section and trailing bytes (after the lists).
+Err scan_tail(const uint8_t* bytes, const FileLayout& layout, std::vector<float>* q_offset, float* q_scale);
+// Entry point (last check of io.rs:517-540).
+Err check_entry(const FileLayout& layout, uint64_t* entry_word);
+// The messages of the checks the device ingest runs (invalid field names).
+Err invalid_field(const char* what);
 // io::write (src/hnsw/io.rs:103-169).
 std::vector<uint8_t> write_index(const HostIndex& ix);
 
