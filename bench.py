@@ -485,7 +485,9 @@ def run_brute(args):
         entry = {"qps_e2e": nq / statistics.median(times), "ms_e2e": 1e3 * statistics.median(times)}
         if stats:
             terms = 3 if prec == H.Precision.BF16X3 else 1
-            kp = (dim * terms + 63) // 64 * 64
+            # MMA work per (query, row) pair: `terms` products over the
+            # 64-padded dimension (the split issues three MMAs per K step).
+            kp = terms * ((dim + 63) // 64 * 64)
             score_ms = statistics.median(s_["score_ms"] for s_ in stats)
             dev_ms = statistics.median(s_["prep_ms"] + s_["sample_ms"] + s_["score_ms"] + s_["rerank_ms"]
                                        for s_ in stats)

@@ -1,10 +1,10 @@
 // Tensor-core brute-force scoring on sm_100a (tcgen05 + TMA + TMEM).
 //
 // Scores q . x for every (query, row) pair as one BF16 GEMM with FP32
-// accumulation in tensor memory, either plainly (K' = D, operands rounded to
-// BF16) or with the 3-term split (K' = 3D: queries [q_hi | q_hi | q_lo],
-// rows [x_hi | x_lo | x_hi], so the sum is q_hi.x_hi + q_hi.x_lo + q_lo.x_hi,
-// i.e. q.x up to the dropped q_lo.x_lo term). The epilogue turns each score
+// accumulation in tensor memory, either plainly (K = D, operands rounded to
+// BF16) or with the 3-term split: operands [hi | lo] (each half padded to a
+// multiple of 64 columns), and per K step three MMAs q_hi.x_hi, q_hi.x_lo,
+// q_lo.x_hi on tiles loaded once, i.e. q.x up to the dropped q_lo.x_lo term. The epilogue turns each score
 // into the metric's distance and either writes it densely (threshold sample)
 // or keeps only (row, distance) pairs at or below a per-query threshold
 // (candidate pass). Exact FP32 re-ranking of the survivors happens in
@@ -13,7 +13,9 @@
 //
 // Kernel structure (one CTA per SM, persistent over 128 x 256 output tiles):
 //   warp 0      TMA producer: A (128 queries x 64 K) and B (256 rows x 64 K)
-//               tiles into a 4-stage shared-memory ring (128-byte swizzle);
+//               tiles into a shared-memory ring (128-byte swizzle): 4 stages
+//               of one A and one B tile, or with the split 2 stages of
+//               A_hi, A_lo, B_hi, B_lo (2/3 of the bytes per MMA);
 //   warp 1      allocates 512 TMEM columns; one thread issues
 //               tcgen05.mma (M=128, N=256, K=16) and tcgen05.commit;
 //   warps 2..5  epilogue: tcgen05.ld of a 128 x 256 FP32 accumulator (two
@@ -32,11 +34,16 @@
 namespace hnswgpu {
 namespace tc {
 
-constexpr int kStages = 4;
 constexpr uint32_t kTileM = 128, kTileN = 256, kTileK = 64;
 constexpr uint32_t kABytes = kTileM * kTileK * 2;   // 16 KB
 constexpr uint32_t kBBytes = kTileN * kTileK * 2;   // 32 KB
-constexpr uint32_t kStageBytes = kABytes + kBBytes;  // 48 KB
+// Ring geometry per variant: tiles per stage of each operand, stages.
+template <bool SPLIT3>
+struct Ring {
+    static constexpr int kTiles = SPLIT3 ? 2 : 1;
+    static constexpr int kStages = SPLIT3 ? 2 : 4;
+    static constexpr uint32_t kStageBytes = kTiles * (kABytes + kBBytes);  // 48 or 96 KB
+};
 constexpr uint32_t kTmemCols = 512;                   // two 256-column accumulators
 constexpr int kThreads = 192;
 constexpr long long kWaitBudget = 4000000000ll;       // clock cycles (~2 s)
@@ -136,13 +143,17 @@ __device__ __forceinline__ float tile_distance(const TcScoreArgs& a, float s, fl
     return 1.0f - s;
 }
 
+template <bool SPLIT3>
 __global__ void __launch_bounds__(kThreads, 1)
     score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
+    constexpr int kStages = Ring<SPLIT3>::kStages, kT = Ring<SPLIT3>::kTiles;
+    constexpr uint32_t kStageBytes = Ring<SPLIT3>::kStageBytes;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte alignment for the swizzled tiles.
+    // 1024-byte alignment for the swizzled tiles. Stage s holds kT A tiles
+    // (hi, lo) then kT B tiles.
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char* sA = smem;
-    unsigned char* sB = smem + kStages * kABytes;
+    auto tileA = [&](uint32_t s, int t) { return smem + s * kStageBytes + uint32_t(t) * kABytes; };
+    auto tileB = [&](uint32_t s, int t) { return smem + s * kStageBytes + kT * kABytes + uint32_t(t) * kBBytes; };
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
     uint64_t* empty = full + kStages;
     uint64_t* acc_full = empty + kStages;
@@ -190,8 +201,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     mbar_expect_tx(&full[s], kStageBytes);
-                    tma_load_2d(sA + s * kABytes, &tmA, &full[s], int(k * kTileK), int(qt * kTileM));
-                    tma_load_2d(sB + s * kBBytes, &tmB, &full[s], int(k * kTileK), int(nt * kTileN));
+#pragma unroll
+                    for (int tt = 0; tt < kT; ++tt) {
+                        const int x = int(k * kTileK + uint32_t(tt) * a.lo_col);
+                        tma_load_2d(tileA(s, tt), &tmA, &full[s], x, int(qt * kTileM));
+                        tma_load_2d(tileB(s, tt), &tmB, &full[s], x, int(nt * kTileN));
+                    }
                     ++it;
                 }
             }
@@ -221,11 +236,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t ad = umma_desc(smem_u32(sA + s * kABytes));
-                    const uint64_t bd = umma_desc(smem_u32(sB + s * kBBytes));
+                    const uint64_t ah = umma_desc(smem_u32(tileA(s, 0)));
+                    const uint64_t bh = umma_desc(smem_u32(tileB(s, 0)));
+                    if (SPLIT3) {
+                        const uint64_t al = umma_desc(smem_u32(tileA(s, kT - 1)));
+                        const uint64_t bl = umma_desc(smem_u32(tileB(s, kT - 1)));
 #pragma unroll
-                    for (uint32_t j = 0; j < kTileK / 16; ++j)
-                        umma_bf16(d, ad + 2 * j, bd + 2 * j, (k | j) != 0 ? 1u : 0u);
+                        for (uint32_t j = 0; j < kTileK / 16; ++j) {
+                            umma_bf16(d, ah + 2 * j, bh + 2 * j, (k | j) != 0 ? 1u : 0u);
+                            umma_bf16(d, ah + 2 * j, bl + 2 * j, 1u);
+                            umma_bf16(d, al + 2 * j, bh + 2 * j, 1u);
+                        }
+                    } else {
+#pragma unroll
+                        for (uint32_t j = 0; j < kTileK / 16; ++j)
+                            umma_bf16(d, ah + 2 * j, bh + 2 * j, (k | j) != 0 ? 1u : 0u);
+                    }
                     umma_commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -320,26 +346,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// Splits rows of fp32 values into BF16 operand rows: plain (K' = D, hi) or
-// 3-term (K' = 3D; query layout hi|hi|lo, row layout hi|lo|hi). Rows are
-// zero padded to kp columns; rows >= n are zero.
+// Splits rows of fp32 values into BF16 operand rows: plain (kp columns: hi,
+// zero padded) or 3-term (two halves of kp / 2 columns: hi, then lo = the
+// BF16 rounding of x - hi, each zero padded). Rows >= n are zero.
 __global__ void split_bf16_kernel(const float* __restrict__ src, uint32_t n, uint32_t dim, uint32_t src_stride,
-                                  __nv_bfloat16* __restrict__ dst, uint32_t rows_padded, uint32_t kp, int terms,
-                                  int query_side) {
+                                  __nv_bfloat16* __restrict__ dst, uint32_t rows_padded, uint32_t kp, int terms) {
     const size_t total = size_t(rows_padded) * kp;
+    const uint32_t half = terms == 3 ? kp / 2 : kp;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
         const uint32_t r = uint32_t(i / kp), c = uint32_t(i % kp);
+        const uint32_t seg = c / half, j = c % half;
         float out = 0.0f;
-        if (r < n) {
-            const uint32_t seg = c / dim, j = c % dim;
-            if (seg < uint32_t(terms)) {
-                const float x = src[size_t(r) * src_stride + j];
-                const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-                const float lo = __bfloat162float(__float2bfloat16_rn(x - __bfloat162float(hi)));
-                // query: hi, hi, lo; row: hi, lo, hi
-                const bool use_lo = terms == 3 && (query_side ? seg == 2 : seg == 1);
-                out = use_lo ? lo : __bfloat162float(hi);
-            }
+        if (r < n && j < dim) {
+            const float x = src[size_t(r) * src_stride + j];
+            const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+            out = seg == 0 ? __bfloat162float(hi) : __bfloat162float(__float2bfloat16_rn(x - __bfloat162float(hi)));
         }
         dst[i] = __float2bfloat16_rn(out);
     }
@@ -457,7 +478,10 @@ bool make_map(CUtensorMap* map, const void* base, uint64_t rows, uint64_t kp, ui
 }
 }  // namespace
 
-uint32_t tc_k_padded(uint32_t dim, int terms) { return (dim * uint32_t(terms) + tc::kTileK - 1) / tc::kTileK * tc::kTileK; }
+uint32_t tc_k_padded(uint32_t dim, int terms) {
+    const uint32_t half = (dim + tc::kTileK - 1) / tc::kTileK * tc::kTileK;
+    return terms == 3 ? 2 * half : half;
+}
 uint32_t tc_rows_padded(uint32_t n, bool query_side) {
     const uint32_t t = query_side ? tc::kTileM : tc::kTileN;
     return (std::max<uint32_t>(n, 1) + t - 1) / t * t;
@@ -467,8 +491,8 @@ cudaError_t tc_split(const float* src, uint32_t n, uint32_t dim, uint32_t src_st
                      uint32_t rows_padded, uint32_t kp, int terms, bool query_side, cudaStream_t stream) {
     const size_t total = size_t(rows_padded) * kp;
     const uint32_t blocks = uint32_t(std::min<size_t>((total + 255) / 256, 148 * 64));
-    tc::split_bf16_kernel<<<blocks, 256, 0, stream>>>(src, n, dim, src_stride, dst, rows_padded, kp, terms,
-                                                      query_side ? 1 : 0);
+    (void)query_side;  // both operands use the same [hi | lo] layout
+    tc::split_bf16_kernel<<<blocks, 256, 0, stream>>>(src, n, dim, src_stride, dst, rows_padded, kp, terms);
     return cudaGetLastError();
 }
 
@@ -484,14 +508,19 @@ cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B
     if (!make_map(&ma, A, qp, kp, tc::kTileM) || !make_map(&mb, B, np_, kp, tc::kTileN)) return cudaErrorInvalidValue;
     TcScoreArgs a = args_in;
     a.q_tiles = qp / tc::kTileM;
-    a.k_chunks = kp / tc::kTileK;
-    const size_t smem = 1024 + size_t(tc::kStages) * tc::kStageBytes + 256;
-    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(tc::score_kernel));
+    const bool split = a.terms == 3;
+    a.lo_col = split ? kp / 2 : 0;
+    a.k_chunks = (split ? kp / 2 : kp) / tc::kTileK;
+    const size_t smem = 1024 + size_t(split ? tc::Ring<true>::kStages * tc::Ring<true>::kStageBytes
+                                            : tc::Ring<false>::kStages * tc::Ring<false>::kStageBytes) +
+                        256;
+    auto kern = split ? tc::score_kernel<true> : tc::score_kernel<false>;
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
     const uint32_t total = a.q_tiles * (a.n_tile_end - a.n_tile_begin);
     if (total == 0) return cudaSuccess;
     const uint32_t grid = std::min<uint32_t>(total, uint32_t(num_sms));
-    tc::score_kernel<<<grid, tc::kThreads, smem, stream>>>(ma, mb, a);
+    kern<<<grid, tc::kThreads, smem, stream>>>(ma, mb, a);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,8 @@ namespace hnswgpu {
 // (256 rows each) for all query tiles (128 queries each).
 struct TcScoreArgs {
     uint32_t q_tiles = 0, k_chunks = 0;   // set by tc_score
+    int terms = 1;                        // 1: plain BF16; 3: split (operands [hi | lo])
+    uint32_t lo_col = 0;                  // set by tc_score: first column of the lo half
     uint32_t n_tile_begin = 0, n_tile_end = 0;
     uint32_t nq = 0, n = 0;               // valid queries / rows
     int metric = 0;
@@ -31,7 +33,7 @@ struct TcScoreArgs {
 
 uint32_t tc_k_padded(uint32_t dim, int terms);
 uint32_t tc_rows_padded(uint32_t n, bool query_side);
-// fp32 rows -> BF16 operand rows (terms 1: hi; terms 3: query hi|hi|lo, row hi|lo|hi).
+// fp32 rows -> BF16 operand rows (terms 1: hi; terms 3: [hi | lo], halves of kp / 2).
 cudaError_t tc_split(const float* src, uint32_t n, uint32_t dim, uint32_t src_stride, __nv_bfloat16* dst,
                      uint32_t rows_padded, uint32_t kp, int terms, bool query_side, cudaStream_t stream);
 cudaError_t tc_row_norms(const float* src, uint32_t n, uint32_t dim, uint32_t stride, float* out, cudaStream_t stream);

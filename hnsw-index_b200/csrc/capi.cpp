@@ -1108,6 +1108,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     CU(b->thr1.ensure(size_t(qp) * 4), "cudaMalloc thresholds");
     CU(b->thr2.ensure(size_t(qp) * 4), "cudaMalloc thresholds");
     TcScoreArgs t;
+    t.terms = terms;
     t.nq = uint32_t(nq);
     t.n = b->n;
     t.metric = b->metric;
