@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "capi_internal.hpp"
+#include "gpu_build.hpp"
 
 using namespace hnswgpu;
 
@@ -1408,6 +1409,87 @@ int hnsw_builder_remove(hnsw_builder* b, uint64_t key, int* removed) {
     if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
     bool r = b->b->remove(key);
     if (removed) *removed = r ? 1 : 0;
+    return HNSW_OK;
+}
+
+int hnsw_builder_compact(hnsw_builder* b, int threads) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    b->b->compact(threads);
+    return HNSW_OK;
+}
+
+void hnsw_gpu_build_opts_default(hnsw_gpu_build_opts* out) {
+    GpuBuildOptions o;
+    out->wave_fraction = o.wave_fraction;
+    out->max_wave = o.max_wave;
+    out->hash_cap = o.hash_cap;
+}
+
+static GpuBuildOptions build_options(const hnsw_gpu_build_opts* opts) {
+    GpuBuildOptions o;
+    if (opts) {
+        o.wave_fraction = opts->wave_fraction;
+        o.max_wave = opts->max_wave;
+        o.hash_cap = opts->hash_cap;
+    }
+    return o;
+}
+
+static void record_stats(hnsw_builder* b, const GpuBuildReport& r) {
+    hnsw_gpu_build_stats& s = b->last;
+    s.waves = r.waves;
+    s.nodes = r.nodes;
+    s.spills = r.spills;
+    s.inexact = r.inexact;
+    s.shrinks = r.shrinks;
+    s.records = r.records;
+    s.device_ms = r.device_ms;
+    s.search_warps_per_block = r.search_warps_per_block;
+    s.search_blocks_per_sm = r.search_blocks_per_sm;
+    s.connect_warps_per_block = r.connect_warps_per_block;
+    s.connect_blocks_per_sm = r.connect_blocks_per_sm;
+    s.hash_cap = r.hash_cap;
+}
+
+int hnsw_builder_insert_batch_gpu(hnsw_builder* b, const uint64_t* keys, const float* v, size_t n, size_t dim,
+                                  int device, const hnsw_gpu_build_opts* opts) {
+    if (!b || (n && (!keys || !v))) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    if (dim != b->b->index().dim) return set_error(HNSW_ERR_DIMENSION_MISMATCH, "dimension mismatch");
+    const GpuBuildOptions o = build_options(opts);
+    if (!(o.wave_fraction > 0.0) || o.wave_fraction > 1.0 || o.max_wave == 0)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "wave_fraction must be in (0, 1] and max_wave >= 1");
+    uint32_t first = 0;
+    int st = from_err(b->b->append_batch(keys, v, n, &first));
+    if (st) return st;
+    GpuBuildReport rep;
+    st = gpu_link(b->b->graph(), first, device, o, &rep);
+    if (st) {
+        b->b->truncate(first);
+        return st;
+    }
+    record_stats(b, rep);
+    return HNSW_OK;
+}
+
+int hnsw_builder_compact_gpu(hnsw_builder* b, int device, const hnsw_gpu_build_opts* opts) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    const GpuBuildOptions o = build_options(opts);
+    if (!(o.wave_fraction > 0.0) || o.wave_fraction > 1.0 || o.max_wave == 0)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "wave_fraction must be in (0, 1] and max_wave >= 1");
+    std::unique_ptr<Builder> fresh = b->b->compacted_unlinked();
+    if (!fresh) return HNSW_OK;
+    GpuBuildReport rep;
+    int st = gpu_link(fresh->graph(), 0, device, o, &rep);
+    if (st) return st;
+    if (b->b->index().quantized) fresh->enable_quantization();
+    b->b = std::move(fresh);
+    record_stats(b, rep);
+    return HNSW_OK;
+}
+
+int hnsw_builder_gpu_stats(const hnsw_builder* b, hnsw_gpu_build_stats* out) {
+    if (!b || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    *out = b->last;
     return HNSW_OK;
 }
 

@@ -206,6 +206,7 @@ struct hnsw_gpu_brute {
 
 struct hnsw_builder {
     std::unique_ptr<Builder> b;
+    hnsw_gpu_build_stats last{};  // figures of the last device link
 };
 
 namespace hnswgpu {

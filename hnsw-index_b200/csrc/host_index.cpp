@@ -625,14 +625,6 @@ void synthetic_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, 
 // ---------------------------------------------------------------------------
 namespace {
 
-// build::sample_level (src/hnsw/build.rs:19-28).
-uint8_t sample_level(uint64_t seed, uint32_t id, double ml) {
-    uint64_t h = mix64(seed ^ mix64(uint64_t(id) + 0x9E3779B97F4A7C15ULL));
-    double u = double((h >> 11) + 1) * (1.0 / double(1ULL << 53));
-    double level = std::floor(-std::log(u) * ml);
-    if (level >= double(kMaxLevel)) return kMaxLevel;
-    return uint8_t(level);
-}
 
 inline int32_t total_key(float f) {
     int32_t b;
@@ -665,6 +657,15 @@ struct SpinLock {
 };
 
 }  // namespace
+
+// build::sample_level (src/hnsw/build.rs:19-28).
+uint8_t sample_level(uint64_t seed, uint32_t id, double ml) {
+    uint64_t h = mix64(seed ^ mix64(uint64_t(id) + 0x9E3779B97F4A7C15ULL));
+    double u = double((h >> 11) + 1) * (1.0 / double(1ULL << 53));
+    double level = std::floor(-std::log(u) * ml);
+    if (level >= double(kMaxLevel)) return kMaxLevel;
+    return uint8_t(level);
+}
 
 struct Builder::Impl {
     std::unique_ptr<SpinLock[]> locks;
@@ -742,6 +743,14 @@ Err Builder::insert(uint64_t key, const float* v) {
 }
 
 Err Builder::insert_batch(const uint64_t* keys, const float* v, size_t count, int threads) {
+    uint32_t first = 0;
+    Err e = append_batch(keys, v, count, &first);
+    if (e) return e;
+    link_range(first, threads);
+    return Err();
+}
+
+Err Builder::append_batch(const uint64_t* keys, const float* v, size_t count, uint32_t* first_out) {
     std::vector<float> prepared;
     prepared.reserve(count * ix_.dim);
     for (size_t i = 0; i < count; ++i) {
@@ -758,7 +767,24 @@ Err Builder::insert_batch(const uint64_t* keys, const float* v, size_t count, in
         }
     if (kMaxNodes - ix_.node_count() < count) return fail(HNSW_ERR_CAPACITY_EXCEEDED);
     ix_.vectors.insert(ix_.vectors.end(), prepared.begin(), prepared.end());
-    uint32_t first = push_nodes(keys, count);
+    *first_out = push_nodes(keys, count);
+    return Err();
+}
+
+void Builder::truncate(uint32_t first) {
+    for (size_t id = first; id < ix_.node_count(); ++id) {
+        auto it = ix_.key_to_id.find(ix_.keys[id]);
+        if (it != ix_.key_to_id.end() && it->second == id) ix_.key_to_id.erase(it);
+    }
+    ix_.vectors.resize(size_t(first) * ix_.dim);
+    ix_.keys.resize(first);
+    ix_.levels.resize(first);
+    ix_.deleted.resize(first);
+    ix_.l0.resize(size_t(first) * (ix_.params.m0 + 1));
+    ix_.upper.resize(first);
+}
+
+void Builder::link_range(uint32_t first, int threads) {
     // link_parallel (src/hnsw/mod.rs:340-349)
     uint32_t end = uint32_t(ix_.node_count()), next = first;
     int nt = threads > 0 ? threads : int(std::max(1u, std::thread::hardware_concurrency()));
@@ -778,7 +804,34 @@ Err Builder::insert_batch(const uint64_t* keys, const float* v, size_t count, in
         for (int t = 0; t < nt; ++t) pool.emplace_back(worker, t);
         for (auto& th : pool) th.join();
     }
-    return Err();
+}
+
+std::unique_ptr<Builder> Builder::compacted_unlinked() const {
+    const size_t n = ix_.node_count();
+    size_t live = 0;
+    for (size_t id = 0; id < n; ++id) live += ix_.deleted[id] ? 0 : 1;
+    if (live == n) return nullptr;
+    std::unique_ptr<Builder> fresh(new Builder(ix_.dim, ix_.metric, ix_.params));
+    std::vector<uint64_t> keys;
+    keys.reserve(live);
+    fresh->ix_.vectors.reserve(live * ix_.dim);
+    for (size_t id = 0; id < n; ++id) {
+        if (ix_.deleted[id]) continue;
+        keys.push_back(ix_.keys[id]);
+        const float* row = ix_.vector(uint32_t(id));
+        fresh->ix_.vectors.insert(fresh->ix_.vectors.end(), row, row + ix_.dim);
+    }
+    fresh->push_nodes(keys.data(), keys.size());
+    return fresh;
+}
+
+void Builder::compact(int threads) {
+    std::unique_ptr<Builder> fresh = compacted_unlinked();
+    if (!fresh) return;
+    fresh->link_range(0, threads);
+    if (ix_.quantized) fresh->enable_quantization();
+    std::swap(ix_, fresh->ix_);
+    std::swap(impl_, fresh->impl_);
 }
 
 bool Builder::remove(uint64_t key) {

@@ -116,6 +116,9 @@ float dot_ref(const float* a, const float* b, size_t n);
 float l2_ref(const float* a, const float* b, size_t n);
 float metric_distance(int metric, const float* a, const float* b, size_t n);
 
+// build::sample_level (src/hnsw/build.rs:19-28).
+uint8_t sample_level(uint64_t seed, uint32_t id, double ml);
+
 // vector::check (src/vector.rs:22-40). Returns 0 or a status, norm in *norm_sq.
 int check_vector(const float* v, size_t dim, double* norm_sq);
 
@@ -129,6 +132,24 @@ public:
     bool remove(uint64_t key);
     void enable_quantization();
     const HostIndex& index() const { return ix_; }
+
+    // The validation and append half of insert_batch: the batch is checked
+    // whole, then its nodes are stored (levels sampled) without links.
+    // *first is the first new id. Used by linkers outside this class.
+    Err append_batch(const uint64_t* keys, const float* v, size_t n, uint32_t* first);
+    // Drops the nodes from `first` on (undoes append_batch).
+    void truncate(uint32_t first);
+    // link_parallel (src/hnsw/mod.rs:340-349) on `threads` host threads.
+    void link_range(uint32_t first, int threads);
+    // The graph a linker writes (lists and entry point).
+    HostIndex& graph() { return ix_; }
+    // compact (src/hnsw/mod.rs:381-400) up to the linking step: a new
+    // builder holding the live nodes (keys, vectors, levels re-sampled by
+    // their new ids), unlinked; null when there are no tombstones.
+    std::unique_ptr<Builder> compacted_unlinked() const;
+    // compact with link_parallel on `threads` host threads; the index is
+    // unchanged when there are no tombstones.
+    void compact(int threads);
 
 private:
     struct Impl;

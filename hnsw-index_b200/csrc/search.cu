@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "device.hpp"
+#include "warp_sort.cuh"
 
 namespace hnswgpu {
 namespace dev {
@@ -77,35 +78,6 @@ struct Ws {
     uint32_t b_chunks, b_count;
     uint64_t b_min, b_max;
 };
-
-__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
-
-// Inserts x into the ascending array A[lo, hi) (capacity permitting one more
-// entry). Returns the insertion position.
-__device__ __forceinline__ uint32_t sorted_insert(uint64_t* A, uint32_t lo, uint32_t hi, uint64_t x) {
-    const int lane = lane_id();
-    uint32_t pos = lo;
-    for (uint32_t base = lo; base < hi; base += 32) {
-        uint32_t i = base + lane;
-        bool lt = i < hi && A[i] < x;
-        pos += __popc(__ballot_sync(kFull, lt));
-    }
-    // Shift [pos, hi) up by one, highest chunk first.
-    if (hi > pos) {
-        uint32_t n = hi - pos;
-        for (int c = int((n - 1) >> 5); c >= 0; --c) {
-            uint32_t i = pos + uint32_t(c) * 32 + lane;
-            bool mv = i < hi;
-            uint64_t v = mv ? A[i] : 0;
-            __syncwarp();
-            if (mv) A[i + 1] = v;
-            __syncwarp();
-        }
-    }
-    if (lane == 0) A[pos] = x;
-    __syncwarp();
-    return pos;
-}
 
 // Visited test-and-set. Returns true if id was not visited before.
 // *full is set when the hash passes its load limit.
@@ -317,68 +289,6 @@ __device__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
         if (bid == from) return best;
         best = (uint64_t(fkey(bd)) << 32) | bid;
     }
-}
-
-// First index in the ascending A[lo, hi) whose entry is not below x (one lane).
-__device__ __forceinline__ uint32_t lower_bound(const uint64_t* A, uint32_t lo, uint32_t hi, uint64_t x) {
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (A[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Merges the entries x held by the lanes in S into the ascending A[lo, hi),
-// keeping only positions below `limit` (truncation of the results array to
-// ef). Entries are distinct. All lanes call.
-__device__ __forceinline__ void batch_merge(uint64_t* A, uint32_t lo, uint32_t hi, uint32_t S, uint64_t x,
-                                            uint32_t limit) {
-    const int lane = lane_id();
-    const bool in = (S >> lane) & 1u;
-    uint32_t rank_s = 0;
-    for (uint32_t bits = S; bits; bits &= bits - 1) {
-        const int j = __ffs(bits) - 1;
-        rank_s += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
-    }
-    const uint32_t pa = in ? lower_bound(A, lo, hi, x) : hi;
-    // The smallest new entry sits at the lowest insertion point.
-    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
-    if (hi > pmin) {
-        for (int base = int((hi - 1) & ~31u); base >= int(pmin & ~31u); base -= 32) {
-            const uint32_t k = uint32_t(base) + uint32_t(lane);
-            const bool mv = k >= pmin && k < hi;
-            const uint64_t v = mv ? A[k] : 0;
-            uint32_t shift = 0;
-            for (uint32_t bits = S; bits; bits &= bits - 1) {
-                const int j = __ffs(bits) - 1;
-                shift += (__shfl_sync(kFull, x, j) < v) ? 1u : 0u;
-            }
-            __syncwarp();
-            if (mv && k + shift < limit) A[k + shift] = v;
-            __syncwarp();
-        }
-    }
-    if (in && pa + rank_s < limit) A[pa + rank_s] = x;
-    __syncwarp();
-}
-
-__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const uint64_t o = __shfl_xor_sync(kFull, v, off);
-        v = o < v ? o : v;
-    }
-    return v;
-}
-
-__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const uint64_t o = __shfl_xor_sync(kFull, v, off);
-        v = o > v ? o : v;
-    }
-    return v;
 }
 
 // Lane of the r-th (from 0) set bit of m; m has more than r bits set.

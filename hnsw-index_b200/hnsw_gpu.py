@@ -208,6 +208,26 @@ _lib.hnsw_builder_insert.argtypes = [_vp, C.c_uint64, _vp, _sz]
 _lib.hnsw_builder_insert_batch.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_int]
 _lib.hnsw_builder_remove.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_int)]
 _lib.hnsw_builder_enable_quantization.argtypes = [_vp]
+_lib.hnsw_builder_compact.argtypes = [_vp, C.c_int]
+
+
+class _BuildOpts(C.Structure):
+    _fields_ = [("wave_fraction", C.c_double), ("max_wave", C.c_uint32), ("hash_cap", C.c_uint32)]
+
+
+class _BuildStats(C.Structure):
+    _fields_ = [("waves", C.c_uint32), ("nodes", C.c_uint32), ("spills", C.c_uint64), ("inexact", C.c_uint64),
+                ("shrinks", C.c_uint64), ("records", C.c_uint64), ("device_ms", C.c_double),
+                ("search_warps_per_block", C.c_uint32), ("search_blocks_per_sm", C.c_uint32),
+                ("connect_warps_per_block", C.c_uint32), ("connect_blocks_per_sm", C.c_uint32),
+                ("hash_cap", C.c_uint32)]
+
+
+_lib.hnsw_gpu_build_opts_default.argtypes = [C.POINTER(_BuildOpts)]
+_lib.hnsw_gpu_build_opts_default.restype = None
+_lib.hnsw_builder_insert_batch_gpu.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_int, C.POINTER(_BuildOpts)]
+_lib.hnsw_builder_compact_gpu.argtypes = [_vp, C.c_int, C.POINTER(_BuildOpts)]
+_lib.hnsw_builder_gpu_stats.argtypes = [_vp, C.POINTER(_BuildStats)]
 _lib.hnsw_builder_to_bytes.argtypes = [_vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(_sz)]
 _lib.hnsw_bytes_free.argtypes = [C.POINTER(C.c_uint8)]
 _lib.hnsw_bytes_free.restype = None
@@ -230,6 +250,8 @@ EXPORTED_SYMBOLS = (
     "hnsw_builder_to_bytes", "hnsw_bytes_free", "hnsw_synthetic_gaussian",
     "hnsw_synthetic_mixture", "hnsw_synthetic_mixture_split", "hnsw_crc32", "hnsw_gpu_autotune",
     "hnsw_gpu_clear_tuning", "hnsw_gpu_set_schedule", "hnsw_gpu_brute_search_filtered",
+    "hnsw_builder_compact", "hnsw_gpu_build_opts_default", "hnsw_builder_insert_batch_gpu",
+    "hnsw_builder_compact_gpu", "hnsw_builder_gpu_stats",
 )
 
 LIBRARY_PATH = _LIB_PATH
@@ -858,6 +880,46 @@ class IndexBuilder:
             raise Error(Status.DIMENSION_MISMATCH,
                         f"dimension mismatch: expected {keys.size * self._dim}, got {v.size}")
         _check(_lib.hnsw_builder_insert_batch(self._h, _ptr(keys), _ptr(v), keys.size, self._dim, threads))
+
+    def insert_batch_gpu(self, keys, vectors, device: int = 0, wave_fraction: Optional[float] = None,
+                         max_wave: Optional[int] = None, hash_cap: Optional[int] = None):
+        """insert_batch with the link step on a GPU (waves of nodes; see hnsw_gpu.h)."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        v = np.ascontiguousarray(vectors, dtype=np.float32).reshape(-1)
+        if v.size != keys.size * self._dim:
+            raise Error(Status.DIMENSION_MISMATCH,
+                        f"dimension mismatch: expected {keys.size * self._dim}, got {v.size}")
+        o = self._build_opts(wave_fraction, max_wave, hash_cap)
+        _check(_lib.hnsw_builder_insert_batch_gpu(self._h, _ptr(keys), _ptr(v), keys.size, self._dim, device,
+                                                  C.byref(o)))
+
+    def compact(self, threads: int = 0):
+        """HnswIndex::compact: rebuild from the live nodes (no-op without tombstones)."""
+        _check(_lib.hnsw_builder_compact(self._h, threads))
+
+    def compact_gpu(self, device: int = 0, wave_fraction: Optional[float] = None, max_wave: Optional[int] = None,
+                    hash_cap: Optional[int] = None):
+        """compact with the link step on a GPU."""
+        o = self._build_opts(wave_fraction, max_wave, hash_cap)
+        _check(_lib.hnsw_builder_compact_gpu(self._h, device, C.byref(o)))
+
+    def gpu_stats(self) -> dict:
+        """Figures of the last device link."""
+        st = _BuildStats()
+        _check(_lib.hnsw_builder_gpu_stats(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in _BuildStats._fields_}
+
+    @staticmethod
+    def _build_opts(wave_fraction, max_wave, hash_cap) -> "_BuildOpts":
+        o = _BuildOpts()
+        _lib.hnsw_gpu_build_opts_default(C.byref(o))
+        if wave_fraction is not None:
+            o.wave_fraction = wave_fraction
+        if max_wave is not None:
+            o.max_wave = max_wave
+        if hash_cap is not None:
+            o.hash_cap = hash_cap
+        return o
 
     def remove(self, key: int) -> bool:
         r = C.c_int()

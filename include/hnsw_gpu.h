@@ -377,6 +377,45 @@ int hnsw_builder_insert_batch(hnsw_builder* b, const uint64_t* keys, const float
                               size_t dim, int threads);
 /* HnswIndex::remove (mod.rs:357-365). *removed = 1 if the key was live. */
 int hnsw_builder_remove(hnsw_builder* b, uint64_t key, int* removed);
+/* HnswIndex::compact (mod.rs:381-400): rebuilds from the live nodes with
+ * link_parallel on `threads` host threads (0 = all cores). No-op without
+ * tombstones. */
+int hnsw_builder_compact(hnsw_builder* b, int threads);
+
+/* Device construction. The batch is validated and appended exactly as by
+ * hnsw_builder_insert_batch (same errors, index unchanged on error); the
+ * new nodes are then linked on `device` in waves: every node of a wave
+ * searches the graph as it stood before the wave, and its reverse edges are
+ * applied list by list in ascending node id with connect's push-or-shrink
+ * rule. Node levels and the wave plan depend only on the inputs, so the
+ * graph is deterministic; with max_wave = 1 every wave is one node and the
+ * graph equals the sequential insert() sequence bit for bit. */
+typedef struct hnsw_gpu_build_opts {
+    double wave_fraction; /* nodes per wave = max(1, floor(linked * fraction)); (0, 1] */
+    uint32_t max_wave;    /* at most this many nodes per wave (>= 1) */
+    uint32_t hash_cap;    /* visited-hash entries per warp; 0 = 32 per unit of ef */
+} hnsw_gpu_build_opts;
+typedef struct hnsw_gpu_build_stats {
+    uint32_t waves, nodes;
+    uint64_t spills;   /* layer searches whose visited set moved to HBM */
+    uint64_t inexact;  /* candidate queues that dropped a live entry (0 in practice) */
+    uint64_t shrinks;  /* full lists re-selected by a reverse edge */
+    uint64_t records;  /* reverse edges */
+    double device_ms;  /* device time of the waves (CUDA events) */
+    uint32_t search_warps_per_block, search_blocks_per_sm;
+    uint32_t connect_warps_per_block, connect_blocks_per_sm;
+    uint32_t hash_cap;
+} hnsw_gpu_build_stats;
+/* Defaults: wave_fraction 0.02, max_wave 65536, hash_cap 0. */
+void hnsw_gpu_build_opts_default(hnsw_gpu_build_opts* out);
+/* HnswIndex::insert_batch (mod.rs:318-338) with the link step on a GPU.
+ * opts may be NULL (defaults). */
+int hnsw_builder_insert_batch_gpu(hnsw_builder* b, const uint64_t* keys, const float* vectors, size_t n,
+                                  size_t dim, int device, const hnsw_gpu_build_opts* opts);
+/* HnswIndex::compact with the link step on a GPU. */
+int hnsw_builder_compact_gpu(hnsw_builder* b, int device, const hnsw_gpu_build_opts* opts);
+/* Figures of the builder's last device link (zeros before the first). */
+int hnsw_builder_gpu_stats(const hnsw_builder* b, hnsw_gpu_build_stats* out);
 /* HnswIndex::enable_quantization (mod.rs:544-547). */
 int hnsw_builder_enable_quantization(hnsw_builder* b);
 /* HnswIndex::to_bytes (mod.rs:639-643). Free the buffer with hnsw_bytes_free. */

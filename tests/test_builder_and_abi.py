@@ -87,6 +87,33 @@ def test_graphs_satisfy_invariants_and_stay_connected(selection, parallel):
     assert 4.0 < mean_degree <= 16.0
 
 
+def test_compaction_drops_tombstones_and_keeps_live_keys():
+    # src/hnsw/tests.rs:266-291 (host link step; recall through the oracle's search).
+    import oracle as O
+
+    base, queries = H.gaussian(1000, 20, 16, 6)
+    b = H.IndexBuilder(16, H.Metric.L2, H.HnswParams())
+    for i in range(1000):
+        b.insert(i, base[i])
+    b.enable_quantization()
+    for key in range(0, 1000, 3):
+        assert b.remove(key)
+    b.compact(threads=2)
+    data = b.to_bytes()
+    info = H.validate_bytes(data)
+    live = 1000 - len(range(0, 1000, 3))
+    assert (info.nodes, info.live, info.quantized) == (live, live, 1)
+    p = parse(data)
+    assert_invariants(p)
+    assert reachable(p) * 100 >= live * 99
+    keep = np.array([k for k in range(1000) if k % 3 != 0], np.uint64)
+    tk, _, tc, _ = O.brute(0, base[keep.astype(np.int64)], queries, 10, keys=keep)
+    fk, _, fc, _ = O.Index(data).search(queries, 10, 100)
+    assert O.recall_at_k(tk, tc, fk, fc, 10) > 0.95
+    b.compact()
+    assert b.to_bytes() == data
+
+
 def test_sequential_build_is_deterministic():
     base, _ = H.gaussian(500, 10, 8, 1)
     assert build_index(base, parallel=False, seed=0) == build_index(base, parallel=False, seed=0)
