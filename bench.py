@@ -804,6 +804,120 @@ def run_serve(args):
 # Small single-kernel cases, sized for ncu captures (a few GB on the device at
 # most, inputs larger than L2, three launches of the kernel of interest).
 # ---------------------------------------------------------------------------
+def build_bytes_search(st, dim) -> float:
+    """Algorithmic bytes of the build's search kernel: a 4D-byte row per
+    distance, 4(M0+1) per layer-0 list read and 4(M+1) per upper list."""
+    return 4.0 * dim * st["dist_search"] + 4.0 * (2 * M + 1) * st["lists0"] + 4.0 * (M + 1) * st["listsU"]
+
+
+def run_build(args):
+    """insert_batch of config 2's 1M x 128 base with the link step on the GPU
+    (M=16, ef_construction=200), against the host builder on all cores."""
+    import hnsw_gpu as H
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nb = args.build_n
+    base, queries = load_data()
+    base = np.ascontiguousarray(base[:nb])
+    keys = np.arange(nb, dtype=np.uint64)
+    params = H.HnswParams(m=M, ef_construction=EF_CONSTRUCTION, seed=LEVEL_SEED)
+    cores = os.cpu_count() or 1
+    sample = min(nb, 200_000)
+    if args.impl == "reference":
+        # The host builder (restatement of insert_batch) on all cores, on a
+        # bounded sample of the same base.
+        times = []
+        for i in range(max(args.warmup, 0) + args.steps):
+            t = time.perf_counter()
+            b = H.IndexBuilder(DIM, H.Metric.L2, params)
+            b.insert_batch(keys[:sample], base[:sample])
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t)
+        v = sample / statistics.median(times)
+        print(json.dumps({
+            "impl": "reference", "metric": "nodes linked per second (insert_batch, 1M x 128 clustered, M=16, efC=200)",
+            "value": v, "unit": "nodes/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "build-1Mx128-clustered", "n_base": nb},
+            "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": cores, "kind": "port",
+                             "sample": f"insert_batch of the first {sample} nodes"},
+            "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+    stats, walls = [], []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        b = H.IndexBuilder(DIM, H.Metric.L2, params)
+        b.insert_batch_gpu(keys, base, device=0, timing=True)
+        wall = time.perf_counter() - t
+        st = b.gpu_stats()
+        log(f"build {i}: wall {wall:.2f} s, device {st['device_ms']:.0f} ms (search {st['search_ms']:.0f}, "
+            f"connect {st['connect_ms']:.0f}), waves {st['waves']}, spills {st['spills']}")
+        if i >= args.warmup:
+            walls.append(wall)
+            stats.append(st)
+    data = b.to_bytes()
+    dev_ms = statistics.median(s_["device_ms"] for s_ in stats)
+    search_ms = statistics.median(s_["search_ms"] for s_ in stats)
+    connect_ms = statistics.median(s_["connect_ms"] for s_ in stats)
+    st = stats[-1]
+    # Recall of the device-built graph and of the host-built one (same search).
+    bf = H.BruteForceIndex(DIM, H.Metric.L2)
+    bf.insert_batch(keys, base)
+    tk, _, tc, _ = bf.search_arrays(queries, K)
+    recalls = {}
+    for name, blob in (("gpu_built", data), ("host_built", None)):
+        if blob is None:
+            if nb != N_BASE:
+                continue
+            blob, _ = index_file(base, 0, lambda: None)
+        gi = H.HnswIndex.from_bytes(blob)
+        recalls[name] = {}
+        for ef in (32, 64, 128):
+            fk, _, fc, _ = gi.search_arrays(queries, K, ef)
+            recalls[name][ef] = O.recall_at_k(tk, tc, fk, fc, K)
+        del gi
+    # Host builder on all cores, bounded sample.
+    cpu_v = None
+    if not args.no_cpu_baseline:
+        t = time.perf_counter()
+        hb = H.IndexBuilder(DIM, H.Metric.L2, params)
+        hb.insert_batch(keys[:sample], base[:sample])
+        cpu_v = sample / (time.perf_counter() - t)
+    peak, peak_kind = measured_peaks()
+    achieved = build_bytes_search(st, DIM) / (search_ms / 1e3) / 1e9
+    h2d = base.nbytes + nb * (2 * M) * 4
+    d2h = nb * (2 * M) * 4
+    line = {
+        "metric": "nodes linked per second (insert_batch, 1M x 128 clustered, M=16, efC=200)",
+        "value": nb / (dev_ms / 1e3), "unit": "nodes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "build-1Mx128-clustered", "n_base": nb, "dim": DIM, "m": M,
+                   "ef_construction": EF_CONSTRUCTION, "wave_fraction": 0.02, "waves": st["waves"],
+                   "search_ms": search_ms, "connect_ms": connect_ms, "spills": st["spills"],
+                   "inexact": st["inexact"], "shrinks": st["shrinks"], "reverse_edges": st["records"],
+                   "distances": {"search": st["dist_search"], "select_pairs": st["dist_select"],
+                                 "connect": st["dist_connect"]},
+                   "lists_read": {"layer0": st["lists0"], "upper": st["listsU"]},
+                   "geometry": {k_: st[k_] for k_ in ("search_warps_per_block", "search_blocks_per_sm",
+                                                      "connect_warps_per_block", "connect_blocks_per_sm",
+                                                      "hash_cap")},
+                   "recall_at_10": recalls, "l2_flush": "inputs larger than L2 (512 MB of rows)"},
+        "roofline": {"bound": "hbm", "kernel": "build_search_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+        "e2e": {"value": nb / statistics.median(walls), "unit": "nodes/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": st["waves"] * 4,
+    }
+    if cpu_v is not None:
+        line["cpu_baseline"] = {"value": cpu_v, "unit": "nodes/s", "cores": cores, "kind": "port",
+                                "sample": f"host insert_batch of the first {sample} nodes"}
+    print(json.dumps(line))
+    return 0
+
+
 def run_case(args):
     import hnsw_gpu as H
 
@@ -862,6 +976,16 @@ def run_case(args):
         bits = random_bitmaps(rng, nb, [0.01])[0]
         for _ in range(3):
             r = timed_call(lambda: index.search_arrays(queries, 10, 256, filter_bits=bits, filter_nbits=nb, mode=0))
+    elif args.workload == "case-build-300kx128":
+        # Build kernels: the first 300k rows of config 2's base (154 MB of
+        # rows, more than L2) linked on the GPU (M=16, ef_construction=200),
+        # one build.
+        base, _ = load_data()
+        base = np.ascontiguousarray(base[:300_000])
+        b = H.IndexBuilder(DIM, H.Metric.L2, H.HnswParams(m=M, ef_construction=EF_CONSTRUCTION, seed=LEVEL_SEED))
+        timed_call(lambda: b.insert_batch_gpu(np.arange(300_000, dtype=np.uint64), base, device=0))
+        print(json.dumps({"workload": args.workload, "host_ms_per_call": times, "stats": b.gpu_stats()}))
+        return 0
     else:  # case-brute-200kx768
         # Brute-force kernels: 200k x 768 cosine, 1000 queries, k=100; FP32
         # twice, then BF16x3 twice.
@@ -883,7 +1007,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="plain-1Mx128",
                     choices=["plain-1Mx128", "brute-1Mx768", "batch-5Mx96", "serve-10Mx128", "case-search-1Mx128",
-                             "case-cold-500kx96", "case-retry-200kx64", "case-brute-200kx768"])
+                             "case-cold-500kx96", "case-retry-200kx64", "case-brute-200kx768", "build-1Mx128",
+                             "case-build-300kx128"])
     ap.add_argument("--case-mode", type=int, default=1)
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
@@ -893,7 +1018,12 @@ def main():
     ap.add_argument("--serve-batch", type=int, default=1024)
     ap.add_argument("--serve-linger", type=int, default=100)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--build-n", type=int, default=1_000_000)
     args = ap.parse_args()
+    if args.workload == "build-1Mx128":
+        if args.steps == 200:
+            args.steps = 3
+        return run_build(args)
     if args.workload == "brute-1Mx768":
         return run_brute(args)
     if args.workload == "batch-5Mx96":

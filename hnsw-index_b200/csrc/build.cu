@@ -51,6 +51,8 @@ struct BWarp {
     bool bitmap;
     uint32_t* spill;
     uint32_t spill_words;
+    // Work counters (warp-uniform).
+    uint32_t nd, nl0, nlU;
 };
 
 __device__ __forceinline__ uint32_t list_cap(const BuildGraph& g, uint32_t layer) { return layer == 0 ? g.m0 : g.m; }
@@ -152,11 +154,13 @@ __device__ uint64_t bgreedy(const BuildGraph& g, BWarp& w, uint64_t best, uint32
         const uint32_t* blk = list_ptr(g, layer, from);
         float bd = pdist(best);
         uint32_t bid = from;
+        ++w.nlU;
         for (uint32_t b = 0; b < cap; b += 32) {
             const uint32_t id = (b + lane < cap) ? __ldg(blk + b + lane) : kEmpty;
             const uint32_t V = __ballot_sync(kFull, id != kEmpty);
             if (V == 0) break;
             fresh_distances(g, w, id, V);
+            w.nd += __popc(V);
             float d = ((V >> lane) & 1u) ? w.fd[lane] : __int_as_float(0x7f800000);
             int idx = lane;
 #pragma unroll
@@ -252,6 +256,8 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
         ++head;
         if (rs >= ef && pdist(cur) > pdist(w.R[rs - 1])) break;
         const uint32_t* row = list_ptr(g, layer, pid(cur));
+        if (layer) ++w.nlU;
+        else ++w.nl0;
         if (lane == 0 && head < tail) prefetch_l2(list_ptr(g, layer, pid(w.C[head])), (layer ? g.mp : g.m0p) * 4);
         for (uint32_t b = 0; b < cap; b += 32) {
             const uint32_t id = (b + lane < cap) ? __ldg(row + b + lane) : kEmpty;
@@ -268,6 +274,7 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
             visited += __popc(F);
             if (F != 0) {
                 fresh_distances(g, w, id, F);
+                w.nd += __popc(F);
                 const bool adm = fresh && id != self;
                 const uint32_t A = __ballot_sync(kFull, adm);
                 const float my_d = fresh ? w.fd[lane] : 0.0f;
@@ -346,7 +353,7 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
 // sel/seld; returns the count.
 __device__ uint32_t bheuristic(const BuildGraph& g, const uint64_t* X, uint32_t n, uint32_t mm, bool keep_pruned,
                                float* stage, uint32_t stage_rows, float* selrows, uint32_t* sel, float* seld,
-                               uint32_t* sslot, uint64_t* disc) {
+                               uint32_t* sslot, uint64_t* disc, uint32_t& npair) {
     const int lane = lane_id();
     const int gi = lane >> 3, g8 = lane & 7;
     const uint32_t dp = g.dp;
@@ -376,6 +383,7 @@ __device__ uint32_t bheuristic(const BuildGraph& g, const uint64_t* X, uint32_t 
                 const float* srow = single ? stage + size_t(sslot[sc]) * dp
                                            : (selrows ? selrows + size_t(sc) * dp : g.vec + size_t(sel[sc]) * dp);
                 const float d = pair_distance(g.metric, srow, crow, int(g.dim), g8);
+                npair += min(4u, nsel - s0);
                 if (__any_sync(kFull, act && !(d >= dc))) {
                     diverse = false;
                     break;
@@ -413,7 +421,7 @@ __device__ uint32_t bheuristic(const BuildGraph& g, const uint64_t* X, uint32_t 
 // candidate is the pool's minimum, taken out by overwriting it with ~0. Rows
 // come from HBM.
 __device__ uint32_t bheuristic_pool(const BuildGraph& g, uint64_t* P, uint32_t n, uint32_t mm, bool keep_pruned,
-                                    uint32_t* sel, float* seld, uint64_t* disc) {
+                                    uint32_t* sel, float* seld, uint64_t* disc, uint32_t& npair) {
     const int lane = lane_id();
     const int gi = lane >> 3, g8 = lane & 7;
     uint32_t nsel = 0, ndisc = 0;
@@ -433,6 +441,7 @@ __device__ uint32_t bheuristic_pool(const BuildGraph& g, uint64_t* P, uint32_t n
             const bool act = s < nsel;
             const float* srow = g.vec + size_t(sel[act ? s : 0u]) * g.dp;
             const float d = pair_distance(g.metric, srow, crow, int(g.dim), g8);
+            npair += min(4u, nsel - s0);
             if (__any_sync(kFull, act && !(d >= dc))) {
                 diverse = false;
                 break;
@@ -478,7 +487,7 @@ __device__ __forceinline__ bool gset_insert(uint32_t* T, uint32_t cap, uint32_t 
 // returns the pool size.
 __device__ uint32_t extend_pool(const BuildGraph& g, const uint64_t* X, uint32_t n, uint32_t base_id,
                                 const float* qrow, uint32_t layer, uint64_t* P, uint32_t pcap, uint32_t* T,
-                                uint32_t tcap, uint32_t* fr, float* fd) {
+                                uint32_t tcap, uint32_t* fr, uint32_t& npair) {
     const int lane = lane_id();
     const int gi = lane >> 3, g8 = lane & 7;
     for (uint32_t i = lane; i < tcap; i += 32) T[i] = kEmpty;
@@ -502,6 +511,7 @@ __device__ uint32_t extend_pool(const BuildGraph& g, const uint64_t* X, uint32_t
             if ((F >> lane) & 1u) fr[__popc(F & ((1u << lane) - 1u))] = id;
             __syncwarp();
             const uint32_t nf = __popc(F);
+            npair += nf;
             for (uint32_t r = 0; r < nf; r += 4) {
                 const uint32_t slot = r + uint32_t(gi);
                 const bool act = slot < nf;
@@ -524,6 +534,7 @@ __device__ void carve_search(BWarp& w, char* p, const BuildArgs& a, uint32_t mm)
     w.q = reinterpret_cast<float*>(p);
     p += a16(size_t(dp) * 4);
     w.selrows = a.sel_rows ? reinterpret_cast<float*>(p) : nullptr;
+    if (a.sel_in_stage) w.selrows = reinterpret_cast<float*>(w.H) + size_t(a.stage_rows) * dp;
     p += a16(size_t(a.sel_rows) * dp * 4);
     w.R = reinterpret_cast<uint64_t*>(p);
     p += a16(size_t(a.ef + 1) * 8);
@@ -545,6 +556,7 @@ __device__ void carve_search(BWarp& w, char* p, const BuildArgs& a, uint32_t mm)
     w.hash_cap = a.hash_cap;
     w.ccap = a.ccap;
     w.bitmap = false;
+    w.nd = w.nl0 = w.nlU = 0;
 }
 
 // Appends the reverse edges sel[j] <- self on `layer` (one record each).
@@ -578,7 +590,7 @@ __global__ void build_search_kernel(BuildArgs a) {
     w.spill = a.spill + size_t(slot) * a.spill_words;
     w.spill_words = a.spill_words;
     const BuildGraph& g = a.g;
-    uint32_t inexact_total = 0, spills_total = 0;
+    uint32_t inexact_total = 0, spills_total = 0, npair = 0;
     for (;;) {
         uint32_t i = 0;
         if (lane == 0) i = atomicAdd(&a.wc->next, 1u);
@@ -591,6 +603,7 @@ __global__ void build_search_kernel(BuildArgs a) {
         __syncwarp();
         const uint32_t level = __ldg(g.levels + self);
         uint64_t ep = pack(query_distance(g, w, a.entry), a.entry);
+        ++w.nd;
         for (uint32_t layer = a.top; layer > level; --layer) ep = bgreedy(g, w, ep, layer);
         if (lane == 0) w.E[0] = ep;
         __syncwarp();
@@ -613,11 +626,11 @@ __global__ void build_search_kernel(BuildArgs a) {
                 uint64_t* P = a.ext + size_t(slot) * a.ext_cap;
                 uint32_t* T = a.ext_hash + size_t(slot) * a.ext_hash_cap;
                 const uint32_t np =
-                    extend_pool(g, w.R, rs, self, w.q, uint32_t(layer), P, a.ext_cap, T, a.ext_hash_cap, w.fr, w.fd);
-                nsel = bheuristic_pool(g, P, np, mm, a.keep_pruned != 0, w.sel, w.seld, w.disc);
+                    extend_pool(g, w.R, rs, self, w.q, uint32_t(layer), P, a.ext_cap, T, a.ext_hash_cap, w.fr, npair);
+                nsel = bheuristic_pool(g, P, np, mm, a.keep_pruned != 0, w.sel, w.seld, w.disc, npair);
             } else {
                 nsel = bheuristic(g, w.R, rs, mm, a.keep_pruned != 0, a.stage_rows ? reinterpret_cast<float*>(w.H) : nullptr,
-                                  a.stage_rows, w.selrows, w.sel, w.seld, w.sslot, w.disc);
+                                  a.stage_rows, w.selrows, w.sel, w.seld, w.sslot, w.disc, npair);
             }
             // install_own_neighbors: the node's list is still empty.
             uint32_t* own = list_ptr(g, uint32_t(layer), self);
@@ -633,9 +646,15 @@ __global__ void build_search_kernel(BuildArgs a) {
             __syncwarp();
         }
     }
-    if (lane == 0 && (inexact_total | spills_total)) {
-        atomicAdd(&a.totals->inexact, (unsigned long long)inexact_total);
-        atomicAdd(&a.totals->spills, (unsigned long long)spills_total);
+    if (lane == 0) {
+        if (inexact_total | spills_total) {
+            atomicAdd(&a.totals->inexact, (unsigned long long)inexact_total);
+            atomicAdd(&a.totals->spills, (unsigned long long)spills_total);
+        }
+        atomicAdd(&a.totals->dist_search, (unsigned long long)w.nd);
+        atomicAdd(&a.totals->dist_select, (unsigned long long)npair);
+        atomicAdd(&a.totals->lists0, (unsigned long long)w.nl0);
+        atomicAdd(&a.totals->listsU, (unsigned long long)w.nlU);
     }
 }
 
@@ -721,7 +740,7 @@ __global__ void build_connect_kernel(BuildArgs a) {
     CWarp w;
     carve_connect(w, base, a, capmax);
     const uint32_t nt = a.wc->ntouched;
-    uint32_t shrinks = 0;
+    uint32_t shrinks = 0, ndist = 0;
     for (uint32_t t = slot; t < nt; t += nwarps) {
         const uint64_t te = a.touched[t];
         const uint32_t layer = uint32_t(te >> 32), u = uint32_t(te);
@@ -784,6 +803,7 @@ __global__ void build_connect_kernel(BuildArgs a) {
                 if ((F >> lane) & 1u) w.fr[__popc(F & ((1u << lane) - 1u))] = i;
                 __syncwarp();
                 const uint32_t nf = __popc(F);
+                ndist += nf;
                 for (uint32_t r = 0; r < nf; r += 4) {
                     const uint32_t s = r + uint32_t(gi);
                     const bool act = s < nf;
@@ -815,11 +835,11 @@ __global__ void build_connect_kernel(BuildArgs a) {
                 uint64_t* P = a.ext + size_t(slot) * a.ext_cap;
                 uint32_t* T = a.ext_hash + size_t(slot) * a.ext_hash_cap;
                 const uint32_t np =
-                    extend_pool(g, w.X2, n, u, w.q, layer, P, a.ext_cap, T, a.ext_hash_cap, w.fr, w.fd);
-                ns = bheuristic_pool(g, P, np, cap, a.keep_pruned != 0, w.sel, w.seld, w.disc);
+                    extend_pool(g, w.X2, n, u, w.q, layer, P, a.ext_cap, T, a.ext_hash_cap, w.fr, ndist);
+                ns = bheuristic_pool(g, P, np, cap, a.keep_pruned != 0, w.sel, w.seld, w.disc, ndist);
             } else {
                 ns = bheuristic(g, w.X2, n, cap, a.keep_pruned != 0, a.c_stage_rows ? w.stage : nullptr,
-                                a.c_stage_rows, w.selrows, w.sel, w.seld, w.sslot, w.disc);
+                                a.c_stage_rows, w.selrows, w.sel, w.seld, w.sslot, w.disc, ndist);
             }
             for (uint32_t j = lane; j < ns; j += 32) {
                 w.lid[j] = w.sel[j];
@@ -834,7 +854,10 @@ __global__ void build_connect_kernel(BuildArgs a) {
         if (!a.extend && lane == 0) a.cnt[key] = 0;
         __syncwarp();
     }
-    if (lane == 0 && shrinks) atomicAdd(&a.totals->shrinks, (unsigned long long)shrinks);
+    if (lane == 0 && (shrinks | ndist)) {
+        atomicAdd(&a.totals->shrinks, (unsigned long long)shrinks);
+        atomicAdd(&a.totals->dist_connect, (unsigned long long)ndist);
+    }
 }
 
 // Extension mode: copies the new lists into the graph and clears the counts.
@@ -879,8 +902,7 @@ cudaError_t gpu_build_occupancy(bool search, int threads, size_t smem, int* bloc
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, f, threads, smem);
 }
 
-cudaError_t launch_build_wave(const BuildArgs& a, uint32_t search_blocks, uint32_t connect_blocks,
-                              uint32_t small_blocks, cudaStream_t stream) {
+cudaError_t launch_build_search(const BuildArgs& a, uint32_t search_blocks, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(a.wc, 0, sizeof(WaveCounters), stream);
     if (e != cudaSuccess) return e;
     const size_t s_smem = a.gscratch ? 0 : size_t(a.bytes_per_warp) * a.warps_per_block;
@@ -888,7 +910,12 @@ cudaError_t launch_build_wave(const BuildArgs& a, uint32_t search_blocks, uint32
                                   cudaSuccess)
         return e;
     dev::build_search_kernel<<<search_blocks, a.warps_per_block * 32, s_smem, stream>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_connect(const BuildArgs& a, uint32_t connect_blocks, uint32_t small_blocks,
+                                 cudaStream_t stream) {
+    cudaError_t e;
     dev::bucket_base_kernel<<<small_blocks, 256, 0, stream>>>(a);
     dev::bucket_fill_kernel<<<small_blocks, 256, 0, stream>>>(a);
     const size_t c_smem = a.c_gscratch ? 0 : size_t(a.c_bytes_per_warp) * a.c_warps_per_block;

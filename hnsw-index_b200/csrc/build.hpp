@@ -53,6 +53,11 @@ struct BuildTotals {
     unsigned long long inexact;  // candidate queues that had to drop a live entry
     unsigned long long shrinks;  // full lists re-selected on a reverse edge
     unsigned long long records;  // reverse edges
+    // Work counters (the roofline's algorithmic traffic): distances of the
+    // layer searches (greedy and beam), of the selections (pairs of rows),
+    // of the connect step (owner to member and pairs), and lists read.
+    unsigned long long dist_search, dist_select, dist_connect;
+    unsigned long long lists0, listsU;
 };
 
 struct BuildArgs {
@@ -66,6 +71,7 @@ struct BuildArgs {
     // `gscratch` when one warp's share does not fit on chip).
     uint32_t ccap = 0, hash_cap = 0, warps_per_block = 1, bytes_per_warp = 0;
     uint32_t stage_rows = 0, sel_rows = 0;  // rows staged for the selection; selected rows kept on chip
+    uint32_t sel_in_stage = 0;  // selected rows live in the hash region after the staged rows
     char* gscratch = nullptr;
     uint32_t* spill = nullptr;  // per warp slot, spill_words words (zero between uses)
     uint32_t spill_words = 0;
@@ -97,10 +103,12 @@ size_t build_connect_bytes(uint32_t dp, uint32_t cap, uint32_t stage_rows, uint3
 // Resident blocks per SM of the search (search = true) or connect kernel.
 cudaError_t gpu_build_occupancy(bool search, int threads, size_t smem, int* blocks);
 
-// One wave: search + own lists, bucket the reverse edges, connect. All on
-// `stream`; the wave counters must be zero on entry (the launcher clears
-// them first). `search_blocks` / `connect_blocks` bound the persistent grids.
-cudaError_t launch_build_wave(const BuildArgs& a, uint32_t search_blocks, uint32_t connect_blocks,
-                              uint32_t small_blocks, cudaStream_t stream);
+// One wave in two launches on `stream`: the search step (clears the wave
+// counters, then searches, selects and writes the own lists) and the connect
+// step (buckets the reverse edges and applies them). `search_blocks` /
+// `connect_blocks` bound the persistent grids.
+cudaError_t launch_build_search(const BuildArgs& a, uint32_t search_blocks, cudaStream_t stream);
+cudaError_t launch_build_connect(const BuildArgs& a, uint32_t connect_blocks, uint32_t small_blocks,
+                                 cudaStream_t stream);
 
 }  // namespace hnswgpu

@@ -1423,6 +1423,7 @@ void hnsw_gpu_build_opts_default(hnsw_gpu_build_opts* out) {
     out->wave_fraction = o.wave_fraction;
     out->max_wave = o.max_wave;
     out->hash_cap = o.hash_cap;
+    out->timing = o.timing;
 }
 
 static GpuBuildOptions build_options(const hnsw_gpu_build_opts* opts) {
@@ -1431,6 +1432,7 @@ static GpuBuildOptions build_options(const hnsw_gpu_build_opts* opts) {
         o.wave_fraction = opts->wave_fraction;
         o.max_wave = opts->max_wave;
         o.hash_cap = opts->hash_cap;
+        o.timing = opts->timing;
     }
     return o;
 }
@@ -1444,6 +1446,13 @@ static void record_stats(hnsw_builder* b, const GpuBuildReport& r) {
     s.shrinks = r.shrinks;
     s.records = r.records;
     s.device_ms = r.device_ms;
+    s.search_ms = r.search_ms;
+    s.connect_ms = r.connect_ms;
+    s.dist_search = r.dist_search;
+    s.dist_select = r.dist_select;
+    s.dist_connect = r.dist_connect;
+    s.lists0 = r.lists0;
+    s.listsU = r.listsU;
     s.search_warps_per_block = r.search_warps_per_block;
     s.search_blocks_per_sm = r.search_blocks_per_sm;
     s.connect_warps_per_block = r.connect_warps_per_block;

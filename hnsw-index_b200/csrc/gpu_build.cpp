@@ -141,33 +141,63 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
     a.keep_pruned = P.keep_pruned;
     a.ef = ef;
     a.ccap = ef + 64;
-    a.hash_cap = opt.hash_cap ? pow2_at_least(opt.hash_cap) : pow2_at_least(std::max<uint64_t>(1024, 32ull * ef));
+    // The visited hash holds about 16 entries per unit of ef (a layer-0
+    // search at ef = 200 visits 2-3k nodes); a search that passes 3/4 of it
+    // continues in its HBM bitmap. After the search the hash region holds
+    // the staged candidate rows of the selection and, when they fit, the
+    // selected rows.
+    a.hash_cap = opt.hash_cap ? pow2_at_least(opt.hash_cap) : pow2_at_least(std::max<uint64_t>(1024, 16ull * ef));
     a.hash_cap = std::max<uint32_t>(a.hash_cap, 64);
     const size_t rowb = size_t(dp) * 4;
-    a.sel_rows = size_t(m) * rowb <= 16384 ? m : 0;
-    a.stage_rows = uint32_t(std::min<size_t>(32, size_t(a.hash_cap) * 4 / rowb));
+    auto layout_stage = [&]() {
+        const size_t hb = size_t(a.hash_cap) * 4;
+        if (size_t(m + 4) * rowb <= hb) {
+            a.sel_in_stage = 1;
+            a.sel_rows = 0;
+            a.stage_rows = uint32_t(std::min<size_t>(32, (hb - size_t(m) * rowb) / rowb));
+        } else {
+            a.sel_in_stage = 0;
+            a.sel_rows = size_t(m) * rowb <= 16384 ? m : 0;
+            a.stage_rows = uint32_t(std::min<size_t>(32, hb / rowb));
+        }
+    };
+    layout_stage();
     size_t bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
     while (bytes > budget / 4 && a.hash_cap > 4096 && !opt.hash_cap) {
         a.hash_cap >>= 1;
-        a.stage_rows = uint32_t(std::min<size_t>(32, size_t(a.hash_cap) * 4 / rowb));
+        layout_stage();
         bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
     }
     const bool s_global = bytes > budget;
     if (s_global) {
         // cp.async stages into shared memory only: no staging from HBM scratch.
         a.stage_rows = 0;
+        a.sel_in_stage = 0;
         bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
     }
     a.bytes_per_warp = uint32_t(bytes);
-    a.warps_per_block = s_global ? 4 : uint32_t(std::max<size_t>(1, std::min<size_t>(4, budget / bytes)));
     uint32_t s_blocks_per_sm = 0;
     if (s_global) {
+        a.warps_per_block = 4;
         s_blocks_per_sm = 2;
     } else {
-        int nb = 0;
-        CU(gpu_build_occupancy(true, a.warps_per_block * 32, size_t(a.bytes_per_warp) * a.warps_per_block, &nb),
-           "occupancy (build search)");
-        s_blocks_per_sm = uint32_t(std::max(1, nb));
+        // Warps per block that maximise resident warps per SM.
+        uint32_t best = 0;
+        for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
+            if (size_t(a.bytes_per_warp) * wpb > budget) continue;
+            int nb = 0;
+            CU(gpu_build_occupancy(true, int(wpb) * 32, size_t(a.bytes_per_warp) * wpb, &nb),
+               "occupancy (build search)");
+            if (uint32_t(nb) * wpb > best) {
+                best = uint32_t(nb) * wpb;
+                a.warps_per_block = wpb;
+                s_blocks_per_sm = uint32_t(nb);
+            }
+        }
+        if (best == 0) {
+            a.warps_per_block = 1;
+            s_blocks_per_sm = 1;
+        }
     }
     const uint32_t s_max_blocks = s_blocks_per_sm * sms;
     const uint32_t s_slots = s_max_blocks * a.warps_per_block;
@@ -183,15 +213,27 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
         cbytes = build_connect_bytes(dp, capmax, 0, 0);
     }
     a.c_bytes_per_warp = uint32_t(cbytes);
-    a.c_warps_per_block = c_global ? 4 : uint32_t(std::max<size_t>(1, std::min<size_t>(4, budget / cbytes)));
     uint32_t c_blocks_per_sm = 0;
     if (c_global) {
+        a.c_warps_per_block = 4;
         c_blocks_per_sm = 2;
     } else {
-        int nb = 0;
-        CU(gpu_build_occupancy(false, a.c_warps_per_block * 32, size_t(a.c_bytes_per_warp) * a.c_warps_per_block, &nb),
-           "occupancy (build connect)");
-        c_blocks_per_sm = uint32_t(std::max(1, nb));
+        uint32_t best = 0;
+        for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
+            if (size_t(a.c_bytes_per_warp) * wpb > budget) continue;
+            int nb = 0;
+            CU(gpu_build_occupancy(false, int(wpb) * 32, size_t(a.c_bytes_per_warp) * wpb, &nb),
+               "occupancy (build connect)");
+            if (uint32_t(nb) * wpb > best) {
+                best = uint32_t(nb) * wpb;
+                a.c_warps_per_block = wpb;
+                c_blocks_per_sm = uint32_t(nb);
+            }
+        }
+        if (best == 0) {
+            a.c_warps_per_block = 1;
+            c_blocks_per_sm = 1;
+        }
     }
     const uint32_t c_max_blocks = c_blocks_per_sm * sms;
     const uint32_t c_slots = c_max_blocks * a.c_warps_per_block;
@@ -298,8 +340,22 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
             cudaEventDestroy(b);
         }
     } eg{ev0, ev1};
+    // Per-phase timing: events after each search step and each connect
+    // step (only when asked; they are recorded on the same stream).
+    std::vector<cudaEvent_t> marks;
+    struct MarkGuard {
+        std::vector<cudaEvent_t>& v;
+        ~MarkGuard() {
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
+        }
+    } mg{marks};
+    if (opt.timing) {
+        marks.resize(2 * waves.size());
+        for (auto& e : marks) CU(cudaEventCreate(&e), "cudaEventCreate");
+    }
     CU(cudaEventRecord(ev0, stream), "cudaEventRecord");
-    for (const Wave& wv : waves) {
+    for (size_t i = 0; i < waves.size(); ++i) {
+        const Wave& wv = waves[i];
         a.first = wv.first;
         a.count = wv.count;
         a.entry = wv.entry;
@@ -307,12 +363,23 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
         const uint32_t sb = std::min(s_max_blocks, (wv.count + a.warps_per_block - 1) / a.warps_per_block);
         const uint32_t cb = std::min(c_max_blocks, (wv.records + a.c_warps_per_block - 1) / a.c_warps_per_block);
         const uint32_t small = std::min<uint32_t>(4 * sms, wv.records / 256 + 1);
-        CU(launch_build_wave(a, std::max(1u, sb), std::max(1u, cb), small, stream), "device build wave");
+        CU(launch_build_search(a, std::max(1u, sb), stream), "device build (search)");
+        if (opt.timing) CU(cudaEventRecord(marks[2 * i], stream), "cudaEventRecord");
+        CU(launch_build_connect(a, std::max(1u, cb), small, stream), "device build (connect)");
+        if (opt.timing) CU(cudaEventRecord(marks[2 * i + 1], stream), "cudaEventRecord");
     }
     CU(cudaEventRecord(ev1, stream), "cudaEventRecord");
     CU(cudaStreamSynchronize(stream), "device build");
     float ms = 0.0f;
     CU(cudaEventElapsedTime(&ms, ev0, ev1), "cudaEventElapsedTime");
+    double search_ms = 0.0, connect_ms = 0.0;
+    for (size_t i = 0; opt.timing && i < waves.size(); ++i) {
+        float t0 = 0.0f, t1 = 0.0f;
+        CU(cudaEventElapsedTime(&t0, i ? marks[2 * i - 1] : ev0, marks[2 * i]), "cudaEventElapsedTime");
+        CU(cudaEventElapsedTime(&t1, marks[2 * i], marks[2 * i + 1]), "cudaEventElapsedTime");
+        search_ms += t0;
+        connect_ms += t1;
+    }
     BuildTotals tot;
     CU(cudaMemcpy(&tot, a.totals, sizeof(tot), cudaMemcpyDeviceToHost), "cudaMemcpy (totals)");
     CU(cudaMemcpy(h0.data(), d_adj0, h0.size() * 4, cudaMemcpyDeviceToHost), "cudaMemcpy (layer 0 back)");
@@ -347,6 +414,13 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
         rep->shrinks = tot.shrinks;
         rep->records = tot.records;
         rep->device_ms = ms;
+        rep->search_ms = search_ms;
+        rep->connect_ms = connect_ms;
+        rep->dist_search = tot.dist_search;
+        rep->dist_select = tot.dist_select;
+        rep->dist_connect = tot.dist_connect;
+        rep->lists0 = tot.lists0;
+        rep->listsU = tot.listsU;
         rep->search_warps_per_block = a.warps_per_block;
         rep->search_blocks_per_sm = s_blocks_per_sm;
         rep->connect_warps_per_block = a.c_warps_per_block;

@@ -212,13 +212,16 @@ _lib.hnsw_builder_compact.argtypes = [_vp, C.c_int]
 
 
 class _BuildOpts(C.Structure):
-    _fields_ = [("wave_fraction", C.c_double), ("max_wave", C.c_uint32), ("hash_cap", C.c_uint32)]
+    _fields_ = [("wave_fraction", C.c_double), ("max_wave", C.c_uint32), ("hash_cap", C.c_uint32),
+                ("timing", C.c_uint32)]
 
 
 class _BuildStats(C.Structure):
     _fields_ = [("waves", C.c_uint32), ("nodes", C.c_uint32), ("spills", C.c_uint64), ("inexact", C.c_uint64),
                 ("shrinks", C.c_uint64), ("records", C.c_uint64), ("device_ms", C.c_double),
-                ("search_warps_per_block", C.c_uint32), ("search_blocks_per_sm", C.c_uint32),
+                ("search_ms", C.c_double), ("connect_ms", C.c_double), ("dist_search", C.c_uint64),
+                ("dist_select", C.c_uint64), ("dist_connect", C.c_uint64), ("lists0", C.c_uint64),
+                ("listsU", C.c_uint64), ("search_warps_per_block", C.c_uint32), ("search_blocks_per_sm", C.c_uint32),
                 ("connect_warps_per_block", C.c_uint32), ("connect_blocks_per_sm", C.c_uint32),
                 ("hash_cap", C.c_uint32)]
 
@@ -882,14 +885,14 @@ class IndexBuilder:
         _check(_lib.hnsw_builder_insert_batch(self._h, _ptr(keys), _ptr(v), keys.size, self._dim, threads))
 
     def insert_batch_gpu(self, keys, vectors, device: int = 0, wave_fraction: Optional[float] = None,
-                         max_wave: Optional[int] = None, hash_cap: Optional[int] = None):
+                         max_wave: Optional[int] = None, hash_cap: Optional[int] = None, timing: bool = False):
         """insert_batch with the link step on a GPU (waves of nodes; see hnsw_gpu.h)."""
         keys = np.ascontiguousarray(keys, dtype=np.uint64)
         v = np.ascontiguousarray(vectors, dtype=np.float32).reshape(-1)
         if v.size != keys.size * self._dim:
             raise Error(Status.DIMENSION_MISMATCH,
                         f"dimension mismatch: expected {keys.size * self._dim}, got {v.size}")
-        o = self._build_opts(wave_fraction, max_wave, hash_cap)
+        o = self._build_opts(wave_fraction, max_wave, hash_cap, timing)
         _check(_lib.hnsw_builder_insert_batch_gpu(self._h, _ptr(keys), _ptr(v), keys.size, self._dim, device,
                                                   C.byref(o)))
 
@@ -898,9 +901,9 @@ class IndexBuilder:
         _check(_lib.hnsw_builder_compact(self._h, threads))
 
     def compact_gpu(self, device: int = 0, wave_fraction: Optional[float] = None, max_wave: Optional[int] = None,
-                    hash_cap: Optional[int] = None):
+                    hash_cap: Optional[int] = None, timing: bool = False):
         """compact with the link step on a GPU."""
-        o = self._build_opts(wave_fraction, max_wave, hash_cap)
+        o = self._build_opts(wave_fraction, max_wave, hash_cap, timing)
         _check(_lib.hnsw_builder_compact_gpu(self._h, device, C.byref(o)))
 
     def gpu_stats(self) -> dict:
@@ -910,9 +913,10 @@ class IndexBuilder:
         return {name: getattr(st, name) for name, _ in _BuildStats._fields_}
 
     @staticmethod
-    def _build_opts(wave_fraction, max_wave, hash_cap) -> "_BuildOpts":
+    def _build_opts(wave_fraction, max_wave, hash_cap, timing=False) -> "_BuildOpts":
         o = _BuildOpts()
         _lib.hnsw_gpu_build_opts_default(C.byref(o))
+        o.timing = int(bool(timing))
         if wave_fraction is not None:
             o.wave_fraction = wave_fraction
         if max_wave is not None:

@@ -393,7 +393,8 @@ int hnsw_builder_compact(hnsw_builder* b, int threads);
 typedef struct hnsw_gpu_build_opts {
     double wave_fraction; /* nodes per wave = max(1, floor(linked * fraction)); (0, 1] */
     uint32_t max_wave;    /* at most this many nodes per wave (>= 1) */
-    uint32_t hash_cap;    /* visited-hash entries per warp; 0 = 32 per unit of ef */
+    uint32_t hash_cap;    /* visited-hash entries per warp; 0 = 16 per unit of ef */
+    uint32_t timing;      /* 1 = record per-phase device times in the stats */
 } hnsw_gpu_build_opts;
 typedef struct hnsw_gpu_build_stats {
     uint32_t waves, nodes;
@@ -402,11 +403,16 @@ typedef struct hnsw_gpu_build_stats {
     uint64_t shrinks;  /* full lists re-selected by a reverse edge */
     uint64_t records;  /* reverse edges */
     double device_ms;  /* device time of the waves (CUDA events) */
+    double search_ms, connect_ms; /* per phase, when opts.timing */
+    uint64_t dist_search;  /* distances of the layer searches */
+    uint64_t dist_select;  /* row pairs compared by the neighbor selections */
+    uint64_t dist_connect; /* distances of the connect step (owner-member and pairs) */
+    uint64_t lists0, listsU; /* neighbor lists read on layer 0 / above */
     uint32_t search_warps_per_block, search_blocks_per_sm;
     uint32_t connect_warps_per_block, connect_blocks_per_sm;
     uint32_t hash_cap;
 } hnsw_gpu_build_stats;
-/* Defaults: wave_fraction 0.02, max_wave 65536, hash_cap 0. */
+/* Defaults: wave_fraction 0.02, max_wave 65536, hash_cap 0, timing 0. */
 void hnsw_gpu_build_opts_default(hnsw_gpu_build_opts* out);
 /* HnswIndex::insert_batch (mod.rs:318-338) with the link step on a GPU.
  * opts may be NULL (defaults). */
