@@ -895,7 +895,7 @@ def run_build(args):
         "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": "build-1Mx128-clustered", "n_base": nb, "dim": DIM, "m": M,
-                   "ef_construction": EF_CONSTRUCTION, "wave_fraction": 0.02, "waves": st["waves"],
+                   "ef_construction": EF_CONSTRUCTION, "wave_fraction": 0.05, "waves": st["waves"],
                    "search_ms": search_ms, "connect_ms": connect_ms, "spills": st["spills"],
                    "inexact": st["inexact"], "shrinks": st["shrinks"], "reverse_edges": st["records"],
                    "distances": {"search": st["dist_search"], "select_pairs": st["dist_select"],

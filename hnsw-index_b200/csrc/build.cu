@@ -35,19 +35,18 @@ namespace {
 __host__ __device__ __forceinline__ size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct BWarp {
-    uint32_t* H;     // visited hash (hash_cap words); the selection stage aliases it
+    uint32_t* H;     // visited hash (hash_cap words); the selection stage aliases its region
     float* q;        // dp: the inserted node's row
     float* selrows;  // sel_rows * dp, or null
-    uint64_t* R;     // ef + 1
-    uint64_t* E;     // ef + 1
-    uint64_t* C;     // ccap + 1
+    uint64_t* R;     // ef + 33: results; after a layer, the next layer's entry points
+    uint64_t* T;     // kTieCap + 1: evicted ties (candidates outside R)
     uint64_t* disc;  // mm
     uint32_t* fr;    // 32
     float* fd;       // 32
     uint32_t* sel;   // mm
     float* seld;     // mm
     uint32_t* sslot; // mm
-    uint32_t hash_cap, ccap;
+    uint32_t hash_cap;
     bool bitmap;
     uint32_t* spill;
     uint32_t spill_words;
@@ -123,13 +122,12 @@ __device__ __forceinline__ bool bvisit(BWarp& w, uint32_t id) {
         const uint32_t bit = 1u << (id & 31);
         return (atomicOr(&w.spill[id >> 5], bit) & bit) == 0;
     }
-    const uint32_t mask = w.hash_cap - 1;
     uint32_t h = uint32_t((uint64_t(id * 0x9E3779B1u) * w.hash_cap) >> 32);
     for (uint32_t probe = 0; probe < w.hash_cap; ++probe) {
         const uint32_t old = atomicCAS(&w.H[h], kEmpty, id);
         if (old == kEmpty) return true;
         if (old == id) return false;
-        h = (h + 1) & mask;
+        h = h + 1 == w.hash_cap ? 0u : h + 1;
     }
     return true;  // unreachable below the load limit
 }
@@ -185,47 +183,77 @@ __device__ uint64_t bgreedy(const BuildGraph& g, BWarp& w, uint64_t best, uint32
     }
 }
 
-// Room for `need` more candidates: compact to the front, drop candidates
-// worse than the worst of ef results (never expanded), and as a last resort
-// drop the largest (counted: the result may then differ from the reference).
-__device__ __forceinline__ void bmake_room(BWarp& w, uint32_t& head, uint32_t& tail, uint32_t need, uint32_t rs,
-                                           uint32_t ef, uint32_t& inexact) {
-    if (tail + need <= w.ccap) return;
+// Layer-search entries: (fkey(d) << 32) | (id << 1) | expanded. The flag bit
+// sits below the id, so the u64 order is still the (total_cmp distance, id)
+// order of Candidate (src/hnsw/search.rs:36-44).
+__device__ __forceinline__ uint64_t upack(float d, uint32_t id) { return (uint64_t(fkey(d)) << 32) | (uint64_t(id) << 1); }
+__device__ __forceinline__ uint64_t to_upack(uint64_t x) { return (x & 0xFFFFFFFF00000000ull) | (uint64_t(uint32_t(x)) << 1); }
+__device__ __forceinline__ uint64_t from_upack(uint64_t x) { return (x & 0xFFFFFFFF00000000ull) | (uint32_t(x) >> 1); }
+
+// Merges the entries x of the lanes in S (distinct, none in A) into the
+// ascending A[0, hi) (room for all of them). Returns the lowest position
+// written. All lanes call.
+__device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t S, uint64_t x) {
     const int lane = lane_id();
-    if (head > 0) {
-        const uint32_t n = tail - head;
-        for (uint32_t b = 0; b < n; b += 32) {
-            const uint32_t j = b + lane;
-            const uint64_t v = j < n ? w.C[head + j] : 0;
+    const bool in = (S >> lane) & 1u;
+    uint32_t rank_s = 0;
+    for (uint32_t bits = S; bits; bits &= bits - 1) {
+        const int j = __ffs(bits) - 1;
+        rank_s += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
+    }
+    const uint32_t pa = in ? lower_bound(A, 0, hi, x) : hi;
+    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
+    if (hi > pmin) {
+        for (int b = int((hi - 1) & ~31u); b >= int(pmin & ~31u); b -= 32) {
+            const uint32_t k = uint32_t(b) + uint32_t(lane);
+            const bool mv = k >= pmin && k < hi;
+            const uint64_t v = mv ? A[k] : 0;
+            uint32_t shift = 0;
+            for (uint32_t bits = S; bits; bits &= bits - 1) {
+                const int j = __ffs(bits) - 1;
+                shift += (__shfl_sync(kFull, x, j) < v) ? 1u : 0u;
+            }
             __syncwarp();
-            if (j < n) w.C[j] = v;
+            if (mv) A[k + shift] = v;
             __syncwarp();
         }
-        head = 0;
-        tail = n;
     }
-    if (tail + need > w.ccap && rs >= ef) {
-        const float wd = pdist(w.R[rs - 1]);
-        uint32_t keep = 0;
-        for (uint32_t b = 0; b < tail; b += 32) {
-            const uint32_t j = b + lane;
-            keep += __popc(__ballot_sync(kFull, j < tail && !(pdist(w.C[j]) > wd)));
-        }
-        tail = keep;
-    }
-    if (tail + need > w.ccap) {
-        tail = w.ccap - need;
-        inexact = 1;
-    }
+    if (in) A[pa + rank_s] = x;
+    __syncwarp();
+    return pmin;
 }
 
-// search_layer (src/hnsw/search.rs:81-142) from the entries E[0, ne) with
-// admission `n != self` (build.rs:71-72). Results ascending in R; returns
-// their count.
+constexpr uint32_t kTieCap = 32;
+
+// A result evicted while unexpanded stays a candidate of the reference's
+// unbounded queue; it can still be expanded only if its distance equals the
+// worst result's (search.rs:113-119). Such entries (all of one distance)
+// wait in the ascending tie list T; entries of a larger distance are dead.
+__device__ __forceinline__ void tie_add(uint64_t* T, uint32_t& nt, uint64_t x, float wd, uint32_t& inexact) {
+    if (nt && pdist(T[0]) > wd) nt = 0;
+    if (nt >= kTieCap) {
+        inexact = 1;
+        return;
+    }
+    sorted_insert(T, 0, nt, x);
+    ++nt;
+}
+
+// search_layer (src/hnsw/search.rs:81-142) from the entry points R[0, ne)
+// (ascending, distinct: the previous layer's results) with admission
+// `n != self` (build.rs:71-72). Results ascending in R; returns their count.
+//
+// One array serves as the results heap and as the live part of the
+// candidate heap: every candidate the reference can still expand is a
+// result not yet expanded (flag bit clear) or an evicted tie in T. The next
+// expansion is the first unexpanded result, else the first tie; the
+// reference's stop rule can only fire on a tie.
 __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, uint32_t layer, uint32_t ne,
                                   uint32_t ef, uint32_t& inexact, uint32_t& spilled) {
     const int lane = lane_id();
     const uint32_t cap = list_cap(g, layer);
+    uint64_t* U = w.R;
+    uint64_t* T = w.T;
     for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
     __syncwarp();
     w.bitmap = false;
@@ -235,30 +263,46 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
         w.bitmap = true;
         spilled = 1;
     }
-    for (uint32_t i = lane; i < ne; i += 32) bvisit(w, pid(w.E[i]));
-    for (uint32_t i = lane; i < ne; i += 32) w.C[i] = w.E[i];
-    uint32_t rs = 0;
-    for (uint32_t b = 0; b < ne; b += 32) {
-        const uint32_t i = b + lane;
-        const uint64_t x = i < ne ? w.E[i] : 0;
-        const bool keep = i < ne && pid(x) != self;
-        const uint32_t K = __ballot_sync(kFull, keep);
-        const uint32_t pos = rs + __popc(K & ((1u << lane) - 1u));
-        if (keep && pos < ef) w.R[pos] = x;
-        rs += __popc(K);
+    for (uint32_t i = lane; i < ne; i += 32) {
+        bvisit(w, pid(U[i]));
+        U[i] = to_upack(U[i]);
     }
-    rs = min(rs, ef);
-    uint32_t head = 0, tail = ne;
     __syncwarp();
+    uint32_t rs = ne, nt = 0, nx = 0;
     for (;;) {
-        if (head == tail) break;
-        const uint64_t cur = w.C[head];
-        ++head;
-        if (rs >= ef && pdist(cur) > pdist(w.R[rs - 1])) break;
-        const uint32_t* row = list_ptr(g, layer, pid(cur));
+        // Next candidate: the first unexpanded result, else the first tie.
+        uint32_t p = rs;
+        for (uint32_t b = nx; b < rs; b += 32) {
+            const uint32_t i = b + lane;
+            const uint32_t M = __ballot_sync(kFull, i < rs && !(U[i] & 1ull));
+            if (M) {
+                p = b + uint32_t(__ffs(int(M)) - 1);
+                break;
+            }
+        }
+        uint64_t cur;
+        if (p < rs) {
+            cur = U[p];
+            __syncwarp();
+            if (lane == 0) U[p] = cur | 1ull;
+            nx = p + 1;
+        } else {
+            if (nt == 0) break;
+            cur = T[0];
+            for (uint32_t b = 0; b + 1 < nt; b += 32) {
+                const uint32_t i = b + lane;
+                const uint64_t v = i + 1 < nt ? T[i + 1] : 0;
+                __syncwarp();
+                if (i + 1 < nt) T[i] = v;
+            }
+            --nt;
+            nx = rs;
+            if (rs >= ef && pdist(cur) > pdist(U[rs - 1])) break;
+        }
+        __syncwarp();
+        const uint32_t* row = list_ptr(g, layer, uint32_t(cur) >> 1);
         if (layer) ++w.nlU;
         else ++w.nl0;
-        if (lane == 0 && head < tail) prefetch_l2(list_ptr(g, layer, pid(w.C[head])), (layer ? g.mp : g.m0p) * 4);
         for (uint32_t b = 0; b < cap; b += 32) {
             const uint32_t id = (b + lane < cap) ? __ldg(row + b + lane) : kEmpty;
             const bool valid = id != kEmpty;
@@ -269,7 +313,6 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
                 spilled = 1;
             }
             const bool fresh = valid && bvisit(w, id);
-            if (fresh) prefetch_l2(g.vec + size_t(id) * g.dp, g.dp * 4);
             const uint32_t F = __ballot_sync(kFull, fresh);
             visited += __popc(F);
             if (F != 0) {
@@ -279,13 +322,17 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
                 const uint32_t A = __ballot_sync(kFull, adm);
                 const float my_d = fresh ? w.fd[lane] : 0.0f;
                 uint32_t P = F;
-                if (rs >= ef) P &= __ballot_sync(kFull, fresh && my_d < pdist(w.R[rs - 1]));
+                if (rs >= ef) P &= __ballot_sync(kFull, fresh && my_d < pdist(U[rs - 1]));
+                // The node itself is never in the graph while it is linked;
+                // it would be a candidate that is not a result.
+                if (P & ~A) inexact = 1;
+                P &= A;
                 if (P == 0) {
                     if (V != kFull) break;
                     continue;
                 }
                 const bool inP = (P >> lane) & 1u;
-                const uint64_t my_x = pack(my_d, id);
+                const uint64_t my_x = upack(my_d, id);
                 // Equal distances among the improving neighbors or with a
                 // result make the evaluation order matter: sequential path.
                 const float dz = __fadd_rn(my_d, 0.0f);
@@ -294,27 +341,38 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
                 uint32_t pr = 0;
                 bool tie = inP && __popc(same) > 1;
                 if (inP) {
-                    pr = lower_bound(w.R, 0, rs, my_x);
-                    if (pr < rs && pdist(w.R[pr]) == my_d) tie = true;
-                    if (pr > 0 && pdist(w.R[pr - 1]) == my_d) tie = true;
+                    pr = lower_bound(U, 0, rs, my_x);
+                    if (pr < rs && pdist(U[pr]) == my_d) tie = true;
+                    if (pr > 0 && pdist(U[pr - 1]) == my_d) tie = true;
                 }
                 if (!__any_sync(kFull, tie)) {
+                    // Rank among the results and the improving neighbors
+                    // before it in list order: it improves iff below ef.
                     uint32_t before = 0;
-                    for (uint32_t bits = A & P; bits; bits &= bits - 1) {
+                    for (uint32_t bits = P; bits; bits &= bits - 1) {
                         const int j = __ffs(bits) - 1;
                         const uint64_t xj = __shfl_sync(kFull, my_x, j);
                         before += (j < lane && xj < my_x) ? 1u : 0u;
                     }
                     const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
-                    const uint32_t IR = I & A;
-                    if (IR) {
-                        batch_merge(w.R, 0, rs, IR, my_x, ef);
-                        rs = min(rs + uint32_t(__popc(IR)), ef);
-                    }
                     if (I) {
-                        bmake_room(w, head, tail, uint32_t(__popc(I)), rs, ef, inexact);
-                        batch_merge(w.C, head, tail, I, my_x, w.ccap);
-                        tail += uint32_t(__popc(I));
+                        nx = min(nx, merge_all(U, rs, I, my_x));
+                        const uint32_t total = rs + uint32_t(__popc(I));
+                        if (total > ef) {
+                            // Evicted entries that tie with the new worst.
+                            const float wd = pdist(U[ef - 1]);
+                            const uint32_t i = ef + uint32_t(lane);
+                            const uint64_t v = i < total ? U[i] : 0;
+                            uint32_t E = __ballot_sync(kFull, i < total && !(v & 1ull) && pdist(v) == wd);
+                            while (E) {
+                                const int j = __ffs(int(E)) - 1;
+                                E &= E - 1;
+                                tie_add(T, nt, __shfl_sync(kFull, v, j), wd, inexact);
+                            }
+                            rs = ef;
+                        } else {
+                            rs = total;
+                        }
                     }
                 } else {
                     while (P) {
@@ -322,15 +380,14 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
                         P &= P - 1;
                         const float d = __shfl_sync(kFull, my_d, i);
                         const uint32_t nid = __shfl_sync(kFull, id, i);
-                        const bool improves = rs < ef || d < pdist(w.R[rs - 1]);
+                        const bool improves = rs < ef || d < pdist(U[rs - 1]);
                         if (!improves) continue;
-                        const uint64_t x = pack(d, nid);
-                        bmake_room(w, head, tail, 1, rs, ef, inexact);
-                        sorted_insert(w.C, head, tail, x);
-                        ++tail;
-                        if ((A >> i) & 1u) {
-                            sorted_insert(w.R, 0, rs, x);
-                            rs = min(rs + 1, ef);
+                        const uint32_t pos = sorted_insert(U, 0, rs, upack(d, nid));
+                        nx = min(nx, pos);
+                        if (++rs > ef) {
+                            rs = ef;
+                            const uint64_t v = U[ef];
+                            if (!(v & 1ull) && pdist(v) == pdist(U[ef - 1])) tie_add(T, nt, v, pdist(v), inexact);
                         }
                     }
                 }
@@ -338,6 +395,8 @@ __device__ uint32_t bsearch_layer(const BuildGraph& g, BWarp& w, uint32_t self, 
             if (V != kFull) break;
         }
     }
+    for (uint32_t i = lane; i < rs; i += 32) U[i] = from_upack(U[i]);
+    __syncwarp();
     if (w.bitmap) {
         for (uint32_t i = lane; i < w.spill_words; i += 32) w.spill[i] = 0;
         __syncwarp();
@@ -530,18 +589,16 @@ __device__ uint32_t extend_pool(const BuildGraph& g, const uint64_t* X, uint32_t
 __device__ void carve_search(BWarp& w, char* p, const BuildArgs& a, uint32_t mm) {
     const uint32_t dp = a.g.dp;
     w.H = reinterpret_cast<uint32_t*>(p);
-    p += a16(size_t(a.hash_cap) * 4);
+    p += a16(size_t(a.region_bytes));
     w.q = reinterpret_cast<float*>(p);
     p += a16(size_t(dp) * 4);
     w.selrows = a.sel_rows ? reinterpret_cast<float*>(p) : nullptr;
     if (a.sel_in_stage) w.selrows = reinterpret_cast<float*>(w.H) + size_t(a.stage_rows) * dp;
     p += a16(size_t(a.sel_rows) * dp * 4);
     w.R = reinterpret_cast<uint64_t*>(p);
-    p += a16(size_t(a.ef + 1) * 8);
-    w.E = reinterpret_cast<uint64_t*>(p);
-    p += a16(size_t(a.ef + 1) * 8);
-    w.C = reinterpret_cast<uint64_t*>(p);
-    p += a16(size_t(a.ccap + 1) * 8);
+    p += a16(size_t(a.ef + 33) * 8);
+    w.T = reinterpret_cast<uint64_t*>(p);
+    p += a16(size_t(kTieCap + 1) * 8);
     w.disc = reinterpret_cast<uint64_t*>(p);
     p += a16(size_t(mm) * 8);
     w.fr = reinterpret_cast<uint32_t*>(p);
@@ -554,7 +611,6 @@ __device__ void carve_search(BWarp& w, char* p, const BuildArgs& a, uint32_t mm)
     p += a16(size_t(mm) * 4);
     w.sslot = reinterpret_cast<uint32_t*>(p);
     w.hash_cap = a.hash_cap;
-    w.ccap = a.ccap;
     w.bitmap = false;
     w.nd = w.nl0 = w.nlU = 0;
 }
@@ -605,7 +661,7 @@ __global__ void build_search_kernel(BuildArgs a) {
         uint64_t ep = pack(query_distance(g, w, a.entry), a.entry);
         ++w.nd;
         for (uint32_t layer = a.top; layer > level; --layer) ep = bgreedy(g, w, ep, layer);
-        if (lane == 0) w.E[0] = ep;
+        if (lane == 0) w.R[0] = ep;
         __syncwarp();
         uint32_t ne = 1;
         for (int layer = int(min(level, a.top)); layer >= 0; --layer) {
@@ -637,12 +693,9 @@ __global__ void build_search_kernel(BuildArgs a) {
             for (uint32_t j = lane; j < nsel; j += 32) own[j] = w.sel[j];
             emit_records(a, w, self, uint32_t(layer), nsel);
             __syncwarp();
-            if (rs > 0) {
-                uint64_t* t = w.E;
-                w.E = w.R;
-                w.R = t;
-                ne = rs;
-            }
+            // The results are the next layer's entry points (the search
+            // always returns its admitted entries, so rs > 0).
+            ne = rs;
             __syncwarp();
         }
     }
@@ -880,10 +933,10 @@ __global__ void build_apply_kernel(BuildArgs a) {
 }  // namespace
 }  // namespace dev
 
-size_t build_search_bytes(uint32_t dp, uint32_t ef, uint32_t ccap, uint32_t hash_cap, uint32_t mm, uint32_t sel_rows) {
+size_t build_search_bytes(uint32_t dp, uint32_t ef, uint32_t region_bytes, uint32_t mm, uint32_t sel_rows) {
     using dev::a16;
-    return a16(size_t(hash_cap) * 4) + a16(size_t(dp) * 4) + a16(size_t(sel_rows) * dp * 4) +
-           2 * a16(size_t(ef + 1) * 8) + a16(size_t(ccap + 1) * 8) + a16(size_t(mm) * 8) + 256 +
+    return a16(size_t(region_bytes)) + a16(size_t(dp) * 4) + a16(size_t(sel_rows) * dp * 4) +
+           a16(size_t(ef + 33) * 8) + a16(size_t(dev::kTieCap + 1) * 8) + a16(size_t(mm) * 8) + 256 +
            3 * a16(size_t(mm) * 4);
 }
 

@@ -69,9 +69,10 @@ struct BuildArgs {
     uint32_t ef = 0;                // max(ef_construction, m)
     // Search scratch per warp (dynamic shared memory, or global memory at
     // `gscratch` when one warp's share does not fit on chip).
-    uint32_t ccap = 0, hash_cap = 0, warps_per_block = 1, bytes_per_warp = 0;
+    uint32_t hash_cap = 0, warps_per_block = 1, bytes_per_warp = 0;
     uint32_t stage_rows = 0, sel_rows = 0;  // rows staged for the selection; selected rows kept on chip
     uint32_t sel_in_stage = 0;  // selected rows live in the hash region after the staged rows
+    uint32_t region_bytes = 0;  // the hash region (>= hash_cap * 4)
     char* gscratch = nullptr;
     uint32_t* spill = nullptr;  // per warp slot, spill_words words (zero between uses)
     uint32_t spill_words = 0;
@@ -95,9 +96,9 @@ struct BuildArgs {
     uint32_t max_records = 0;
 };
 
-// Per-warp search scratch bytes for ef, candidate capacity, hash entries,
-// selection size mm and row floats dp.
-size_t build_search_bytes(uint32_t dp, uint32_t ef, uint32_t ccap, uint32_t hash_cap, uint32_t mm, uint32_t sel_rows);
+// Per-warp search scratch bytes for ef, hash region bytes, selection size
+// mm and row floats dp.
+size_t build_search_bytes(uint32_t dp, uint32_t ef, uint32_t region_bytes, uint32_t mm, uint32_t sel_rows);
 size_t build_connect_bytes(uint32_t dp, uint32_t cap, uint32_t stage_rows, uint32_t sel_rows);
 
 // Resident blocks per SM of the search (search = true) or connect kernel.

@@ -140,40 +140,43 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
     a.extend = P.selection && P.extend_candidates;
     a.keep_pruned = P.keep_pruned;
     a.ef = ef;
-    a.ccap = ef + 64;
     // The visited hash holds about 16 entries per unit of ef (a layer-0
-    // search at ef = 200 visits 2-3k nodes); a search that passes 3/4 of it
+    // search at ef = 200 visits 1-2k nodes); a search that passes 3/4 of it
     // continues in its HBM bitmap. After the search the hash region holds
-    // the staged candidate rows of the selection and, when they fit, the
-    // selected rows.
-    a.hash_cap = opt.hash_cap ? pow2_at_least(opt.hash_cap) : pow2_at_least(std::max<uint64_t>(1024, 16ull * ef));
-    a.hash_cap = std::max<uint32_t>(a.hash_cap, 64);
+    // the staged candidate rows of the selection and, when they fit in a
+    // region of at most 24 KB, the selected rows.
     const size_t rowb = size_t(dp) * 4;
-    auto layout_stage = [&]() {
+    a.hash_cap = opt.hash_cap ? std::max<uint32_t>(opt.hash_cap, 64)
+                              : round_up(std::max<uint32_t>(1024, std::min<uint32_t>(16 * ef, 1u << 20)), 32);
+    auto layout_region = [&]() {
         const size_t hb = size_t(a.hash_cap) * 4;
-        if (size_t(m + 4) * rowb <= hb) {
+        const size_t want = size_t(m + 8) * rowb;
+        if (want <= std::max<size_t>(hb, 24 * 1024)) {
+            a.region_bytes = uint32_t(std::max(hb, want));
             a.sel_in_stage = 1;
             a.sel_rows = 0;
-            a.stage_rows = uint32_t(std::min<size_t>(32, (hb - size_t(m) * rowb) / rowb));
+            a.stage_rows = uint32_t(std::min<size_t>(32, (a.region_bytes - size_t(m) * rowb) / rowb));
         } else {
+            a.region_bytes = uint32_t(hb);
             a.sel_in_stage = 0;
-            a.sel_rows = size_t(m) * rowb <= 16384 ? m : 0;
+            a.sel_rows = 0;
             a.stage_rows = uint32_t(std::min<size_t>(32, hb / rowb));
         }
+        if (!opt.hash_cap) a.hash_cap = a.region_bytes / 4;
     };
-    layout_stage();
-    size_t bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
+    layout_region();
+    size_t bytes = build_search_bytes(dp, ef, a.region_bytes, m, a.sel_rows);
     while (bytes > budget / 4 && a.hash_cap > 4096 && !opt.hash_cap) {
-        a.hash_cap >>= 1;
-        layout_stage();
-        bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
+        a.hash_cap = round_up(a.hash_cap / 2, 32);
+        layout_region();
+        bytes = build_search_bytes(dp, ef, a.region_bytes, m, a.sel_rows);
     }
     const bool s_global = bytes > budget;
     if (s_global) {
         // cp.async stages into shared memory only: no staging from HBM scratch.
         a.stage_rows = 0;
         a.sel_in_stage = 0;
-        bytes = build_search_bytes(dp, ef, a.ccap, a.hash_cap, m, a.sel_rows);
+        bytes = build_search_bytes(dp, ef, a.region_bytes, m, a.sel_rows);
     }
     a.bytes_per_warp = uint32_t(bytes);
     uint32_t s_blocks_per_sm = 0;

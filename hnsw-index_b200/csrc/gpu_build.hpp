@@ -8,7 +8,7 @@
 namespace hnswgpu {
 
 struct GpuBuildOptions {
-    double wave_fraction = 0.02;  // nodes per wave = max(1, floor(linked * fraction))
+    double wave_fraction = 0.05;  // nodes per wave = max(1, floor(linked * fraction))
     uint32_t max_wave = 65536;
     uint32_t hash_cap = 0;        // visited-hash entries per warp (0: 16 per unit of ef)
     uint32_t timing = 0;          // record per-phase device times

@@ -412,7 +412,7 @@ typedef struct hnsw_gpu_build_stats {
     uint32_t connect_warps_per_block, connect_blocks_per_sm;
     uint32_t hash_cap;
 } hnsw_gpu_build_stats;
-/* Defaults: wave_fraction 0.02, max_wave 65536, hash_cap 0, timing 0. */
+/* Defaults: wave_fraction 0.05, max_wave 65536, hash_cap 0, timing 0. */
 void hnsw_gpu_build_opts_default(hnsw_gpu_build_opts* out);
 /* HnswIndex::insert_batch (mod.rs:318-338) with the link step on a GPU.
  * opts may be NULL (defaults). */
