@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <queue>
 #include <thread>
 #include <unordered_set>
@@ -705,15 +706,19 @@ uint32_t Builder::push_nodes(const uint64_t* keys, size_t count) {
     size_t total = first + count;
     ix_.l0.resize(total * (ix_.params.m0 + 1), 0);
     ix_.upper.resize(total);
-    for (size_t i = 0; i < count; ++i) {
-        uint32_t id = first + uint32_t(i);
-        uint8_t level = sample_level(ix_.params.seed, id, ix_.params.level_multiplier);
-        ix_.upper[id].assign(size_t(level) * (ix_.params.m + 1), 0);
-        ix_.keys.push_back(keys[i]);
-        ix_.levels.push_back(level);
-        ix_.deleted.push_back(0);
-        ix_.key_to_id[keys[i]] = id;
-    }
+    ix_.levels.resize(total);
+    parallel_chunks(count, [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            const uint32_t id = first + uint32_t(i);
+            const uint8_t level = sample_level(ix_.params.seed, id, ix_.params.level_multiplier);
+            ix_.levels[id] = level;
+            if (level) ix_.upper[id].assign(size_t(level) * (ix_.params.m + 1), 0);
+        }
+    });
+    ix_.keys.insert(ix_.keys.end(), keys, keys + count);
+    ix_.deleted.resize(total, 0);
+    ix_.key_to_id.reserve(ix_.key_to_id.size() + count);
+    for (size_t i = 0; i < count; ++i) ix_.key_to_id[keys[i]] = first + uint32_t(i);
     if (impl_->nlocks < total) {
         size_t cap = std::max(total, impl_->nlocks * 2);
         impl_->locks.reset(new SpinLock[cap]);
@@ -751,22 +756,68 @@ Err Builder::insert_batch(const uint64_t* keys, const float* v, size_t count, in
 }
 
 Err Builder::append_batch(const uint64_t* keys, const float* v, size_t count, uint32_t* first_out) {
-    std::vector<float> prepared;
-    prepared.reserve(count * ix_.dim);
-    for (size_t i = 0; i < count; ++i) {
-        Err e = prepare(v + i * ix_.dim, &prepared);
-        if (e) return e;
-    }
-    std::unordered_set<uint64_t> seen;
-    seen.reserve(count);
-    for (size_t i = 0; i < count; ++i)
-        if (ix_.key_to_id.count(keys[i]) || !seen.insert(keys[i]).second) {
-            Err e = fail(HNSW_ERR_DUPLICATE_KEY);
-            e.a = keys[i];
-            return e;
+    // prepare_batch: every row is checked in parallel (read only); the error
+    // reported is the first failing row's, as in a sequential pass.
+    const size_t dim = ix_.dim, base = ix_.vectors.size();
+    std::atomic<size_t> first_bad{count};
+    int bad_status = 0;
+    std::mutex err_mu;
+    const bool cosine = ix_.metric == HNSW_METRIC_COSINE;
+    parallel_chunks(count, [&](size_t b, size_t e) {
+        for (size_t i = b; i < e && i < first_bad.load(std::memory_order_relaxed); ++i) {
+            double norm = 0.0;
+            int st = check_vector(v + i * dim, dim, &norm);
+            if (!st && cosine && norm == 0.0) st = HNSW_ERR_ZERO_VECTOR;
+            if (st) {
+                std::lock_guard<std::mutex> lock(err_mu);
+                if (i < first_bad.load()) {
+                    first_bad.store(i);
+                    bad_status = st;
+                }
+                return;
+            }
         }
+    });
+    if (first_bad.load() < count) return fail(bad_status);
+    // Duplicate keys: the first key (in batch order) that is live or repeats
+    // an earlier one, found with an open-addressing set.
+    {
+        size_t cap = 16;
+        while (cap < 2 * count) cap <<= 1;
+        std::vector<uint64_t> table(cap, 0);
+        std::vector<uint8_t> used(cap, 0);
+        for (size_t i = 0; i < count; ++i) {
+            const uint64_t k = keys[i];
+            bool dup = ix_.key_to_id.count(k) != 0;
+            if (!dup) {
+                size_t h = size_t(mix64(k)) & (cap - 1);
+                while (used[h] && table[h] != k) h = (h + 1) & (cap - 1);
+                if (used[h]) dup = true;
+                else {
+                    used[h] = 1;
+                    table[h] = k;
+                }
+            }
+            if (dup) {
+                Err e = fail(HNSW_ERR_DUPLICATE_KEY);
+                e.a = k;
+                return e;
+            }
+        }
+    }
     if (kMaxNodes - ix_.node_count() < count) return fail(HNSW_ERR_CAPACITY_EXCEEDED);
-    ix_.vectors.insert(ix_.vectors.end(), prepared.begin(), prepared.end());
+    ix_.vectors.insert(ix_.vectors.end(), v, v + count * dim);
+    if (cosine)
+        // vector::normalized (src/vector.rs:42-45), in place.
+        parallel_chunks(count, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) {
+                float* row = ix_.vectors.data() + base + i * dim;
+                double norm = 0.0;
+                check_vector(row, dim, &norm);
+                const double inv = 1.0 / std::sqrt(norm);
+                for (size_t j = 0; j < dim; ++j) row[j] = float(double(row[j]) * inv);
+            }
+        });
     *first_out = push_nodes(keys, count);
     return Err();
 }
