@@ -183,62 +183,6 @@ __device__ uint64_t bgreedy(const BuildGraph& g, BWarp& w, uint64_t best, uint32
     }
 }
 
-// Layer-search entries: (fkey(d) << 32) | (id << 1) | expanded. The flag bit
-// sits below the id, so the u64 order is still the (total_cmp distance, id)
-// order of Candidate (src/hnsw/search.rs:36-44).
-__device__ __forceinline__ uint64_t upack(float d, uint32_t id) { return (uint64_t(fkey(d)) << 32) | (uint64_t(id) << 1); }
-__device__ __forceinline__ uint64_t to_upack(uint64_t x) { return (x & 0xFFFFFFFF00000000ull) | (uint64_t(uint32_t(x)) << 1); }
-__device__ __forceinline__ uint64_t from_upack(uint64_t x) { return (x & 0xFFFFFFFF00000000ull) | (uint32_t(x) >> 1); }
-
-// Merges the entries x of the lanes in S (distinct, none in A) into the
-// ascending A[0, hi) (room for all of them). Returns the lowest position
-// written. All lanes call.
-__device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t S, uint64_t x) {
-    const int lane = lane_id();
-    const bool in = (S >> lane) & 1u;
-    uint32_t rank_s = 0;
-    for (uint32_t bits = S; bits; bits &= bits - 1) {
-        const int j = __ffs(bits) - 1;
-        rank_s += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
-    }
-    const uint32_t pa = in ? lower_bound(A, 0, hi, x) : hi;
-    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
-    if (hi > pmin) {
-        for (int b = int((hi - 1) & ~31u); b >= int(pmin & ~31u); b -= 32) {
-            const uint32_t k = uint32_t(b) + uint32_t(lane);
-            const bool mv = k >= pmin && k < hi;
-            const uint64_t v = mv ? A[k] : 0;
-            uint32_t shift = 0;
-            for (uint32_t bits = S; bits; bits &= bits - 1) {
-                const int j = __ffs(bits) - 1;
-                shift += (__shfl_sync(kFull, x, j) < v) ? 1u : 0u;
-            }
-            __syncwarp();
-            if (mv) A[k + shift] = v;
-            __syncwarp();
-        }
-    }
-    if (in) A[pa + rank_s] = x;
-    __syncwarp();
-    return pmin;
-}
-
-constexpr uint32_t kTieCap = 32;
-
-// A result evicted while unexpanded stays a candidate of the reference's
-// unbounded queue; it can still be expanded only if its distance equals the
-// worst result's (search.rs:113-119). Such entries (all of one distance)
-// wait in the ascending tie list T; entries of a larger distance are dead.
-__device__ __forceinline__ void tie_add(uint64_t* T, uint32_t& nt, uint64_t x, float wd, uint32_t& inexact) {
-    if (nt && pdist(T[0]) > wd) nt = 0;
-    if (nt >= kTieCap) {
-        inexact = 1;
-        return;
-    }
-    sorted_insert(T, 0, nt, x);
-    ++nt;
-}
-
 // search_layer (src/hnsw/search.rs:81-142) from the entry points R[0, ne)
 // (ascending, distinct: the previous layer's results) with admission
 // `n != self` (build.rs:71-72). Results ascending in R; returns their count.

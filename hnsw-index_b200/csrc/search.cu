@@ -713,6 +713,179 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     return int(rs);
 }
 
+// layer0 for a query that admits every node (no filter, no tombstones).
+// Results and live candidates then share one ascending array U: every entry
+// is a result, with an "expanded" bit below the id (upack), and the next
+// expansion is the first unexpanded entry. A result evicted before it was
+// expanded stays a candidate of the reference's unbounded heap only if its
+// distance equals the new worst result's (any larger one would meet the stop
+// rule first, search.rs:113-119), so those wait in the tie list T. The
+// expansion order, the visited set and every comparison are those of
+// layer0, so the results are the same; one merge per round instead of two.
+// U lives in the candidate array's space (cand_cap + 1 >= ef_cap + 33), T in
+// the results array's; the results are copied back to w.R at the end.
+// Returns rs, or -1 when the query outgrows the scratch (retried).
+__device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t ef) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    uint64_t* U = w.C;
+    uint64_t* T = w.R;
+    if (w.bitmap_mode) {
+        for (uint32_t i = lane; i < w.bitmap_words; i += 32) w.H[i] = 0;
+    } else {
+        for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
+    }
+    __syncwarp();
+    const uint32_t hash_limit = (w.hash_cap >> 2) * 3;
+    uint32_t visited = 1;
+    if (lane == 0) {
+        visit(w, pid(ep));
+        U[0] = to_upack(ep);
+    }
+    __syncwarp();
+    uint32_t rs = 1, nt = 0, nx = 0, lost = 0;
+    for (;;) {
+        // p: the next expansion; pn: the one after it, unless this round
+        // inserts something before it (its list is prefetched into L2).
+        uint32_t p = rs, pn = rs;
+        for (uint32_t b = nx; b < rs; b += 32) {
+            const uint32_t i = b + lane;
+            const uint32_t M = __ballot_sync(kFull, i < rs && !(U[i] & 1ull));
+            if (M) {
+                p = b + uint32_t(__ffs(int(M)) - 1);
+                const uint32_t M2 = M & (M - 1);
+                if (M2) pn = b + uint32_t(__ffs(int(M2)) - 1);
+                break;
+            }
+        }
+        uint64_t cur;
+        if (p < rs) {
+            cur = U[p];
+            __syncwarp();
+            if (lane == 0) {
+                U[p] = cur | 1ull;
+                if (pn < rs) prefetch_l2(ix.adj0 + size_t(uint32_t(U[pn]) >> 1) * ix.m0p, ix.m0p * 4);
+            }
+            nx = p + 1;
+        } else {
+            if (nt == 0) break;
+            cur = T[0];
+            for (uint32_t b = 0; b + 1 < nt; b += 32) {
+                const uint32_t i = b + lane;
+                const uint64_t v = i + 1 < nt ? T[i + 1] : 0;
+                __syncwarp();
+                if (i + 1 < nt) T[i] = v;
+            }
+            --nt;
+            nx = rs;
+            if (rs >= ef && pdist(cur) > pdist(U[rs - 1])) break;
+        }
+        __syncwarp();
+        c.cnt.exp0++;
+        const uint32_t* row = ix.adj0 + size_t(uint32_t(cur) >> 1) * ix.m0p;
+        for (uint32_t base = 0; base < ix.m0; base += 32) {
+            const uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+            const bool valid = id != kEmpty;
+            const uint32_t V = __ballot_sync(kFull, valid);
+            if (V == 0) break;
+            if (!w.bitmap_mode && visited + __popc(V) > hash_limit) {
+                if (!w.spill_bits) return -1;
+                for (uint32_t i = lane; i < w.hash_cap; i += 32) {
+                    const uint32_t v = w.H[i];
+                    if (v != kEmpty) atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
+                }
+                __syncwarp();
+                w.H = w.spill_bits;
+                w.bitmap_mode = true;
+                w.bitmap_words = w.spill_words;
+                w.spilled_bits = true;
+            }
+            const bool fresh = valid && visit(w, id);
+            if (fresh && !w.stage) {
+                if (c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
+                else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
+            }
+            const uint32_t F = __ballot_sync(kFull, fresh);
+            visited += __popc(F);
+            if (F != 0) {
+                chunk_distances(c, id, F);
+                c.cnt.dist0 += __popc(F);
+                const float my_d = fresh ? w.fd[lane] : 0.0f;
+                uint32_t P = F;
+                if (rs >= ef) P &= __ballot_sync(kFull, fresh && my_d < pdist(U[rs - 1]));
+                if (P == 0) {
+                    if (V != kFull) break;
+                    continue;
+                }
+                const bool inP = (P >> lane) & 1u;
+                const uint64_t my_x = upack(my_d, id);
+                const float dz = __fadd_rn(my_d, 0.0f);
+                const unsigned same =
+                    __match_any_sync(kFull, inP ? __float_as_uint(dz) : (0x7FC00000u | uint32_t(lane)));
+                uint32_t pr = 0;
+                bool tie = inP && __popc(same) > 1;
+                if (inP) {
+                    pr = lower_bound(U, 0, rs, my_x);
+                    if (pr < rs && pdist(U[pr]) == my_d) tie = true;
+                    if (pr > 0 && pdist(U[pr - 1]) == my_d) tie = true;
+                }
+                if (!__any_sync(kFull, tie)) {
+                    uint32_t before = 0;
+                    for (uint32_t bits = P; bits; bits &= bits - 1) {
+                        const int j = __ffs(bits) - 1;
+                        const uint64_t xj = __shfl_sync(kFull, my_x, j);
+                        before += (j < lane && xj < my_x) ? 1u : 0u;
+                    }
+                    const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
+                    if (I) {
+                        nx = min(nx, merge_all(U, rs, I, my_x));
+                        const uint32_t total = rs + uint32_t(__popc(I));
+                        if (total > ef) {
+                            const float wd = pdist(U[ef - 1]);
+                            const uint32_t i = ef + uint32_t(lane);
+                            const uint64_t v = i < total ? U[i] : 0;
+                            uint32_t E = __ballot_sync(kFull, i < total && !(v & 1ull) && pdist(v) == wd);
+                            while (E) {
+                                const int j = __ffs(int(E)) - 1;
+                                E &= E - 1;
+                                tie_add(T, nt, __shfl_sync(kFull, v, j), wd, lost);
+                            }
+                            rs = ef;
+                        } else {
+                            rs = total;
+                        }
+                    }
+                } else {
+                    while (P) {
+                        const int i = __ffs(P) - 1;
+                        P &= P - 1;
+                        const float d = __shfl_sync(kFull, my_d, i);
+                        const uint32_t nid = __shfl_sync(kFull, id, i);
+                        const bool improves = rs < ef || d < pdist(U[rs - 1]);
+                        if (!improves) continue;
+                        const uint32_t pos = sorted_insert(U, 0, rs, upack(d, nid));
+                        nx = min(nx, pos);
+                        if (++rs > ef) {
+                            rs = ef;
+                            const uint64_t v = U[ef];
+                            if (!(v & 1ull) && pdist(v) == pdist(U[ef - 1])) tie_add(T, nt, v, pdist(v), lost);
+                        }
+                    }
+                }
+                // A full tie list would drop a live candidate: retry with
+                // the general queue instead.
+                if (lost) return -1;
+            }
+            if (V != kFull) break;
+        }
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < rs; i += 32) w.R[i] = from_upack(U[i]);
+    __syncwarp();
+    return int(rs);
+}
+
 // Exact scan of the nodes a selective filter admits (the planner's route,
 // advised by src/hnsw/mod.rs:421-425): every admitted live node gets its f32
 // distance in the reference kernel order, and the best ef by (distance, id)
@@ -805,7 +978,8 @@ __device__ int32_t prepare(QueryCtx& c, const float* q) {
 }
 
 // One query, start to finish. Returns the status written.
-template <bool COLD>
+// V: 0 lean, 1 cold-list variant, 2 single-array variant (every node admitted).
+template <int V>
 __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
     const DeviceIndexView& ix = a.ix;
     const int lane = lane_id();
@@ -845,7 +1019,8 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
             c.cnt.dist_up++;
             uint64_t ep = pack(d0, ix.entry);
             for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
-            rs = layer0<COLD>(c, ep, ef);
+            if constexpr (V == 2) rs = layer0_single(c, ep, ef);
+            else rs = layer0<V == 1>(c, ep, ef);
             if (rs < 0) return ST_OVERFLOW;
         }
         // Quantized: exact distances for the survivors (src/hnsw/mod.rs:494-498).
@@ -1002,7 +1177,7 @@ __device__ void end_spill(Ws& w) {
 // The fast kernel. COLD = false: candidate queues spill to a per-warp global
 // array and, beyond it, to the retry pass. COLD = true: the shared array's
 // upper half moves to the cold list directly.
-template <bool COLD>
+template <int V>
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1014,18 +1189,18 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
         if (a.spill_bits && slot < a.spill_slots) {
             w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;
             w.spill_words = a.spill_words;
-            if (!COLD && a.spill_cands) {
+            if (V == 0 && a.spill_cands) {
                 w.spill_cands = a.spill_cands + size_t(slot) * (a.spill_cand_cap + 1);
                 w.spill_cand_cap = a.spill_cand_cap;
             }
         }
-        if (COLD) attach_cold(w, a, slot, a.cold_next);
+        if (V == 1) attach_cold(w, a, slot, a.cold_next);
         for (;;) {
             uint32_t qi = 0;
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
             qi = __shfl_sync(kFull, qi, 0);
             if (qi >= a.nq) break;
-            const int32_t st = run_query<COLD>(a, w, qi);
+            const int32_t st = run_query<V>(a, w, qi);
             end_spill(w);
             if (st == ST_OVERFLOW && lane == 0) {
                 a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
@@ -1035,7 +1210,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     } else {
         const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
         if (qi >= a.nq) return;
-        if (run_query<COLD>(a, w, qi) == ST_OVERFLOW && lane == 0) {
+        if (run_query<V>(a, w, qi) == ST_OVERFLOW && lane == 0) {
             a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
             a.out_status[qi] = ST_OVERFLOW;
         }
@@ -1103,7 +1278,7 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
         const uint32_t qi = a.overflow_list[t];
         // Writes ST_OVERFLOW again if even this scratch is too small; the
         // last-resort pass then takes the query.
-        if (run_query<true>(a, w, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)
+        if (run_query<1>(a, w, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)
             a.overflow_list2[atomicAdd(a.overflow_count2, 1u)] = qi;
     }
 }
@@ -1166,11 +1341,21 @@ uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t 
     return uint32_t(al(b));
 }
 
+// The single-array variant serves batches in which every query admits every
+// node (no filter bitmaps, no tombstones) when the geometry leaves room for
+// its arrays: ef_cap + 33 entries in the candidate array, the tie list in
+// the results array.
+static bool single_array_batch(const SearchArgs& args, const SearchGeometry& g) {
+    return !args.filter_bits && !args.ix.has_dead && !args.planned && g.ef_cap >= dev::kTieCap &&
+           g.cand_cap >= g.ef_cap + 32;
+}
+
 cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, int num_sms, cudaStream_t stream) {
     SearchGeometry geo = geo_in;
     geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
     const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
-    auto kern = geo.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
+    auto kern = single_array_batch(args, geo) ? dev::search_kernel<2>
+                                              : (geo.cold ? dev::search_kernel<1> : dev::search_kernel<0>);
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
     dim3 block(32 * geo.warps_per_block);
@@ -1195,13 +1380,17 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     SearchGeometry g = g_in;
     g.bytes_per_warp = geometry_bytes_per_warp(g, dp, dc);
     const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
-    auto kern = g.cold ? dev::search_kernel<true> : dev::search_kernel<false>;
-    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(32 * g.warps_per_block), smem);
-    if (e != cudaSuccess) return e;
-    *warps = uint32_t(std::max(per_sm, 1)) * g.warps_per_block * uint32_t(num_sms);
+    // Spill slots for whichever variant a batch takes: the larger residency.
+    int best = 1;
+    for (auto kern : {g.cold ? dev::search_kernel<1> : dev::search_kernel<0>, dev::search_kernel<2>}) {
+        cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(32 * g.warps_per_block), smem);
+        if (e != cudaSuccess) return e;
+        best = std::max(best, per_sm);
+    }
+    *warps = uint32_t(best) * g.warps_per_block * uint32_t(num_sms);
     return cudaSuccess;
 }
 

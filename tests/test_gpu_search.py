@@ -315,6 +315,25 @@ def test_visited_and_candidate_overflow_paths(mode):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("quant", [False, True])
+def test_distance_ties_bit_exact(mode, quant):
+    """Small-integer points with ~40 copies each: most distances tie, so the
+    heap order falls back to ids (src/hnsw/search.rs:36-44) and results that
+    tie with the worst one are evicted unexpanded. Unfiltered batches take the
+    single-array layer-0 variant, whose tie list overflows here and sends
+    those queries to the retry pass; every answer must still be the oracle's."""
+    rng = np.random.default_rng(11)
+    base = rng.integers(0, 3, size=(3000, 4)).astype(np.float32)
+    queries = np.vstack([rng.integers(0, 3, size=(150, 4)), rng.integers(-1, 4, size=(50, 4))]).astype(np.float32)
+    data = build_index(base, metric=0, m=8, seed=3, quantize=quant)
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    for k, ef in [(1, 1), (10, 16), (10, 40), (32, 64), (50, 200)]:
+        got = gi.search_arrays(queries, k, ef, mode=mode, quantized=quant)
+        assert_same(got, oi.search(queries, k, ef, quantized=quant), f"k={k} ef={ef}")
+
+
+@pytest.mark.parametrize("mode", [0, 1])
 def test_modes_on_quantized_filtered_tombstoned_mixture(mode):
     base, queries = H.mixture(6000, 96, 32, 30, 0.4, 8)
     rng = np.random.default_rng(5)
