@@ -121,19 +121,27 @@ __device__ __forceinline__ bool admit(const QueryCtx& c, uint32_t id) {
     return key < c.fnbits && ((__ldg(c.fbits + (key >> 6)) >> (key & 63)) & 1ull);
 }
 
+// Distance kinds a kernel is built for. DK_ANY decides per query at run time
+// (f32 rows or int8 codes, any metric, rows loaded directly or staged);
+// DK_L2 and DK_DOT are f32 rows loaded directly with the L2 sum or the dot
+// sum (inner product, cosine), so the kernel carries one distance loop
+// instead of all of them: less code in the traversal loop to fetch.
+constexpr int DK_ANY = 0, DK_L2 = 1, DK_DOT = 2;
+
 // Distance from the query to node `id` for the group of 8 lanes (valid in
 // every lane of the group). All 32 lanes call; `id` may differ per group.
+template <int DK = DK_ANY>
 __device__ __forceinline__ float group_distance(const QueryCtx& c, uint32_t id, int g8) {
     const DeviceIndexView& ix = c.a->ix;
-    if (c.quant) {
+    if (DK == DK_ANY && c.quant) {
         int dot = group_i8dot(ix.codes + size_t(id) * ix.dc, c.w->qc, int(ix.dc), g8);
         long long l2 = 0;
         if (c.metric == 0) l2 = (long long)c.qnorm + (long long)__ldg(ix.code_norm + id) - 2ll * (long long)dot;
         return sq_distance(c.metric, dot, l2, c.s2);
     }
     const float* row = ix.vec + size_t(id) * ix.dp;
-    float s = c.metric == 0 ? group_sum<true>(row, c.w->qf, int(ix.dim), g8)
-                            : group_sum<false>(row, c.w->qf, int(ix.dim), g8);
+    const bool l2 = DK == DK_ANY ? c.metric == 0 : DK == DK_L2;
+    float s = l2 ? group_sum<true>(row, c.w->qf, int(ix.dim), g8) : group_sum<false>(row, c.w->qf, int(ix.dim), g8);
     s = __shfl_sync(kFull, s, (lane_id() & ~7));
     return metric_from_sum(c.metric, s);
 }
@@ -166,19 +174,21 @@ __device__ __forceinline__ float group_exact(const QueryCtx& c, uint32_t id, int
 
 // Computes distances for the neighbors at positions fr[0..nf) of the
 // current chunk (ids in lane order `ids`), writing fd[pos].
+template <int DK = DK_ANY>
 __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uint32_t F) {
     Ws& w = *c.w;
     const int lane = lane_id();
     const int g = lane >> 3, g8 = lane & 7;
+    const bool stage = DK == DK_ANY && w.stage != nullptr;
     // Ranks of fresh lanes -> compact list of positions.
     if ((F >> lane) & 1u) {
         const uint32_t rk = __popc(F & ((1u << lane) - 1u));
         w.fr[rk] = uint32_t(lane);
-        if (w.stage) w.fi[rk] = my_id;
+        if (stage) w.fi[rk] = my_id;
     }
     __syncwarp();
     const uint32_t nf = __popc(F);
-    if (w.stage) {
+    if (stage) {
         // All rows of a round in flight at once, one wait, then the
         // distances from shared memory.
         const DeviceIndexView& ix = c.a->ix;
@@ -206,9 +216,10 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
         }
         return;
     }
-    if (!c.quant) {
+    if (DK != DK_ANY || !c.quant) {
         // f32 rows: two rows per group while at least five remain.
         const DeviceIndexView& ix = c.a->ix;
+        const bool l2 = DK == DK_ANY ? c.metric == 0 : DK == DK_L2;
         uint32_t r = 0;
         for (; r + 4 < nf; r += 8) {
             const uint32_t sa = r + uint32_t(g), sb = r + 4 + uint32_t(g);
@@ -216,7 +227,7 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
             const uint32_t pa = aa ? w.fr[sa] : w.fr[0], pb = ab ? w.fr[sb] : w.fr[0];
             const uint32_t ida = __shfl_sync(kFull, my_id, int(pa)), idb = __shfl_sync(kFull, my_id, int(pb));
             float s0, s1;
-            if (c.metric == 0)
+            if (l2)
                 group_sum2<true>(ix.vec + size_t(ida) * ix.dp, ix.vec + size_t(idb) * ix.dp, w.qf, int(ix.dim), g8, s0,
                                  s1);
             else
@@ -232,7 +243,7 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
             const bool active = slot < nf;
             const uint32_t pos = active ? w.fr[slot] : w.fr[0];
             const uint32_t id = __shfl_sync(kFull, my_id, int(pos));
-            const float d = group_distance(c, id, g8);
+            const float d = group_distance<DK>(c, id, g8);
             if (active && g8 == 0) w.fd[pos] = d;
         }
         __syncwarp();
@@ -250,7 +261,8 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
 }
 
 // greedy_closest (src/hnsw/search.rs:49-68) on an upper layer.
-__device__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
+template <int DK = DK_ANY>
+__device__ __forceinline__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
     const int lane = lane_id();
@@ -264,7 +276,7 @@ __device__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uint32_t layer) {
             uint32_t id = (base + lane < ix.m) ? __ldg(blk + base + lane) : kEmpty;
             uint32_t V = __ballot_sync(kFull, id != kEmpty);
             if (V == 0) break;
-            chunk_distances(c, id, V);
+            chunk_distances<DK>(c, id, V);
             c.cnt.dist_up += __popc(V);
             // First strict minimum in list order (IEEE comparison, as d < best.distance).
             float d = ((V >> lane) & 1u) ? w.fd[lane] : __int_as_float(0x7f800000);
@@ -725,6 +737,7 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
 // U lives in the candidate array's space (cand_cap + 1 >= ef_cap + 33), T in
 // the results array's; the results are copied back to w.R at the end.
 // Returns rs, or -1 when the query outgrows the scratch (retried).
+template <int DK>
 __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
@@ -802,14 +815,14 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
                 w.spilled_bits = true;
             }
             const bool fresh = valid && visit(w, id);
-            if (fresh && !w.stage) {
-                if (c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
+            if (fresh && (DK != DK_ANY || !w.stage)) {
+                if (DK == DK_ANY && c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
                 else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
             }
             const uint32_t F = __ballot_sync(kFull, fresh);
             visited += __popc(F);
             if (F != 0) {
-                chunk_distances(c, id, F);
+                chunk_distances<DK>(c, id, F);
                 c.cnt.dist0 += __popc(F);
                 const float my_d = fresh ? w.fd[lane] : 0.0f;
                 uint32_t P = F;
@@ -979,7 +992,8 @@ __device__ int32_t prepare(QueryCtx& c, const float* q) {
 
 // One query, start to finish. Returns the status written.
 // V: 0 lean, 1 cold-list variant, 2 single-array variant (every node admitted).
-template <int V>
+// DK: the distance kinds compiled in (DK_ANY unless V == 2).
+template <int V, int DK = DK_ANY>
 __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi) {
     const DeviceIndexView& ix = a.ix;
     const int lane = lane_id();
@@ -990,7 +1004,7 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
     c.metric = ix.metric;
     // Codes exist only on quantized indexes; a quantized request on any
     // other index fails with QuantizationDisabled after validation.
-    c.quant = a.quantized != 0 && ix.quantized != 0;
+    c.quant = DK == DK_ANY && a.quantized != 0 && ix.quantized != 0;
     c.s2 = __fmul_rn(ix.scale, ix.scale);
     c.qnorm = 0;
     c.use_filter = a.filter_bits != nullptr && (a.filter_used == nullptr || a.filter_used[qi] != 0);
@@ -1014,12 +1028,12 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
             float d0;
             {
                 const int g8 = lane & 7;
-                d0 = group_distance(c, ix.entry, g8);
+                d0 = group_distance<DK>(c, ix.entry, g8);
             }
             c.cnt.dist_up++;
             uint64_t ep = pack(d0, ix.entry);
-            for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer(c, ep, layer);
-            if constexpr (V == 2) rs = layer0_single(c, ep, ef);
+            for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer<DK>(c, ep, layer);
+            if constexpr (V == 2) rs = layer0_single<DK>(c, ep, ef);
             else rs = layer0<V == 1>(c, ep, ef);
             if (rs < 0) return ST_OVERFLOW;
         }
@@ -1177,7 +1191,7 @@ __device__ void end_spill(Ws& w) {
 // The fast kernel. COLD = false: candidate queues spill to a per-warp global
 // array and, beyond it, to the retry pass. COLD = true: the shared array's
 // upper half moves to the cold list directly.
-template <int V>
+template <int V, int DK = DK_ANY>
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1200,7 +1214,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
             qi = __shfl_sync(kFull, qi, 0);
             if (qi >= a.nq) break;
-            const int32_t st = run_query<V>(a, w, qi);
+            const int32_t st = run_query<V, DK>(a, w, qi);
             end_spill(w);
             if (st == ST_OVERFLOW && lane == 0) {
                 a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
@@ -1210,7 +1224,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     } else {
         const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
         if (qi >= a.nq) return;
-        if (run_query<V>(a, w, qi) == ST_OVERFLOW && lane == 0) {
+        if (run_query<V, DK>(a, w, qi) == ST_OVERFLOW && lane == 0) {
             a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
             a.out_status[qi] = ST_OVERFLOW;
         }
@@ -1350,12 +1364,20 @@ static bool single_array_batch(const SearchArgs& args, const SearchGeometry& g) 
            g.cand_cap >= g.ef_cap + 32;
 }
 
+// The search kernel a batch takes: the single-array variant when it applies,
+// built for its distance kind when the batch uses f32 rows loaded directly.
+using SearchKernel = void (*)(SearchArgs, SearchGeometry);
+static SearchKernel pick_search_kernel(const SearchArgs& args, const SearchGeometry& g) {
+    if (!single_array_batch(args, g)) return g.cold ? dev::search_kernel<1> : dev::search_kernel<0>;
+    if (args.quantized || g.stage_rows) return dev::search_kernel<2, dev::DK_ANY>;
+    return args.ix.metric == 0 ? dev::search_kernel<2, dev::DK_L2> : dev::search_kernel<2, dev::DK_DOT>;
+}
+
 cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, int num_sms, cudaStream_t stream) {
     SearchGeometry geo = geo_in;
     geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
     const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
-    auto kern = single_array_batch(args, geo) ? dev::search_kernel<2>
-                                              : (geo.cold ? dev::search_kernel<1> : dev::search_kernel<0>);
+    const SearchKernel kern = pick_search_kernel(args, geo);
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
     dim3 block(32 * geo.warps_per_block);
@@ -1382,7 +1404,8 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
     // Spill slots for whichever variant a batch takes: the larger residency.
     int best = 1;
-    for (auto kern : {g.cold ? dev::search_kernel<1> : dev::search_kernel<0>, dev::search_kernel<2>}) {
+    for (SearchKernel kern : {g.cold ? dev::search_kernel<1> : dev::search_kernel<0>, dev::search_kernel<2, dev::DK_ANY>,
+                              dev::search_kernel<2, dev::DK_L2>, dev::search_kernel<2, dev::DK_DOT>}) {
         cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
         if (e != cudaSuccess) return e;
         int per_sm = 0;
