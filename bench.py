@@ -931,8 +931,8 @@ def run_case(args):
         return r
 
     if args.workload == "case-search-1Mx128":
-        # search_kernel<2> (single-array variant, unfiltered): config 2's
-        # index and queries, ef=64.
+        # search_kernel<2, DK_L2> (single-array variant, unfiltered, f32 L2):
+        # config 2's index and queries, ef=64.
         base, queries = load_data()
         data, _ = index_file(base, 0, lambda: None)
         index = H.HnswIndex.from_bytes(data)
