@@ -93,15 +93,26 @@ def index_file(base, rank, barrier):
 
 def start_clock_sampler(device_index: int, path: str):
     try:
-        return subprocess.Popen(
+        proc = subprocess.Popen(
             ["nvidia-smi", "-i", str(device_index),
              "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "100"],
+             "--format=csv,noheader,nounits", "-lms", "50"],
             stdout=open(path, "w"), stderr=subprocess.DEVNULL)
     except Exception:
         return None
+    # nvidia-smi takes a moment to start: wait (at most 5 s) for its first
+    # sample so that a short timed region is still sampled.
+    deadline = time.time() + 5.0
+    while time.time() < deadline and proc.poll() is None:
+        try:
+            if os.path.getsize(path) > 0:
+                break
+        except OSError:
+            pass
+        time.sleep(0.01)
+    return proc
 
 
 def stop_clock_sampler(proc, path: str):
@@ -112,26 +123,44 @@ def stop_clock_sampler(proc, path: str):
         proc.wait(timeout=5)
     except Exception:
         proc.kill()
-    sm, mx, reasons = [], None, set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    rows = []
     try:
         for line in open(path):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
     except OSError:
         return None
-    if not sm:
+    return summarize_clock_rows(rows)
+
+
+def summarize_clock_rows(rows):
+    """(sm MHz, max MHz, [hw_slowdown, hw_thermal, sw_thermal, sw_power_cap])
+    per sample -> the clocks record. The first sample was taken before the
+    timed region started; it is dropped when later ones exist."""
+    if len(rows) > 1:
+        rows = rows[1:]
+    if not rows:
         return None
-    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = {n for _, _, flags in rows for n, v in zip(names, flags) if v.lower() == "active"}
+    return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": rows[-1][1], "reasons": sorted(reasons),
+            "samples": len(rows)}
+
+
+def sampled(fn, device_index: int = 0, tag: str = "run"):
+    """fn() with the clocks sampled while it runs: (fn's result, clocks record)."""
+    path = f"/tmp/hnsw_bench_clocks_{tag}.csv"
+    proc = start_clock_sampler(device_index, path)
+    try:
+        r = fn()
+    finally:
+        clocks = stop_clock_sampler(proc, path)
+    return r, clocks
 
 
 def measured_peaks():
@@ -467,20 +496,31 @@ def run_brute(args):
     bf = H.BruteForceIndex(dim, H.Metric.Cosine)
     bf.insert_batch(np.arange(nb, dtype=np.uint64), base)
     log(f"brute open in {time.time() - t:.1f} s")
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+    have_peaks = os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if have_peaks else {
+        "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
     out = {}
     results = {}
+    clocks = None
     for prec in (H.Precision.BF16X3, H.Precision.BF16, H.Precision.FP32):
         steps = args.steps if prec != H.Precision.FP32 else 1
         bf.search_arrays(queries, k, prec)  # warm-up (also builds the BF16 rows)
         times, stats = [], []
-        for _ in range(steps):
-            t = time.perf_counter()
-            res = bf.search_arrays(queries, k, prec)
-            times.append(time.perf_counter() - t)
-            if prec != H.Precision.FP32:
-                stats.append(bf.last_stats())
+
+        def run_steps():
+            r = None
+            for _ in range(steps):
+                t = time.perf_counter()
+                r = bf.search_arrays(queries, k, prec)
+                times.append(time.perf_counter() - t)
+                if prec != H.Precision.FP32:
+                    stats.append(bf.last_stats())
+            return r
+
+        if prec == H.Precision.BF16X3:
+            res, clocks = sampled(run_steps, tag="brute")
+        else:
+            res = run_steps()
         results[prec.name] = res
         entry = {"qps_e2e": nq / statistics.median(times), "ms_e2e": 1e3 * statistics.median(times)}
         if stats:
@@ -552,9 +592,11 @@ def run_brute(args):
                    "identical_to_fp32": same, "fp64_sample": fp64},
         "roofline": {"bound": "tensor", "achieved": out["BF16X3"]["tensor_tflops_executed"],
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                     "frac": out["BF16X3"]["tensor_frac_of_burst"], "traffic": None, "peak_kind": "measured burst"},
+                     "frac": out["BF16X3"]["tensor_frac_of_burst"], "traffic": None,
+                     "peak_kind": "measured burst" if have_peaks else "fallback burst"},
         "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": cores, "kind": "port",
                          "sample": f"{cs} queries, oracle FP32 brute force"},
+        "clocks": clocks,
     }
     print(json.dumps(line))
     return 0
@@ -646,7 +688,8 @@ def run_batch(args):
     out["autotune_s"] = time.time() - t
     out["autotune_best"] = best
     out["autotune_trials"] = len(trials)
-    qps, tuned_res = timed_search(index, queries, 100, 16, args.steps, mode=2, **common)
+    (qps, tuned_res), clocks = sampled(lambda: timed_search(index, queries, 100, 16, args.steps, mode=2, **common),
+                                       tag="batch")
     out["autotuned_qps"] = qps
     out["tuned_equals_heuristic"] = bool(np.array_equal(tuned_res[0], res[0]) and np.array_equal(tuned_res[2], res[2]))
     index.set_schedule(ef_cap=512, hash_cap=16384, warps_per_block=1, cold=1)
@@ -705,6 +748,7 @@ def run_batch(args):
                    "filters": nbank, "index_build_s": build_s, **out},
         "cpu_baseline": {"value": cpu_qps, "unit": "queries/s", "cores": cores, "kind": "port",
                          "sample": f"{cs} queries, oracle search_with(quantized, filter)"},
+        "clocks": clocks,
     }
     print(json.dumps(line))
     return 0
@@ -762,12 +806,15 @@ def run_serve(args):
                    linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
     srv.replay(queries[:5000], np.cumsum(rq.exponential(1e6 / 30_000, 5000)), ks[:5000], efs[:5000], fids[:5000])
     sweep = []
+    clocks = []
     for rate in (10_000, 30_000, 100_000, 300_000, 1_000_000):
         n = int(min(pool, max(5000, rate * 1.0)))
         arr = np.cumsum(rq.exponential(1e6 / rate, n))
+        sampler = start_clock_sampler(0, "/tmp/hnsw_bench_clocks_serve.csv")
         t = time.perf_counter()
         keys, dist, cnt, st, lat = srv.replay(queries[:n], arr, ks[:n], efs[:n], fids[:n])
         wall = time.perf_counter() - t
+        clocks.append(stop_clock_sampler(sampler, "/tmp/hnsw_bench_clocks_serve.csv"))
         ok = st == 0
         lat_ok = lat[ok]
         same = 0
@@ -795,6 +842,7 @@ def run_serve(args):
                    "linger_us": args.serve_linger, "launched_batches": batches, "launched_queries": launched,
                    "tuned_schedule": tuned,
                    "sweep": sweep},
+        "clocks": next((c for c in reversed(clocks) if c), None),
     }
     print(json.dumps(line))
     return 0
@@ -846,11 +894,16 @@ def run_build(args):
             "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return 0
     stats, walls = [], []
+    clocks = None
     for i in range(args.warmup + args.steps):
+        last = i == args.warmup + args.steps - 1
+        sampler = start_clock_sampler(0, "/tmp/hnsw_bench_clocks_build.csv") if last else None
         t = time.perf_counter()
         b = H.IndexBuilder(DIM, H.Metric.L2, params)
         b.insert_batch_gpu(keys, base, device=0, timing=True)
         wall = time.perf_counter() - t
+        if last:
+            clocks = stop_clock_sampler(sampler, "/tmp/hnsw_bench_clocks_build.csv")
         st = b.gpu_stats()
         log(f"build {i}: wall {wall:.2f} s, device {st['device_ms']:.0f} ms (search {st['search_ms']:.0f}, "
             f"connect {st['connect_ms']:.0f}), waves {st['waves']}, spills {st['spills']}")
@@ -910,6 +963,7 @@ def run_build(args):
         "e2e": {"value": nb / statistics.median(walls), "unit": "nodes/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": st["waves"] * 4,
+        "clocks": clocks,
     }
     if cpu_v is not None:
         line["cpu_baseline"] = {"value": cpu_v, "unit": "nodes/s", "cores": cores, "kind": "port",
