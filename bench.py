@@ -1,6 +1,6 @@
-"""Benchmark of the device HNSW query path on the plain-GPU config.
+"""Benchmark of the device HNSW query path on the 1M x 128 clustered workload.
 
-Workload (the configuration the headline metric is quoted on): 1,000,000
+Workload (the one the headline metric is quoted on): 1,000,000
 base vectors, dim 128, f32, Gaussian mixture of 1,000 centers (centers
 N(0,1), points center + N(0, 0.3^2) per coordinate, seed 1); 10,000 queries
 from the same mixture (seed 2); L2, M=16, M0=32, efConstruction=200; k=10;
@@ -643,7 +643,7 @@ def timed_search(index, queries, k, ef, steps, **kw):
 
 
 # ---------------------------------------------------------------------------
-# Batching workload (config 4): 5M x 96 inner product, int8 traversal +
+# Batching workload: 5M x 96 inner product, int8 traversal +
 # exact re-rank, 5% tombstones, per-query filters, uneven k and ef.
 # ---------------------------------------------------------------------------
 def run_batch(args):
@@ -755,7 +755,7 @@ def run_batch(args):
 
 
 # ---------------------------------------------------------------------------
-# Serving workload (config 5): 10M x 128 L2, open-loop Poisson arrivals.
+# Serving workload: 10M x 128 L2, open-loop Poisson arrivals.
 # ---------------------------------------------------------------------------
 def run_serve(args):
     import hnsw_gpu as H
@@ -859,7 +859,7 @@ def build_bytes_search(st, dim) -> float:
 
 
 def run_build(args):
-    """insert_batch of config 2's 1M x 128 base with the link step on the GPU
+    """insert_batch of the default workload's 1M x 128 clustered base with the link step on the GPU
     (M=16, ef_construction=200), against the host builder on all cores."""
     import hnsw_gpu as H
 
@@ -986,7 +986,7 @@ def run_case(args):
 
     if args.workload == "case-search-1Mx128":
         # search_kernel<2, DK_L2> (single-array variant, unfiltered, f32 L2):
-        # config 2's index and queries, ef=64.
+        # the default workload's 1M x 128 index and queries, ef=64.
         base, queries = load_data()
         data, _ = index_file(base, 0, lambda: None)
         index = H.HnswIndex.from_bytes(data)
@@ -1032,7 +1032,7 @@ def run_case(args):
         for _ in range(3):
             r = timed_call(lambda: index.search_arrays(queries, 10, 256, filter_bits=bits, filter_nbits=nb, mode=0))
     elif args.workload == "case-build-300kx128":
-        # Build kernels: the first 300k rows of config 2's base (154 MB of
+        # Build kernels: the first 300k rows of the default workload's 1M x 128 base (154 MB of
         # rows, more than L2) linked on the GPU (M=16, ef_construction=200),
         # one build.
         base, _ = load_data()

@@ -31,20 +31,20 @@ def assert_same(gpu, ref, label=""):
 
 @pytest.fixture(scope="module")
 def gaussian_10k():
-    """Config 1: 10k x 128 N(0,1) seed 42, queries seed 43, L2, M=16, seed 7."""
+    """10k x 128 N(0,1) base from seed 42, queries from seed 43, L2, M=16, level seed 7."""
     base, _ = H.gaussian(10_000, 0, 128, 42)
     _, queries = H.gaussian(0, 1000, 128, 43)
     data = build_index(base, metric=0, m=16, seed=7)
     return base, queries, data
 
 
-def test_config1_bit_exact(gaussian_10k):
+def test_gaussian_10k_bit_exact(gaussian_10k):
     base, queries, data = gaussian_10k
     gi = H.HnswIndex.from_bytes(data)
     oi = O.Index(data)
     gpu = gi.search_arrays(queries, 10, 64)
     ref = oi.search(queries, 10, 64)
-    assert_same(gpu, ref, "config 1")
+    assert_same(gpu, ref, "gaussian 10k x 128")
     tk, _, tc, _ = O.brute(0, base, queries, 10)
     r_gpu = O.recall_at_k(tk, tc, gpu[0], gpu[2], 10)
     r_ref = O.recall_at_k(tk, tc, ref[0], ref[2], 10)
@@ -352,7 +352,7 @@ def test_modes_on_quantized_filtered_tombstoned_mixture(mode):
                            filter_stride=words, ks=ks, efs=efs, mode=mode)
     ref = oi.search(queries, 100, 16, quantized=True, filter_bits=bits, filter_nbits=6000,
                     filter_stride=words, ks=ks, efs=efs)
-    assert_same(got, ref, f"config-4-like mode={mode}")
+    assert_same(got, ref, f"IP mixture, int8, filters, tombstones, mode={mode}")
 
 
 def test_shared_filter_bitmaps_by_id():
