@@ -249,15 +249,18 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
         __syncwarp();
         return;
     }
-    for (uint32_t r = 0; r < nf; r += 4) {
-        uint32_t slot = r + uint32_t(g);
-        bool active = slot < nf;
-        uint32_t pos = active ? w.fr[slot] : w.fr[0];
-        uint32_t id = __shfl_sync(kFull, my_id, int(pos));
-        float d = group_distance(c, id, g8);
-        if (active && g8 == 0) w.fd[pos] = d;
+    if constexpr (DK == DK_ANY) {
+        // int8 codes, one row per group.
+        for (uint32_t r = 0; r < nf; r += 4) {
+            uint32_t slot = r + uint32_t(g);
+            bool active = slot < nf;
+            uint32_t pos = active ? w.fr[slot] : w.fr[0];
+            uint32_t id = __shfl_sync(kFull, my_id, int(pos));
+            float d = group_distance(c, id, g8);
+            if (active && g8 == 0) w.fd[pos] = d;
+        }
+        __syncwarp();
     }
-    __syncwarp();
 }
 
 // greedy_closest (src/hnsw/search.rs:49-68) on an upper layer.
