@@ -488,6 +488,7 @@ int hnsw_gpu_index_open(const uint8_t* bytes, size_t len, uint64_t max_memory, i
         return set_error(HNSW_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(ce));
     if (device < 0 || device >= ndev) return set_error(HNSW_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     DeviceGuard dg(device);
+    TraceRange trace("hnsw.index_open");
     std::unique_ptr<hnsw_gpu_index> gi(new hnsw_gpu_index());
     gi->device = device;
     gi->slots.device = device;
@@ -663,6 +664,7 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
     if (!queries || !out_keys || !out_dist || !out_count || !out_status)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "null buffer");
     DeviceGuard dg(gi->device);
+    TraceRange trace("hnsw.search_batch");
     Slot* s = nullptr;
     r = gi->slots.acquire(&s);
     if (r != HNSW_OK) return r;
@@ -718,6 +720,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     if (reps == 0) reps = 3;
     if (reps > 50) return set_error(HNSW_ERR_INVALID_ARGUMENT, "at most 50 timed runs per schedule");
     DeviceGuard dg(gi->device);
+    TraceRange trace("hnsw.autotune");
     Slot* s = nullptr;
     r = gi->slots.acquire(&s);
     if (r != HNSW_OK) return r;
@@ -875,6 +878,7 @@ int hnsw_gpu_search_batch_device(hnsw_gpu_index* gi, const float* d_queries, siz
     const uint32_t ef_bound = std::max(o->k, o->ef);
     const uint32_t stride = o->out_stride ? o->out_stride : std::max<uint32_t>(o->k, 1);
     DeviceGuard dg(gi->device);
+    TraceRange trace("hnsw.search_batch_device");
     std::lock_guard<std::mutex> lock(gi->dev_mu);
     if (!gi->dev_slot) {
         Slot* s = nullptr;
@@ -954,6 +958,7 @@ int hnsw_gpu_graph_create(hnsw_gpu_index* gi, const float* d_queries, size_t nq,
 int hnsw_gpu_graph_launch(hnsw_gpu_graph* g, void* stream) {
     if (!g) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null graph");
     DeviceGuard dg(g->index->device);
+    TraceRange trace("hnsw.graph_launch");
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g->slot->stream;
     CU(cudaGraphLaunch(g->exec, st), "graph launch");
     return HNSW_OK;
@@ -1046,6 +1051,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
                                uint64_t* out_keys, float* out_dist, uint32_t* out_count, int32_t* out_status) {
     std::lock_guard<std::mutex> lock(b->mu);
     DeviceGuard dg(b->device);
+    TraceRange trace("hnsw.brute_search_tensor");
     cudaStream_t st = b->stream;
     const int terms = precision == HNSW_PRECISION_BF16X3 ? 3 : 1;
     const int ti = terms == 3 ? 1 : 0;
@@ -1202,6 +1208,7 @@ static int brute_search_fp32(hnsw_gpu_brute* b, const float* queries, size_t nq,
                              int32_t* out_status) {
     std::lock_guard<std::mutex> lock(b->mu);
     DeviceGuard dg(b->device);
+    TraceRange trace("hnsw.brute_search_fp32");
     cudaStream_t st = b->stream;
     const uint32_t kk = std::max<uint32_t>(k, 1);
     BruteArgs a;

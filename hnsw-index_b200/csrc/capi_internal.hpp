@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -105,6 +106,17 @@ struct SlotPool {
         std::lock_guard<std::mutex> g(mu);
         free.emplace_back(s);
     }
+};
+
+// A named range on the NVTX timeline around a host-side phase (staging,
+// enqueue, copies, a build wave). Profilers that attach an NVTX tool (Nsight
+// Systems, Nsight Compute with --nvtx) show it; without one it costs a
+// function call.
+struct TraceRange {
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
 };
 
 struct DeviceGuard {

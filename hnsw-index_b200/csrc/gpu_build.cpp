@@ -356,6 +356,7 @@ int gpu_link(HostIndex& ix, uint32_t first, int device, const GpuBuildOptions& o
         marks.resize(2 * waves.size());
         for (auto& e : marks) CU(cudaEventCreate(&e), "cudaEventCreate");
     }
+    TraceRange trace("hnsw.build_waves");
     CU(cudaEventRecord(ev0, stream), "cudaEventRecord");
     for (size_t i = 0; i < waves.size(); ++i) {
         const Wave& wv = waves[i];

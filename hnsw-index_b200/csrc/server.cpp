@@ -100,6 +100,7 @@ struct hnsw_gpu_server {
 namespace {
 
 int stage_and_launch(hnsw_gpu_server* s, BatchSlot& b, std::vector<uint64_t>& tickets) {
+    TraceRange trace("hnsw.server_batch");
     const uint32_t n = uint32_t(tickets.size());
     const uint32_t dim = s->dim, K = s->cfg.max_k;
     bool any_filter = false;
