@@ -7,8 +7,8 @@
 //
 // Every function names the reference file:line it restates (paths are within
 // the hnsw-index crate). Pinned by the reference's own known answers (see
-// tests/test_oracle_golden.py): SplitMix64 outputs, the Python-generator golden
-// components, CRC-32 check values, scalar kernel known answers, metric known
+// tests/test_oracle_golden.py): SplitMix64 outputs, the golden components of
+// the synthetic generator (tests/recall.rs:130-138), CRC-32 check values, scalar kernel known answers, metric known
 // answers (IP -0.0), brute-force tie breaking, the complete-graph exactness
 // case and the recall pins.
 //
