@@ -98,7 +98,7 @@ def start_clock_sampler(device_index: int, path: str):
              "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "50"],
+             "--format=csv,noheader,nounits", "-lms", "100"],
             stdout=open(path, "w"), stderr=subprocess.DEVNULL)
     except Exception:
         return None
