@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import hnsw_gpu as H
-from conftest import ROOT, build_index
+from conftest import ROOT, build_index, gpu_available
 
 
 def parse(data: bytes):
@@ -183,3 +183,18 @@ def test_library_exports_every_declared_function():
     for name in names:
         assert hasattr(lib, name), f"{name} declared in include/hnsw_gpu.h but not exported"
     assert set(H.EXPORTED_SYMBOLS) <= set(names)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the behaviour on a host without a CUDA device")
+def test_device_paths_fail_loudly_without_a_gpu():
+    # There is no CPU search path behind the device API: without a CUDA
+    # device, opening an index and loading brute-force rows are CUDA errors.
+    base, _ = H.gaussian(200, 0, 8, 1)
+    data = build_index(base)
+    with pytest.raises(H.Error) as e:
+        H.HnswIndex.from_bytes(data)
+    assert e.value.status == H.Status.CUDA
+    bf = H.BruteForceIndex(8, H.Metric.L2)
+    with pytest.raises(H.Error) as e:
+        bf.insert_batch(np.arange(200, dtype=np.uint64), base)
+    assert e.value.status == H.Status.CUDA
