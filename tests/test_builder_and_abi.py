@@ -198,3 +198,40 @@ def test_device_paths_fail_loudly_without_a_gpu():
     with pytest.raises(H.Error) as e:
         bf.insert_batch(np.arange(200, dtype=np.uint64), base)
     assert e.value.status == H.Status.CUDA
+
+
+def test_null_handles_are_rejected_without_touching_the_device():
+    # Every entry point checks its handle before any CUDA call: a null
+    # handle is INVALID_ARGUMENT with a message, and the close/free calls
+    # accept null (no compute is launched, so this runs on any host).
+    lib = ctypes.CDLL(H.LIBRARY_PATH)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    lib.hnsw_last_error.restype = ctypes.c_char_p
+    calls = {
+        "hnsw_gpu_index_info": ([vp, vp], (None, None)),
+        "hnsw_gpu_set_tombstones": ([vp, vp, sz], (None, None, 0)),
+        "hnsw_gpu_search_batch": ([vp, vp, sz, sz, vp, vp, vp, vp, vp], (None, None, 1, 8, None, None, None, None,
+                                                                         None)),
+        "hnsw_gpu_search_batch_device": ([vp, vp, sz, sz, vp, vp, vp, vp, vp, vp],
+                                         (None, None, 1, 8, None, None, None, None, None, None)),
+        "hnsw_gpu_graph_launch": ([vp, vp], (None, None)),
+        "hnsw_gpu_clear_tuning": ([vp], (None,)),
+        "hnsw_gpu_set_counters": ([vp, ctypes.c_int], (None, 1)),
+        "hnsw_gpu_read_counters": ([vp, vp, sz], (None, None, 1)),
+        "hnsw_gpu_server_start": ([vp, vp, vp], (None, None, None)),
+        "hnsw_gpu_server_stats": ([vp, vp, vp], (None, None, None)),
+        "hnsw_builder_insert": ([vp, ctypes.c_uint64, vp, sz], (None, 1, None, 8)),
+        "hnsw_builder_enable_quantization": ([vp], (None,)),
+    }
+    for name, (argtypes, args) in calls.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = ctypes.c_int
+        assert fn(*args) == H.Status.INVALID_ARGUMENT, name
+        assert lib.hnsw_last_error(), name
+    for name in ("hnsw_gpu_index_close", "hnsw_gpu_graph_destroy", "hnsw_gpu_server_stop", "hnsw_gpu_brute_close",
+                 "hnsw_builder_free"):
+        fn = getattr(lib, name)
+        fn.argtypes = [vp]
+        fn.restype = None
+        fn(None)
