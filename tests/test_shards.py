@@ -174,3 +174,23 @@ def test_two_gloo_ranks_sharded_hnsw_equals_merge_of_shard_searches(tmp_path):
     _assert_same(got, _sequential_merge(*stack, k), "sharded hnsw")
     truth = O.brute(0, base, queries, k, keys=keys)
     assert O.recall_at_k(truth[0], truth[2], got[0], got[2], k) >= 0.9
+
+
+@pytest.mark.gpu
+def test_merge_topk_on_the_device_equals_the_host_merge():
+    # The exchange merges on the device that holds the gathered rows (a GPU
+    # under NCCL): same result as on the host, bit for bit.
+    rng = np.random.default_rng(1)
+    S, nq, s, k = 4, 257, 16, 10
+    keys = rng.choice(2**62, size=(S, nq, s), replace=False).astype(np.uint64)
+    keys[1] |= np.uint64(1 << 63)
+    dist = rng.choice(np.array([0.0, -0.0, 0.25, 0.5, 1.0, 2.0], np.float32), size=(S, nq, s)).astype(np.float32)
+    count = rng.integers(0, s + 1, size=(S, nq))
+    status = np.where(rng.random((S, nq)) < 0.02, 3, 0).astype(np.int32)
+    args = (torch.from_numpy(keys.view(np.int64)), torch.from_numpy(dist.view(np.int32)),
+            torch.from_numpy(count.astype(np.int64)), torch.from_numpy(status))
+    host = SH.merge_topk(*args, k)
+    dev = SH.merge_topk(*(a.cuda() for a in args), k)
+    for h, d in zip(host, dev):
+        assert d.is_cuda
+        assert torch.equal(h, d.cpu())
