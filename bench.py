@@ -990,6 +990,10 @@ def run_case(args):
         base, queries = load_data()
         data, _ = index_file(base, 0, lambda: None)
         index = H.HnswIndex.from_bytes(data)
+        if args.case_hash:
+            # A fixed schedule (e.g. the one the autotuner picks for this
+            # workload: 4096-entry hash, one warp per block, plain mode).
+            index.set_schedule(ef_cap=64, hash_cap=args.case_hash, warps_per_block=args.case_wpb)
         for _ in range(3):
             r = timed_call(lambda: index.search_arrays(queries, K, 64, mode=args.case_mode))
     elif args.workload == "case-cold-500kx96":
@@ -1065,6 +1069,8 @@ def main():
                              "case-cold-500kx96", "case-retry-200kx64", "case-brute-200kx768", "build-1Mx128",
                              "case-build-300kx128"])
     ap.add_argument("--case-mode", type=int, default=1)
+    ap.add_argument("--case-hash", type=int, default=0)
+    ap.add_argument("--case-wpb", type=int, default=1)
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
     ap.add_argument("--batch-n", type=int, default=5_000_000)

@@ -121,9 +121,12 @@ def search_sharded(search: Callable[..., Result], queries: np.ndarray, k: int, e
     dist_ = np.zeros((nq, k), np.float32)
     count = np.zeros(nq, np.uint32)
     status = np.zeros(nq, np.int32)
-    if nq and k:
+    if nq:
+        # Called for k = 0 too: the local search validates every query
+        # before it looks at k (src/hnsw/mod.rs:460-477), so a NaN or zero
+        # query still reports its status; a zero-width result is empty.
         kk, dd, cc, ss = search(queries, k, ef, **search_kw)
-        w = min(k, kk.shape[1])
+        w = min(k, kk.shape[1] if kk.ndim == 2 else 0)
         keys[:, :w], dist_[:, :w] = kk[:, :w], dd[:, :w]
         count[:], status[:] = np.minimum(cc, k), ss
     # One int64 tensor per rank: keys | distance bits | count | status.

@@ -140,7 +140,7 @@ def _run_ranks(tmp_path, world, *args):
     return res[0]["keys"], res[0]["dist"], res[0]["count"], res[0]["status"]
 
 
-@pytest.mark.parametrize("metric,k", [(0, 10), (1, 25), (0, 700)])
+@pytest.mark.parametrize("metric,k", [(0, 10), (1, 25), (0, 700), (0, 0)])
 def test_two_gloo_ranks_sharded_brute_force_equals_unsharded(tmp_path, metric, k):
     import hnsw_gpu as H
     import oracle as O
