@@ -20,7 +20,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <queue>
 #include <thread>
 #include <vector>
@@ -519,6 +521,310 @@ void parallel_for(size_t n, int threads, F&& f) {
     for (auto& th : pool) th.join();
 }
 
+
+// ---------------------------------------------------------------------------
+// Construction, restated for making index files on the reference side:
+// HnswIndex::insert / insert_batch (src/hnsw/mod.rs:225-349), sample_level,
+// link, install_own_neighbors, connect, write_shrunk, select_neighbors and
+// extend_candidates (src/hnsw/build.rs:19-222), the fixed-capacity lists of
+// src/hnsw/graph.rs:26-135 (count word, then ids; writers publish the ids
+// before the count), and search_layer over any layer with several entry
+// points (src/hnsw/search.rs:81-142). One thread links the nodes in id order,
+// which is the sequence of `insert` calls; more threads link them
+// concurrently as link_parallel does (mod.rs:336-346), each node behind its
+// own lock, the entry point behind the promotion lock.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kNoEntry = ~0ull;
+constexpr unsigned kMaxLevel = 31;
+
+uint8_t sample_level(uint64_t seed, uint32_t id, double ml) {  // build.rs:19-28
+    const uint64_t h = mix64(seed ^ mix64(uint64_t(id) + 0x9E3779B97F4A7C15ULL));
+    const double u = double((h >> 11) + 1) * (1.0 / double(1ULL << 53));
+    const double level = std::floor(-std::log(u) * ml);
+    return level >= double(kMaxLevel) ? uint8_t(kMaxLevel) : uint8_t(level);
+}
+
+struct Graph {
+    size_t dim = 0;
+    int metric = 0;
+    uint32_t m = 0, m0 = 0, efc = 0;
+    double ml = 0.0;
+    int selection = 1;  // 0 simple, 1 heuristic
+    bool extend = false, keep = false;
+    uint64_t seed = 0;
+    uint32_t n = 0;
+    std::vector<float> vectors;
+    std::vector<uint64_t> keys;
+    std::vector<uint8_t> levels;
+    std::vector<std::atomic<uint32_t>> l0;     // (m0 + 1) words per node
+    std::vector<std::atomic<uint32_t>> upper;  // level * (m + 1) words per node
+    std::vector<size_t> up_off;
+    std::vector<std::mutex> locks;
+    std::atomic<uint64_t> entry{kNoEntry};
+    std::mutex promotion;
+
+    const float* vec(uint32_t id) const { return vectors.data() + size_t(id) * dim; }
+    float dist(const float* a, uint32_t b) const { return metric_distance(metric, a, vec(b), dim); }
+    uint32_t capacity(unsigned layer) const { return layer == 0 ? m0 : m; }
+    std::atomic<uint32_t>* block(uint32_t id, unsigned layer) {
+        if (layer == 0) return l0.data() + size_t(id) * (m0 + 1);
+        return upper.data() + up_off[id] + size_t(layer - 1) * (m + 1);
+    }
+    void read(uint32_t id, unsigned layer, std::vector<uint32_t>& out) {  // Links::read_into
+        out.clear();
+        std::atomic<uint32_t>* b = block(id, layer);
+        const uint32_t c = std::min(b[0].load(std::memory_order_acquire), capacity(layer));
+        for (uint32_t j = 0; j < c; ++j) out.push_back(b[1 + j].load(std::memory_order_relaxed));
+    }
+    void set(uint32_t id, unsigned layer, const std::vector<uint32_t>& ids) {  // Links::set
+        std::atomic<uint32_t>* b = block(id, layer);
+        for (size_t j = 0; j < ids.size(); ++j) b[1 + j].store(ids[j], std::memory_order_relaxed);
+        b[0].store(uint32_t(ids.size()), std::memory_order_release);
+    }
+    bool try_push(uint32_t id, unsigned layer, uint32_t nb) {  // Links::try_push
+        std::atomic<uint32_t>* b = block(id, layer);
+        const uint32_t c = b[0].load(std::memory_order_relaxed);
+        if (c >= capacity(layer)) return false;
+        b[1 + c].store(nb, std::memory_order_relaxed);
+        b[0].store(c + 1, std::memory_order_release);
+        return true;
+    }
+};
+
+struct BuildScratch {
+    std::vector<uint16_t> marks;
+    uint16_t epoch = 0;
+    std::vector<uint32_t> ids;
+    void reset(size_t n) {
+        if (marks.size() < n) marks.resize(n, 0);
+        epoch = uint16_t(epoch + 1);
+        if (epoch == 0) {
+            std::fill(marks.begin(), marks.end(), 0);
+            epoch = 1;
+        }
+    }
+    bool insert(uint32_t id) {
+        if (marks[id] == epoch) return false;
+        marks[id] = epoch;
+        return true;
+    }
+};
+
+// greedy_closest (search.rs:49-68) on the graph under construction.
+Cand build_greedy(Graph& g, BuildScratch& sc, Cand best, unsigned layer, const float* q) {
+    for (;;) {
+        const uint32_t from = best.id;
+        g.read(from, layer, sc.ids);
+        for (uint32_t nb : sc.ids) {
+            const float d = g.dist(q, nb);
+            if (d < best.d) best = Cand{d, nb};
+        }
+        if (best.id == from) return best;
+    }
+}
+
+// search_layer (search.rs:81-142) with the admission `n != self`.
+std::vector<Cand> build_search_layer(Graph& g, BuildScratch& sc, const std::vector<Cand>& eps, size_t ef,
+                                     unsigned layer, const float* q, uint32_t self) {
+    sc.reset(g.n);
+    std::priority_queue<Cand, std::vector<Cand>, CandGreater> cands;
+    std::priority_queue<Cand, std::vector<Cand>, CandLess> results;
+    for (const Cand& ep : eps) {
+        if (!sc.insert(ep.id)) continue;
+        cands.push(ep);
+        if (ep.id != self) {
+            results.push(ep);
+            if (results.size() > ef) results.pop();
+        }
+    }
+    std::vector<uint32_t> list;
+    while (!cands.empty()) {
+        const Cand cur = cands.top();
+        cands.pop();
+        if (results.size() >= ef && !results.empty() && cur.d > results.top().d) break;
+        g.read(cur.id, layer, list);
+        for (uint32_t nb : list) {
+            if (!sc.insert(nb)) continue;
+            const float d = g.dist(q, nb);
+            const bool improves = results.size() < ef || (!results.empty() && d < results.top().d);
+            if (!improves) continue;
+            cands.push(Cand{d, nb});
+            if (nb != self) {
+                results.push(Cand{d, nb});
+                if (results.size() > ef) results.pop();
+            }
+        }
+    }
+    std::vector<Cand> out;
+    out.reserve(results.size());
+    while (!results.empty()) {
+        out.push_back(results.top());
+        results.pop();
+    }
+    std::sort(out.begin(), out.end(), CandLess());
+    return out;
+}
+
+// extend_candidates (build.rs:198-220).
+std::vector<Cand> extend_candidates(Graph& g, uint32_t base_id, const float* base, const std::vector<Cand>& cands,
+                                    unsigned layer) {
+    std::vector<uint32_t> seen;
+    for (const Cand& c : cands) seen.push_back(c.id);
+    seen.push_back(base_id);
+    std::sort(seen.begin(), seen.end());
+    std::vector<Cand> out = cands;
+    std::vector<uint32_t> list;
+    for (const Cand& c : cands) {
+        g.read(c.id, layer, list);
+        for (uint32_t nb : list) {
+            auto it = std::lower_bound(seen.begin(), seen.end(), nb);
+            if (it != seen.end() && *it == nb) continue;
+            seen.insert(it, nb);
+            out.push_back(Cand{g.dist(base, nb), nb});
+        }
+    }
+    std::sort(out.begin(), out.end(), CandLess());
+    return out;
+}
+
+// select_neighbors (build.rs:153-196): simple, or the heuristic.
+std::vector<uint32_t> select_neighbors(Graph& g, uint32_t base_id, const float* base, const std::vector<Cand>& cands,
+                                       size_t m, unsigned layer) {
+    std::vector<uint32_t> out;
+    if (g.selection == 0) {
+        for (size_t i = 0; i < cands.size() && i < m; ++i) out.push_back(cands[i].id);
+        return out;
+    }
+    std::vector<Cand> extended;
+    const std::vector<Cand>* pool = &cands;
+    if (g.extend) {
+        extended = extend_candidates(g, base_id, base, cands, layer);
+        pool = &extended;
+    }
+    std::vector<Cand> selected, discarded;
+    for (const Cand& c : *pool) {
+        if (selected.size() >= m) break;
+        const float* v = g.vec(c.id);
+        bool diverse = true;
+        for (const Cand& s : selected)
+            if (!(metric_distance(g.metric, v, g.vec(s.id), g.dim) >= c.d)) {
+                diverse = false;
+                break;
+            }
+        if (diverse) selected.push_back(c);
+        else if (g.keep) discarded.push_back(c);
+    }
+    const size_t room = m - selected.size();
+    for (size_t i = 0; i < discarded.size() && i < room; ++i) selected.push_back(discarded[i]);
+    for (const Cand& c : selected) out.push_back(c.id);
+    return out;
+}
+
+// write_shrunk (build.rs:136-151); the caller holds the node's lock.
+void write_shrunk(Graph& g, uint32_t node, const std::vector<uint32_t>& ids, unsigned layer) {
+    const uint32_t cap = g.capacity(layer);
+    if (ids.size() <= cap) {
+        g.set(node, layer, ids);
+        return;
+    }
+    const float* base = g.vec(node);
+    std::vector<Cand> cands;
+    for (uint32_t c : ids) cands.push_back(Cand{g.dist(base, c), c});
+    std::sort(cands.begin(), cands.end(), CandLess());
+    g.set(node, layer, select_neighbors(g, node, base, cands, cap, layer));
+}
+
+// install_own_neighbors (build.rs:100-117).
+void install_own(Graph& g, uint32_t id, const std::vector<uint32_t>& selected, unsigned layer) {
+    std::lock_guard<std::mutex> lock(g.locks[id]);
+    std::vector<uint32_t> merged;
+    g.read(id, layer, merged);
+    if (merged.empty()) {
+        g.set(id, layer, selected);
+        return;
+    }
+    for (uint32_t nb : selected)
+        if (std::find(merged.begin(), merged.end(), nb) == merged.end()) merged.push_back(nb);
+    write_shrunk(g, id, merged, layer);
+}
+
+// connect (build.rs:121-132).
+void connect(Graph& g, uint32_t node, uint32_t fresh, unsigned layer) {
+    std::lock_guard<std::mutex> lock(g.locks[node]);
+    std::vector<uint32_t> cur;
+    g.read(node, layer, cur);
+    if (std::find(cur.begin(), cur.end(), fresh) != cur.end() || g.try_push(node, layer, fresh)) return;
+    cur.push_back(fresh);
+    write_shrunk(g, node, cur, layer);
+}
+
+// link (build.rs:40-96).
+void link(Graph& g, BuildScratch& sc, uint32_t id) {
+    const unsigned level = g.levels[id];
+    const float* q = g.vec(id);
+    uint64_t entry = g.entry.load(std::memory_order_acquire);
+    std::unique_lock<std::mutex> promotion;
+    if (entry == kNoEntry || level > unsigned(entry >> 32)) {
+        std::unique_lock<std::mutex> guard(g.promotion);
+        entry = g.entry.load(std::memory_order_acquire);
+        if (entry == kNoEntry) {
+            g.entry.store((uint64_t(level) << 32) | id, std::memory_order_release);
+            return;
+        }
+        if (level > unsigned(entry >> 32)) promotion = std::move(guard);
+    }
+    const uint32_t entry_id = uint32_t(entry);
+    const unsigned top = unsigned(entry >> 32);
+    Cand ep{g.dist(q, entry_id), entry_id};
+    for (unsigned layer = top; layer > level; --layer) ep = build_greedy(g, sc, ep, layer, q);
+    const size_t ef = std::max<size_t>(g.efc, g.m);
+    std::vector<Cand> eps{ep};
+    for (int layer = int(std::min(level, top)); layer >= 0; --layer) {
+        std::vector<Cand> found = build_search_layer(g, sc, eps, ef, unsigned(layer), q, id);
+        std::vector<uint32_t> selected = select_neighbors(g, id, q, found, g.m, unsigned(layer));
+        install_own(g, id, selected, unsigned(layer));
+        for (uint32_t nb : selected) connect(g, nb, id, unsigned(layer));
+        if (!found.empty()) eps = std::move(found);
+    }
+    if (promotion.owns_lock()) g.entry.store((uint64_t(level) << 32) | id, std::memory_order_release);
+}
+
+// Format v1 writer (src/hnsw/io.rs:102-178), CRC-32 trailer.
+std::vector<uint8_t> write_v1(Graph& g, const std::vector<uint8_t>& deleted) {
+    std::vector<uint8_t> out;
+    auto put = [&](const void* p, size_t k) {
+        const uint8_t* b = static_cast<const uint8_t*>(p);
+        out.insert(out.end(), b, b + k);
+    };
+    auto put32 = [&](uint32_t v) { put(&v, 4); };
+    put("HNSWIDX\0", 8);
+    put32(1);
+    const uint8_t tags[4] = {uint8_t(g.metric), uint8_t(g.selection),
+                             uint8_t(g.selection ? (uint8_t(g.extend) | (uint8_t(g.keep) << 1)) : 0), 0};
+    put(tags, 4);
+    put32(uint32_t(g.dim));
+    put32(g.m);
+    put32(g.m0);
+    put32(g.efc);
+    put(&g.ml, 8);
+    put(&g.seed, 8);
+    put32(g.n);
+    const uint64_t e = g.entry.load();
+    put32(e == kNoEntry ? 0xFFFFFFFFu : uint32_t(e));
+    put(g.keys.data(), g.keys.size() * 8);
+    put(g.levels.data(), g.levels.size());
+    put(deleted.data(), deleted.size());
+    put(g.vectors.data(), g.vectors.size() * 4);
+    std::vector<uint32_t> list;
+    for (uint32_t id = 0; id < g.n; ++id)
+        for (unsigned layer = 0; layer <= g.levels[id]; ++layer) {
+            g.read(id, layer, list);
+            put32(uint32_t(list.size()));
+            put(list.data(), list.size() * 4);
+        }
+    put32(crc32(out.data(), out.size()));
+    return out;
+}
 }  // namespace
 
 extern "C" {
@@ -570,6 +876,100 @@ void orc_clustered(size_t nb, size_t nq, size_t dim, size_t clusters, double spr
     };
     sample(nb, base);
     sample(nq, queries);
+}
+
+
+// ---- construction ----
+// HnswIndex::insert_batch into an empty index (src/hnsw/mod.rs:318-349) of
+// n rows with keys, then to_bytes. threads == 1 links the nodes in id order
+// (the same graph as n calls of insert); threads != 1 links them
+// concurrently (0: every core), whose graph depends on scheduling, as the
+// reference's does (mod.rs:306-312). deleted_keys (count nd) are then
+// removed (tombstoned). Returns the file size and writes it to *out
+// (orc_free_bytes releases it), or 0 when a row fails validation.
+size_t orc_build(size_t dim, int metric, uint32_t m, uint32_t m0, uint32_t efc, double ml, int selection,
+                 int extend, int keep, uint64_t seed, const uint64_t* keys, const float* vectors, size_t n,
+                 const uint64_t* deleted_keys, size_t nd, int threads, uint8_t** out) {
+    *out = nullptr;
+    Graph g;
+    g.dim = dim;
+    g.metric = metric;
+    g.m = m;
+    g.m0 = m0;
+    g.efc = efc;
+    g.ml = ml;
+    g.selection = selection;
+    g.extend = extend != 0;
+    g.keep = keep != 0;
+    g.seed = seed;
+    g.n = uint32_t(n);
+    g.vectors.resize(n * dim);
+    for (size_t i = 0; i < n; ++i)  // prepare_batch (src/vector.rs:55-88)
+        if (prepare_query(metric, vectors + i * dim, dim, g.vectors.data() + i * dim) != OK) return 0;
+    g.keys.assign(keys, keys + n);
+    g.levels.resize(n);
+    g.up_off.resize(n);
+    size_t up = 0;
+    for (uint32_t id = 0; id < n; ++id) {
+        g.levels[id] = sample_level(seed, id, ml);
+        g.up_off[id] = up;
+        up += size_t(g.levels[id]) * (m + 1);
+    }
+    g.l0 = std::vector<std::atomic<uint32_t>>(n * (m0 + 1));
+    g.upper = std::vector<std::atomic<uint32_t>>(up);
+    g.locks = std::vector<std::mutex>(n);
+    if (threads == 1) {
+        BuildScratch sc;
+        for (uint32_t id = 0; id < n; ++id) link(g, sc, id);
+    } else {
+        BuildScratch first;
+        if (n) link(g, first, 0);  // link_parallel: the first node alone sets the entry point
+        const int nt = threads > 0 ? threads : int(std::max(1u, std::thread::hardware_concurrency()));
+        std::atomic<uint32_t> next{1};
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                BuildScratch sc;
+                for (;;) {
+                    const uint32_t id = next.fetch_add(1);
+                    if (id >= n) break;
+                    link(g, sc, id);
+                }
+            });
+        for (auto& th : pool) th.join();
+    }
+    std::vector<uint8_t> deleted(n, 0);
+    for (size_t j = 0; j < nd; ++j)
+        for (uint32_t id = 0; id < n; ++id)
+            if (g.keys[id] == deleted_keys[j] && !deleted[id]) {
+                deleted[id] = 1;
+                break;
+            }
+    std::vector<uint8_t> bytes = write_v1(g, deleted);
+    *out = static_cast<uint8_t*>(std::malloc(bytes.size()));
+    std::memcpy(*out, bytes.data(), bytes.size());
+    return bytes.size();
+}
+void orc_free_bytes(uint8_t* p) { std::free(p); }
+
+// Mixture with the base (and the centers) from base_seed and the queries
+// from query_seed: the draw order of Dataset::clustered (src/synthetic.rs:
+// 102-124: the centers, then per point next_below and dim Gaussians), with
+// the spread as a parameter and the query points on their own stream.
+void orc_mixture_split(size_t nb, size_t nq, size_t dim, size_t clusters, double spread, uint64_t base_seed,
+                       uint64_t query_seed, float* base, float* queries) {
+    SplitMix64 r{base_seed};
+    std::vector<double> centers(clusters * dim);
+    for (auto& c : centers) c = r.gaussian();
+    auto sample = [&](SplitMix64& g, size_t count, float* out) {
+        for (size_t p = 0; p < count; ++p) {
+            const size_t c = size_t(g.below(clusters));
+            for (size_t j = 0; j < dim; ++j) out[p * dim + j] = float(centers[c * dim + j] + spread * g.gaussian());
+        }
+    };
+    sample(r, nb, base);
+    SplitMix64 q{query_seed};
+    sample(q, nq, queries);
 }
 
 // ---- index ----

@@ -57,6 +57,10 @@ for name, res, args in [
                                   _vp, _vp, _vp, C.c_int]),
     ("orc_brute_f64", None, [C.c_int, _vp, _sz, _sz, _vp, _sz, _sz, _vp, _vp, C.c_int]),
     ("orc_recall_at_k", C.c_double, [_vp, _vp, _sz, _vp, _vp, _sz, _sz, _sz]),
+    ("orc_build", _sz, [_sz, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_int, C.c_int, C.c_int,
+                        C.c_uint64, _vp, _vp, _sz, _vp, _sz, C.c_int, C.POINTER(C.POINTER(C.c_uint8))]),
+    ("orc_free_bytes", None, [C.POINTER(C.c_uint8)]),
+    ("orc_mixture_split", None, [_sz, _sz, _sz, _sz, C.c_double, C.c_uint64, C.c_uint64, _vp, _vp]),
 ]:
     f = getattr(_lib, name)
     f.restype = res
@@ -153,6 +157,39 @@ def clustered(nb, nq, dim, clusters, spread, seed):
     q = np.zeros((nq, dim), np.float32)
     _lib.orc_clustered(nb, nq, dim, clusters, spread, seed, _p(base), _p(q))
     return base, q
+
+
+def mixture_split(nb, nq, dim, clusters, spread, base_seed, query_seed):
+    """Clustered data with the base (and centers) from base_seed and the
+    queries on their own stream from query_seed (src/synthetic.rs:102-124 order)."""
+    base = np.zeros((nb, dim), np.float32)
+    q = np.zeros((nq, dim), np.float32)
+    _lib.orc_mixture_split(nb, nq, dim, clusters, spread, base_seed, query_seed, _p(base), _p(q))
+    return base, q
+
+
+def build(base, keys=None, metric=0, m=16, m0=None, ef_construction=200, level_multiplier=None,
+          selection=1, extend_candidates=False, keep_pruned=False, seed=0, threads=0, deleted_keys=()):
+    """HnswIndex::insert_batch into an empty index, then to_bytes (format v1).
+    threads=1 links in id order (the graph of repeated `insert`); otherwise
+    the nodes are linked concurrently (0: all cores)."""
+    import math
+
+    base = _f32(base)
+    n, dim = base.shape
+    keys = np.arange(n, dtype=np.uint64) if keys is None else np.ascontiguousarray(keys, np.uint64)
+    dk = np.ascontiguousarray(np.asarray(deleted_keys, np.uint64))
+    m0 = 2 * m if m0 is None else m0
+    ml = 1.0 / math.log(m) if level_multiplier is None else level_multiplier
+    out = C.POINTER(C.c_uint8)()
+    size = _lib.orc_build(dim, int(metric), m, m0, ef_construction, ml, int(selection), int(extend_candidates),
+                          int(keep_pruned), seed, _p(keys), _p(base), n, _p(dk) if dk.size else None, dk.size,
+                          int(threads), C.byref(out))
+    if size == 0:
+        raise ValueError("a row failed validation")
+    data = C.string_at(out, size)
+    _lib.orc_free_bytes(out)
+    return data
 
 
 class Index:

@@ -226,10 +226,9 @@ def test_recall_at_k_known_answers():
 
 
 def _seq_build(base, m):
-    b = H.IndexBuilder(base.shape[1], H.Metric.L2, H.HnswParams(m=m))
-    for i in range(base.shape[0]):
-        b.insert(i, base[i])
-    return b.to_bytes()
+    # The oracle's own restatement of construction, one node at a time in id
+    # order (the graph of repeated HnswIndex::insert).
+    return O.build(base, metric=0, m=m, threads=1)
 
 
 @pytest.fixture(scope="module")
