@@ -44,6 +44,8 @@ K = 10
 EF_SWEEP = (16, 32, 64, 128, 256)
 RECALL_TARGET = 0.95
 SELECT_QUERIES = 1000  # ef is chosen on the first 1000 queries (both arms)
+PARITY_QUERIES = 2000  # queries compared with the oracle at full size
+FP64_QUERIES = 200     # queries checked against the FP64 oracle
 CACHE = os.environ.get("HNSW_BENCH_CACHE", "/tmp/hnsw_b200_bench")
 METRIC = "QPS at recall@10>=0.95 (1M x 128 clustered, k=10)"
 
@@ -68,18 +70,25 @@ def load_data():
     return H.mixture_split(N_BASE, N_QUERY, DIM, CLUSTERS, SIGMA, BASE_SEED, QUERY_SEED)
 
 
-def index_file(base, rank, barrier):
-    """Builds the index once per box (host builder, all cores) and caches it."""
+def product_build(base):
+    """insert_batch with the library's host builder on all cores, then to_bytes."""
     import hnsw_gpu as H
 
+    b = H.IndexBuilder(DIM, H.Metric.L2, H.HnswParams(m=M, ef_construction=EF_CONSTRUCTION, seed=LEVEL_SEED))
+    b.insert_batch(np.arange(N_BASE, dtype=np.uint64), base)
+    return b.to_bytes()
+
+
+def index_file(base, rank, barrier, build=product_build):
+    """Builds the index once per box and caches it; both arms then read the
+    same file (whichever arm runs first builds it: the reference arm with the
+    oracle's restatement of insert_batch, the GPU arm with the library's)."""
     os.makedirs(CACHE, exist_ok=True)
     path = os.path.join(CACHE, f"index-{workload_tag()}.hnsw")
     build_s = None
     if rank == 0 and not os.path.exists(path):
         t = time.time()
-        b = H.IndexBuilder(DIM, H.Metric.L2, H.HnswParams(m=M, ef_construction=EF_CONSTRUCTION, seed=LEVEL_SEED))
-        b.insert_batch(np.arange(N_BASE, dtype=np.uint64), base)
-        data = b.to_bytes()
+        data = build(base)
         build_s = time.time() - t
         tmp = path + f".tmp{os.getpid()}"
         with open(tmp, "wb") as f:
@@ -200,6 +209,94 @@ def choose_ef(recalls):
     return EF_SWEEP[-1]
 
 
+def shared_config(ef, recall_first_1000):
+    """The workload both arms run, identical in the GPU and reference lines.
+    The recall on the ef-selection queries is identical when the results are."""
+    return {"workload": "plain-1Mx128-clustered", "n_base": N_BASE, "n_queries": N_QUERY, "dim": DIM,
+            "clusters": CLUSTERS, "sigma": SIGMA, "seeds": [BASE_SEED, QUERY_SEED], "M": M, "M0": 2 * M,
+            "ef_construction": EF_CONSTRUCTION, "level_seed": LEVEL_SEED, "k": K, "ef": ef,
+            "ef_rule": f"smallest ef in {list(EF_SWEEP)} with recall@10 >= {RECALL_TARGET} on the first "
+                       f"{SELECT_QUERIES} queries",
+            "recall_at_10_first_1000": recall_first_1000,
+            "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush"}
+
+
+def compare_results(a, b, n):
+    """Queries among the first n whose keys, distance bits, counts and statuses
+    agree in the result sets a and b, and the largest relative distance
+    difference over positions where both hold the same key."""
+    same, rel = 0, 0.0
+    for i in range(n):
+        c = int(a[2][i])
+        ok = c == int(b[2][i]) and int(a[3][i]) == int(b[3][i])
+        ok = ok and np.array_equal(a[0][i, :c], b[0][i, :c])
+        ok = ok and np.array_equal(a[1][i, :c].view(np.uint32), b[1][i, :c].view(np.uint32))
+        same += int(ok)
+        m = min(c, int(b[2][i]))
+        eq = a[0][i, :m] == b[0][i, :m]
+        if eq.any():
+            da = a[1][i, :m][eq].astype(np.float64)
+            db = b[1][i, :m][eq].astype(np.float64)
+            rel = max(rel, float(np.max(np.abs(da - db) / np.maximum(np.abs(db), 1e-30))))
+    return same, rel
+
+
+def fp64_error(O, base, queries, res, k, cores):
+    """Distances and top-k of a result set against an FP64 oracle (exact
+    squared L2 in double precision) on a query sample: the largest absolute
+    and relative distance error over the returned keys, and the mean number
+    of returned keys per query outside the FP64 top-k."""
+    k64, _ = O.brute_f64(0, base, queries, k, threads=cores)
+    max_abs = max_rel = 0.0
+    outside = 0
+    for i in range(len(queries)):
+        c = int(res[2][i])
+        keys = res[0][i, :c].astype(np.int64)
+        d64 = ((base[keys].astype(np.float64) - queries[i].astype(np.float64)) ** 2).sum(1)
+        err = np.abs(res[1][i, :c].astype(np.float64) - d64)
+        if c:
+            max_abs = max(max_abs, float(err.max()))
+            max_rel = max(max_rel, float((err / np.maximum(d64, 1e-30)).max()))
+        outside += len(set(keys.tolist()) - set(k64[i].astype(np.int64).tolist()))
+    return {"queries": len(queries), "max_abs_distance_error": max_abs, "max_rel_distance_error": max_rel,
+            "topk_disagreement_per_query": outside / max(len(queries), 1)}
+
+
+def config1_block(H, O, cores):
+    """The small plain workload (10,000 x 128 N(0,1) from seed 42, 1,000
+    queries from seed 43, L2, M=16, efC=200, level seed 7, k=10, ef=64): the
+    oracle's search_batch on all host cores, one warm-up pass measuring
+    recall@10 then the median of 3 timed passes (the hnsw-bench method), and
+    the GPU's search_batch on the same file, checked bit for bit."""
+    base, _ = H.gaussian(10_000, 0, 128, 42)
+    _, queries = H.gaussian(0, 1000, 128, 43)
+    b = H.IndexBuilder(128, H.Metric.L2, H.HnswParams(m=16, ef_construction=200, seed=7))
+    b.insert_batch(np.arange(10_000, dtype=np.uint64), base)
+    data = b.to_bytes()
+    oi = O.Index(data)
+    tk, _, tc, _ = O.brute(0, base, queries, 10, threads=cores)
+    ref = oi.search(queries, 10, 64, threads=cores)
+    recall = O.recall_at_k(tk, tc, ref[0], ref[2], 10)
+    times = []
+    for _ in range(3):
+        t = time.perf_counter()
+        oi.search(queries, 10, 64, threads=cores)
+        times.append(time.perf_counter() - t)
+    gi = H.HnswIndex.from_bytes(data)
+    got = gi.search_arrays(queries, 10, 64)
+    gt = []
+    for _ in range(3):
+        t = time.perf_counter()
+        gi.search_arrays(queries, 10, 64)
+        gt.append(time.perf_counter() - t)
+    gi.close()
+    same, _ = compare_results(got, ref, len(queries))
+    return {"workload": "plain-10kx128-gaussian", "ef": 64, "k": 10, "recall_at_10": recall,
+            "cpu_qps": len(queries) / statistics.median(times), "cpu_cores": cores,
+            "cpu_method": "oracle search_batch, warm-up pass then median of 3", "load_average": os.getloadavg(),
+            "gpu_e2e_qps": len(queries) / statistics.median(gt), "identical_to_oracle": f"{same}/{len(queries)}"}
+
+
 # ---------------------------------------------------------------------------
 # Reference arm: the oracle's search_batch on the host cores.
 # ---------------------------------------------------------------------------
@@ -210,8 +307,12 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    base, queries = load_data()
-    data, _ = index_file(base, 0, lambda: None)
+    # Data and index file from the oracle alone (the reference's generator
+    # and insert_batch, restated); the library is not loaded by this arm.
+    base, queries = O.mixture_split(N_BASE, N_QUERY, DIM, CLUSTERS, SIGMA, BASE_SEED, QUERY_SEED)
+    data, build_s = index_file(base, 0, lambda: None,
+                               build=lambda b: O.build(b, metric=0, m=M, ef_construction=EF_CONSTRUCTION,
+                                                       seed=LEVEL_SEED, threads=0))
     ix = O.Index(data)
     cores = os.cpu_count() or 1
     # ef choice on the first 1000 queries, as in the GPU arm.
@@ -235,8 +336,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "plain-1Mx128-clustered", "ef": ef, "k": K, "recall_at_10": recalls[ef],
-                   "sweep_recall_1000q": recalls, "sample_queries": len(sample)},
+        "config": shared_config(ef, recalls[ef]),
+        "details": {"sweep_recall_first_1000": recalls, "sample_queries": len(sample), "index_build_s": build_s,
+                    "index_builder": "oracle insert_batch (all cores)" if build_s is not None else "cached file"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
                          "sample": f"{len(sample)} queries per step at ef={ef}, {args.steps} steps"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -290,7 +392,6 @@ def run_gpu(args):
         if rank == 0:
             np.savez(truth_path + ".tmp.npz", keys=tk, counts=tc)
             os.replace(truth_path + ".tmp.npz", truth_path)
-    del base
 
     # ef sweep: recall on all queries and on the selection subset.
     recalls, recalls_sel = {}, {}
@@ -347,11 +448,17 @@ def run_gpu(args):
     plain_qps = N_QUERY / (statistics.median(plain_ms) / 1e3)
     pers_ms = timed(ef, 1, max(3, args.steps // 2), 1)
     pers_qps = N_QUERY / (statistics.median(pers_ms) / 1e3)
-    sweep_qps, tuned = {}, {}
+    sweep_qps, tuned, mode_best = {}, {}, {}
     for e in EF_SWEEP:
-        tuned[e], _ = index.autotune(queries[:5000], K, e, reps=3)
+        tuned[e], trials = index.autotune(queries[:5000], K, e, reps=3)
         ms = timed(e, 2, 3, 1)
         sweep_qps[e] = N_QUERY / (statistics.median(ms) / 1e3)
+        if e == ef:
+            # Each mode's fastest schedule on the tuning sample (same batch, same ef).
+            for t_ in trials:
+                name = "persistent" if t_["mode"] == 1 else "plain"
+                if name not in mode_best or t_["ms"] < mode_best[name]["ms"]:
+                    mode_best[name] = t_
 
     clock_path = f"/tmp/hnsw_bench_clocks_{rank}.csv"
     sampler = start_clock_sampler(local, clock_path)
@@ -363,6 +470,9 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * N_QUERY * args.steps / (total_ms / 1e3)
+    # The last timed step's outputs, as the device holds them.
+    timed_res = (o_keys.cpu().numpy().view(np.uint64), o_dist.cpu().numpy(), o_cnt.cpu().numpy().view(np.uint32),
+                 o_st.cpu().numpy())
 
     # End to end through the host-buffer API (pinned host memory).
     q_pin = torch.from_numpy(queries).pin_memory()
@@ -426,44 +536,62 @@ def run_gpu(args):
     achieved = alg_bytes / mean_s / 1e9
     traffic = profiled_traffic()
 
-    cpu = None
+    cpu, parity, fp64, config1 = None, None, None, None
     if rank == 0 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
         oi = O.Index(data)
         cores = os.cpu_count() or 1
-        sample = queries[:2000]
+        sample = queries[:PARITY_QUERIES]
         oi.search(sample[:200], K, ef, threads=cores)
         times = []
         for _ in range(2):
             t = time.perf_counter()
-            oi.search(sample, K, ef, threads=cores)
+            ref = oi.search(sample, K, ef, threads=cores)
             times.append(time.perf_counter() - t)
         cpu = {"value": len(sample) / statistics.median(times), "unit": "queries/s", "cores": cores,
                "kind": "port", "sample": f"{len(sample)} of the {N_QUERY} queries at ef={ef}, median of 2 passes"}
+        # Full-size parity: the oracle's search_batch (src/hnsw/mod.rs:520-536)
+        # on the same file and queries against the GPU's timed and e2e outputs.
+        e2e_res = (kk, dd, cc, ss)
+        same_timed, _ = compare_results(timed_res, e2e_res, N_QUERY)
+        same_ref, rel_err = compare_results(e2e_res, ref, len(sample))
+        recall_ref_sel = O.recall_at_k(tk[:SELECT_QUERIES], tc[:SELECT_QUERIES], ref[0][:SELECT_QUERIES],
+                                       ref[2][:SELECT_QUERIES], K)
+        parity = {"queries": len(sample), "identical": same_ref, "max_rel_dist_err": rel_err,
+                  "timed_outputs_equal_e2e": same_timed == N_QUERY,
+                  "recall_at_10_first_1000_gpu": recalls_sel[ef], "recall_at_10_first_1000_oracle": recall_ref_sel,
+                  "recall_diff": abs(recalls_sel[ef] - recall_ref_sel)}
+        fp64 = fp64_error(O, base, queries[:FP64_QUERIES], e2e_res, K, cores)
+        config1 = config1_block(H, O, cores)
 
     if world > 1:
         dist.barrier()
     if rank == 0:
         srt = sorted(step_ms)
+        pob = None
+        if "plain" in mode_best and "persistent" in mode_best:
+            pob = mode_best["plain"]["ms"] / mode_best["persistent"]["ms"]
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {
-                "workload": "plain-1Mx128-clustered", "n_base": N_BASE, "n_queries_per_gpu": N_QUERY, "dim": DIM,
-                "clusters": CLUSTERS, "sigma": SIGMA, "M": M, "M0": 2 * M, "ef_construction": EF_CONSTRUCTION,
-                "k": K, "ef": ef, "recall_at_10": recalls[ef], "sweep_recall": recalls, "sweep_qps": sweep_qps,
+            "config": shared_config(ef, recalls_sel[ef]),
+            "details": {
+                "n_queries_per_gpu": N_QUERY, "recall_at_10_all": recalls[ef], "sweep_recall": recalls,
+                "sweep_recall_first_1000": recalls_sel, "sweep_qps": sweep_qps,
                 "schedule": tuned[ef], "plain_heuristic_qps": plain_qps, "persistent_heuristic_qps": pers_qps,
                 "tuned_over_plain": value / world / plain_qps,
+                "best_schedule_per_mode": mode_best, "persistent_over_plain": pob,
                 "per_call_qps": per_call_qps, "tuned_over_per_call": value / per_call_qps,
                 "served": served,
                 "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
-                "l2": "inputs larger than L2 (vectors 512 MB + adjacency 128 MB), no flush",
                 "parallelism": f"replicas x{world}", "index_build_s": build_s,
-                "layer0_distances_per_query": visit_stats,
+                "layer0_distances_per_query": visit_stats, "config1": config1,
             },
+            "parity": parity,
+            "fp64_sample": fp64,
             "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 3 * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -472,17 +600,33 @@ def run_gpu(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
-        print(json.dumps(line))
     index.close()
+    del base
+    if rank == 0 and world == 1 and not args.no_extra:
+        # The brute-force and batching workloads, compact, in the same run.
+        extra = {}
+        for name, fn in (("brute-1Mx768-cosine", run_brute), ("batch-5Mx96-ip", run_batch)):
+            t = time.time()
+            try:
+                extra[name] = fn(args, emit=False)
+            except Exception as e:  # reported, and the headline stands
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
+            extra[name]["wall_s"] = time.time() - t
+        line["other_configs"] = extra
+    if rank == 0:
+        print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+    if parity is not None and parity["identical"] != parity["queries"]:
+        log(f"PARITY FAILURE: {parity}")
+        return 1
     return 0
 
 
 # ---------------------------------------------------------------------------
 # Brute-force precision workload (not the default line): 1M x 768 cosine.
 # ---------------------------------------------------------------------------
-def run_brute(args):
+def run_brute(args, emit=True):
     import hnsw_gpu as H
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -502,8 +646,9 @@ def run_brute(args):
     out = {}
     results = {}
     clocks = None
+    nsteps = args.steps if emit else args.extra_steps
     for prec in (H.Precision.BF16X3, H.Precision.BF16, H.Precision.FP32):
-        steps = args.steps if prec != H.Precision.FP32 else 1
+        steps = nsteps if prec != H.Precision.FP32 else 1
         bf.search_arrays(queries, k, prec)  # warm-up (also builds the BF16 rows)
         times, stats = [], []
 
@@ -559,7 +704,8 @@ def run_brute(args):
     qs = queries[:sample].astype(np.float64)
     qn = (qs / np.sqrt((qs * qs).sum(1, keepdims=True))).astype(np.float32)
     t = time.time()
-    k64, d64 = O.brute_f64(2, rows, qn, k)
+    cores = os.cpu_count() or 1
+    k64, d64 = O.brute_f64(2, rows, qn, k, threads=cores)
     log(f"fp64 oracle on {sample} queries in {time.time() - t:.1f} s")
     fp64 = {}
     for name in ("BF16X3", "BF16", "FP32"):
@@ -585,7 +731,7 @@ def run_brute(args):
     cpu_qps = cs / (time.perf_counter() - t)
     line = {
         "metric": "brute-force QPS (1M x 768 cosine, k=100, BF16x3 + exact FP32 re-rank)",
-        "value": out["BF16X3"]["qps_device"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "value": out["BF16X3"]["qps_device"], "unit": "queries/s", "n_gpus": 1, "steps": nsteps,
         "warmup": 1, "higher_is_better": True, "dtype": "bf16x3", "data": "synthetic",
         "config": {"workload": "brute-1Mx768-cosine", "n_base": nb, "n_queries": nq, "dim": dim, "k": k,
                    "clusters": 4096, "sigma": 0.5, "seeds": [3, 4], "precisions": out,
@@ -598,6 +744,9 @@ def run_brute(args):
                          "sample": f"{cs} queries, oracle FP32 brute force"},
         "clocks": clocks,
     }
+    bf.close()
+    if not emit:
+        return line
     print(json.dumps(line))
     return 0
 
@@ -646,7 +795,7 @@ def timed_search(index, queries, k, ef, steps, **kw):
 # Batching workload: 5M x 96 inner product, int8 traversal +
 # exact re-rank, 5% tombstones, per-query filters, uneven k and ef.
 # ---------------------------------------------------------------------------
-def run_batch(args):
+def run_batch(args, emit=True):
     import hnsw_gpu as H
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -660,14 +809,16 @@ def run_batch(args):
     dead = np.sort(rng.choice(nb, nb // 20, replace=False)).astype(np.uint64)
 
     def build():
+        # insert_batch with the link step on the device (deterministic waves).
         b = H.IndexBuilder(dim, H.Metric.InnerProduct, H.HnswParams(m=24, ef_construction=200, seed=0))
-        b.insert_batch(np.arange(nb, dtype=np.uint64), base)
+        b.insert_batch_gpu(np.arange(nb, dtype=np.uint64), base, device=0)
         for key in dead.tolist():
             b.remove(int(key))
         b.enable_quantization()
         return b.to_bytes()
 
-    data, build_s = cached_index(f"batch-{nb}-{dim}-5-6-m24-dead7-q", build)
+    data, build_s = cached_index(f"batch-{nb}-{dim}-5-6-m24-dead7-q-gpu", build)
+    steps = args.steps if emit else args.extra_steps
     index = H.HnswIndex.from_bytes(data)
     rq = np.random.default_rng(8)
     ks = rq.choice([1, 10, 100], nq).astype(np.uint32)
@@ -678,8 +829,8 @@ def run_batch(args):
     common = dict(quantized=True, ks=ks, efs=efs, filter_bits=bank, filter_nbits=nb, filter_stride=words,
                   filter_ids=fids)
     out = {}
-    out["persistent_heuristic_qps"], res = timed_search(index, queries, 100, 16, args.steps, mode=1, **common)
-    out["plain_heuristic_qps"], _ = timed_search(index, queries, 100, 16, args.steps, mode=0, **common)
+    out["persistent_heuristic_qps"], res = timed_search(index, queries, 100, 16, steps, mode=1, **common)
+    out["plain_heuristic_qps"], _ = timed_search(index, queries, 100, 16, steps, mode=0, **common)
     # Autotune on a sample of the same request mix, then time the tuned schedule.
     ns = min(nq, 8000)
     t = time.time()
@@ -688,12 +839,12 @@ def run_batch(args):
     out["autotune_s"] = time.time() - t
     out["autotune_best"] = best
     out["autotune_trials"] = len(trials)
-    (qps, tuned_res), clocks = sampled(lambda: timed_search(index, queries, 100, 16, args.steps, mode=2, **common),
+    (qps, tuned_res), clocks = sampled(lambda: timed_search(index, queries, 100, 16, steps, mode=2, **common),
                                        tag="batch")
     out["autotuned_qps"] = qps
     out["tuned_equals_heuristic"] = bool(np.array_equal(tuned_res[0], res[0]) and np.array_equal(tuned_res[2], res[2]))
     index.set_schedule(ef_cap=512, hash_cap=16384, warps_per_block=1, cold=1)
-    out["fixed_schedule_qps"], fixed_res = timed_search(index, queries, 100, 16, args.steps, mode=1, **common)
+    out["fixed_schedule_qps"], fixed_res = timed_search(index, queries, 100, 16, steps, mode=1, **common)
     index.set_schedule()
     out["fixed_equals_heuristic"] = bool(np.array_equal(fixed_res[0], res[0]))
     # One query per call (the reference's search_with called per query).
@@ -705,7 +856,7 @@ def run_batch(args):
     out["per_call_qps"] = npc / (time.perf_counter() - t)
     # Selectivity planner: filters admitting at most 2% of the live nodes
     # take the exact scan of their admitted nodes instead of the graph walk.
-    out["planner_qps"], plan_res = timed_search(index, queries, 100, 16, args.steps, mode=2, exact_below=0.02,
+    out["planner_qps"], plan_res = timed_search(index, queries, 100, 16, steps, mode=2, exact_below=0.02,
                                                 **common)
     # Recall@10 on a sample against exact filtered search (float64 scores).
     samp = 100
@@ -742,7 +893,7 @@ def run_batch(args):
     out["identical_to_oracle"] = f"{same}/{cs}"
     line = {
         "metric": "QPS, batched persistent search (5M x 96 IP, int8 + re-rank, filters, tombstones, uneven k/ef)",
-        "value": out["autotuned_qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "value": out["autotuned_qps"], "unit": "queries/s", "n_gpus": 1, "steps": steps,
         "higher_is_better": True, "dtype": "int8+f32", "data": "synthetic",
         "config": {"workload": "batch-5Mx96-ip", "n_base": nb, "n_queries": nq, "tombstoned": int(dead.size),
                    "filters": nbank, "index_build_s": build_s, **out},
@@ -750,6 +901,9 @@ def run_batch(args):
                          "sample": f"{cs} queries, oracle search_with(quantized, filter)"},
         "clocks": clocks,
     }
+    index.close()
+    if not emit:
+        return line
     print(json.dumps(line))
     return 0
 
@@ -1079,6 +1233,9 @@ def main():
     ap.add_argument("--serve-batch", type=int, default=1024)
     ap.add_argument("--serve-linger", type=int, default=100)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the brute-force and batching blocks of the default run")
+    ap.add_argument("--extra-steps", type=int, default=2)
     ap.add_argument("--build-n", type=int, default=1_000_000)
     args = ap.parse_args()
     if args.workload == "build-1Mx128":

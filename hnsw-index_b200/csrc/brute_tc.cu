@@ -46,7 +46,7 @@ struct Ring {
 };
 constexpr uint32_t kTmemCols = 512;                   // two 256-column accumulators
 constexpr int kThreads = 192;
-constexpr long long kWaitBudget = 4000000000ll;       // clock cycles (~2 s)
+constexpr long long kWaitBudget = 4000000000ll;       // drain waits, clock cycles (~2 s)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -75,13 +75,13 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
 }
 // Waits for the phase with the given parity; false (and the error word set)
 // if the clock budget runs out or another role already failed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* err, long long budget) {
     const long long t0 = clock64();
     for (uint32_t i = 0;; ++i) {
         if (mbar_try(bar, parity)) return true;
         if ((i & 255) == 255) {
             if (*reinterpret_cast<volatile uint32_t*>(err)) return false;
-            if (clock64() - t0 > kWaitBudget) {
+            if (clock64() - t0 > budget) {
                 atomicExch(err, 1u);
                 return false;
             }
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
                 for (uint32_t k = 0; k < a.k_chunks; ++k) {
                     const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
-                    if (!mbar_wait(&empty[s], ph ^ 1u, a.err)) {
+                    if (!mbar_wait(&empty[s], ph ^ 1u, a.err, a.wait_budget)) {
                         ok = false;
                         break;
                     }
@@ -223,15 +223,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             uint32_t it = 0, tile_it = 0;
-            for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
+            // Test switch: nothing arrives on mma_done before the commit
+            // below, so this wait runs out and the CTA takes the error path.
+            const bool stalled = a.stall && !mbar_wait(mma_done, 0, a.err, a.wait_budget);
+            for (uint32_t t = stalled ? total : blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
                 const uint32_t b = tile_it & 1u, use = tile_it >> 1;
-                if (!mbar_wait(&acc_empty[b], (use & 1u) ^ 1u, a.err)) break;
+                if (!mbar_wait(&acc_empty[b], (use & 1u) ^ 1u, a.err, a.wait_budget)) break;
                 tc_fence_after();
                 const uint32_t d = tmem_base + b * kTileN;
                 bool ok = true;
                 for (uint32_t k = 0; k < a.k_chunks; ++k, ++it) {
                     const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
-                    if (!mbar_wait(&full[s], ph, a.err)) {
+                    if (!mbar_wait(&full[s], ph, a.err, a.wait_budget)) {
                         ok = false;
                         break;
                     }
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
             const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
             const uint32_t b = tile_it & 1u, use = tile_it >> 1;
-            const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err));
+            const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err, a.wait_budget));
             if (!got) break;
             tc_fence_after();
             const uint32_t q = qt * kTileM + lane_base + uint32_t(lane);

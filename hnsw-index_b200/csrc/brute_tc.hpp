@@ -29,6 +29,12 @@ struct TcScoreArgs {
     uint64_t* cand = nullptr;
     uint32_t cand_cap = 0;
     uint32_t* err = nullptr;              // set to 1 if a bounded wait runs out
+    // Clock budget of every pipeline wait (cycles); on expiry the CTA sets
+    // *err, drains its copies and MMAs, frees its TMEM and returns.
+    long long wait_budget = 4000000000ll;
+    // Test switch for the timeout path: the MMA issuer first waits on a
+    // barrier that nothing arrives at, so its bounded wait runs out.
+    uint32_t stall = 0;
 };
 
 uint32_t tc_k_padded(uint32_t dim, int terms);

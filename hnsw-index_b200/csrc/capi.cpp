@@ -1122,6 +1122,8 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     t.qnorm2 = b->qnorm2.as<float>();
     t.xnorm2 = b->metric == HNSW_METRIC_L2 ? b->xnorm2.as<float>() : nullptr;
     t.err = b->err.as<uint32_t>();
+    t.wait_budget = b->wait_budget;
+    t.stall = b->stall;
     t.n_tile_begin = 0;
     t.n_tile_end = sample_rows / 256;
     t.dense = b->dense.as<float>();
@@ -1314,6 +1316,17 @@ int hnsw_gpu_brute_stats(const hnsw_gpu_brute* b, hnsw_brute_stats* out) {
 
 // For callers that must not allocate device memory once they are running:
 // all scratch comes from a fixed 8 MiB array compiled into the library.
+int hnsw_gpu_brute_set_wait_limits(hnsw_gpu_brute* b, uint64_t budget_cycles, int inject_stall) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    std::lock_guard<std::mutex> lock(b->mu);
+    b->wait_budget = budget_cycles == 0 ? 4000000000ll
+                                        : (long long)std::min<uint64_t>(budget_cycles, uint64_t(1) << 62);
+    b->stall = inject_stall ? 1u : 0u;
+    return HNSW_OK;
+}
+
+void hnsw_gpu_debug_fail_allocations(int count) { g_fail_allocations.store(count > 0 ? count : 0); }
+
 int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* b, const float* d_queries, size_t nq, size_t dim,
                                         uint32_t k, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
                                         int32_t* d_status, void* stream) {
@@ -1333,8 +1346,8 @@ int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* b, const float* d_querie
     uint32_t slices = 0;
     if (!noalloc_layout(uint32_t(nq), b->dp, kk, want, &qbytes, &slices))
         return set_error(HNSW_ERR_INVALID_ARGUMENT,
-                         "batch too large for the no-alloc scratch: nq * (4 * padded dim + 8 * min(k, n)) must "
-                         "stay below 8 MiB");
+                         "batch too large for the no-alloc scratch: round_up(nq * 4 * round_up(dim, 32), 256) + "
+                         "nq * 8 * max(1, min(k, n)) must not exceed 8 MiB");
     BruteArgs a;
     a.base = b->base.as<float>();
     a.keys = b->keys.as<uint64_t>();

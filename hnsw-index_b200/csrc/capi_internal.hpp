@@ -7,6 +7,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <functional>
 #include <memory>
@@ -36,12 +37,23 @@ int cuda_fail(cudaError_t e, const char* where);
 
 inline uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
+// Device allocations still to fail on purpose (hnsw_gpu_debug_fail_allocations):
+// a host-side test hook for the out-of-device-memory paths.
+inline std::atomic<int> g_fail_allocations{0};
+inline bool injected_alloc_failure() {
+    int n = g_fail_allocations.load(std::memory_order_relaxed);
+    while (n > 0)
+        if (g_fail_allocations.compare_exchange_weak(n, n - 1, std::memory_order_relaxed)) return true;
+    return false;
+}
+
 // Growable device buffer.
 struct DBuf {
     void* p = nullptr;
     size_t bytes = 0;
     cudaError_t ensure(size_t need) {
         if (need <= bytes) return cudaSuccess;
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;  // buffer left as it was
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
@@ -202,6 +214,8 @@ struct hnsw_gpu_brute {
     DBuf aop, dense, thr1, thr2, margin, qnorm2, ccount, cand, err;
     uint64_t last_candidates = 0, last_queries = 0;
     float last_ms[4] = {0, 0, 0, 0};
+    long long wait_budget = 4000000000ll;  // tensor-core pipeline waits, clock cycles
+    uint32_t stall = 0;                    // test switch: the MMA issuer's wait runs out
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream = nullptr;
     ~hnsw_gpu_brute() {

@@ -38,6 +38,7 @@ struct DevMem {
     template <class T>
     cudaError_t alloc(T** out, size_t count) {
         void* p = nullptr;
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, std::max<size_t>(count * sizeof(T), 16));
         if (e != cudaSuccess) return e;
         ptrs.push_back(p);

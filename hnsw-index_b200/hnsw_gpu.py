@@ -190,6 +190,9 @@ class _BruteStats(C.Structure):
 
 
 _lib.hnsw_gpu_brute_stats.argtypes = [_vp, C.POINTER(_BruteStats)]
+_lib.hnsw_gpu_brute_set_wait_limits.argtypes = [_vp, C.c_uint64, C.c_int]
+_lib.hnsw_gpu_debug_fail_allocations.argtypes = [C.c_int]
+_lib.hnsw_gpu_debug_fail_allocations.restype = None
 
 
 class _BruteFilter(C.Structure):
@@ -719,6 +722,11 @@ class SearchGraph:
             pass
 
 
+def debug_fail_allocations(count: int):
+    """Test hook: the next `count` device allocations fail as out of memory."""
+    _lib.hnsw_gpu_debug_fail_allocations(int(count))
+
+
 def validate_bytes(data: bytes, max_memory: Optional[int] = None) -> _Info:
     """Host-only validation with every check of HnswIndex::from_bytes."""
     buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
@@ -822,6 +830,12 @@ class BruteForceIndex:
         keys, dist, count, _ = self.search_arrays(np.asarray(query, np.float32).reshape(1, -1), k,
                                                   filter_bits=bits, filter_nbits=nbits, filter_by_row=by_row)
         return [Neighbor(int(keys[0, j]), float(dist[0, j])) for j in range(int(count[0]))]
+
+    def set_wait_limits(self, budget_cycles: int = 0, inject_stall: bool = False):
+        """Clock budget of the tensor-core pipeline's waits (0: the default);
+        inject_stall makes the next tensor-core searches run out of it
+        (hnsw_gpu_brute_set_wait_limits)."""
+        _check(_lib.hnsw_gpu_brute_set_wait_limits(self._h, budget_cycles, int(inject_stall)))
 
     def last_stats(self) -> dict:
         """Candidates and device stage times of the last tensor-core search."""

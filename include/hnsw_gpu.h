@@ -327,6 +327,24 @@ typedef struct hnsw_brute_stats {
 } hnsw_brute_stats;
 int hnsw_gpu_brute_stats(const hnsw_gpu_brute* brute, hnsw_brute_stats* out);
 
+/* Limits of the tensor-core pipeline's waits (BF16 / BF16x3 searches). Every
+ * wait of the scoring kernel on its shared-memory barriers gives up after
+ * `budget_cycles` SM clock cycles (0 restores the default, about 2 s): the
+ * kernel then records the failure, lets its copies and MMAs finish, frees its
+ * tensor memory and returns, and the search returns HNSW_ERR_TIMEOUT with the
+ * handle still usable. `inject_stall` != 0 makes the MMA issuer first wait on
+ * a barrier that nothing arrives at, so that wait runs out: a switch for
+ * testing the timeout path without faulting the GPU (0 in normal use). No
+ * counterpart in the reference (CPU-only; its errors are src/error.rs). */
+int hnsw_gpu_brute_set_wait_limits(hnsw_gpu_brute* brute, uint64_t budget_cycles, int inject_stall);
+
+/* Test hook: the next `count` device allocations the library attempts fail
+ * as cudaErrorMemoryAllocation would, so callers can exercise the
+ * HNSW_ERR_OUT_OF_DEVICE_MEMORY paths (0 clears it). The failing call leaves
+ * its handle as it was; later calls allocate normally. Process-wide. No
+ * counterpart in the reference. */
+void hnsw_gpu_debug_fail_allocations(int count);
+
 /* Allocation-free variant of hnsw_gpu_brute_search_batch, FP32 precision,
  * for callers that cannot allocate device memory while they run: code on a
  * latency-critical path, in a process whose memory policy forbids cudaMalloc
@@ -336,14 +354,22 @@ int hnsw_gpu_brute_stats(const hnsw_gpu_brute* brute, hnsw_brute_stats* out);
  * keys/dist nq x k; count and status nq). Scratch comes from one fixed
  * 8 MiB array in the library's device memory, held by every GPU that loads
  * the library until the process exits; a batch must satisfy
- * nq * (4 * round_up(dim, 32) + 8 * min(k, n)) < 8 MiB, otherwise the call
- * returns HNSW_ERR_INVALID_ARGUMENT without launching. The first call on a
- * device looks up the array's device address (once per device, with that
- * device current); make that first call before any stream capture. All calls
- * share the one array, so calls whose work overlaps on the GPU (different
- * streams, no ordering between them) race and corrupt each other's results;
- * order them on one stream. Enqueued on `stream` (NULL = the handle's
- * stream); returns once enqueued. */
+ *   round_up(nq * 4 * round_up(dim, 32), 256) + nq * 8 * max(1, min(k, n))
+ *     <= 8 MiB (8388608 bytes),
+ * otherwise the call returns HNSW_ERR_INVALID_ARGUMENT without launching
+ * (n = rows in the index; the first term holds the prepared queries, the
+ * second one top-k list per query and row slice, at least one slice). The
+ * first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture. All calls share the one array, so calls whose work overlaps on
+ * the GPU (different streams, no ordering between them) race and corrupt
+ * each other's results; order them on one stream. Enqueued on `stream`;
+ * NULL means the handle's own stream, which is NOT ordered with the caller's
+ * streams (the legacy default stream included): a caller passing NULL must
+ * finish writing d_queries first (e.g. synchronise its stream) and must
+ * synchronise the device before reading the outputs. Pass cudaStreamLegacy
+ * ((void*)1) to order the call with the legacy default stream. Returns once
+ * enqueued. */
 int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* brute, const float* d_queries, size_t nq, size_t dim,
                                         uint32_t k, uint64_t* d_keys, float* d_dist, uint32_t* d_count,
                                         int32_t* d_status, void* stream);
