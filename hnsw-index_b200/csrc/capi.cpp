@@ -544,6 +544,7 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     g.cold_chunks = sc->cold_chunks;
     g.stage_rows = sc->stage_rows;
     g.cold = sc->cold ? 1 : 0;
+    g.lookahead = sc->lookahead > 2 ? 2 : sc->lookahead;
     if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
     index->fixed = g;
@@ -757,7 +758,8 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     std::vector<float> times(reps);
     auto same = [](const SearchGeometry& x, const SearchGeometry& y) {
         return x.ef_cap == y.ef_cap && x.cand_cap == y.cand_cap && x.hash_cap == y.hash_cap &&
-               x.warps_per_block == y.warps_per_block && x.stage_rows == y.stage_rows && x.cold == y.cold;
+               x.warps_per_block == y.warps_per_block && x.stage_rows == y.stage_rows && x.cold == y.cold &&
+               x.lookahead == y.lookahead;
     };
     // Times one schedule; returns false on an error (status in r).
     auto timed = [&](const SearchGeometry& g, int32_t mode, int32_t heuristic, float* ms) {
@@ -856,6 +858,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         e->schedule.cold_chunks = t.g.cold_chunks;
         e->schedule.stage_rows = t.g.stage_rows;
         e->schedule.cold = t.g.cold;
+        e->schedule.lookahead = t.g.lookahead;
         e->mode = t.mode;
         e->heuristic = t.heuristic;
         e->ms = t.ms;

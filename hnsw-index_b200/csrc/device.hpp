@@ -50,6 +50,10 @@ struct SearchGeometry {
     // Fast-kernel variant with the cold candidate list (persistent warps
     // move queue overflow there directly instead of to a global array).
     uint32_t cold = 0;
+    // Single-array variant, M0 <= 32: stage the next candidate's neighbor
+    // list in shared memory and prefetch its unvisited rows a round ahead
+    // (1: once the round's rows are requested, 2: once its distances are done).
+    uint32_t lookahead = 0;
 };
 
 struct SearchArgs {

@@ -106,9 +106,11 @@ __device__ __forceinline__ uint64_t to_upack(uint64_t x) { return (x & 0xFFFFFFF
 __device__ __forceinline__ uint64_t from_upack(uint64_t x) { return (x & 0xFFFFFFFF00000000ull) | (uint32_t(x) >> 1); }
 
 // Merges the entries x of the lanes in S (distinct, none in A) into the
-// ascending A[0, hi) (room for all of them). Returns the lowest position
-// written. All lanes call.
-__device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t S, uint64_t x) {
+// ascending A[0, hi) (room for all of them). `at` is, in the lanes of S,
+// lower_bound(A, 0, hi, x) when the caller has it already (else ~0u: it is
+// computed here). Returns the lowest position written. All lanes call.
+__device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t S, uint64_t x,
+                                              uint32_t at = ~0u) {
     const int lane = lane_id();
     const bool in = (S >> lane) & 1u;
     uint32_t rank_s = 0;
@@ -116,7 +118,7 @@ __device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t
         const int j = __ffs(bits) - 1;
         rank_s += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
     }
-    const uint32_t pa = in ? lower_bound(A, 0, hi, x) : hi;
+    const uint32_t pa = in ? (at != ~0u ? at : lower_bound(A, 0, hi, x)) : hi;
     const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
     if (hi > pmin) {
         for (int b = int((hi - 1) & ~31u); b >= int(pmin & ~31u); b -= 32) {

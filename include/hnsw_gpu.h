@@ -182,6 +182,13 @@ typedef struct hnsw_schedule {
     uint32_t cold;            /* 1: the fast kernel's variant that keeps candidate queues of any
                                  length (cold list), for selective filters; 0: leaner variant,
                                  overflow goes to the retry pass */
+    uint32_t lookahead;       /* batches where every node is admitted (no filter, no tombstones),
+                                 M0 <= 32: while a round expands one candidate, the neighbor
+                                 list of the next one in the queue is copied into shared memory
+                                 and the rows of its unvisited neighbors are prefetched into L2
+                                 (used when that candidate is expanded next), once the round's
+                                 own rows are requested (1) or once its distances are computed
+                                 (2); 0 = off */
 } hnsw_schedule;
 int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
 
