@@ -123,6 +123,44 @@ struct SearchArgs {
     int publish = 0;
 };
 
+// Resident serving kernel (serve_kernel): warps that take requests from a
+// ring as the host publishes them. The ring and its tail and stop words live
+// in mapped host memory; one doorbell warp polls the host tail and copies it
+// into device memory, where the serving warps read it. A warp claims the
+// next published request with a compare-and-swap on `claim`, copies its
+// inputs into its own staging row, runs it, and publishes the results and
+// the status in the ring's output row (mapped host memory, status last).
+// Every wait is bounded: a warp leaves after `idle_budget` clock cycles
+// without work or when the stop word is set, so the kernel always ends; the
+// host launches it again when requests arrive.
+struct ServeArgs {
+    const volatile uint64_t* host_tail = nullptr;  // requests published (mapped host memory)
+    const volatile uint32_t* host_stop = nullptr;  // nonzero: leave (mapped host memory)
+    volatile uint64_t* tail = nullptr;             // device copy of host_tail
+    volatile uint32_t* stop = nullptr;             // device copy of host_stop
+    unsigned long long* claim = nullptr;           // requests taken (device memory)
+    const volatile float* rq = nullptr;            // ring: ring_cap x dim queries
+    const volatile uint32_t* rk = nullptr;         // ring: k
+    const volatile uint32_t* ref = nullptr;        // ring: ef
+    const volatile int32_t* rfid = nullptr;        // ring: filter id (-1: none)
+    uint32_t ring_cap = 0;
+    // Per-warp staging rows (device memory): the request being served.
+    float* wq = nullptr;        // warps x dim
+    uint32_t* wk = nullptr;
+    uint32_t* wef = nullptr;
+    uint8_t* wfu = nullptr;
+    uint32_t* wfid = nullptr;
+    long long idle_budget = 0;  // cycles a warp waits for work before it leaves
+    uint32_t* served = nullptr; // requests served (device counter, statistics)
+};
+
+// Serving kernel over a fixed geometry (every request's max(ef, k) <=
+// geo.ef_cap); outputs in the ring's rows, out_stride = args.out_stride.
+cudaError_t launch_serve(const SearchArgs& args, const SearchGeometry& geo, const ServeArgs& sv, int num_sms,
+                         cudaStream_t stream, uint32_t* warps_out);
+// Warps the serving kernel keeps resident for a geometry (its launch size).
+cudaError_t serve_warps(const SearchGeometry& g, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps);
+
 constexpr uint32_t kLastResortWarps = 4;
 
 constexpr uint32_t kColdChunkShift = 10;

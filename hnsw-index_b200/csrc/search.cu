@@ -1367,6 +1367,110 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     }
 }
 
+// Resident serving kernel (ServeArgs, device.hpp). Global warp 0 is the
+// doorbell: it copies the host's tail and stop words into device memory.
+// The other warps claim published requests one at a time. A request with a
+// filter, or on an index with tombstones, takes the cold-list variant;
+// others take the single-array one. A query that outgrows the warp's scratch
+// publishes HNSW_ERR_SCRATCH_OVERFLOW and the host runs it again with the
+// batch path's retry passes.
+__global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry g, ServeArgs sv) {
+    extern __shared__ __align__(16) char smem[];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + warp;
+    const int lane = lane_id();
+    if (gw == 0) {
+        // Doorbell. Polls the host words about once a microsecond; leaves
+        // on stop, or once nothing new was published for twice the serving
+        // warps' idle budget (they leave first).
+        if (lane == 0) {
+            uint64_t seen = *sv.tail;
+            long long last = clock64();
+            for (uint32_t it = 0; it < (1u << 30); ++it) {
+                const uint32_t stop = *sv.host_stop;
+                const uint64_t t = *sv.host_tail;
+                if (t != seen) {
+                    __threadfence_system();  // the ring rows behind the tail are visible before it
+                    *sv.tail = t;
+                    __threadfence();
+                    seen = t;
+                    last = clock64();
+                }
+                if (stop) {
+                    *sv.stop = 1u;
+                    __threadfence();
+                    break;
+                }
+                if (clock64() - last > 2 * sv.idle_budget) break;
+                __nanosleep(1000);
+            }
+        }
+        return;
+    }
+    Ws w;
+    carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g);
+    if (a.spill_bits && gw < a.spill_slots) {
+        w.spill_bits = a.spill_bits + size_t(gw) * a.spill_words;
+        w.spill_words = a.spill_words;
+    }
+    attach_cold(w, a, gw, a.cold_next);
+    const uint32_t dim = a.ix.dim;
+    for (uint32_t served = 0; served < (1u << 30); ++served) {
+        // Claim the next published request (lane 0), with a bounded wait.
+        unsigned long long r = ~0ull;
+        if (lane == 0) {
+            const long long idle0 = clock64();
+            uint32_t nap = 64;
+            for (uint32_t it = 0; it < (1u << 30); ++it) {
+                const unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(sv.claim);
+                const uint64_t t = *sv.tail;
+                if (h < t) {
+                    if (atomicCAS(sv.claim, h, h + 1) == h) {
+                        r = h;
+                        break;
+                    }
+                    continue;  // another warp took it: look again at once
+                }
+                if (*sv.stop) break;
+                if (clock64() - idle0 > sv.idle_budget) break;
+                __nanosleep(nap);
+                nap = min(nap * 2u, 2048u);
+            }
+        }
+        r = __shfl_sync(kFull, r, 0);
+        if (r == ~0ull) break;
+        __threadfence();  // the tail was read before the ring row
+        const uint32_t slot = uint32_t(r % sv.ring_cap);
+        // Copy the request into this warp's staging row (volatile loads: the
+        // ring lives in mapped host memory and its rows are reused).
+        for (uint32_t i = lane; i < dim; i += 32) sv.wq[size_t(gw) * dim + i] = sv.rq[size_t(slot) * dim + i];
+        if (lane == 0) {
+            const int32_t fid = sv.rfid[slot];
+            sv.wk[gw] = sv.rk[slot];
+            sv.wef[gw] = sv.ref[slot];
+            sv.wfu[gw] = fid >= 0 ? 1 : 0;
+            sv.wfid[gw] = fid >= 0 ? uint32_t(fid) : 0u;
+        }
+        __syncwarp();
+        const bool general = a.ix.has_dead || (a.filter_bits != nullptr && sv.wfu[gw] != 0);
+        int32_t st;
+        if (general) st = run_query<1>(a, w, gw, slot);
+        else st = run_query<2>(a, w, gw, slot);
+        end_spill(w);
+        if (st == ST_OVERFLOW) {
+            __threadfence_system();
+            __syncwarp();
+            if (lane == 0) {
+                a.out_count[slot] = 0u;
+                __threadfence_system();
+                a.out_status[slot] = ST_OVERFLOW;
+            }
+        }
+        if (lane == 0 && sv.served) atomicAdd(sv.served, 1u);
+        __syncwarp();
+    }
+}
+
 // One warp per query: whether its filter admits at most a.plan_max nodes.
 __global__ void plan_kernel(SearchArgs a, uint8_t* planned) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -1501,6 +1605,36 @@ cudaError_t launch_search_retry(const SearchArgs& args, uint32_t warps, cudaStre
     if (e != cudaSuccess) return e;
     dev::search_retry_kernel<<<(warps + wpb - 1) / wpb, 32 * wpb, smem, stream>>>(args);
     return cudaGetLastError();
+}
+
+cudaError_t launch_serve(const SearchArgs& args, const SearchGeometry& geo_in, const ServeArgs& sv, int num_sms,
+                         cudaStream_t stream, uint32_t* warps_out) {
+    SearchGeometry geo = geo_in;
+    geo.bytes_per_warp = geometry_bytes_per_warp(geo, args.ix.dp, args.ix.dc);
+    const size_t smem = size_t(geo.bytes_per_warp) * geo.warps_per_block;
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dev::serve_kernel));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::serve_kernel, int(32 * geo.warps_per_block), smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const uint32_t blocks = uint32_t(num_sms * per_sm);
+    if (warps_out) *warps_out = blocks * geo.warps_per_block;
+    dev::serve_kernel<<<blocks, 32 * geo.warps_per_block, smem, stream>>>(args, geo, sv);
+    return cudaGetLastError();
+}
+
+cudaError_t serve_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps) {
+    SearchGeometry g = g_in;
+    g.bytes_per_warp = geometry_bytes_per_warp(g, dp, dc);
+    const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dev::serve_kernel));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::serve_kernel, int(32 * g.warps_per_block), smem);
+    if (e != cudaSuccess) return e;
+    *warps = uint32_t(std::max(per_sm, 1)) * g.warps_per_block * uint32_t(num_sms);
+    return cudaSuccess;
 }
 
 cudaError_t launch_plan(const SearchArgs& args, uint8_t* planned, cudaStream_t stream) {

@@ -613,7 +613,8 @@ class _ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
                 ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
                 ("filter_nbits", C.c_uint64), ("quantized", C.c_int32), ("filter_bank", C.c_void_p),
-                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32), ("mode", C.c_int32)]
+                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32), ("mode", C.c_int32),
+                ("resident", C.c_int32), ("idle_us", C.c_uint32)]
 
 
 _lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
@@ -630,11 +631,13 @@ _lib.hnsw_gpu_server_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c
 
 
 class Server:
-    """Request loop over a resident HnswIndex (continuous batching)."""
+    """Request loop over a resident HnswIndex: continuous batching, or with
+    resident=True a resident serving kernel whose warps take requests one at
+    a time from a ring as they arrive."""
 
     def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
                  max_ef=512, linger_us=100, filter_nbits=0, filter_bank: Optional[np.ndarray] = None,
-                 quantized=False, filter_by_node=False, mode=1):
+                 quantized=False, filter_by_node=False, mode=1, resident=False, idle_us=20000):
         cfg = _ServerConfig()
         _lib.hnsw_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
@@ -642,6 +645,7 @@ class Server:
         cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
         cfg.filter_by_node = int(filter_by_node)
         cfg.mode = int(mode)
+        cfg.resident, cfg.idle_us = int(resident), idle_us
         bank = None if filter_bank is None else np.ascontiguousarray(filter_bank, np.uint64)
         if bank is not None:
             cfg.filter_bank = _ptr(bank)

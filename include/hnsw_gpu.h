@@ -248,6 +248,15 @@ typedef struct hnsw_server_config {
     int32_t filter_by_node; /* the bank's bitmaps are indexed by node id, not key */
     int32_t mode;           /* HNSW_MODE_* of the batches; default PERSISTENT (the device work queue
                                spreads a small batch's queries over every SM); AUTO uses the tuned mode */
+    int32_t resident;       /* 1: a resident serving kernel instead of batches. Requests go into a
+                               ring in mapped host memory as they are submitted; the kernel's warps
+                               (each with its own scratch, sized for max_ef and max_k) take them one
+                               at a time as they come free, so a slow query holds one warp, not a
+                               batch. Every device wait is bounded: the kernel leaves after idle_us
+                               without requests and is launched again when they come. Queries that
+                               outgrow a warp's scratch finish on the batch path's retry passes
+                               (one batch slot of max_batch queries is kept for them). */
+    uint32_t idle_us;       /* resident mode: how long the kernel waits for requests (default 20000) */
 } hnsw_server_config;
 
 void hnsw_server_config_default(hnsw_server_config* cfg);
