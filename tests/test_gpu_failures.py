@@ -56,7 +56,8 @@ def test_tensor_core_wait_runs_out_then_the_handle_still_works(precision):
 
 
 def test_allocation_failure_reports_out_of_device_memory_and_recovers():
-    base, queries = H.gaussian(3000, 50, 32, 6)
+    base, queries = H.gaussian(3000, 400, 32, 6)
+    queries, more = queries[:50], queries
     data = build_index(base, metric=0, m=8, seed=4)
     gi = H.HnswIndex.from_bytes(data)
     ref = O.Index(data).search(queries, 10, 40)
@@ -68,18 +69,19 @@ def test_allocation_failure_reports_out_of_device_memory_and_recovers():
     finally:
         H.debug_fail_allocations(0)
     _same(gi.search_arrays(queries, 10, 40), ref)
-    # The same on the brute-force handle, in the middle of its allocations.
+    # The same on the brute-force handle, at its first allocation and in the
+    # middle of them; each batch is larger than the last, so its buffers grow.
     bf = H.BruteForceIndex(32, H.Metric.L2)
     bf.insert_batch(np.arange(3000, dtype=np.uint64), base)
-    for n in (1, 3):
+    for n, q in ((1, queries), (3, more)):
         try:
             H.debug_fail_allocations(n)
             with pytest.raises(H.Error) as e:
-                bf.search_arrays(queries, 10)
+                bf.search_arrays(q, 10)
             assert e.value.status == H.Status.OUT_OF_DEVICE_MEMORY
         finally:
             H.debug_fail_allocations(0)
-        _same(bf.search_arrays(queries, 10), O.brute(0, base, queries, 10))
+        _same(bf.search_arrays(q, 10), O.brute(0, base, q, 10))
 
 
 def test_allocation_failure_at_open_leaves_nothing_behind():
