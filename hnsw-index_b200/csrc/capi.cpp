@@ -743,8 +743,9 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     // Coordinate descent per mode from the heuristic's choice: the
     // cold-list variant (persistent), warps per block {1,2,4,8}, visited hash
     // {16,32,64} entries per result slot (powers of two within 1024..32768),
-    // staged rows {0,16,32}, then warps per block again; a change is kept
-    // when it is faster. ef_cap is the bucket's bound.
+    // staged rows {0,16,32}, lookahead {1,2} where it applies, then warps per
+    // block again; a change is kept when it is faster. ef_cap is the
+    // bucket's bound.
     const uint32_t ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_bound, 32)));
     const uint32_t row_bytes = (o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4;
     const bool filtered = o.filter_bits != nullptr;
@@ -837,6 +838,14 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
                 g.stage_rows = stage;
                 if (!consider(g)) return r;
             }
+            // Lookahead applies to batches that take the single-array variant
+            // with f32 rows read in place (no filter, no tombstones, M0 <= 32).
+            if (!filtered && !gi->view.has_dead && !o.quantized && cur.stage_rows == 0 && gi->view.m0 <= 32)
+                for (uint32_t la : {1u, 2u}) {
+                    SearchGeometry g = cur;
+                    g.lookahead = la;
+                    if (!consider(g)) return r;
+                }
         }
     }
     const Trial* win[2] = {nullptr, nullptr};

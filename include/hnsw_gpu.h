@@ -196,7 +196,8 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
  * Times the search of a sample batch (host buffers, same options as
  * hnsw_gpu_search_batch) under every feasible schedule of the grid
  * mode x warps per block {1, 2, 4, 8} x visited-hash size {16, 32, 64} x
- * ef_cap (rounded up to a power of two, 1024..32768 entries), plus the
+ * ef_cap (rounded up to a power of two, 1024..32768 entries) x staged rows x
+ * lookahead (batches it applies to), by coordinate descent from the
  * heuristic's own choice, `reps` timed runs each after one warm-up (median,
  * CUDA events). The fastest schedule of each mode is stored in the index's
  * tuning table for the ef bucket of the sample's max(ef, k) (buckets of 32),
