@@ -143,6 +143,70 @@ __device__ __forceinline__ float tile_distance(const TcScoreArgs& a, float s, fl
     return 1.0f - s;
 }
 
+// Epilogue of one accumulator: this lane's query q against the 256 rows
+// row_base .. row_base + 255 held in TMEM columns taddr .. taddr + 255 of its
+// lane. Dense mode writes every distance of the sample's row range;
+// candidate mode appends the (row, distance) pairs at or below the query's
+// threshold, with one reservation per (query, tile). All 32 lanes call.
+__device__ __forceinline__ void epilogue_tile(const TcScoreArgs& a, uint32_t taddr, uint32_t q, uint32_t row_base) {
+    const bool qvalid = q < a.nq;
+    const float thr = (qvalid && a.thr) ? a.thr[q] : 0.0f;
+    const float qn = (qvalid && a.qnorm2) ? a.qnorm2[q] : 0.0f;
+    if (a.dense) {
+        for (uint32_t c = 0; c < kTileN / 32; ++c) {
+            uint32_t v[32];
+            __syncwarp();
+            tmem_ld32(taddr + c * 32, v);
+            const uint32_t row0 = row_base + c * 32;
+#pragma unroll
+            for (int j = 0; j < 32 && qvalid; ++j) {
+                const uint32_t row = row0 + uint32_t(j);
+                const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+                if (row >= a.row0 && row < a.row0 + a.ld)
+                    a.dense[size_t(q) * a.ld + (row - a.row0)] = row < a.n ? dist : __int_as_float(0x7f800000);
+            }
+        }
+        return;
+    }
+    // Pass 1: how many of this query's 256 rows pass the threshold.
+    uint32_t total_pass = 0;
+#pragma unroll 1
+    for (uint32_t c = 0; c < kTileN / 32; ++c) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + c * 32, v);
+        const uint32_t row0 = row_base + c * 32;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const uint32_t row = row0 + uint32_t(j);
+            const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+            total_pass += (qvalid && row < a.n && dist <= thr) ? 1u : 0u;
+        }
+    }
+    // One reservation per (query, tile); pass 2 writes the entries.
+    uint32_t slot = 0;
+    if (total_pass) slot = atomicAdd(a.cand_count + q, total_pass);
+    if (__any_sync(0xFFFFFFFFu, total_pass != 0)) {
+#pragma unroll 1
+        for (uint32_t c = 0; c < kTileN / 32; ++c) {
+            uint32_t v[32];
+            __syncwarp();
+            tmem_ld32(taddr + c * 32, v);
+            const uint32_t row0 = row_base + c * 32;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const uint32_t row = row0 + uint32_t(j);
+                const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+                if (qvalid && row < a.n && dist <= thr) {
+                    if (slot < a.cand_cap)
+                        a.cand[size_t(q) * a.cand_cap + slot] = (uint64_t(__float_as_uint(dist)) << 32) | row;
+                    ++slot;
+                }
+            }
+        }
+    }
+}
+
 template <bool SPLIT3>
 __global__ void __launch_bounds__(kThreads, 1)
     score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
@@ -276,66 +340,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err, a.wait_budget));
             if (!got) break;
             tc_fence_after();
-            const uint32_t q = qt * kTileM + lane_base + uint32_t(lane);
-            const bool qvalid = q < a.nq;
-            const float thr = (qvalid && a.thr) ? a.thr[q] : 0.0f;
-            const float qn = (qvalid && a.qnorm2) ? a.qnorm2[q] : 0.0f;
-            const uint32_t acc_col = b * kTileN;
-            const uint32_t taddr = tmem_base + (lane_base << 16) + acc_col;
-            if (a.dense) {
-                for (uint32_t c = 0; c < kTileN / 32; ++c) {
-                    uint32_t v[32];
-                    __syncwarp();
-                    tmem_ld32(taddr + c * 32, v);
-                    const uint32_t row0 = nt * kTileN + c * 32;
-#pragma unroll
-                    for (int j = 0; j < 32 && qvalid; ++j) {
-                        const uint32_t row = row0 + uint32_t(j);
-                        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-                        if (row >= a.row0 && row < a.row0 + a.ld)
-                            a.dense[size_t(q) * a.ld + (row - a.row0)] = row < a.n ? dist : __int_as_float(0x7f800000);
-                    }
-                }
-            } else {
-                // Pass 1: how many of this query's 256 rows pass the threshold.
-                uint32_t total_pass = 0;
-#pragma unroll 1
-                for (uint32_t c = 0; c < kTileN / 32; ++c) {
-                    uint32_t v[32];
-                    __syncwarp();
-                    tmem_ld32(taddr + c * 32, v);
-                    const uint32_t row0 = nt * kTileN + c * 32;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const uint32_t row = row0 + uint32_t(j);
-                        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-                        total_pass += (qvalid && row < a.n && dist <= thr) ? 1u : 0u;
-                    }
-                }
-                // One reservation per (query, tile); pass 2 writes the entries.
-                uint32_t slot = 0;
-                if (total_pass) slot = atomicAdd(a.cand_count + q, total_pass);
-                if (__any_sync(0xFFFFFFFFu, total_pass != 0)) {
-#pragma unroll 1
-                    for (uint32_t c = 0; c < kTileN / 32; ++c) {
-                        uint32_t v[32];
-                        __syncwarp();
-                        tmem_ld32(taddr + c * 32, v);
-                        const uint32_t row0 = nt * kTileN + c * 32;
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const uint32_t row = row0 + uint32_t(j);
-                            const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-                            if (qvalid && row < a.n && dist <= thr) {
-                                if (slot < a.cand_cap)
-                                    a.cand[size_t(q) * a.cand_cap + slot] =
-                                        (uint64_t(__float_as_uint(dist)) << 32) | row;
-                                ++slot;
-                            }
-                        }
-                    }
-                }
-            }
+            epilogue_tile(a, tmem_base + (lane_base << 16) + b * kTileN, qt * kTileM + lane_base + uint32_t(lane),
+                          nt * kTileN);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
@@ -346,6 +352,235 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Paired variant (cta_group::2): the two CTAs of a cluster compute one
+// 256 x 256 output tile. CTA r holds queries r*128 .. r*128+127 of the pair's
+// 256 (its A tile) and base rows r*128 .. r*128+127 of the tile's 256 (its
+// half of B); one thread of CTA 0 issues tcgen05.mma with M = 256, which reads
+// both CTAs' shared memory and writes each CTA's 128 query rows (x 256 rows)
+// into its own tensor memory. Per CTA and K step that is half the B bytes of
+// the single-CTA kernel for the same products, so more K steps fit in the
+// ring (6 stages of 32 KB, or 3 of 64 KB with the split). Each CTA's TMA
+// loads complete on its own barrier; CTA 1's warp 1 relays each completed
+// stage to CTA 0 with a remote arrive. MMA completions are committed to both
+// CTAs' barriers (multicast commit). No load uses cluster multicast. Every
+// wait is bounded as in score_kernel; the CTAs meet at a cluster barrier
+// before tensor memory is freed, after CTA 0's MMAs and each CTA's copies
+// have completed.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kHalfN = kTileN / 2;                 // base rows per CTA
+constexpr uint32_t kBHalfBytes = kHalfN * kTileK * 2;   // 16 KB
+template <bool SPLIT3>
+struct Ring2 {
+    static constexpr int kTiles = SPLIT3 ? 2 : 1;
+    static constexpr int kStages = SPLIT3 ? 3 : 6;
+    static constexpr uint32_t kStageBytes = kTiles * (kABytes + kBHalfBytes);  // 32 or 64 KB
+};
+// Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 256 (pair), N = 256.
+constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((kTileN >> 3) << 17) | ((256u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc2), "r"(accumulate));
+}
+// Arrives (once) on the barrier at `bar`'s offset in every CTA of `mask`
+// when this thread's MMAs so far have completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar, uint16_t mask) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+        ::"r"(smem_u32(bar)), "h"(mask)
+        : "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Arrive on the barrier at `bar`'s offset in CTA `rank` of the cluster.
+__device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar, uint32_t rank) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(bar)), "r"(rank));
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <bool SPLIT3>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    score_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      TcScoreArgs a) {
+    constexpr int kStages = Ring2<SPLIT3>::kStages, kT = Ring2<SPLIT3>::kTiles;
+    constexpr uint32_t kStageBytes = Ring2<SPLIT3>::kStageBytes;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // Both CTAs lay shared memory out identically: the MMA reads the peer's
+    // operands at the same offsets.
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    auto tileA = [&](uint32_t s, int t) { return smem + s * kStageBytes + uint32_t(t) * kABytes; };
+    auto tileB = [&](uint32_t s, int t) { return smem + s * kStageBytes + kT * kABytes + uint32_t(t) * kBHalfBytes; };
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    uint64_t* peer_full = full + kStages;
+    uint64_t* empty = peer_full + kStages;
+    uint64_t* acc_full = empty + kStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* mma_done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const uint32_t pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const uint32_t q_pairs = a.q_tiles >> 1;
+    const uint32_t n_tiles = a.n_tile_end - a.n_tile_begin;
+    const uint32_t total = q_pairs * n_tiles;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&peer_full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 8);  // four epilogue warps in each CTA
+        }
+        mbar_init(mma_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // Producer (both CTAs): this CTA's A tile and half of B per K step.
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t t = pair; ok && t < total; t += npairs) {
+                const uint32_t nt = a.n_tile_begin + t / q_pairs, qp2 = t % q_pairs;
+                for (uint32_t k = 0; k < a.k_chunks; ++k) {
+                    const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                    if (!mbar_wait(&empty[s], ph ^ 1u, a.err, a.wait_budget)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], kStageBytes);
+#pragma unroll
+                    for (int tt = 0; tt < kT; ++tt) {
+                        const int x = int(k * kTileK + uint32_t(tt) * a.lo_col);
+                        tma_load_2d(tileA(s, tt), &tmA, &full[s], x, int((2 * qp2 + rank) * kTileM));
+                        tma_load_2d(tileB(s, tt), &tmB, &full[s], x, int(nt * kTileN + rank * kHalfN));
+                    }
+                    ++it;
+                }
+            }
+            const uint32_t inflight = it < uint32_t(kStages) ? it : uint32_t(kStages);
+            for (uint32_t j = 0; j < inflight; ++j) {
+                const uint32_t i2 = it - 1 - j;
+                const long long t0 = clock64();
+                while (!mbar_try(&full[i2 % kStages], (i2 / kStages) & 1u) && clock64() - t0 < kWaitBudget) {
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && !leader) {
+            // Relay (CTA 1): each stage of this CTA that has landed is
+            // reported to CTA 0's MMA issuer.
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t t = pair; ok && t < total; t += npairs)
+                for (uint32_t k = 0; k < a.k_chunks; ++k, ++it) {
+                    const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                    if (!mbar_wait(&full[s], ph, a.err, a.wait_budget)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_remote(&peer_full[s], 0);
+                }
+        } else if (lane == 0) {
+            // MMA issuer (CTA 0).
+            uint32_t it = 0, tile_it = 0;
+            for (uint32_t t = pair; t < total; t += npairs, ++tile_it) {
+                const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+                if (!mbar_wait(&acc_empty[b], (use & 1u) ^ 1u, a.err, a.wait_budget)) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + b * kTileN;
+                bool ok = true;
+                for (uint32_t k = 0; k < a.k_chunks; ++k, ++it) {
+                    const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                    if (!mbar_wait(&full[s], ph, a.err, a.wait_budget) ||
+                        !mbar_wait(&peer_full[s], ph, a.err, a.wait_budget)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ah = umma_desc(smem_u32(tileA(s, 0)));
+                    const uint64_t bh = umma_desc(smem_u32(tileB(s, 0)));
+                    if (SPLIT3) {
+                        const uint64_t al = umma_desc(smem_u32(tileA(s, kT - 1)));
+                        const uint64_t bl = umma_desc(smem_u32(tileB(s, kT - 1)));
+#pragma unroll
+                        for (uint32_t j = 0; j < kTileK / 16; ++j) {
+                            umma_bf16_pair(d, ah + 2 * j, bh + 2 * j, (k | j) != 0 ? 1u : 0u);
+                            umma_bf16_pair(d, ah + 2 * j, bl + 2 * j, 1u);
+                            umma_bf16_pair(d, al + 2 * j, bh + 2 * j, 1u);
+                        }
+                    } else {
+#pragma unroll
+                        for (uint32_t j = 0; j < kTileK / 16; ++j)
+                            umma_bf16_pair(d, ah + 2 * j, bh + 2 * j, (k | j) != 0 ? 1u : 0u);
+                    }
+                    umma_commit_pair(&empty[s], 0x3);
+                }
+                if (!ok) break;
+                umma_commit_pair(&acc_full[b], 0x3);
+            }
+            // Every MMA issued has completed before the CTAs part.
+            umma_commit_pair(mma_done, 0x1);
+            const long long t0 = clock64();
+            while (!mbar_try(mma_done, 0) && clock64() - t0 < kWaitBudget) {
+            }
+        }
+    } else {
+        // Epilogue (both CTAs): this CTA's 128 query rows x the tile's 256 rows.
+        const uint32_t lane_base = 32u * uint32_t(warp & 3);
+        uint32_t tile_it = 0;
+        for (uint32_t t = pair; t < total; t += npairs, ++tile_it) {
+            const uint32_t nt = a.n_tile_begin + t / q_pairs, qp2 = t % q_pairs;
+            const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+            const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err, a.wait_budget));
+            if (!got) break;
+            tc_fence_after();
+            epilogue_tile(a, tmem_base + (lane_base << 16) + b * kTileN,
+                          (2 * qp2 + rank) * kTileM + lane_base + uint32_t(lane), nt * kTileN);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                if (leader) mbar_arrive(&acc_empty[b]);
+                else mbar_arrive_remote(&acc_empty[b], 0);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols));
     }
 }
 
@@ -485,8 +720,8 @@ uint32_t tc_k_padded(uint32_t dim, int terms) {
     const uint32_t half = (dim + tc::kTileK - 1) / tc::kTileK * tc::kTileK;
     return terms == 3 ? 2 * half : half;
 }
-uint32_t tc_rows_padded(uint32_t n, bool query_side) {
-    const uint32_t t = query_side ? tc::kTileM : tc::kTileN;
+uint32_t tc_rows_padded(uint32_t n, bool query_side, bool pairs) {
+    const uint32_t t = query_side ? (pairs ? 2 * tc::kTileM : tc::kTileM) : tc::kTileN;
     return (std::max<uint32_t>(n, 1) + t - 1) / t * t;
 }
 
@@ -508,12 +743,28 @@ cudaError_t tc_row_norms(const float* src, uint32_t n, uint32_t dim, uint32_t st
 cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B, uint32_t np_, uint32_t kp,
                      const TcScoreArgs& args_in, int num_sms, cudaStream_t stream) {
     CUtensorMap ma, mb;
-    if (!make_map(&ma, A, qp, kp, tc::kTileM) || !make_map(&mb, B, np_, kp, tc::kTileN)) return cudaErrorInvalidValue;
+    const bool pairs = args_in.pairs != 0;
+    if (pairs && qp % (2 * tc::kTileM) != 0) return cudaErrorInvalidValue;
+    if (!make_map(&ma, A, qp, kp, tc::kTileM) || !make_map(&mb, B, np_, kp, pairs ? tc::kHalfN : tc::kTileN))
+        return cudaErrorInvalidValue;
     TcScoreArgs a = args_in;
     a.q_tiles = qp / tc::kTileM;
     const bool split = a.terms == 3;
     a.lo_col = split ? kp / 2 : 0;
     a.k_chunks = (split ? kp / 2 : kp) / tc::kTileK;
+    if (pairs) {
+        const size_t smem2 = 1024 + size_t(split ? tc::Ring2<true>::kStages * tc::Ring2<true>::kStageBytes
+                                                 : tc::Ring2<false>::kStages * tc::Ring2<false>::kStageBytes) +
+                             256;
+        auto kern2 = split ? tc::score_pair_kernel<true> : tc::score_pair_kernel<false>;
+        cudaError_t e2 = raise_smem_limit(reinterpret_cast<const void*>(kern2));
+        if (e2 != cudaSuccess) return e2;
+        const uint32_t total2 = (a.q_tiles / 2) * (a.n_tile_end - a.n_tile_begin);
+        if (total2 == 0) return cudaSuccess;
+        const uint32_t npairs = std::max<uint32_t>(1, std::min<uint32_t>(total2, uint32_t(num_sms) / 2));
+        kern2<<<2 * npairs, tc::kThreads, smem2, stream>>>(ma, mb, a);
+        return cudaGetLastError();
+    }
     const size_t smem = 1024 + size_t(split ? tc::Ring<true>::kStages * tc::Ring<true>::kStageBytes
                                             : tc::Ring<false>::kStages * tc::Ring<false>::kStageBytes) +
                         256;

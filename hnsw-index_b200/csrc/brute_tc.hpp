@@ -35,10 +35,14 @@ struct TcScoreArgs {
     // Test switch for the timeout path: the MMA issuer first waits on a
     // barrier that nothing arrives at, so its bounded wait runs out.
     uint32_t stall = 0;
+    // 1: the paired kernel (two CTAs of a cluster per 256 x 256 tile,
+    // tcgen05.mma with cta_group::2); query tiles then come in pairs, so the
+    // query operand rows must be padded to a multiple of 256.
+    uint32_t pairs = 0;
 };
 
 uint32_t tc_k_padded(uint32_t dim, int terms);
-uint32_t tc_rows_padded(uint32_t n, bool query_side);
+uint32_t tc_rows_padded(uint32_t n, bool query_side, bool pairs = false);
 // fp32 rows -> BF16 operand rows (terms 1: hi; terms 3: [hi | lo], halves of kp / 2).
 cudaError_t tc_split(const float* src, uint32_t n, uint32_t dim, uint32_t src_stride, __nv_bfloat16* dst,
                      uint32_t rows_padded, uint32_t kp, int terms, bool query_side, cudaStream_t stream);

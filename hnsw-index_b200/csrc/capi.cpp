@@ -1069,7 +1069,8 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     const int ti = terms == 3 ? 1 : 0;
     const uint32_t kp = tc_k_padded(b->dim, terms);
     const uint32_t np = tc_rows_padded(b->n, false);
-    const uint32_t qp = tc_rows_padded(uint32_t(nq), true);
+    const bool pairs = b->tc_pairs != 0;
+    const uint32_t qp = tc_rows_padded(uint32_t(nq), true, pairs);
     if (b->bop_kp[ti] != kp) {
         CU(b->bop[ti].ensure(size_t(np) * kp * 2), "cudaMalloc BF16 rows");
         CU(tc_split(b->base.as<float>(), b->n, b->dim, b->dp, b->bop[ti].as<__nv_bfloat16>(), np, kp, terms, false, st),
@@ -1136,6 +1137,7 @@ static int brute_search_tensor(hnsw_gpu_brute* b, const float* queries, size_t n
     t.err = b->err.as<uint32_t>();
     t.wait_budget = b->wait_budget;
     t.stall = b->stall;
+    t.pairs = pairs ? 1u : 0u;
     t.n_tile_begin = 0;
     t.n_tile_end = sample_rows / 256;
     t.dense = b->dense.as<float>();
@@ -1334,6 +1336,13 @@ int hnsw_gpu_brute_set_wait_limits(hnsw_gpu_brute* b, uint64_t budget_cycles, in
     b->wait_budget = budget_cycles == 0 ? 4000000000ll
                                         : (long long)std::min<uint64_t>(budget_cycles, uint64_t(1) << 62);
     b->stall = inject_stall ? 1u : 0u;
+    return HNSW_OK;
+}
+
+int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* b, int enabled) {
+    if (!b) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null handle");
+    std::lock_guard<std::mutex> lock(b->mu);
+    b->tc_pairs = enabled ? 1u : 0u;
     return HNSW_OK;
 }
 

@@ -216,6 +216,7 @@ struct hnsw_gpu_brute {
     float last_ms[4] = {0, 0, 0, 0};
     long long wait_budget = 4000000000ll;  // tensor-core pipeline waits, clock cycles
     uint32_t stall = 0;                    // test switch: the MMA issuer's wait runs out
+    uint32_t tc_pairs = 0;                 // paired (cta_group::2) tensor-core kernel
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream = nullptr;
     ~hnsw_gpu_brute() {

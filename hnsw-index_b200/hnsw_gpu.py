@@ -191,6 +191,7 @@ class _BruteStats(C.Structure):
 
 _lib.hnsw_gpu_brute_stats.argtypes = [_vp, C.POINTER(_BruteStats)]
 _lib.hnsw_gpu_brute_set_wait_limits.argtypes = [_vp, C.c_uint64, C.c_int]
+_lib.hnsw_gpu_brute_set_pairs.argtypes = [_vp, C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.argtypes = [C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.restype = None
 
@@ -841,6 +842,10 @@ class BruteForceIndex:
         inject_stall makes the next tensor-core searches run out of it
         (hnsw_gpu_brute_set_wait_limits)."""
         _check(_lib.hnsw_gpu_brute_set_wait_limits(self._h, budget_cycles, int(inject_stall)))
+
+    def set_pairs(self, enabled: bool = True):
+        """Tensor-core kernel shape: paired CTAs per 256 x 256 tile (hnsw_gpu_brute_set_pairs)."""
+        _check(_lib.hnsw_gpu_brute_set_pairs(self._h, int(enabled)))
 
     def last_stats(self) -> dict:
         """Candidates and device stage times of the last tensor-core search."""

@@ -355,6 +355,14 @@ int hnsw_gpu_brute_stats(const hnsw_gpu_brute* brute, hnsw_brute_stats* out);
  * counterpart in the reference (CPU-only; its errors are src/error.rs). */
 int hnsw_gpu_brute_set_wait_limits(hnsw_gpu_brute* brute, uint64_t budget_cycles, int inject_stall);
 
+/* Tensor-core kernel shape for BF16 / BF16x3 searches: 0 = one CTA per
+ * 128 x 256 output tile; 1 = the two CTAs of a cluster share a 256 x 256
+ * tile (tcgen05.mma with cta_group::2: each CTA loads its 128 queries and
+ * half of the 256 base rows, so a K step moves a third fewer bytes per
+ * product and the ring holds more of them). Results are the same either
+ * way. No counterpart in the reference. */
+int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* brute, int enabled);
+
 /* Test hook: the next `count` device allocations the library attempts fail
  * as cudaErrorMemoryAllocation would, so callers can exercise the
  * HNSW_ERR_OUT_OF_DEVICE_MEMORY paths (0 clears it). The failing call leaves

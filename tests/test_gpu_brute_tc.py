@@ -67,3 +67,39 @@ def test_tensor_small_and_edge_cases():
     keys = (np.arange(300, dtype=np.uint64) * 13 + 5)[::-1].copy()
     tcres, fp = run(1, base, queries, 20, H.Precision.BF16, keys=keys)
     same(tcres, fp)
+
+
+# The paired kernel (two CTAs per 256 x 256 tile, cta_group::2 MMAs): the
+# same results, bit for bit, and the scores still filter.
+
+def run_pairs(metric, base, queries, k, precision, max_candidates=None):
+    bf = H.BruteForceIndex(base.shape[1], H.Metric(metric))
+    bf.insert_batch(np.arange(base.shape[0], dtype=np.uint64), base)
+    bf.set_pairs(True)
+    tcres = bf.search_arrays(queries, k, precision)
+    if max_candidates is not None:
+        per_query = bf.last_candidates_per_query()
+        assert 0 < per_query <= max_candidates, per_query
+    again = bf.search_arrays(queries, k, precision)
+    bf.set_pairs(False)
+    single = bf.search_arrays(queries, k, precision)
+    return tcres, again, single, bf.search_arrays(queries, k, H.Precision.FP32)
+
+
+@pytest.mark.parametrize("precision", [H.Precision.BF16X3, H.Precision.BF16])
+def test_paired_kernel_matches_fp32(precision):
+    base, queries = H.mixture(30000, 300, 768, 128, 0.5, 8)
+    tcres, again, single, fp = run_pairs(2, base, queries, 100, precision, max_candidates=8000)
+    same(tcres, fp)
+    same(again, fp)
+    same(single, fp)
+
+
+@pytest.mark.parametrize("metric", [0, 1])
+def test_paired_kernel_metrics_and_ragged_batches(metric):
+    # 130 queries: the second query tile of the pair is mostly padding.
+    base, queries = H.mixture(7000, 130, 100, 30, 0.4, 17 + metric)
+    tcres, again, single, fp = run_pairs(metric, base, queries, 10, H.Precision.BF16X3, max_candidates=4000)
+    same(tcres, fp)
+    same(again, fp)
+    same(tcres, O.brute(metric, base, queries, 10))
