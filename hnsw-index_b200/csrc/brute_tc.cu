@@ -408,6 +408,32 @@ __device__ __forceinline__ void mbar_arrive_remote(uint64_t* bar, uint32_t rank)
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(bar)), "r"(rank));
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
 }
+// mbar_wait for a barrier that threads of the peer CTA arrive on (remote
+// arrivals with release at cluster scope): the acquire is at cluster scope too.
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, uint32_t* err, long long budget) {
+    const long long t0 = clock64();
+    for (uint32_t i = 0;; ++i) {
+        if (mbar_try_cluster(bar, parity)) return true;
+        if ((i & 255) == 255) {
+            if (*reinterpret_cast<volatile uint32_t*>(err)) return false;
+            if (clock64() - t0 > budget) {
+                atomicExch(err, 1u);
+                return false;
+            }
+        }
+    }
+}
 __device__ __forceinline__ void cluster_sync() {
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
@@ -516,14 +542,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             uint32_t it = 0, tile_it = 0;
             for (uint32_t t = pair; t < total; t += npairs, ++tile_it) {
                 const uint32_t b = tile_it & 1u, use = tile_it >> 1;
-                if (!mbar_wait(&acc_empty[b], (use & 1u) ^ 1u, a.err, a.wait_budget)) break;
+                if (!mbar_wait_cluster(&acc_empty[b], (use & 1u) ^ 1u, a.err, a.wait_budget)) break;
                 tc_fence_after();
                 const uint32_t d = tmem_base + b * kTileN;
                 bool ok = true;
                 for (uint32_t k = 0; k < a.k_chunks; ++k, ++it) {
                     const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
                     if (!mbar_wait(&full[s], ph, a.err, a.wait_budget) ||
-                        !mbar_wait(&peer_full[s], ph, a.err, a.wait_budget)) {
+                        !mbar_wait_cluster(&peer_full[s], ph, a.err, a.wait_budget)) {
                         ok = false;
                         break;
                     }
