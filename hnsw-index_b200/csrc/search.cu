@@ -1417,9 +1417,13 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
     const uint32_t dim = a.ix.dim;
     for (uint32_t served = 0; served < (1u << 30); ++served) {
         // Claim the next published request (lane 0), with a bounded wait.
+        // The idle clock restarts whenever anything new is published, so the
+        // warps leave together after a quiet period of the whole ring (not
+        // one by one while requests still arrive for others to take).
         unsigned long long r = ~0ull;
         if (lane == 0) {
-            const long long idle0 = clock64();
+            long long idle0 = clock64();
+            uint64_t seen_t = *sv.tail;
             uint32_t nap = 64;
             for (uint32_t it = 0; it < (1u << 30); ++it) {
                 const unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(sv.claim);
@@ -1430,6 +1434,11 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
                         break;
                     }
                     continue;  // another warp took it: look again at once
+                }
+                if (t != seen_t) {
+                    seen_t = t;
+                    idle0 = clock64();
+                    nap = 64;
                 }
                 if (*sv.stop) break;
                 if (clock64() - idle0 > sv.idle_budget) break;

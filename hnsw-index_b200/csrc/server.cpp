@@ -381,6 +381,7 @@ void dispatch_loop(hnsw_gpu_server* s) {
     DeviceGuard dg(s->index->device);
     std::vector<uint64_t> take;
     std::vector<uint64_t> retry;
+    double stop_deadline = 0.0;
     while (true) {
         std::unique_lock<std::mutex> lock(s->mu);
         if (s->cfg.resident) {
@@ -415,6 +416,31 @@ void dispatch_loop(hnsw_gpu_server* s) {
             }
             if (any) s->cv_done.notify_all();
             if (s->stop && s->pending.empty() && s->ring.inflight.empty() && retry.empty() && !busy_batch) break;
+            if (s->stop) {
+                // Stopping: requests get idle_us plus 10 s to finish; any left
+                // then (a kernel that cannot make progress) end with TIMEOUT so
+                // that stopping always returns.
+                if (stop_deadline == 0.0) stop_deadline = now_us() + 1e7 + double(s->cfg.idle_us);
+                if (now_us() > stop_deadline && !busy_batch) {
+                    const double t = now_us();
+                    auto fail = [&](uint64_t ticket) {
+                        Request& q = s->at(ticket);
+                        q.status = HNSW_ERR_TIMEOUT;
+                        q.count = 0;
+                        q.t_done = t;
+                        q.state = ReqState::Done;
+                    };
+                    for (uint64_t pos : s->ring.inflight) fail(s->ring.ticket_of[pos % s->ring.cap]);
+                    for (uint64_t ticket : s->pending) fail(ticket);
+                    for (uint64_t ticket : retry) fail(ticket);
+                    s->ring.inflight.clear();
+                    s->pending.clear();
+                    retry.clear();
+                    s->error = HNSW_ERR_TIMEOUT;
+                    s->cv_done.notify_all();
+                    break;
+                }
+            }
             if (!any) {
                 if (s->ring.inflight.empty() && s->pending.empty() && !busy_batch && retry.empty()) {
                     s->cv_work.wait_for(lock, std::chrono::milliseconds(2));

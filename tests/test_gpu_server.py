@@ -135,10 +135,12 @@ def test_resident_kernel_requests_equal_oracle(served):
     q = queries[:300]
     ks, efs, fids, bank = make_requests(q, nbits, 4)
     srv = H.Server(gi, max_batch=64, max_inflight=1, filter_nbits=nbits, filter_bank=bank, resident=True)
-    tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), int(fids[i])) for i in range(len(q))]
-    results = [srv.wait(t) for t in tickets]
-    launches, served_n = srv.stats()
-    srv.stop()
+    try:
+        tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), int(fids[i])) for i in range(len(q))]
+        results = [srv.wait(t, timeout_ms=20000) for t in tickets]
+        launches, served_n = srv.stats()
+    finally:
+        srv.stop()
     assert served_n == len(q) and launches >= 1
     ref = oracle_results(oi, q, ks, efs, fids, bank, nbits)
     for i, (keys, dist, status, lat) in enumerate(results):
@@ -163,11 +165,13 @@ def test_resident_kernel_open_loop_and_relaunch_after_idle(served):
     # launched again for the second.
     srv = H.Server(gi, max_batch=64, max_inflight=1, filter_nbits=nbits, filter_bank=bank, resident=True,
                    idle_us=2000)
-    keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, fids)
-    time.sleep(0.05)
-    keys2, dist2, cnt2, st2, _ = srv.replay(queries[:50], arrivals[:50], ks[:50], efs[:50], fids[:50])
-    launches, served_n = srv.stats()
-    srv.stop()
+    try:
+        keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, fids)
+        time.sleep(0.05)
+        keys2, dist2, cnt2, st2, _ = srv.replay(queries[:50], arrivals[:50], ks[:50], efs[:50], fids[:50])
+        launches, served_n = srv.stats()
+    finally:
+        srv.stop()
     assert (st == 0).all() and (st2 == 0).all()
     assert launches >= 2 and served_n == len(queries) + 50
     ref = oracle_results(oi, queries, ks, efs, fids, bank, nbits)
@@ -188,9 +192,11 @@ def test_resident_kernel_with_tombstones_and_int8():
     gi = H.HnswIndex.from_bytes(data)
     oi = O.Index(data)
     srv = H.Server(gi, max_batch=32, max_inflight=1, max_k=20, max_ef=128, quantized=True, resident=True)
-    tickets = [srv.submit(queries[i], 10, 40 + (i % 5) * 20) for i in range(len(queries))]
-    results = [srv.wait(t) for t in tickets]
-    srv.stop()
+    try:
+        tickets = [srv.submit(queries[i], 10, 40 + (i % 5) * 20) for i in range(len(queries))]
+        results = [srv.wait(t, timeout_ms=20000) for t in tickets]
+    finally:
+        srv.stop()
     for i, (keys, dist, status, _) in enumerate(results):
         ref = oi.search(queries[i:i + 1], 10, 40 + (i % 5) * 20, quantized=True)
         assert status == 0
