@@ -1371,9 +1371,11 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
 // doorbell: it copies the host's tail and stop words into device memory.
 // The other warps claim published requests one at a time. A request with a
 // filter, or on an index with tombstones, takes the cold-list variant;
-// others take the single-array one. A query that outgrows the warp's scratch
-// publishes HNSW_ERR_SCRATCH_OVERFLOW and the host runs it again with the
-// batch path's retry passes.
+// others take the single-array one (and the cold-list variant if they
+// outgrow it). A query that outgrows even that publishes
+// HNSW_ERR_SCRATCH_OVERFLOW and the host runs it again with the batch path's
+// retry passes, after asking this kernel to leave (stop word) so that the
+// retry kernels get SMs.
 __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry g, ServeArgs sv) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1463,8 +1465,17 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
         __syncwarp();
         const bool general = a.ix.has_dead || (a.filter_bits != nullptr && sv.wfu[gw] != 0);
         int32_t st;
-        if (general) st = run_query<1>(a, w, gw, slot);
-        else st = run_query<2>(a, w, gw, slot);
+        if (general) {
+            st = run_query<1>(a, w, gw, slot);
+        } else {
+            st = run_query<2>(a, w, gw, slot);
+            if (st == ST_OVERFLOW) {
+                // Outgrew the single array (a long run of equal distances):
+                // the cold-list variant takes it on the same scratch.
+                end_spill(w);
+                st = run_query<1>(a, w, gw, slot);
+            }
+        }
         end_spill(w);
         if (st == ST_OVERFLOW) {
             __threadfence_system();

@@ -230,6 +230,9 @@ int launch_resident(hnsw_gpu_server* s) {
     const uint32_t chunks = uint32_t(sl->cold_pool.bytes / (size_t(kColdChunk) * 8));
     CU(sl->work.ensure(32), "cudaMalloc work counters");
     CU(cudaMemsetAsync(sl->work.p, 0, 32, st), "memset work counters");
+    // A stop word raised to make the previous launch yield is lowered again.
+    *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 0;
+    CU(cudaMemsetAsync(static_cast<unsigned char*>(R.words.p) + 16, 0, 4, st), "clear serving stop word");
     SearchArgs a;
     a.ix = gi->view;
     a.queries = R.wq.as<float>();
@@ -370,6 +373,12 @@ bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry) {
         any = true;
     }
     if (R.running && cudaEventQuery(R.done) != cudaErrorNotReady) R.running = false;
+    if (R.running && !retry.empty()) {
+        // Overflowed queries need the retry kernels, which need SMs the
+        // serving kernel holds: ask it to leave after its current requests.
+        *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 1;
+        any = true;
+    }
     if (!R.running && !R.inflight.empty()) {
         const int e = launch_resident(s);
         if (e != HNSW_OK) s->error = e;
