@@ -320,7 +320,7 @@ int launch_resident(hnsw_gpu_server* s) {
 // status is out (overflowed queries go to `retry` for the batch path),
 // publish pending requests into free rows, and launch the serving kernel
 // when it is not running and requests wait. Returns whether anything moved.
-bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry) {
+bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry, bool retry_busy) {
     ResidentRing& R = s->ring;
     const uint32_t K = s->cfg.max_k;
     bool any = false;
@@ -373,13 +373,14 @@ bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry) {
         any = true;
     }
     if (R.running && cudaEventQuery(R.done) != cudaErrorNotReady) R.running = false;
-    if (R.running && !retry.empty()) {
+    const bool retrying = !retry.empty() || retry_busy;
+    if (R.running && retrying) {
         // Overflowed queries need the retry kernels, which need SMs the
-        // serving kernel holds: ask it to leave after its current requests.
+        // serving kernel holds: ask it to leave after its current requests,
+        // and launch it again once the retry batch is done.
         *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 1;
-        any = true;
     }
-    if (!R.running && !R.inflight.empty()) {
+    if (!R.running && !R.inflight.empty() && !retrying) {
         const int e = launch_resident(s);
         if (e != HNSW_OK) s->error = e;
     }
@@ -401,7 +402,7 @@ void dispatch_loop(hnsw_gpu_server* s) {
                 if (cudaEventQuery(b.done) == cudaSuccess) harvest(s, b, true);
                 else busy_batch = true;
             }
-            bool any = resident_step(s, retry);
+            bool any = resident_step(s, retry, busy_batch);
             if (!retry.empty() && !busy_batch) {
                 BatchSlot& b = s->batches[0];
                 b.busy = true;
