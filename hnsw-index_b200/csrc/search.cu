@@ -1428,6 +1428,10 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
             uint64_t seen_t = *sv.tail;
             uint32_t nap = 64;
             for (uint32_t it = 0; it < (1u << 30); ++it) {
+                // The stop word first: a kernel asked to leave (server stop,
+                // or to yield SMs to the retry passes) takes no new request;
+                // published ones stay in the ring for the next launch.
+                if (*sv.stop) break;
                 const unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(sv.claim);
                 const uint64_t t = *sv.tail;
                 if (h < t) {
@@ -1442,7 +1446,6 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
                     idle0 = clock64();
                     nap = 64;
                 }
-                if (*sv.stop) break;
                 if (clock64() - idle0 > sv.idle_budget) break;
                 __nanosleep(nap);
                 nap = min(nap * 2u, 2048u);
