@@ -532,8 +532,8 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
         index->fixed = SearchGeometry{0, 0, 0, 0, 0};
         return HNSW_OK;
     }
-    const bool pow2 = sc->hash_cap >= 64 && (sc->hash_cap & (sc->hash_cap - 1)) == 0;
-    if (sc->ef_cap < 32 || sc->ef_cap > 1024 || sc->ef_cap % 32 || sc->cand_cap < sc->ef_cap || !pow2 ||
+    const bool hash_ok = sc->hash_cap >= 64 && sc->hash_cap % 64 == 0 && sc->hash_cap <= (1u << 20);
+    if (sc->ef_cap < 32 || sc->ef_cap > 1024 || sc->ef_cap % 32 || sc->cand_cap < sc->ef_cap || !hash_ok ||
         sc->warps_per_block < 1 || sc->warps_per_block > 8 || sc->stage_rows > 32)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule out of range");
     SearchGeometry g;
@@ -544,7 +544,6 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* sc) {
     g.cold_chunks = sc->cold_chunks;
     g.stage_rows = sc->stage_rows;
     g.cold = sc->cold ? 1 : 0;
-    g.lookahead = sc->lookahead > 2 ? 2 : sc->lookahead;
     if (size_t(geometry_bytes_per_warp(g, index->view.dp, index->view.dc)) * g.warps_per_block > 220 * 1024)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "schedule needs more than 220 KB of shared memory per block");
     index->fixed = g;
@@ -742,10 +741,10 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     });
     // Coordinate descent per mode from the heuristic's choice: the
     // cold-list variant (persistent), warps per block {1,2,4,8}, visited hash
-    // {16,32,64} entries per result slot (powers of two within 1024..32768),
-    // staged rows {0,16,32}, lookahead {1,2} where it applies, then warps per
-    // block again; a change is kept when it is faster. ef_cap is the
-    // bucket's bound.
+    // {16,24,32,40,48,64} entries per result slot (multiples of 64 within
+    // 1024..32768),
+    // staged rows {0,16,32}, then warps per block again; a change is kept
+    // when it is faster. ef_cap is the bucket's bound.
     const uint32_t ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_bound, 32)));
     const uint32_t row_bytes = (o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4;
     const bool filtered = o.filter_bits != nullptr;
@@ -759,8 +758,7 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     std::vector<float> times(reps);
     auto same = [](const SearchGeometry& x, const SearchGeometry& y) {
         return x.ef_cap == y.ef_cap && x.cand_cap == y.cand_cap && x.hash_cap == y.hash_cap &&
-               x.warps_per_block == y.warps_per_block && x.stage_rows == y.stage_rows && x.cold == y.cold &&
-               x.lookahead == y.lookahead;
+               x.warps_per_block == y.warps_per_block && x.stage_rows == y.stage_rows && x.cold == y.cold;
     };
     // Times one schedule; returns false on an error (status in r).
     auto timed = [&](const SearchGeometry& g, int32_t mode, int32_t heuristic, float* ms) {
@@ -825,9 +823,10 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
                 if (!consider(g)) return r;
             }
             if (pass == 1) break;
-            for (uint32_t per : {16u, 32u, 64u}) {
-                uint32_t hc = 1024;
-                while (hc < ef_cap * per && hc < 32768) hc <<= 1;
+            // Hash sizes need not be powers of two: 24 or 40 entries per
+            // result slot can fit one more warp per SM than 32 or 48.
+            for (uint32_t per : {16u, 24u, 32u, 40u, 48u, 64u}) {
+                const uint32_t hc = std::min<uint32_t>(32768, std::max<uint32_t>(1024, round_up(ef_cap * per, 64)));
                 SearchGeometry g = cur;
                 g.ef_cap = ef_cap;
                 g.hash_cap = hc;
@@ -838,14 +837,6 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
                 g.stage_rows = stage;
                 if (!consider(g)) return r;
             }
-            // Lookahead applies to batches that take the single-array variant
-            // with f32 rows read in place (no filter, no tombstones, M0 <= 32).
-            if (!filtered && !gi->view.has_dead && !o.quantized && cur.stage_rows == 0 && gi->view.m0 <= 32)
-                for (uint32_t la : {1u, 2u}) {
-                    SearchGeometry g = cur;
-                    g.lookahead = la;
-                    if (!consider(g)) return r;
-                }
         }
     }
     const Trial* win[2] = {nullptr, nullptr};
@@ -867,7 +858,6 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
         e->schedule.cold_chunks = t.g.cold_chunks;
         e->schedule.stage_rows = t.g.stage_rows;
         e->schedule.cold = t.g.cold;
-        e->schedule.lookahead = t.g.lookahead;
         e->mode = t.mode;
         e->heuristic = t.heuristic;
         e->ms = t.ms;

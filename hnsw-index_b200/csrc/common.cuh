@@ -94,9 +94,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// Waits for every committed group of this thread (a hardware wait).
-__device__ __forceinline__ void cp_async_wait_committed() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Asks the memory system to bring `bytes` (multiple of 16, 16-byte aligned
 // source) into L2 without occupying registers or shared memory.

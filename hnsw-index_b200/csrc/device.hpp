@@ -38,7 +38,7 @@ struct DeviceIndexView {
 struct SearchGeometry {
     uint32_t ef_cap = 64;     // results capacity (>= every ef of the batch)
     uint32_t cand_cap = 160;  // candidate queue capacity
-    uint32_t hash_cap = 4096; // visited hash entries (power of two)
+    uint32_t hash_cap = 4096; // visited hash entries (multiple of 64)
     uint32_t warps_per_block = 4;
     uint32_t bytes_per_warp = 0;
     uint32_t cold_chunks = 0;  // cold-list pool size in chunks; 0 = automatic
@@ -50,10 +50,6 @@ struct SearchGeometry {
     // Fast-kernel variant with the cold candidate list (persistent warps
     // move queue overflow there directly instead of to a global array).
     uint32_t cold = 0;
-    // Single-array variant, M0 <= 32: stage the next candidate's neighbor
-    // list in shared memory and prefetch its unvisited rows a round ahead
-    // (1: once the round's rows are requested, 2: once its distances are done).
-    uint32_t lookahead = 0;
 };
 
 struct SearchArgs {

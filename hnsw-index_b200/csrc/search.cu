@@ -44,7 +44,6 @@ struct Ws {
     uint32_t* H;       // hash_cap entries, or a bitmap when bitmap_mode
     uint32_t* fr;      // 32: fresh neighbor positions
     float* fd;         // 32: distances of fresh neighbors
-    uint32_t* nl;      // 64: the next candidate's neighbor list, staged a round ahead (lookahead)
     // Staged gathers (null stage: off): stage_rows rows of stage_row_bytes,
     // the fresh ids in rank order, and their code norms.
     uint8_t* stage;
@@ -80,20 +79,6 @@ struct Ws {
     uint64_t b_min, b_max;
 };
 
-// Whether id is in the visited set (read only).
-__device__ __forceinline__ bool visited_probe(const Ws& w, uint32_t id) {
-    if (w.bitmap_mode) return (w.H[id >> 5] >> (id & 31)) & 1u;
-    const uint32_t mask = w.hash_cap - 1;
-    uint32_t h = uint32_t((uint64_t(id * 0x9E3779B1u) * w.hash_cap) >> 32);
-    for (uint32_t probe = 0; probe < w.hash_cap; ++probe) {
-        const uint32_t v = w.H[h];
-        if (v == id) return true;
-        if (v == kEmpty) return false;
-        h = (h + 1) & mask;
-    }
-    return false;
-}
-
 // Visited test-and-set. Returns true if id was not visited before.
 // *full is set when the hash passes its load limit.
 __device__ __forceinline__ bool visit(Ws& w, uint32_t id) {
@@ -102,13 +87,14 @@ __device__ __forceinline__ bool visit(Ws& w, uint32_t id) {
         uint32_t old = atomicOr(&w.H[id >> 5], bit);
         return (old & bit) == 0;
     }
-    const uint32_t mask = w.hash_cap - 1;
+    // Any capacity (not only powers of two): the multiplicative hash maps
+    // ids onto [0, hash_cap) and probing wraps around at the end.
     uint32_t h = uint32_t((uint64_t(id * 0x9E3779B1u) * w.hash_cap) >> 32);
     for (uint32_t probe = 0; probe < w.hash_cap; ++probe) {
         uint32_t old = atomicCAS(&w.H[h], kEmpty, id);
         if (old == kEmpty) return true;
         if (old == id) return false;
-        h = (h + 1) & mask;
+        h = h + 1 == w.hash_cap ? 0u : h + 1;
     }
     return true;  // unreachable while the load limit holds
 }
@@ -755,29 +741,7 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
 // U lives in the candidate array's space (cand_cap + 1 >= ef_cap + 33), T in
 // the results array's; the results are copied back to w.R at the end.
 // Returns rs, or -1 when the query outgrows the scratch (retried).
-// Lookahead: the rows of the staged list's neighbors that are not visited
-// yet are prefetched into L2 (the list's copy into shared memory is waited for
-// first; it was issued at the start of the round).
-__device__ __forceinline__ void prefetch_staged_rows(const QueryCtx& c, const Ws& w) {
-    const DeviceIndexView& ix = c.a->ix;
-    const int lane = lane_id();
-    cp_async_wait_committed();
-    __syncwarp();
-    const uint32_t sid = uint32_t(lane) < ix.m0 ? w.nl[lane] : kEmpty;
-    if (sid != kEmpty && !visited_probe(w, sid)) prefetch_l2(ix.vec + size_t(sid) * ix.dp, ix.dp * 4);
-    __syncwarp();
-}
-
-// LA (lookahead, M0 <= 32): while a round expands candidate p, the neighbor
-// list of pn (the next unexpanded entry, which is the next expansion unless
-// this round inserts something before it) is copied into shared memory with
-// cp.async, and once the round's own rows are in flight (LA = 1) or its
-// distances are computed (LA = 2), the rows of pn's neighbors that are not
-// visited yet are prefetched into L2. When pn is expanded next, its list
-// comes from shared memory and its rows from L2. Nothing but memory traffic
-// depends on the guess: the staged list is used only when its node is the
-// one expanded, and the visited set is only read.
-template <int DK, int LA = 0>
+template <int DK>
 __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
@@ -798,7 +762,6 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
     }
     __syncwarp();
     uint32_t rs = 1, nt = 0, nx = 0, lost = 0;
-    uint32_t nl_id = kEmpty;  // node whose list sits in w.nl (lookahead)
     for (;;) {
         // p: the next expansion; pn: the one after it, unless this round
         // inserts something before it (its list is prefetched into L2).
@@ -814,14 +777,12 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
             }
         }
         uint64_t cur;
-        uint32_t spec = kEmpty;  // lookahead: the node whose list is staged this round
         if (p < rs) {
             cur = U[p];
-            if (LA && pn < rs) spec = uint32_t(U[pn]) >> 1;
             __syncwarp();
             if (lane == 0) {
                 U[p] = cur | 1ull;
-                if (!LA && pn < rs) prefetch_l2(ix.adj0 + size_t(uint32_t(U[pn]) >> 1) * ix.m0p, ix.m0p * 4);
+                if (pn < rs) prefetch_l2(ix.adj0 + size_t(uint32_t(U[pn]) >> 1) * ix.m0p, ix.m0p * 4);
             }
             nx = p + 1;
         } else {
@@ -839,29 +800,9 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
         }
         __syncwarp();
         c.cnt.exp0++;
-        const uint32_t cid = uint32_t(cur) >> 1;
-        const uint32_t* row = ix.adj0 + size_t(cid) * ix.m0p;
-        uint32_t staged_id = kEmpty;
-        bool from_smem = false;
-        if (LA) {
-            // This round's list: from shared memory when it was staged for
-            // this node, else from global memory. Then stage the next one.
-            cp_async_wait_committed();
-            __syncwarp();
-            from_smem = nl_id == cid;
-            if (from_smem) staged_id = uint32_t(lane) < ix.m0 ? w.nl[lane] : kEmpty;
-            __syncwarp();
-            nl_id = spec;
-            if (spec != kEmpty) {
-                if (uint32_t(lane) < (ix.m0p >> 2))
-                    cp_async16(w.nl + 4 * lane, ix.adj0 + size_t(spec) * ix.m0p + 4 * lane);
-                cp_async_commit();
-            }
-        }
+        const uint32_t* row = ix.adj0 + size_t(uint32_t(cur) >> 1) * ix.m0p;
         for (uint32_t base = 0; base < ix.m0; base += 32) {
-            uint32_t id;
-            if (LA && from_smem) id = staged_id;
-            else id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+            const uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
             const bool valid = id != kEmpty;
             const uint32_t V = __ballot_sync(kFull, valid);
             if (V == 0) break;
@@ -884,10 +825,8 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
             }
             const uint32_t F = __ballot_sync(kFull, fresh);
             visited += __popc(F);
-            if (LA == 1 && nl_id != kEmpty) prefetch_staged_rows(c, w);
             if (F != 0) {
                 chunk_distances<DK>(c, id, F);
-                if (LA == 2 && nl_id != kEmpty) prefetch_staged_rows(c, w);
                 c.cnt.dist0 += __popc(F);
                 const float my_d = fresh ? w.fd[lane] : 0.0f;
                 uint32_t P = F;
@@ -958,7 +897,6 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
             if (V != kFull) break;
         }
     }
-    if (LA) cp_async_wait_committed();
     __syncwarp();
     for (uint32_t i = lane; i < rs; i += 32) w.R[i] = from_upack(U[i]);
     __syncwarp();
@@ -1060,7 +998,7 @@ __device__ int32_t prepare(QueryCtx& c, const float* q) {
 // row qi of the arguments (query, k, ef, filter), the outputs row qo.
 // V: 0 lean, 1 cold-list variant, 2 single-array variant (every node admitted).
 // DK: the distance kinds compiled in (DK_ANY unless V == 2).
-template <int V, int DK = DK_ANY, int LA = 0>
+template <int V, int DK = DK_ANY>
 __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_t qi, uint32_t qo) {
     const DeviceIndexView& ix = a.ix;
     const int lane = lane_id();
@@ -1100,7 +1038,7 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
             c.cnt.dist_up++;
             uint64_t ep = pack(d0, ix.entry);
             for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer<DK>(c, ep, layer);
-            if constexpr (V == 2) rs = layer0_single<DK, LA>(c, ep, ef);
+            if constexpr (V == 2) rs = layer0_single<DK>(c, ep, ef);
             else rs = layer0<V == 1>(c, ep, ef);
             if (rs < 0) return ST_OVERFLOW;
         }
@@ -1186,8 +1124,6 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const Search
     off += 32 * 4;
     w.fd = reinterpret_cast<float*>(base + off);
     off += 32 * 4;
-    w.nl = reinterpret_cast<uint32_t*>(base + off);
-    off += 64 * 4;
     w.stage = nullptr;
     w.stage_rows = 0;
     w.stage_row_bytes = 0;
@@ -1260,7 +1196,7 @@ __device__ void end_spill(Ws& w) {
 // The fast kernel. COLD = false: candidate queues spill to a per-warp global
 // array and, beyond it, to the retry pass. COLD = true: the shared array's
 // upper half moves to the cold list directly.
-template <int V, int DK = DK_ANY, int LA = 0>
+template <int V, int DK = DK_ANY>
 __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
@@ -1283,7 +1219,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
             if (lane == 0) qi = atomicAdd(a.work_next, 1u);
             qi = __shfl_sync(kFull, qi, 0);
             if (qi >= a.nq) break;
-            const int32_t st = run_query<V, DK, LA>(a, w, qi, qi);
+            const int32_t st = run_query<V, DK>(a, w, qi, qi);
             end_spill(w);
             if (st == ST_OVERFLOW && lane == 0) {
                 a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
@@ -1293,7 +1229,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     } else {
         const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
         if (qi >= a.nq) return;
-        if (run_query<V, DK, LA>(a, w, qi, qi) == ST_OVERFLOW && lane == 0) {
+        if (run_query<V, DK>(a, w, qi, qi) == ST_OVERFLOW && lane == 0) {
             a.overflow_list[atomicAdd(a.overflow_count, 1u)] = qi;
             a.out_status[qi] = ST_OVERFLOW;
         }
@@ -1320,7 +1256,6 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.qc = reinterpret_cast<int8_t*>(base + align_up(size_t(ix.dp) * 4, 16));
     w.fr = reinterpret_cast<uint32_t*>(base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16));
     w.fd = reinterpret_cast<float*>(w.fr + 32);
-    w.nl = nullptr;
     w.stage = nullptr;
     w.stage_rows = 0;
     w.stage_row_bytes = 0;
@@ -1544,7 +1479,7 @@ __global__ void encode_codes_kernel(const float* __restrict__ vec, uint32_t n, u
 uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t dc) {
     auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
     size_t b = al(size_t(dp) * 4) + al(dc) + al(size_t(g.ef_cap + 1) * 8) + al(size_t(g.cand_cap + 1) * 8) + 256 +
-               256 + size_t(g.hash_cap) * 4;
+               size_t(g.hash_cap) * 4;
     if (g.stage_rows) {
         const size_t rb = g.stage_row_bytes ? g.stage_row_bytes : size_t(dp) * 4;
         b += 256 + al(size_t(g.stage_rows) * rb);
@@ -1567,11 +1502,6 @@ using SearchKernel = void (*)(SearchArgs, SearchGeometry);
 static SearchKernel pick_search_kernel(const SearchArgs& args, const SearchGeometry& g) {
     if (!single_array_batch(args, g)) return g.cold ? dev::search_kernel<1> : dev::search_kernel<0>;
     if (args.quantized || g.stage_rows) return dev::search_kernel<2, dev::DK_ANY>;
-    if (g.lookahead && args.ix.m0 <= 32) {
-        if (g.lookahead == 2)
-            return args.ix.metric == 0 ? dev::search_kernel<2, dev::DK_L2, 2> : dev::search_kernel<2, dev::DK_DOT, 2>;
-        return args.ix.metric == 0 ? dev::search_kernel<2, dev::DK_L2, 1> : dev::search_kernel<2, dev::DK_DOT, 1>;
-    }
     return args.ix.metric == 0 ? dev::search_kernel<2, dev::DK_L2> : dev::search_kernel<2, dev::DK_DOT>;
 }
 
@@ -1607,9 +1537,7 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     // Spill slots for whichever variant a batch takes: the larger residency.
     int best = 1;
     for (SearchKernel kern : {g.cold ? dev::search_kernel<1> : dev::search_kernel<0>, dev::search_kernel<2, dev::DK_ANY>,
-                              dev::search_kernel<2, dev::DK_L2>, dev::search_kernel<2, dev::DK_DOT>,
-                              dev::search_kernel<2, dev::DK_L2, 1>, dev::search_kernel<2, dev::DK_DOT, 1>,
-                              dev::search_kernel<2, dev::DK_L2, 2>, dev::search_kernel<2, dev::DK_DOT, 2>}) {
+                              dev::search_kernel<2, dev::DK_L2>, dev::search_kernel<2, dev::DK_DOT>}) {
         cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
         if (e != cudaSuccess) return e;
         int per_sm = 0;

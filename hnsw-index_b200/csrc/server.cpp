@@ -623,7 +623,6 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
         const uint32_t ef_max = std::max(cfg.max_ef, cfg.max_k);
         R.geo = pick_geometry(ef_max, index->view.dp, index->view.dc, true, cfg.filter_count > 0);
         R.geo.stage_rows = 0;
-        R.geo.lookahead = 0;
         CU(serve_warps(R.geo, index->view.dp, index->view.dc, index->num_sms, &R.warps), "serving occupancy");
         int r = index->slots.acquire(&R.slot);
         if (r != HNSW_OK) return r;

@@ -160,7 +160,7 @@ _lib.hnsw_gpu_set_counters.argtypes = [_vp, C.c_int]
 class _Schedule(C.Structure):
     _fields_ = [("ef_cap", C.c_uint32), ("cand_cap", C.c_uint32), ("hash_cap", C.c_uint32),
                 ("warps_per_block", C.c_uint32), ("cold_chunks", C.c_uint32), ("stage_rows", C.c_uint32),
-                ("cold", C.c_uint32), ("lookahead", C.c_uint32)]
+                ("cold", C.c_uint32)]
 
 
 _lib.hnsw_gpu_set_schedule.argtypes = [_vp, C.POINTER(_Schedule)]
@@ -538,13 +538,13 @@ class HnswIndex:
         self._info = info
 
     def set_schedule(self, ef_cap=None, cand_cap=None, hash_cap=None, warps_per_block=None, cold_chunks=0,
-                     stage_rows=0, cold=0, lookahead=0):
+                     stage_rows=0, cold=0):
         """Fixes the traversal scratch geometry; no arguments restores the automatic choice."""
         if ef_cap is None:
             _check(_lib.hnsw_gpu_set_schedule(self._h, None))
             return
         sc = _Schedule(ef_cap, cand_cap or 2 * ef_cap + 32, hash_cap, warps_per_block, cold_chunks, stage_rows,
-                       int(cold), int(lookahead))
+                       int(cold))
         _check(_lib.hnsw_gpu_set_schedule(self._h, C.byref(sc)))
 
     def autotune(self, queries, k: int, ef: int, reps: int = 3, **search_kw):
@@ -564,7 +564,6 @@ class HnswIndex:
             s = e.schedule
             return {"ef_cap": s.ef_cap, "cand_cap": s.cand_cap, "hash_cap": s.hash_cap,
                     "warps_per_block": s.warps_per_block, "stage_rows": s.stage_rows, "cold": s.cold,
-                    "lookahead": s.lookahead,
                     "mode": e.mode,
                     "heuristic": bool(e.heuristic),
                     "ms": e.ms}

@@ -171,7 +171,7 @@ void hnsw_gpu_graph_destroy(hnsw_gpu_graph* graph);
 typedef struct hnsw_schedule {
     uint32_t ef_cap;          /* >= every max(ef, k) of a batch; multiple of 32, <= 1024 */
     uint32_t cand_cap;        /* candidate array entries */
-    uint32_t hash_cap;        /* visited-hash entries, power of two */
+    uint32_t hash_cap;        /* visited-hash entries, a multiple of 64 (at least 64) */
     uint32_t warps_per_block; /* 1..8 */
     uint32_t cold_chunks;     /* pool of the queues' cold lists, in chunks of 1024 candidates;
                                  0 = automatic (8 per node or 32 per warp). A smaller pool sends
@@ -182,13 +182,6 @@ typedef struct hnsw_schedule {
     uint32_t cold;            /* 1: the fast kernel's variant that keeps candidate queues of any
                                  length (cold list), for selective filters; 0: leaner variant,
                                  overflow goes to the retry pass */
-    uint32_t lookahead;       /* batches where every node is admitted (no filter, no tombstones),
-                                 M0 <= 32: while a round expands one candidate, the neighbor
-                                 list of the next one in the queue is copied into shared memory
-                                 and the rows of its unvisited neighbors are prefetched into L2
-                                 (used when that candidate is expanded next), once the round's
-                                 own rows are requested (1) or once its distances are computed
-                                 (2); 0 = off */
 } hnsw_schedule;
 int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
 
@@ -196,9 +189,8 @@ int hnsw_gpu_set_schedule(hnsw_gpu_index* index, const hnsw_schedule* schedule);
  * Times the search of a sample batch (host buffers, same options as
  * hnsw_gpu_search_batch) under every feasible schedule of the grid
  * mode x warps per block {1, 2, 4, 8} x visited-hash size {16, 32, 64} x
- * ef_cap (rounded up to a power of two, 1024..32768 entries) x staged rows x
- * lookahead (batches it applies to), by coordinate descent from the
- * heuristic's own choice, `reps` timed runs each after one warm-up (median,
+ * ef_cap (rounded up to a multiple of 64, 1024..32768 entries) x staged
+ * rows, by coordinate descent from the heuristic's own choice, `reps` timed runs each after one warm-up (median,
  * CUDA events). The fastest schedule of each mode is stored in the index's
  * tuning table for the ef bucket of the sample's max(ef, k) (buckets of 32),
  * used from then on by searches in that bucket unless a fixed schedule is
