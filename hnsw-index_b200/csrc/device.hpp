@@ -148,6 +148,13 @@ struct ServeArgs {
     uint32_t* wfid = nullptr;
     long long idle_budget = 0;  // cycles a warp waits for work before it leaves
     uint32_t* served = nullptr; // requests served (device counter, statistics)
+    // Requests are checked again on the device (the host checked them at
+    // submission): k in [1, out_stride], filter id below filter_rows. A
+    // request that fails publishes HNSW_ERR_INVALID_ARGUMENT, and the first
+    // failure is recorded in err[0] (what: 1 claim past the tail, 2 bad k,
+    // 3 bad filter id) and err[1] (the ring position's low 32 bits).
+    uint32_t filter_rows = 0;
+    uint32_t* err = nullptr;
 };
 
 // Serving kernel over a fixed geometry (every request's max(ef, k) <=

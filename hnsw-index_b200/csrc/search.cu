@@ -28,7 +28,7 @@
 namespace hnswgpu {
 namespace dev {
 
-enum : int32_t { ST_OK = 0, ST_NON_FINITE = 3, ST_ZERO = 4, ST_QDISABLED = 7, ST_OVERFLOW = 25 };
+enum : int32_t { ST_OK = 0, ST_NON_FINITE = 3, ST_ZERO = 4, ST_QDISABLED = 7, ST_BAD_ARGUMENT = 24, ST_OVERFLOW = 25 };
 
 struct Counters {
     uint32_t dist0 = 0, exp0 = 0, dist_up = 0, exp_up = 0;
@@ -1393,14 +1393,32 @@ __global__ void __launch_bounds__(256) serve_kernel(SearchArgs a, SearchGeometry
         // Copy the request into this warp's staging row (volatile loads: the
         // ring lives in mapped host memory and its rows are reused).
         for (uint32_t i = lane; i < dim; i += 32) sv.wq[size_t(gw) * dim + i] = sv.rq[size_t(slot) * dim + i];
+        uint32_t bad = 0;
         if (lane == 0) {
             const int32_t fid = sv.rfid[slot];
-            sv.wk[gw] = sv.rk[slot];
+            const uint32_t k = sv.rk[slot];
+            if (r >= *sv.tail) bad = 1;
+            else if (k == 0 || k > a.out_stride) bad = 2;
+            else if (fid >= 0 && a.filter_bits != nullptr && uint32_t(fid) >= sv.filter_rows) bad = 3;
+            sv.wk[gw] = k;
             sv.wef[gw] = sv.ref[slot];
             sv.wfu[gw] = fid >= 0 ? 1 : 0;
             sv.wfid[gw] = fid >= 0 ? uint32_t(fid) : 0u;
+            if (bad && sv.err && atomicCAS(sv.err, 0u, bad) == 0u) sv.err[1] = uint32_t(r);
         }
+        bad = __shfl_sync(kFull, bad, 0);
         __syncwarp();
+        if (bad) {
+            // Not run: the request is published with an argument error.
+            if (lane == 0) {
+                a.out_count[slot] = 0u;
+                __threadfence_system();
+                a.out_status[slot] = ST_BAD_ARGUMENT;
+                if (sv.served) atomicAdd(sv.served, 1u);
+            }
+            __syncwarp();
+            continue;
+        }
         const bool general = a.ix.has_dead || (a.filter_bits != nullptr && sv.wfu[gw] != 0);
         int32_t st;
         if (general) {

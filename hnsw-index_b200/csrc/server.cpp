@@ -307,6 +307,8 @@ int launch_resident(hnsw_gpu_server* s) {
     if (cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, gi->device) != cudaSuccess || clock_khz <= 0)
         clock_khz = 1965000;
     sv.idle_budget = (long long)s->cfg.idle_us * (clock_khz / 1000);
+    sv.filter_rows = s->cfg.filter_count;
+    sv.err = reinterpret_cast<uint32_t*>(w + 24);
     uint32_t launched = 0;
     CU(launch_serve(a, R.geo, sv, gi->num_sms, st, &launched), "serving kernel");
     CU(cudaEventRecord(R.done, st), "record serving event");
@@ -349,8 +351,11 @@ bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry, bool retry_
         it = R.inflight.erase(it);
         any = true;
     }
+    // Ring position p uses row p % cap, so a position is published only when
+    // the oldest unharvested one is less than cap positions behind it (rows
+    // finish out of order; a count of inflight rows would not say which).
     bool published = false;
-    while (!s->pending.empty() && R.inflight.size() < R.cap) {
+    while (!s->pending.empty() && (R.inflight.empty() || R.published - R.inflight.front() < R.cap)) {
         const uint64_t ticket = s->pending.front();
         s->pending.pop_front();
         Request& r = s->at(ticket);
@@ -372,7 +377,15 @@ bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry, bool retry_
         *reinterpret_cast<volatile uint64_t*>(R.h_tail) = R.published;
         any = true;
     }
-    if (R.running && cudaEventQuery(R.done) != cudaErrorNotReady) R.running = false;
+    if (R.running && cudaEventQuery(R.done) != cudaErrorNotReady) {
+        R.running = false;
+        // A request the kernel refused (its own checks of the ring row).
+        uint32_t err[2] = {0, 0};
+        if (cudaMemcpy(err, static_cast<unsigned char*>(R.words.p) + 24, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+            s->error = HNSW_ERR_CUDA;
+        else if (err[0] && s->error == HNSW_OK)
+            s->error = HNSW_ERR_INVALID_ARGUMENT;
+    }
     const bool retrying = !retry.empty() || retry_busy;
     if (R.running && retrying) {
         // Overflowed queries need the retry kernels, which need SMs the
@@ -618,7 +631,13 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
         CU(cudaHostAlloc(&R.h_status, C * 4, cudaHostAllocMapped), "mapped ring statuses");
         *reinterpret_cast<volatile uint64_t*>(R.h_tail) = 0;
         *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 0;
-        for (size_t i = 0; i < C; ++i) R.h_status[i] = kUnpublished;
+        for (size_t i = 0; i < C; ++i) {
+            R.h_status[i] = kUnpublished;
+            R.h_k[i] = 0;
+            R.h_ef[i] = 0;
+            R.h_fid[i] = -1;
+        }
+        std::memset(R.h_q, 0, C * s->dim * 4);
         R.ticket_of.assign(C, 0);
         const uint32_t ef_max = std::max(cfg.max_ef, cfg.max_k);
         R.geo = pick_geometry(ef_max, index->view.dp, index->view.dc, true, cfg.filter_count > 0);
