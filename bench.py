@@ -421,13 +421,13 @@ def run_gpu(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
 
-    def step(ef_, mode):
+    def step(ef_, mode, trav=0):
         index.search_device(q_dev.data_ptr(), N_QUERY, K, ef_, o_keys.data_ptr(), o_dist.data_ptr(),
-                            o_cnt.data_ptr(), o_st.data_ptr(), stream=stream.cuda_stream, mode=mode)
+                            o_cnt.data_ptr(), o_st.data_ptr(), stream=stream.cuda_stream, mode=mode, traversal=trav)
 
-    def timed(ef_, mode, steps, warmup):
+    def timed(ef_, mode, steps, warmup, trav=0):
         for _ in range(warmup):
-            step(ef_, mode)
+            step(ef_, mode, trav)
         torch.cuda.synchronize(dev)
         if world > 1:
             barrier()
@@ -435,7 +435,7 @@ def run_gpu(args):
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         for i in range(steps):
             starts[i].record(stream)
-            step(ef_, mode)
+            step(ef_, mode, trav)
             ends[i].record(stream)
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -491,6 +491,26 @@ def run_gpu(args):
     h2d = N_QUERY * DIM * 4
     d2h = N_QUERY * K * 12 + N_QUERY * 8
 
+    # Tensor-core traversal (BF16 / BF16X3 distances while walking the graph,
+    # exact f32 re-rank of the ef results): device time per batch, recall@10
+    # beside the f32 search's on the same queries, and the share of queries
+    # whose list equals the f32 search's.
+    tc_traversal = {}
+    if world == 1:
+        f32_keys, _, f32_cnt, _ = index.search_arrays(queries, K, ef, mode=1)
+        r_f32 = H.recall_at_k(tk, tc, f32_keys, f32_cnt, K)
+        for name, trav in (("bf16", H.Traversal.BF16), ("bf16x3", H.Traversal.BF16X3)):
+            ms = timed(ef, 1, max(3, args.steps // 4), 2, trav)
+            tkeys, tdist, tcnt, tst = index.search_arrays(queries, K, ef, mode=1, traversal=trav)
+            same = sum(int(tcnt[i] == f32_cnt[i] and np.array_equal(tkeys[i, :tcnt[i]], f32_keys[i, :f32_cnt[i]]))
+                       for i in range(N_QUERY))
+            rec = H.recall_at_k(tk, tc, tkeys, tcnt, K)
+            tc_traversal[name] = {"qps_device": N_QUERY / (statistics.median(ms) / 1e3), "ms": statistics.median(ms),
+                                  "recall_at_10": rec, "recall_at_10_f32": r_f32, "recall_diff": rec - r_f32,
+                                  "identical_lists_vs_f32": f"{same}/{N_QUERY}",
+                                  "statuses_ok": int((tst == 0).sum())}
+            log(f"traversal {name}: {tc_traversal[name]}")
+
     # One search call per query (the per-call API path), on a sample.
     npc = 2000
     t = time.perf_counter()
@@ -500,38 +520,35 @@ def run_gpu(args):
 
     # Served load: open-loop Poisson arrivals through the request loop
     # (continuous batching; each request completes when its own query does).
-    served, served_resident = [], []
+    served = []
     if world == 1 and not args.no_serve:
         ref_keys = kk
         rng = np.random.default_rng(21)
         reps = 20
         pool_q = np.tile(queries, (reps, 1))
-        for resident in (False, True):
-            srv = H.Server(index, max_batch=args.serve_batch, max_inflight=1 if resident else 8, max_pending=1 << 18,
-                           max_k=K, max_ef=ef, linger_us=args.serve_linger, resident=resident)
-            out = served_resident if resident else served
-            # Warm-up replays: the first launches on each batch slot size its
-            # device buffers (growing one frees the old, which synchronises
-            # the device), so drive every slot at a high rate before measuring.
-            for rate in (300_000, 2_000_000):
-                srv.replay(pool_q[:50_000], np.cumsum(rng.exponential(1e6 / rate, 50_000)),
-                           np.full(50_000, K, np.uint32), np.full(50_000, ef, np.uint32))
-            for rate in (100_000, 300_000, 1_000_000, 2_000_000):
-                n = int(min(len(pool_q), max(20_000, rate // 2)))
-                arr = np.cumsum(rng.exponential(1e6 / rate, n))
-                t = time.perf_counter()
-                skeys, _, scnt, sst, lat = srv.replay(pool_q[:n], arr, np.full(n, K, np.uint32),
-                                                      np.full(n, ef, np.uint32))
-                wall = time.perf_counter() - t
-                ok = sst == 0
-                same = bool(np.array_equal(skeys[ok][:, :K], ref_keys[np.nonzero(ok)[0] % N_QUERY]))
-                out.append({"offered_qps": rate, "requests": n, "completed": int(ok.sum()),
-                            "rejected": int((sst == H.Status.ADMISSION_REJECTED).sum()),
-                            "achieved_qps": float(ok.sum() / wall),
-                            "p50_ms": float(np.percentile(lat[ok], 50) / 1e3),
-                            "p99_ms": float(np.percentile(lat[ok], 99) / 1e3), "identical_to_batched": same})
-                log(("resident " if resident else "batches ") + str(out[-1]))
-            srv.stop()
+        srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 18, max_k=K, max_ef=ef,
+                       linger_us=args.serve_linger)
+        # Warm-up replays: the first launches on each batch slot size its
+        # device buffers (growing one frees the old, which synchronises the
+        # device), so drive every slot at a high rate before measuring.
+        for rate in (300_000, 2_000_000):
+            srv.replay(pool_q[:50_000], np.cumsum(rng.exponential(1e6 / rate, 50_000)),
+                       np.full(50_000, K, np.uint32), np.full(50_000, ef, np.uint32))
+        for rate in (100_000, 300_000, 1_000_000, 2_000_000):
+            n = int(min(len(pool_q), max(20_000, rate // 2)))
+            arr = np.cumsum(rng.exponential(1e6 / rate, n))
+            t = time.perf_counter()
+            skeys, _, scnt, sst, lat = srv.replay(pool_q[:n], arr, np.full(n, K, np.uint32), np.full(n, ef, np.uint32))
+            wall = time.perf_counter() - t
+            ok = sst == 0
+            same = bool(np.array_equal(skeys[ok][:, :K], ref_keys[np.nonzero(ok)[0] % N_QUERY]))
+            served.append({"offered_qps": rate, "requests": n, "completed": int(ok.sum()),
+                           "rejected": int((sst == H.Status.ADMISSION_REJECTED).sum()),
+                           "achieved_qps": float(ok.sum() / wall),
+                           "p50_ms": float(np.percentile(lat[ok], 50) / 1e3),
+                           "p99_ms": float(np.percentile(lat[ok], 99) / 1e3), "identical_to_batched": same})
+            log("batches " + str(served[-1]))
+        srv.stop()
 
     mean_s = statistics.mean(step_ms) / 1e3
     peak, peak_kind = measured_peaks()
@@ -587,10 +604,11 @@ def run_gpu(args):
                 "tuned_over_plain": value / world / plain_qps,
                 "best_schedule_per_mode": mode_best, "persistent_over_plain": pob,
                 "per_call_qps": per_call_qps, "tuned_over_per_call": value / per_call_qps,
-                "served": served, "served_resident_kernel": served_resident,
+                "served": served,
                 "step_p50_ms": srt[len(srt) // 2], "step_p99_ms": srt[min(len(srt) - 1, int(0.99 * len(srt)))],
                 "parallelism": f"replicas x{world}", "index_build_s": build_s,
                 "layer0_distances_per_query": visit_stats, "config1": config1,
+                "tc_traversal": tc_traversal,
             },
             "parity": parity,
             "fp64_sample": fp64,
@@ -926,10 +944,10 @@ def run_batch(args, emit=True):
 # Serving workload: 10M x 128 L2, open-loop Poisson arrivals.
 # ---------------------------------------------------------------------------
 def run_serve(args, emit=True):
-    """Open-loop Poisson arrivals at 10M x 128 (int8 resident beside f32,
-    k in {10, 100}, ef log-uniform 32-512, 30% filtered at 5-50%), through
-    the resident serving kernel and through batches; plus the latency floor:
-    single queries searched alone, one per call."""
+    """Open-loop Poisson arrivals at 10M x 128 (int8 codes beside f32 rows,
+    k in {10, 100}, ef log-uniform 32-512, 30% filtered at 5-50%) through the
+    request loop (continuous batching); plus the latency floor: single
+    queries searched alone, one per call."""
     import hnsw_gpu as H
 
     nb, dim, pool = args.serve_n, 128, 200_000
@@ -1005,36 +1023,29 @@ def run_serve(args, emit=True):
             log(out[-1])
         return out, clocks
 
-    rates = tuple(int(r) for r in args.serve_rates.split(","))
-    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=1, max_pending=1 << 17, max_k=100, max_ef=512,
-                   filter_nbits=nb, filter_bank=bank, quantized=True, resident=True)
+    # The default run (emit=False) sweeps three loads to stay within minutes.
+    rates = tuple(int(r) for r in args.serve_rates.split(",")) if emit else (10_000, 30_000, 100_000)
+    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 17, max_k=100, max_ef=512,
+                   linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
     srv.replay(queries[:5000], np.cumsum(rq.exponential(1e6 / 30_000, 5000)), ks[:5000], efs[:5000], fids[:5000])
-    resident, clocks = sweep(srv, rates)
+    batch, clocks = sweep(srv, rates)
     launches, served_n = srv.stats()
     srv.stop()
-    batch = []
-    if not args.serve_resident_only:
-        srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 17, max_k=100, max_ef=512,
-                       linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
-        srv.replay(queries[:5000], np.cumsum(rq.exponential(1e6 / 30_000, 5000)), ks[:5000], efs[:5000], fids[:5000])
-        batch, _ = sweep(srv, rates)
-        srv.stop()
     index.close()
     # Headline: the highest served rate with every request admitted and p99
     # within 2 ms, else the highest served rate with every request admitted.
-    ok2 = [s_ for s_ in resident if s_["rejected"] == 0 and s_["p99_ms"] <= 2.0]
-    pool_ = ok2 or [s_ for s_ in resident if s_["rejected"] == 0]
+    ok2 = [s_ for s_ in batch if s_["rejected"] == 0 and s_["p99_ms"] <= 2.0]
+    pool_ = ok2 or [s_ for s_ in batch if s_["rejected"] == 0]
     best = max(pool_, key=lambda s_: s_["achieved_qps"], default=None)
     line = {
-        "metric": "served QPS (10M x 128 L2, open-loop Poisson, resident serving kernel; p50/p99 per load in config)",
+        "metric": "served QPS (10M x 128 L2, open-loop Poisson, continuous batching; p50/p99 per load in config)",
         "value": best["achieved_qps"] if best else 0.0, "unit": "queries/s", "n_gpus": 1,
         "higher_is_better": True, "dtype": "int8+f32", "data": "synthetic",
         "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s, "file_gb": file_gb,
                    "open_s": open_s, "host_validate_s": host_validate_s,
                    "batched_qps_same_requests": batched_qps, "max_batch": args.serve_batch,
                    "p99_within_2ms_at_headline": bool(ok2), "latency_floor_single_request": floor,
-                   "resident_kernel_launches": launches, "resident_served": served_n,
-                   "sweep_resident": resident, "sweep_batches": batch},
+                   "batch_launches": launches, "served": served_n, "sweep_batches": batch},
         "clocks": clocks,
     }
     if not emit:
@@ -1277,7 +1288,6 @@ def main():
     ap.add_argument("--serve-rates", default="10000,30000,100000,300000,1000000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-ref", type=int, default=20000)
-    ap.add_argument("--serve-resident-only", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the brute-force and batching blocks of the default run")

@@ -137,6 +137,27 @@ static int ensure_retry(hnsw_gpu_index* gi, Slot* s, uint32_t ef_cap) {
 // The schedule comes from, in order: `force` (the autotuner's trials), the
 // fixed schedule, the tuning table, the occupancy heuristic. HNSW_MODE_AUTO
 // resolves to the tuned mode of the bucket, else persistent.
+// Builds the tensor-core traversal rows on first use (and the low parts on
+// the first BF16X3 search). The build is waited for before the lock is
+// released, so a search on any stream that finds them ready can read them.
+static int ensure_tc_rows(hnsw_gpu_index* gi, bool lo, cudaStream_t stream) {
+    std::lock_guard<std::mutex> l(gi->tc_mu);
+    if (gi->tc_hi_ready && (!lo || gi->tc_lo_ready)) return HNSW_OK;
+    const DeviceIndexView& v = gi->view;
+    const uint32_t dt = round_up(v.dim, 32);
+    const size_t row_bytes = size_t(v.n) * dt * 2;
+    CU(gi->tc_hi.ensure(std::max<size_t>(row_bytes, 16)), "cudaMalloc tensor-core rows");
+    if (lo) CU(gi->tc_lo.ensure(std::max<size_t>(row_bytes, 16)), "cudaMalloc tensor-core low parts");
+    if (v.metric == HNSW_METRIC_L2) CU(gi->tc_norm.ensure(std::max<size_t>(size_t(v.n) * 4, 4)), "cudaMalloc row norms");
+    CU(launch_tc_rows(v.vec, v.n, v.dim, v.dp, dt, gi->tc_hi.as<uint4>(), lo ? gi->tc_lo.as<uint4>() : nullptr,
+                      v.metric == HNSW_METRIC_L2 ? gi->tc_norm.as<float>() : nullptr, stream),
+       "tensor-core rows");
+    CU(cudaStreamSynchronize(stream), "tensor-core rows");
+    gi->tc_hi_ready = true;
+    if (lo) gi->tc_lo_ready = true;
+    return HNSW_OK;
+}
+
 int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_t nq, const hnsw_search_opts& o_in,
                           const uint32_t* d_ks, const uint32_t* d_efs, const uint64_t* d_fbits, const uint8_t* d_fused,
                           const uint32_t* d_fids,
@@ -145,6 +166,16 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     hnsw_search_opts o = o_in;
     if (o.mode != HNSW_MODE_PLAIN && o.mode != HNSW_MODE_PERSISTENT && o.mode != HNSW_MODE_AUTO)
         return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown search mode");
+    if (o.traversal < HNSW_TRAVERSAL_F32 || o.traversal > HNSW_TRAVERSAL_BF16X3)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown traversal");
+    if (o.traversal && o.quantized)
+        return set_error(HNSW_ERR_INVALID_ARGUMENT, "the tensor-core traversal does not combine with quantized search");
+    if (o.traversal) {
+        const int r = ensure_tc_rows(gi, o.traversal == HNSW_TRAVERSAL_BF16X3, stream);
+        if (r != HNSW_OK) return r;
+    }
+    const uint32_t tcb = o.traversal ? round_up(gi->view.dim, 32) * 2u * (o.traversal == HNSW_TRAVERSAL_BF16X3 ? 2u : 1u)
+                                     : 0u;
     SearchGeometry geo{0, 0, 0, 0, 0};
     if (force) {
         geo = *force;
@@ -161,9 +192,17 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
     geo.stage_row_bytes =
         geo.stage_rows ? ((o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4) : 0;
-    // A schedule tuned on int8 rows may not fit f32 rows.
-    if (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024)
+    geo.tc_bytes = tcb;
+    // A schedule tuned on int8 rows may not fit f32 rows (or the tensor-core
+    // query operands): the heuristic's, with the visited hash halved until
+    // it fits.
+    if (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024) {
         geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
+        geo.tc_bytes = tcb;
+        while (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024 &&
+               geo.hash_cap > 1024)
+            geo.hash_cap >>= 1;
+    }
     if (!persistent) geo.cold = 0;  // cold lists need the persistent warps' chunk tables
     // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
     // out by the fast (cold variant) and retry kernels, [4] last-resort count.
@@ -182,6 +221,13 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.ks = d_ks;
     a.efs = d_efs;
     a.quantized = o.quantized;
+    a.traversal = o.traversal;
+    if (o.traversal) {
+        a.ix.tc_hi = gi->tc_hi.as<uint4>();
+        a.ix.tc_lo = o.traversal == HNSW_TRAVERSAL_BF16X3 ? gi->tc_lo.as<uint4>() : nullptr;
+        a.ix.xnorm = gi->view.metric == HNSW_METRIC_L2 ? gi->tc_norm.as<float>() : nullptr;
+        a.ix.dt = round_up(gi->view.dim, 32);
+    }
     a.filter_bits = d_fbits;
     a.filter_nbits = o.filter_nbits;
     a.filter_stride = o.filter_stride;

@@ -184,6 +184,11 @@ struct hnsw_gpu_index {
     std::mutex tune_mu;
     Tuned tuned[33];
     cudaEvent_t dev_done = nullptr;
+    // Tensor-core traversal rows, built on first use (tc_mu): BF16 high
+    // parts, low parts (BF16X3), f32 squared norms (L2).
+    std::mutex tc_mu;
+    DBuf tc_hi, tc_lo, tc_norm;
+    bool tc_hi_ready = false, tc_lo_ready = false;
     ~hnsw_gpu_index() {
         DeviceGuard g(device);
         if (dev_done) {
@@ -191,7 +196,8 @@ struct hnsw_gpu_index {
             cudaEventDestroy(dev_done);
         }
         dev_slot.reset();
-        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead}) b->release();
+        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead, &tc_hi, &tc_lo, &tc_norm})
+            b->release();
         std::lock_guard<std::mutex> l(slots.mu);
         slots.free.clear();
     }

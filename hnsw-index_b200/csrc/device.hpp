@@ -32,6 +32,14 @@ struct DeviceIndexView {
     const uint32_t* adjU = nullptr;    // blocks * mp
     const uint64_t* keys = nullptr;    // n
     const uint32_t* dead = nullptr;    // ceil(n/32) tombstone bitmap
+    // Tensor-core traversal: BF16 copies of the rows, dt (dim rounded up to
+    // 32) values per node, permuted within each 32-value block so that lane
+    // t of an mma quad finds its operand words in one 16-byte load
+    // (tc_row_pos); the low parts of the hi/lo split; the f32 squared norms.
+    const uint4* tc_hi = nullptr;      // n * dt / 8
+    const uint4* tc_lo = nullptr;      // n * dt / 8 (BF16X3 only)
+    const float* xnorm = nullptr;      // n
+    uint32_t dt = 0;
 };
 
 // Per-launch scratch geometry (picked by the launcher per call).
@@ -47,6 +55,7 @@ struct SearchGeometry {
     // computed (0 = rows are read from global memory group by group).
     uint32_t stage_rows = 0;
     uint32_t stage_row_bytes = 0;  // set per launch: dc (int8 traversal) or dp * 4
+    uint32_t tc_bytes = 0;         // set per launch: the query's BF16 operands (tensor-core traversal)
     // Fast-kernel variant with the cold candidate list (persistent warps
     // move queue overflow there directly instead of to a global array).
     uint32_t cold = 0;
@@ -113,56 +122,29 @@ struct SearchArgs {
     // of its admitted nodes; plan_max is the admitted-count bound.
     const uint8_t* planned = nullptr;
     uint32_t plan_max = 0;
+    // Distances while walking the graph: 0 f32 (the reference's), 1 BF16
+    // and 2 BF16x3 on the tensor cores with an exact f32 re-rank.
+    int traversal = 0;
     // Outputs live in mapped host memory and each query's status is its
     // completion flag: the status is written last, after a system-scope
     // fence, so a host thread that sees it can read the query's results.
     int publish = 0;
 };
 
-// Resident serving kernel (serve_kernel): warps that take requests from a
-// ring as the host publishes them. The ring and its tail and stop words live
-// in mapped host memory; one doorbell warp polls the host tail and copies it
-// into device memory, where the serving warps read it. A warp claims the
-// next published request with a compare-and-swap on `claim`, copies its
-// inputs into its own staging row, runs it, and publishes the results and
-// the status in the ring's output row (mapped host memory, status last).
-// Every wait is bounded: a warp leaves after `idle_budget` clock cycles
-// without work or when the stop word is set, so the kernel always ends; the
-// host launches it again when requests arrive.
-struct ServeArgs {
-    const volatile uint64_t* host_tail = nullptr;  // requests published (mapped host memory)
-    const volatile uint32_t* host_stop = nullptr;  // nonzero: leave (mapped host memory)
-    volatile uint64_t* tail = nullptr;             // device copy of host_tail
-    volatile uint32_t* stop = nullptr;             // device copy of host_stop
-    unsigned long long* claim = nullptr;           // requests taken (device memory)
-    const volatile float* rq = nullptr;            // ring: ring_cap x dim queries
-    const volatile uint32_t* rk = nullptr;         // ring: k
-    const volatile uint32_t* ref = nullptr;        // ring: ef
-    const volatile int32_t* rfid = nullptr;        // ring: filter id (-1: none)
-    uint32_t ring_cap = 0;
-    // Per-warp staging rows (device memory): the request being served.
-    float* wq = nullptr;        // warps x dim
-    uint32_t* wk = nullptr;
-    uint32_t* wef = nullptr;
-    uint8_t* wfu = nullptr;
-    uint32_t* wfid = nullptr;
-    long long idle_budget = 0;  // cycles a warp waits for work before it leaves
-    uint32_t* served = nullptr; // requests served (device counter, statistics)
-    // Requests are checked again on the device (the host checked them at
-    // submission): k in [1, out_stride], filter id below filter_rows. A
-    // request that fails publishes HNSW_ERR_INVALID_ARGUMENT, and the first
-    // failure is recorded in err[0] (what: 1 claim past the tail, 2 bad k,
-    // 3 bad filter id) and err[1] (the ring position's low 32 bits).
-    uint32_t filter_rows = 0;
-    uint32_t* err = nullptr;
-};
+// Kernels of the tensor-core traversal (search_tc.cu): variant v (0 lean,
+// 1 cold list, 2 single array) and the retry pass, for traversal 1 (BF16)
+// or 2 (BF16x3); and the builder of the BF16 rows and f32 squared norms.
+using SearchKernel = void (*)(SearchArgs, SearchGeometry);
+using RetryKernel = void (*)(SearchArgs);
+SearchKernel tc_search_kernel(int v, int traversal);
+RetryKernel tc_retry_kernel(int traversal);
+cudaError_t launch_tc_rows(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, uint32_t dt, uint4* hi, uint4* lo,
+                           float* xnorm, cudaStream_t stream);
 
-// Serving kernel over a fixed geometry (every request's max(ef, k) <=
-// geo.ef_cap); outputs in the ring's rows, out_stride = args.out_stride.
-cudaError_t launch_serve(const SearchArgs& args, const SearchGeometry& geo, const ServeArgs& sv, int num_sms,
-                         cudaStream_t stream, uint32_t* warps_out);
-// Warps the serving kernel keeps resident for a geometry (its launch size).
-cudaError_t serve_warps(const SearchGeometry& g, uint32_t dp, uint32_t dc, int num_sms, uint32_t* warps);
+// Bytes of a warp's BF16 query operands for the tensor-core traversal.
+__host__ __device__ inline uint32_t tc_query_bytes(const SearchArgs& a) {
+    return a.traversal ? a.ix.dt * 2u * (a.traversal == 2 ? 2u : 1u) : 0u;
+}
 
 constexpr uint32_t kLastResortWarps = 4;
 

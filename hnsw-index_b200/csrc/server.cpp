@@ -74,33 +74,6 @@ constexpr int32_t kRetrying = HNSW_ERR_SCRATCH_OVERFLOW;
 
 }  // namespace
 
-// Resident mode: the request ring in mapped host memory, the serving
-// kernel's device words and per-warp staging rows, and its scratch slot.
-struct ResidentRing {
-    uint32_t cap = 0;                 // ring rows (= request table rows)
-    float* h_q = nullptr;             // cap x dim
-    uint32_t* h_k = nullptr;
-    uint32_t* h_ef = nullptr;
-    int32_t* h_fid = nullptr;
-    uint64_t* h_tail = nullptr;       // requests published
-    uint32_t* h_stop = nullptr;
-    uint64_t* h_keys = nullptr;       // outputs, cap x max_k
-    float* h_dist = nullptr;
-    uint32_t* h_count = nullptr;
-    int32_t* h_status = nullptr;
-    DBuf words;                       // claim (8 B), tail (8 B), stop (4 B), served (4 B)
-    DBuf wq, wk, wef, wfu, wfid;      // per-warp staging rows
-    Slot* slot = nullptr;             // spill areas and cold-list pool of the serving warps
-    cudaEvent_t done = nullptr;
-    bool running = false;
-    uint32_t warps = 0;
-    SearchGeometry geo;
-    uint64_t published = 0;
-    std::vector<uint64_t> ticket_of;  // ticket held by each ring row
-    std::deque<uint64_t> inflight;    // ring positions published and not completed
-    uint64_t launches = 0;
-};
-
 struct hnsw_gpu_server {
     hnsw_gpu_index* index = nullptr;
     hnsw_server_config cfg{};
@@ -120,7 +93,6 @@ struct hnsw_gpu_server {
     std::thread dispatcher;
     int error = HNSW_OK;
     uint64_t launched_batches = 0, launched_queries = 0;
-    ResidentRing ring;
 
     Request& at(uint64_t ticket) { return req[ticket % cap]; }
 };
@@ -218,262 +190,11 @@ bool harvest(hnsw_gpu_server* s, BatchSlot& b, bool all) {
     return any;
 }
 
-// Launches the serving kernel over the ring (caller holds mu).
-int launch_resident(hnsw_gpu_server* s) {
-    ResidentRing& R = s->ring;
-    hnsw_gpu_index* gi = s->index;
-    Slot* sl = R.slot;
-    cudaStream_t st = sl->stream;
-    const uint32_t n = gi->view.n;
-    const uint32_t words = ((n + 31) / 32 + 3) & ~3u;
-    const uint32_t tab_cap = (n + kColdChunk - 1) / kColdChunk + 2;
-    const uint32_t chunks = uint32_t(sl->cold_pool.bytes / (size_t(kColdChunk) * 8));
-    CU(sl->work.ensure(32), "cudaMalloc work counters");
-    CU(cudaMemsetAsync(sl->work.p, 0, 32, st), "memset work counters");
-    // A stop word raised to make the previous launch yield is lowered again.
-    *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 0;
-    CU(cudaMemsetAsync(static_cast<unsigned char*>(R.words.p) + 16, 0, 4, st), "clear serving stop word");
-    SearchArgs a;
-    a.ix = gi->view;
-    a.queries = R.wq.as<float>();
-    a.nq = R.cap;
-    a.k = s->cfg.max_k;
-    a.ef = s->cfg.max_ef;
-    a.ks = R.wk.as<uint32_t>();
-    a.efs = R.wef.as<uint32_t>();
-    a.quantized = s->cfg.quantized;
-    if (s->words && s->cfg.filter_count) {
-        a.filter_bits = s->bank.as<uint64_t>();
-        a.filter_nbits = s->cfg.filter_nbits;
-        a.filter_stride = s->words;
-        a.filter_used = R.wfu.as<uint8_t>();
-        a.filter_ids = R.wfid.as<uint32_t>();
-        a.filter_by_node = s->cfg.filter_by_node;
-    }
-    uint64_t* dk = nullptr;
-    float* dd = nullptr;
-    uint32_t* dc = nullptr;
-    int32_t* ds = nullptr;
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dk), R.h_keys, 0), "mapped keys");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dd), R.h_dist, 0), "mapped dist");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dc), R.h_count, 0), "mapped counts");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ds), R.h_status, 0), "mapped statuses");
-    a.out_keys = dk;
-    a.out_dist = dd;
-    a.out_count = dc;
-    a.out_status = ds;
-    a.out_stride = s->cfg.max_k;
-    a.publish = 1;
-    a.persistent = 1;
-    a.spill_bits = sl->spill_bits.as<uint32_t>();
-    a.spill_words = words;
-    a.spill_slots = R.warps;
-    a.cold_pool = sl->cold_pool.as<uint64_t>();
-    a.cold_chunks = chunks;
-    a.cold_next = sl->work.as<uint32_t>() + 2;
-    a.cold_tab = sl->cold_tab.as<uint32_t>();
-    a.cold_tab_cap = tab_cap;
-    a.cold_slots = R.warps;
-    ServeArgs sv;
-    uint64_t* hw_tail = nullptr;
-    uint32_t* hw_stop = nullptr;
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&hw_tail), R.h_tail, 0), "mapped tail");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&hw_stop), R.h_stop, 0), "mapped stop");
-    sv.host_tail = hw_tail;
-    sv.host_stop = hw_stop;
-    unsigned char* w = static_cast<unsigned char*>(R.words.p);
-    sv.claim = reinterpret_cast<unsigned long long*>(w);
-    sv.tail = reinterpret_cast<volatile uint64_t*>(w + 8);
-    sv.stop = reinterpret_cast<volatile uint32_t*>(w + 16);
-    sv.served = reinterpret_cast<uint32_t*>(w + 20);
-    float* rq = nullptr;
-    uint32_t *rk = nullptr, *ref = nullptr;
-    int32_t* rfid = nullptr;
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&rq), R.h_q, 0), "mapped ring queries");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&rk), R.h_k, 0), "mapped ring k");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ref), R.h_ef, 0), "mapped ring ef");
-    CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&rfid), R.h_fid, 0), "mapped ring filters");
-    sv.rq = rq;
-    sv.rk = rk;
-    sv.ref = ref;
-    sv.rfid = rfid;
-    sv.ring_cap = R.cap;
-    sv.wq = R.wq.as<float>();
-    sv.wk = R.wk.as<uint32_t>();
-    sv.wef = R.wef.as<uint32_t>();
-    sv.wfu = R.wfu.as<uint8_t>();
-    sv.wfid = R.wfid.as<uint32_t>();
-    int clock_khz = 0;
-    if (cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, gi->device) != cudaSuccess || clock_khz <= 0)
-        clock_khz = 1965000;
-    sv.idle_budget = (long long)s->cfg.idle_us * (clock_khz / 1000);
-    sv.filter_rows = s->cfg.filter_count;
-    sv.err = reinterpret_cast<uint32_t*>(w + 24);
-    uint32_t launched = 0;
-    CU(launch_serve(a, R.geo, sv, gi->num_sms, st, &launched), "serving kernel");
-    CU(cudaEventRecord(R.done, st), "record serving event");
-    R.running = true;
-    ++R.launches;
-    ++s->launched_batches;
-    return HNSW_OK;
-}
-
-// Resident mode, one pass (the caller holds mu): harvest the ring rows whose
-// status is out (overflowed queries go to `retry` for the batch path),
-// publish pending requests into free rows, and launch the serving kernel
-// when it is not running and requests wait. Returns whether anything moved.
-bool resident_step(hnsw_gpu_server* s, std::vector<uint64_t>& retry, bool retry_busy) {
-    ResidentRing& R = s->ring;
-    const uint32_t K = s->cfg.max_k;
-    bool any = false;
-    const double t = now_us();
-    for (auto it = R.inflight.begin(); it != R.inflight.end();) {
-        const uint32_t row = uint32_t(*it % R.cap);
-        const int32_t st = reinterpret_cast<volatile int32_t*>(R.h_status)[row];
-        if (st == kUnpublished) {
-            ++it;
-            continue;
-        }
-        std::atomic_thread_fence(std::memory_order_acquire);
-        const uint64_t ticket = R.ticket_of[row];
-        if (st == kRetrying) {
-            retry.push_back(ticket);
-        } else {
-            Request& r = s->at(ticket);
-            const uint64_t rrow = ticket % s->cap;
-            r.status = st;
-            r.count = st == 0 ? std::min(R.h_count[row], r.k) : 0;
-            std::memcpy(&s->keys[rrow * K], R.h_keys + size_t(row) * K, size_t(r.count) * 8);
-            std::memcpy(&s->dist[rrow * K], R.h_dist + size_t(row) * K, size_t(r.count) * 4);
-            r.t_done = t;
-            r.state = ReqState::Done;
-        }
-        it = R.inflight.erase(it);
-        any = true;
-    }
-    // Ring position p uses row p % cap, so a position is published only when
-    // the oldest unharvested one is less than cap positions behind it (rows
-    // finish out of order; a count of inflight rows would not say which).
-    bool published = false;
-    while (!s->pending.empty() && (R.inflight.empty() || R.published - R.inflight.front() < R.cap)) {
-        const uint64_t ticket = s->pending.front();
-        s->pending.pop_front();
-        Request& r = s->at(ticket);
-        r.state = ReqState::Inflight;
-        const uint64_t pos = R.published++;
-        const uint32_t row = uint32_t(pos % R.cap);
-        R.ticket_of[row] = ticket;
-        std::memcpy(R.h_q + size_t(row) * s->dim, &s->q[(ticket % s->cap) * s->dim], size_t(s->dim) * 4);
-        R.h_k[row] = r.k;
-        R.h_ef[row] = r.ef;
-        R.h_fid[row] = r.filter_id;
-        reinterpret_cast<volatile int32_t*>(R.h_status)[row] = kUnpublished;
-        R.inflight.push_back(pos);
-        ++s->launched_queries;
-        published = true;
-    }
-    if (published) {
-        std::atomic_thread_fence(std::memory_order_release);
-        *reinterpret_cast<volatile uint64_t*>(R.h_tail) = R.published;
-        any = true;
-    }
-    if (R.running && cudaEventQuery(R.done) != cudaErrorNotReady) {
-        R.running = false;
-        // A request the kernel refused (its own checks of the ring row).
-        uint32_t err[2] = {0, 0};
-        if (cudaMemcpy(err, static_cast<unsigned char*>(R.words.p) + 24, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
-            s->error = HNSW_ERR_CUDA;
-        else if (err[0] && s->error == HNSW_OK)
-            s->error = HNSW_ERR_INVALID_ARGUMENT;
-    }
-    const bool retrying = !retry.empty() || retry_busy;
-    if (R.running && retrying) {
-        // Overflowed queries need the retry kernels, which need SMs the
-        // serving kernel holds: ask it to leave after its current requests,
-        // and launch it again once the retry batch is done.
-        *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 1;
-    }
-    if (!R.running && !R.inflight.empty() && !retrying) {
-        const int e = launch_resident(s);
-        if (e != HNSW_OK) s->error = e;
-    }
-    return any;
-}
-
 void dispatch_loop(hnsw_gpu_server* s) {
     DeviceGuard dg(s->index->device);
     std::vector<uint64_t> take;
-    std::vector<uint64_t> retry;
-    double stop_deadline = 0.0;
     while (true) {
         std::unique_lock<std::mutex> lock(s->mu);
-        if (s->cfg.resident) {
-            // Serving kernel first; overflowed queries wait for the batch slot.
-            bool busy_batch = false;
-            for (BatchSlot& b : s->batches) {
-                if (!b.busy) continue;
-                if (cudaEventQuery(b.done) == cudaSuccess) harvest(s, b, true);
-                else busy_batch = true;
-            }
-            bool any = resident_step(s, retry, busy_batch);
-            if (!retry.empty() && !busy_batch) {
-                BatchSlot& b = s->batches[0];
-                b.busy = true;
-                const size_t nb = std::min<size_t>(retry.size(), s->cfg.max_batch);
-                b.tickets.assign(retry.begin(), retry.begin() + nb);
-                retry.erase(retry.begin(), retry.begin() + nb);
-                const int r = stage_and_launch(s, b, b.tickets);
-                if (r != HNSW_OK) {
-                    s->error = r;
-                    for (uint64_t t : b.tickets) {
-                        Request& q = s->at(t);
-                        q.status = r;
-                        q.count = 0;
-                        q.t_done = now_us();
-                        q.state = ReqState::Done;
-                    }
-                    b.busy = false;
-                    b.tickets.clear();
-                }
-                any = true;
-            }
-            if (any) s->cv_done.notify_all();
-            if (s->stop && s->pending.empty() && s->ring.inflight.empty() && retry.empty() && !busy_batch) break;
-            if (s->stop) {
-                // Stopping: requests get idle_us plus 10 s to finish; any left
-                // then (a kernel that cannot make progress) end with TIMEOUT so
-                // that stopping always returns.
-                if (stop_deadline == 0.0) stop_deadline = now_us() + 1e7 + double(s->cfg.idle_us);
-                if (now_us() > stop_deadline && !busy_batch) {
-                    const double t = now_us();
-                    auto fail = [&](uint64_t ticket) {
-                        Request& q = s->at(ticket);
-                        q.status = HNSW_ERR_TIMEOUT;
-                        q.count = 0;
-                        q.t_done = t;
-                        q.state = ReqState::Done;
-                    };
-                    for (uint64_t pos : s->ring.inflight) fail(s->ring.ticket_of[pos % s->ring.cap]);
-                    for (uint64_t ticket : s->pending) fail(ticket);
-                    for (uint64_t ticket : retry) fail(ticket);
-                    s->ring.inflight.clear();
-                    s->pending.clear();
-                    retry.clear();
-                    s->error = HNSW_ERR_TIMEOUT;
-                    s->cv_done.notify_all();
-                    break;
-                }
-            }
-            if (!any) {
-                if (s->ring.inflight.empty() && s->pending.empty() && !busy_batch && retry.empty()) {
-                    s->cv_work.wait_for(lock, std::chrono::milliseconds(2));
-                } else {
-                    lock.unlock();
-                    std::this_thread::sleep_for(std::chrono::microseconds(5));
-                }
-            }
-            continue;
-        }
         // Retire finished batches.
         bool retired = false;
         int inflight = 0;
@@ -558,8 +279,6 @@ void hnsw_server_config_default(hnsw_server_config* c) {
     c->filter_bank = nullptr;
     c->filter_count = 0;
     c->mode = HNSW_MODE_PERSISTENT;
-    c->resident = 0;
-    c->idle_us = 20000;
 }
 
 int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_in, hnsw_gpu_server** out) {
@@ -613,57 +332,6 @@ int hnsw_gpu_server_start(hnsw_gpu_index* index, const hnsw_server_config* cfg_i
         CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_count), b.h_count, 0), "mapped counts");
         CU(cudaHostGetDevicePointer(reinterpret_cast<void**>(&b.d_status), b.h_status, 0), "mapped statuses");
     }
-    if (cfg.resident) {
-        ResidentRing& R = s->ring;
-        if (!s->cfg.idle_us) s->cfg.idle_us = 20000;
-        if (s->cap > (uint64_t(1) << 30)) return set_error(HNSW_ERR_INVALID_ARGUMENT, "ring too large");
-        R.cap = uint32_t(s->cap);
-        const size_t C = R.cap;
-        CU(cudaHostAlloc(&R.h_q, C * s->dim * 4, cudaHostAllocMapped), "mapped ring queries");
-        CU(cudaHostAlloc(&R.h_k, C * 4, cudaHostAllocMapped), "mapped ring k");
-        CU(cudaHostAlloc(&R.h_ef, C * 4, cudaHostAllocMapped), "mapped ring ef");
-        CU(cudaHostAlloc(&R.h_fid, C * 4, cudaHostAllocMapped), "mapped ring filters");
-        CU(cudaHostAlloc(&R.h_tail, 64, cudaHostAllocMapped), "mapped ring tail");
-        CU(cudaHostAlloc(&R.h_stop, 64, cudaHostAllocMapped), "mapped ring stop");
-        CU(cudaHostAlloc(&R.h_keys, C * cfg.max_k * 8, cudaHostAllocMapped), "mapped ring keys");
-        CU(cudaHostAlloc(&R.h_dist, C * cfg.max_k * 4, cudaHostAllocMapped), "mapped ring dist");
-        CU(cudaHostAlloc(&R.h_count, C * 4, cudaHostAllocMapped), "mapped ring counts");
-        CU(cudaHostAlloc(&R.h_status, C * 4, cudaHostAllocMapped), "mapped ring statuses");
-        *reinterpret_cast<volatile uint64_t*>(R.h_tail) = 0;
-        *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 0;
-        for (size_t i = 0; i < C; ++i) {
-            R.h_status[i] = kUnpublished;
-            R.h_k[i] = 0;
-            R.h_ef[i] = 0;
-            R.h_fid[i] = -1;
-        }
-        std::memset(R.h_q, 0, C * s->dim * 4);
-        R.ticket_of.assign(C, 0);
-        const uint32_t ef_max = std::max(cfg.max_ef, cfg.max_k);
-        R.geo = pick_geometry(ef_max, index->view.dp, index->view.dc, true, cfg.filter_count > 0);
-        R.geo.stage_rows = 0;
-        CU(serve_warps(R.geo, index->view.dp, index->view.dc, index->num_sms, &R.warps), "serving occupancy");
-        int r = index->slots.acquire(&R.slot);
-        if (r != HNSW_OK) return r;
-        Slot* sl = R.slot;
-        const uint32_t n = index->view.n;
-        const uint32_t words = ((n + 31) / 32 + 3) & ~3u;
-        const uint32_t tab_cap = (n + kColdChunk - 1) / kColdChunk + 2;
-        const uint64_t want = std::max<uint64_t>((uint64_t(n) * 8 + kColdChunk - 1) / kColdChunk, uint64_t(R.warps) * 32);
-        const uint32_t chunks = uint32_t(std::min<uint64_t>(want, 1u << 18));
-        CU(sl->spill_bits.ensure(size_t(R.warps) * words * 4), "cudaMalloc serving spill bitmaps");
-        CU(cudaMemset(sl->spill_bits.p, 0, sl->spill_bits.bytes), "memset serving spill bitmaps");
-        CU(sl->cold_pool.ensure(size_t(chunks) * kColdChunk * 8), "cudaMalloc serving cold pool");
-        CU(sl->cold_tab.ensure(size_t(R.warps) * tab_cap * 4), "cudaMalloc serving chunk tables");
-        CU(R.words.ensure(32), "cudaMalloc serving words");
-        CU(cudaMemset(R.words.p, 0, 32), "memset serving words");
-        CU(R.wq.ensure(size_t(R.warps) * s->dim * 4), "cudaMalloc staging queries");
-        CU(R.wk.ensure(size_t(R.warps) * 4), "cudaMalloc staging k");
-        CU(R.wef.ensure(size_t(R.warps) * 4), "cudaMalloc staging ef");
-        CU(R.wfu.ensure(size_t(R.warps)), "cudaMalloc staging filter flags");
-        CU(R.wfid.ensure(size_t(R.warps) * 4), "cudaMalloc staging filter ids");
-        CU(cudaEventCreateWithFlags(&R.done, cudaEventDisableTiming), "serving event");
-    }
     hnsw_gpu_server* raw = s.get();
     raw->dispatcher = std::thread(dispatch_loop, raw);
     *out = s.release();
@@ -679,19 +347,6 @@ void hnsw_gpu_server_stop(hnsw_gpu_server* s) {
     s->cv_work.notify_all();
     if (s->dispatcher.joinable()) s->dispatcher.join();
     DeviceGuard dg(s->index->device);
-    ResidentRing& R = s->ring;
-    if (R.h_stop) {
-        // The kernel leaves at the stop word, or after its idle budget.
-        *reinterpret_cast<volatile uint32_t*>(R.h_stop) = 1;
-        std::atomic_thread_fence(std::memory_order_seq_cst);
-        if (R.done) cudaEventSynchronize(R.done);
-    }
-    if (R.done) cudaEventDestroy(R.done);
-    for (void* p : {(void*)R.h_q, (void*)R.h_k, (void*)R.h_ef, (void*)R.h_fid, (void*)R.h_tail, (void*)R.h_stop,
-                    (void*)R.h_keys, (void*)R.h_dist, (void*)R.h_count, (void*)R.h_status})
-        if (p) cudaFreeHost(p);
-    for (DBuf* b : {&R.words, &R.wq, &R.wk, &R.wef, &R.wfu, &R.wfid}) b->release();
-    if (R.slot) s->index->slots.release(R.slot);
     for (BatchSlot& b : s->batches) {
         if (b.done) cudaEventDestroy(b.done);
         for (void* p : {(void*)b.h_q, (void*)b.h_ks, (void*)b.h_efs, (void*)b.h_fused, (void*)b.h_fids,

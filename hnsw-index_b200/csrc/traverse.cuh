@@ -23,6 +23,8 @@
 
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "device.hpp"
 #include "warp_sort.cuh"
@@ -41,6 +43,7 @@ struct Counters {
 struct Ws {
     float* qf;         // dp floats: prepared query
     int8_t* qc;        // dc bytes: query code
+    uint4* qt;         // tensor-core traversal: the query's BF16 operands (hi, then lo)
     uint64_t* R;       // ef_cap + 1
     uint64_t* C;       // cand_cap + 1
     uint32_t* H;       // hash_cap entries, or a bitmap when bitmap_mode
@@ -109,6 +112,7 @@ struct QueryCtx {
     bool quant;
     float s2;
     int qnorm;  // squared norm of the query code (L2 on codes)
+    float qn2;  // squared f32 norm of the prepared query (tensor-core L2)
     bool use_filter;
     bool by_node;
     const uint64_t* fbits;
@@ -129,7 +133,113 @@ __device__ __forceinline__ bool admit(const QueryCtx& c, uint32_t id) {
 // DK_L2 and DK_DOT are f32 rows loaded directly with the L2 sum or the dot
 // sum (inner product, cosine), so the kernel carries one distance loop
 // instead of all of them: less code in the traversal loop to fetch.
-constexpr int DK_ANY = 0, DK_L2 = 1, DK_DOT = 2;
+// DK_TC1 and DK_TC3 compute the distances of each neighbor list on the
+// tensor cores (BF16, or the 3-term hi/lo split) for the tensor-core
+// traversal; the results are re-ranked with exact f32 distances.
+constexpr int DK_ANY = 0, DK_L2 = 1, DK_DOT = 2, DK_TC1 = 3, DK_TC3 = 4;
+__host__ __device__ constexpr bool is_tc(int dk) { return dk == DK_TC1 || dk == DK_TC3; }
+
+// Position (in BF16 values) of dimension d in a tensor-core row: within each
+// block of 32 values, lane t of an mma quad reads one 16-byte word holding
+// k = 2t, 2t+1, 2t+8, 2t+9 of the block's first 16 dimensions, then the
+// same of its second 16 (the A/B fragment order of mma.m16n8k16).
+__host__ __device__ __forceinline__ uint32_t tc_row_pos(uint32_t d) {
+    const uint32_t o = d & 31u, kb = o >> 4, r = o & 15u;
+    return (d & ~31u) + 8u * ((r & 7u) >> 1) + 4u * kb + 2u * (r >> 3) + (r & 1u);
+}
+
+// D += A.B for one m16n8k16 tile: BF16 operands, FP32 accumulation.
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Distances of the neighbors at the list positions in F (lane p holds the
+// id at position p) on the tensor cores, into w.fd[p]. The 32 positions are
+// the rows of two 16-row A tiles and the query is every column of B, so one
+// m16n8k16 per 16 dimensions and tile. Lane (g, t) = (lane / 4, lane % 4)
+// loads positions g, g+8, g+16, g+24, one 16-byte word per 32 dimensions of
+// each (tc_row_pos); the dot of position p ends in lane 4 (p % 8) + p / 8.
+// X3 adds x_hi.q_lo and x_lo.q_hi to x_hi.q_hi. L2 uses |q|^2 + |x|^2 - 2 q.x.
+template <bool X3>
+__device__ __forceinline__ void tc_chunk_distances(QueryCtx& c, uint32_t my_id, uint32_t F) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t stride = ix.dt >> 3, blocks = ix.dt >> 5;
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    size_t off[4];
+    bool on[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t id = __shfl_sync(kFull, my_id, g + 8 * j);
+        on[j] = (F >> (g + 8 * j)) & 1u;
+        off[j] = size_t(on[j] ? id : 0u) * stride + uint32_t(t);
+    }
+    float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
+    for (uint32_t b = 0; b < blocks; ++b) {
+        uint4 x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = on[j] ? __ldg(ix.tc_hi + off[j] + 4u * b) : z;
+        const uint4 q = w.qt[4u * b + uint32_t(t)];
+        mma_bf16_16816(acc0, x[0].x, x[1].x, x[0].y, x[1].y, q.x, q.y);
+        mma_bf16_16816(acc1, x[2].x, x[3].x, x[2].y, x[3].y, q.x, q.y);
+        mma_bf16_16816(acc0, x[0].z, x[1].z, x[0].w, x[1].w, q.z, q.w);
+        mma_bf16_16816(acc1, x[2].z, x[3].z, x[2].w, x[3].w, q.z, q.w);
+        if constexpr (X3) {
+            const uint4 ql = w.qt[stride + 4u * b + uint32_t(t)];
+            mma_bf16_16816(acc0, x[0].x, x[1].x, x[0].y, x[1].y, ql.x, ql.y);
+            mma_bf16_16816(acc1, x[2].x, x[3].x, x[2].y, x[3].y, ql.x, ql.y);
+            mma_bf16_16816(acc0, x[0].z, x[1].z, x[0].w, x[1].w, ql.z, ql.w);
+            mma_bf16_16816(acc1, x[2].z, x[3].z, x[2].w, x[3].w, ql.z, ql.w);
+            uint4 y[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) y[j] = on[j] ? __ldg(ix.tc_lo + off[j] + 4u * b) : z;
+            mma_bf16_16816(acc0, y[0].x, y[1].x, y[0].y, y[1].y, q.x, q.y);
+            mma_bf16_16816(acc1, y[2].x, y[3].x, y[2].y, y[3].y, q.x, q.y);
+            mma_bf16_16816(acc0, y[0].z, y[1].z, y[0].w, y[1].w, q.z, q.w);
+            mma_bf16_16816(acc1, y[2].z, y[3].z, y[2].w, y[3].w, q.z, q.w);
+        }
+    }
+    // acc0[0] / acc0[2]: positions g / g+8; acc1[0] / acc1[2]: g+16 / g+24.
+    const float v = t == 0 ? acc0[0] : t == 1 ? acc0[2] : t == 2 ? acc1[0] : acc1[2];
+    const float dot = __shfl_sync(kFull, v, 4 * (lane & 7) + (lane >> 3));
+    if ((F >> lane) & 1u) {
+        float d;
+        if (c.metric == 0) d = c.qn2 + __ldg(ix.xnorm + my_id) - 2.0f * dot;
+        else d = metric_from_sum(c.metric, dot);
+        w.fd[lane] = d;
+    }
+    __syncwarp();
+}
+
+// The query's BF16 operands (hi, and for X3 lo = bf16(q - hi)) in the
+// tensor-core row order, and its squared norm; all lanes call after prepare.
+template <bool X3>
+__device__ __forceinline__ void tc_prepare_query(QueryCtx& c) {
+    const DeviceIndexView& ix = c.a->ix;
+    Ws& w = *c.w;
+    const int lane = lane_id();
+    __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(w.qt);
+    __nv_bfloat16* lo = hi + ix.dt;
+    float sq = 0.0f;
+    for (uint32_t d = lane; d < ix.dt; d += 32) {
+        const float x = d < ix.dim ? w.qf[d] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[tc_row_pos(d)] = h;
+        if (X3) lo[tc_row_pos(d)] = __float2bfloat16_rn(__fsub_rn(x, __bfloat162float(h)));
+        sq = __fadd_rn(sq, __fmul_rn(x, x));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sq = __fadd_rn(sq, __shfl_xor_sync(kFull, sq, off));
+    c.qn2 = sq;
+    __syncwarp();
+}
 
 // Distance from the query to node `id` for the group of 8 lanes (valid in
 // every lane of the group). All 32 lanes call; `id` may differ per group.
@@ -182,6 +292,10 @@ __device__ __forceinline__ void chunk_distances(QueryCtx& c, uint32_t my_id, uin
     Ws& w = *c.w;
     const int lane = lane_id();
     const int g = lane >> 3, g8 = lane & 7;
+    if constexpr (is_tc(DK)) {
+        tc_chunk_distances<DK == DK_TC3>(c, my_id, F);
+        return;
+    }
     const bool stage = DK == DK_ANY && w.stage != nullptr;
     // Ranks of fresh lanes -> compact list of positions.
     if ((F >> lane) & 1u) {
@@ -327,7 +441,7 @@ __device__ __forceinline__ void cold_reset(Ws& w) {
 
 // Appends the entries x of the lanes in S to the cold list. Returns false
 // when the pool has no chunk left. All lanes call.
-__device__ bool cold_append(Ws& w, uint32_t S, uint64_t x) {
+static __device__ bool cold_append(Ws& w, uint32_t S, uint64_t x) {
     const int lane = lane_id();
     const uint32_t n = __popc(S);
     if (n == 0) return true;
@@ -428,7 +542,7 @@ __device__ __forceinline__ void cold_load4(const Ws& w, uint32_t b, uint64_t (&v
 // exist (`full`), cold entries worse than the worst result are dropped
 // first: they can never be expanded. The 64 words at w.fr serve as the
 // histogram of a radix selection of the cut.
-__device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, float worst) {
+static __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, float worst) {
     const int lane = lane_id();
     const uint32_t lt = (1u << lane) - 1u;
     head = tail = 0;
@@ -566,7 +680,7 @@ __device__ void cold_refill(Ws& w, uint32_t& head, uint32_t& tail, bool full, fl
 // COLD: the cold list is compiled in (retry kernels, and the fast kernel's
 // variant for batches whose queues outgrow shared memory, e.g. selective
 // filters); without it the hot loop keeps fewer registers live.
-template <bool COLD>
+template <bool COLD, int DK = DK_ANY>
 __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
@@ -624,14 +738,19 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                 w.spilled_bits = true;
             }
             const bool fresh = valid && visit(w, id);
-            if (fresh && !w.stage) {
+            if (is_tc(DK)) {
+                if (fresh) {
+                    prefetch_l2(ix.tc_hi + size_t(id) * (ix.dt >> 3), ix.dt * 2);
+                    if (DK == DK_TC3) prefetch_l2(ix.tc_lo + size_t(id) * (ix.dt >> 3), ix.dt * 2);
+                }
+            } else if (fresh && !w.stage) {
                 if (c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
                 else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
             }
             const uint32_t F = __ballot_sync(kFull, fresh);
             visited += __popc(F);
             if (F != 0) {
-                chunk_distances(c, id, F);
+                chunk_distances<DK>(c, id, F);
                 c.cnt.dist0 += __popc(F);
                 const bool adm = fresh && admit(c, id);
                 const uint32_t A = __ballot_sync(kFull, adm);
@@ -821,7 +940,12 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
                 w.spilled_bits = true;
             }
             const bool fresh = valid && visit(w, id);
-            if (fresh && (DK != DK_ANY || !w.stage)) {
+            if (is_tc(DK)) {
+                if (fresh) {
+                    prefetch_l2(ix.tc_hi + size_t(id) * (ix.dt >> 3), ix.dt * 2);
+                    if (DK == DK_TC3) prefetch_l2(ix.tc_lo + size_t(id) * (ix.dt >> 3), ix.dt * 2);
+                }
+            } else if (fresh && (DK != DK_ANY || !w.stage)) {
                 if (DK == DK_ANY && c.quant) prefetch_l2(ix.codes + size_t(id) * ix.dc, ix.dc);
                 else prefetch_l2(ix.vec + size_t(id) * ix.dp, ix.dp * 4);
             }
@@ -909,7 +1033,7 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
 // advised by src/hnsw/mod.rs:421-425): every admitted live node gets its f32
 // distance in the reference kernel order, and the best ef by (distance, id)
 // stay in w.R; the caller sorts them by (distance, key). Returns the count.
-__device__ int exact_scan(QueryCtx& c, uint32_t ef) {
+static __device__ int exact_scan(QueryCtx& c, uint32_t ef) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
     const int lane = lane_id();
@@ -952,7 +1076,7 @@ __device__ int exact_scan(QueryCtx& c, uint32_t ef) {
 // Prepares the query (vector::check + normalisation, src/vector.rs:22-45,
 // 90-104; and the int8 code, src/quantization.rs:73-81) into the workspace.
 // Returns a status.
-__device__ int32_t prepare(QueryCtx& c, const float* q) {
+static __device__ int32_t prepare(QueryCtx& c, const float* q) {
     const DeviceIndexView& ix = c.a->ix;
     Ws& w = *c.w;
     const int lane = lane_id();
@@ -1024,6 +1148,9 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
     uint32_t count = 0;
     int32_t st = prepare(c, a.queries + size_t(qi) * ix.dim);
     if (st == ST_OK && a.quantized && !ix.quantized) st = ST_QDISABLED;
+    if constexpr (is_tc(DK)) {
+        if (st == ST_OK) tc_prepare_query<DK == DK_TC3>(c);
+    }
     if (st == ST_OK && k != 0 && ix.live != 0 && ix.entry != kEmpty) {
         ef = max(ef, k);
         if (ef > w.ef_cap) return ST_OVERFLOW;
@@ -1033,7 +1160,10 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
         } else {
             // search_graph (src/hnsw/search.rs:146-161)
             float d0;
-            {
+            if constexpr (is_tc(DK)) {
+                chunk_distances<DK>(c, lane == 0 ? ix.entry : 0u, 1u);
+                d0 = w.fd[0];
+            } else {
                 const int g8 = lane & 7;
                 d0 = group_distance<DK>(c, ix.entry, g8);
             }
@@ -1041,11 +1171,12 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
             uint64_t ep = pack(d0, ix.entry);
             for (uint32_t layer = ix.top; layer >= 1; --layer) ep = greedy_layer<DK>(c, ep, layer);
             if constexpr (V == 2) rs = layer0_single<DK>(c, ep, ef);
-            else rs = layer0<V == 1>(c, ep, ef);
+            else rs = layer0<V == 1, DK>(c, ep, ef);
             if (rs < 0) return ST_OVERFLOW;
         }
-        // Quantized: exact distances for the survivors (src/hnsw/mod.rs:494-498).
-        if (c.quant) {
+        // Quantized or tensor-core traversal: exact distances for the
+        // survivors (src/hnsw/mod.rs:494-498).
+        if (c.quant || is_tc(DK)) {
             const int g = lane >> 3, g8 = lane & 7;
             for (int r = 0; r < rs; r += 4) {
                 int slot = r + g;
@@ -1104,20 +1235,23 @@ __host__ __device__ __forceinline__ size_t align_up(size_t x, size_t a) { return
 // (results + candidates: about 25 KB per warp at 1024).
 __host__ __device__ __forceinline__ bool retry_shared_heaps(uint32_t ef_cap) { return ef_cap <= 1024; }
 
-__host__ __device__ __forceinline__ size_t retry_bytes_per_warp(uint32_t dp, uint32_t dc, uint32_t ef_cap) {
-    size_t b = align_up(size_t(dp) * 4, 16) + align_up(size_t(dc), 16) + 256;
+__host__ __device__ __forceinline__ size_t retry_bytes_per_warp(uint32_t dp, uint32_t dc, uint32_t ef_cap,
+                                                                uint32_t tcb = 0) {
+    size_t b = align_up(size_t(dp) * 4, 16) + align_up(size_t(dc), 16) + 256 + align_up(size_t(tcb), 16);
     if (retry_shared_heaps(ef_cap))
         b += align_up(size_t(ef_cap + 1) * 8, 16) + align_up(size_t(2 * ef_cap + 32 + 1) * 8, 16);
     return b;
 }
 
-__device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const SearchGeometry& g) {
+static __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const SearchGeometry& g) {
     const uint32_t ef_cap = g.ef_cap, cand_cap = g.cand_cap, hash_cap = g.hash_cap;
     size_t off = 0;
     w.qf = reinterpret_cast<float*>(base + off);
     off = align_up(off + size_t(ix.dp) * 4, 16);
     w.qc = reinterpret_cast<int8_t*>(base + off);
     off = align_up(off + size_t(ix.dc), 16);
+    w.qt = reinterpret_cast<uint4*>(base + off);
+    off = align_up(off + size_t(g.tc_bytes), 16);
     w.R = reinterpret_cast<uint64_t*>(base + off);
     off = align_up(off + size_t(ef_cap + 1) * 8, 16);
     w.C = reinterpret_cast<uint64_t*>(base + off);
@@ -1165,7 +1299,7 @@ __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const Search
 }
 
 // Gives the warp its cold-list row of the pool (`slot` < cold_slots).
-__device__ void attach_cold(Ws& w, const SearchArgs& a, uint32_t slot, uint32_t* next) {
+static __device__ void attach_cold(Ws& w, const SearchArgs& a, uint32_t slot, uint32_t* next) {
     if (!a.cold_pool || slot >= a.cold_slots) return;
     w.pool = a.cold_pool;
     w.pool_next = next;
@@ -1176,7 +1310,7 @@ __device__ void attach_cold(Ws& w, const SearchArgs& a, uint32_t slot, uint32_t*
 }
 
 // Clears a spill bitmap and points the workspace back at shared memory.
-__device__ void end_spill(Ws& w) {
+static __device__ void end_spill(Ws& w) {
     const int lane = lane_id();
     if (w.spilled_bits) {
         uint4* b = reinterpret_cast<uint4*>(w.spill_bits);
@@ -1253,19 +1387,21 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     // Query vectors and small buffers in shared memory, then the heaps when
     // they fit; the visited set in global memory.
     const bool sh = retry_shared_heaps(a.g_ef_cap);
-    const size_t per = retry_bytes_per_warp(ix.dp, ix.dc, a.g_ef_cap);
+    const uint32_t tcb = tc_query_bytes(a);
+    const size_t per = retry_bytes_per_warp(ix.dp, ix.dc, a.g_ef_cap, tcb);
     char* base = smem + size_t(warp) * per;
     w.qf = reinterpret_cast<float*>(base);
     w.qc = reinterpret_cast<int8_t*>(base + align_up(size_t(ix.dp) * 4, 16));
     w.fr = reinterpret_cast<uint32_t*>(base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16));
     w.fd = reinterpret_cast<float*>(w.fr + 32);
+    w.qt = reinterpret_cast<uint4*>(base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256);
     w.stage = nullptr;
     w.stage_rows = 0;
     w.stage_row_bytes = 0;
     w.fi = nullptr;
     w.fnorm = nullptr;
     if (sh) {
-        char* heaps = base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256;
+        char* heaps = base + align_up(size_t(ix.dp) * 4, 16) + align_up(size_t(ix.dc), 16) + 256 + align_up(size_t(tcb), 16);
         w.R = reinterpret_cast<uint64_t*>(heaps);
         w.C = reinterpret_cast<uint64_t*>(heaps + align_up(size_t(a.g_ef_cap + 1) * 8, 16));
         w.cand_cap = 2 * a.g_ef_cap + 32;

@@ -105,6 +105,16 @@ class Metric(enum.IntEnum):
     Cosine = 2
 
 
+class Traversal(enum.IntEnum):
+    """hnsw_search_opts.traversal: distances while the graph is walked. F32
+    is the reference's search bit for bit; BF16 / BF16X3 use the tensor cores
+    and re-rank the ef results with exact f32 distances."""
+
+    F32 = 0
+    BF16 = 1
+    BF16X3 = 2
+
+
 class Neighbor(NamedTuple):
     """Neighbor (src/neighbor.rs:7-12)."""
 
@@ -131,7 +141,7 @@ class _Opts(C.Structure):
         ("quantized", C.c_int32), ("filter_bits", C.c_void_p), ("filter_nbits", C.c_uint64),
         ("filter_stride", C.c_uint64), ("filter_used", C.c_void_p), ("out_stride", C.c_uint32),
         ("mode", C.c_int32), ("filter_ids", C.c_void_p), ("filter_by_node", C.c_int32),
-        ("exact_below", C.c_float),
+        ("exact_below", C.c_float), ("traversal", C.c_int32),
     ]
 
 
@@ -444,7 +454,7 @@ class HnswIndex:
 
     @staticmethod
     def _opts(nq, k, ef, quantized=False, filter_bits=None, filter_nbits=0, filter_stride=0, filter_used=None,
-              ks=None, efs=None, mode=0, filter_ids=None, filter_by_node=False, exact_below=0.0):
+              ks=None, efs=None, mode=0, filter_ids=None, filter_by_node=False, exact_below=0.0, traversal=0):
         """hnsw_search_opts for a batch, and the arrays it points into (keep them alive)."""
         ks_a = None if ks is None else np.ascontiguousarray(ks, dtype=np.uint32)
         efs_a = None if efs is None else np.ascontiguousarray(efs, dtype=np.uint32)
@@ -463,6 +473,7 @@ class HnswIndex:
         o.filter_ids = _ptr(fi)
         o.filter_by_node = int(filter_by_node)
         o.exact_below = float(exact_below)
+        o.traversal = int(traversal)
         o.out_stride = max(kmax, 1)
         o.mode = mode
         return o, (ks_a, efs_a, fb, fu, fi)
@@ -472,9 +483,11 @@ class HnswIndex:
                       filter_stride: int = 0, filter_used: Optional[np.ndarray] = None,
                       ks: Optional[np.ndarray] = None, efs: Optional[np.ndarray] = None,
                       mode: int = 0, raise_on_error: bool = True, filter_ids: Optional[np.ndarray] = None,
-                      filter_by_node: bool = False, exact_below: float = 0.0):
+                      filter_by_node: bool = False, exact_below: float = 0.0, traversal: int = 0):
         """Batched search returning arrays (keys, dist, count, status).
-        exact_below > 0 turns on the selectivity planner (hnsw_search_opts)."""
+        exact_below > 0 turns on the selectivity planner; traversal
+        (Traversal.BF16 / BF16X3) walks the graph with tensor-core distances
+        and re-ranks with exact f32 ones (hnsw_search_opts)."""
         q = np.ascontiguousarray(queries, dtype=np.float32)
         if q.ndim == 1:
             if q.size % max(self.dim(), 1):
@@ -484,7 +497,8 @@ class HnswIndex:
         nq, dim = q.shape
         o, keep = self._opts(nq, k, ef, quantized=quantized, filter_bits=filter_bits, filter_nbits=filter_nbits,
                              filter_stride=filter_stride, filter_used=filter_used, ks=ks, efs=efs, mode=mode,
-                             filter_ids=filter_ids, filter_by_node=filter_by_node, exact_below=exact_below)
+                             filter_ids=filter_ids, filter_by_node=filter_by_node, exact_below=exact_below,
+                             traversal=traversal)
         stride = o.out_stride
         keys = np.zeros((nq, stride), dtype=np.uint64)
         dist = np.zeros((nq, stride), dtype=np.float32)
@@ -596,11 +610,12 @@ class HnswIndex:
 
     def search_device(self, d_queries: int, nq: int, k: int, ef: int, d_keys: int, d_dist: int,
                       d_count: int, d_status: int, stream: Optional[int] = None, quantized: bool = False,
-                      mode: int = 0, out_stride: int = 0):
+                      mode: int = 0, out_stride: int = 0, traversal: int = 0):
         """hnsw_gpu_search_batch_device with raw device pointers."""
         o = _Opts()
         o.k, o.ef = k, ef
         o.quantized = int(quantized)
+        o.traversal = int(traversal)
         o.out_stride = out_stride or k
         o.mode = mode
         # stream None = the library's own stream; 0 = the legacy default stream.
@@ -613,8 +628,7 @@ class _ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("max_inflight", C.c_uint32), ("max_pending", C.c_uint32),
                 ("max_k", C.c_uint32), ("max_ef", C.c_uint32), ("linger_us", C.c_uint32),
                 ("filter_nbits", C.c_uint64), ("quantized", C.c_int32), ("filter_bank", C.c_void_p),
-                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32), ("mode", C.c_int32),
-                ("resident", C.c_int32), ("idle_us", C.c_uint32)]
+                ("filter_count", C.c_uint32), ("filter_by_node", C.c_int32), ("mode", C.c_int32)]
 
 
 _lib.hnsw_server_config_default.argtypes = [C.POINTER(_ServerConfig)]
@@ -631,13 +645,11 @@ _lib.hnsw_gpu_server_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c
 
 
 class Server:
-    """Request loop over a resident HnswIndex: continuous batching, or with
-    resident=True a resident serving kernel whose warps take requests one at
-    a time from a ring as they arrive."""
+    """Request loop over a resident HnswIndex: continuous batching."""
 
     def __init__(self, index: HnswIndex, *, max_batch=2048, max_inflight=4, max_pending=1 << 16, max_k=100,
                  max_ef=512, linger_us=100, filter_nbits=0, filter_bank: Optional[np.ndarray] = None,
-                 quantized=False, filter_by_node=False, mode=1, resident=False, idle_us=20000):
+                 quantized=False, filter_by_node=False, mode=1):
         cfg = _ServerConfig()
         _lib.hnsw_server_config_default(C.byref(cfg))
         cfg.max_batch, cfg.max_inflight, cfg.max_pending = max_batch, max_inflight, max_pending
@@ -645,7 +657,6 @@ class Server:
         cfg.filter_nbits, cfg.quantized = filter_nbits, int(quantized)
         cfg.filter_by_node = int(filter_by_node)
         cfg.mode = int(mode)
-        cfg.resident, cfg.idle_us = int(resident), idle_us
         bank = None if filter_bank is None else np.ascontiguousarray(filter_bank, np.uint64)
         if bank is not None:
             cfg.filter_bank = _ptr(bank)

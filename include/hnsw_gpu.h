@@ -124,7 +124,22 @@ typedef struct hnsw_search_opts {
                                    documentation advises for very selective filters
                                    (src/hnsw/mod.rs:421-425). Needs node bitmaps, or keys equal to
                                    node ids; other queries are unaffected */
+    int32_t traversal;          /* HNSW_TRAVERSAL_*: how distances are computed while the graph is
+                                   walked. F32 (0, default) is the reference's search, bit for bit.
+                                   BF16 (1) and BF16X3 (2) compute each neighbor list's distances on
+                                   the tensor cores (BF16 operands, FP32 accumulation; X3 adds the
+                                   two cross terms of the hi/lo split), then re-rank the ef results
+                                   with exact f32 distances, as the quantized search re-ranks its int8
+                                   traversal (src/hnsw/mod.rs:494-498). Results carry exact
+                                   distances; the walk may differ from the f32 one where distances
+                                   nearly tie. Not combined with `quantized` */
 } hnsw_search_opts;
+
+enum {
+    HNSW_TRAVERSAL_F32 = 0,
+    HNSW_TRAVERSAL_BF16 = 1,
+    HNSW_TRAVERSAL_BF16X3 = 2
+};
 
 enum {
     HNSW_MODE_PLAIN = 0,      /* one warp per query, one launch per call */
@@ -241,15 +256,6 @@ typedef struct hnsw_server_config {
     int32_t filter_by_node; /* the bank's bitmaps are indexed by node id, not key */
     int32_t mode;           /* HNSW_MODE_* of the batches; default PERSISTENT (the device work queue
                                spreads a small batch's queries over every SM); AUTO uses the tuned mode */
-    int32_t resident;       /* 1: a resident serving kernel instead of batches. Requests go into a
-                               ring in mapped host memory as they are submitted; the kernel's warps
-                               (each with its own scratch, sized for max_ef and max_k) take them one
-                               at a time as they come free, so a slow query holds one warp, not a
-                               batch. Every device wait is bounded: the kernel leaves after idle_us
-                               without requests and is launched again when they come. Queries that
-                               outgrow a warp's scratch finish on the batch path's retry passes
-                               (one batch slot of max_batch queries is kept for them). */
-    uint32_t idle_us;       /* resident mode: how long the kernel waits for requests (default 20000) */
 } hnsw_server_config;
 
 void hnsw_server_config_default(hnsw_server_config* cfg);

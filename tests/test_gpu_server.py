@@ -122,85 +122,3 @@ def test_admission_rejects_when_queue_is_full(served):
         assert status == 0
     srv.stop()
     assert rejected > 0 and len(accepted) >= 16
-
-
-# Resident serving kernel: the kernel's warps take requests from the ring
-# one at a time (resident=True); the same equality with the oracle holds.
-
-def test_resident_kernel_requests_equal_oracle(served):
-    base, queries, data = served
-    gi = H.HnswIndex.from_bytes(data)
-    oi = O.Index(data)
-    nbits = 20000
-    q = queries[:300]
-    ks, efs, fids, bank = make_requests(q, nbits, 4)
-    srv = H.Server(gi, max_batch=64, max_inflight=1, filter_nbits=nbits, filter_bank=bank, resident=True)
-    try:
-        tickets = [srv.submit(q[i], int(ks[i]), int(efs[i]), int(fids[i])) for i in range(len(q))]
-        results = [srv.wait(t, timeout_ms=20000) for t in tickets]
-        launches, served_n = srv.stats()
-    finally:
-        srv.stop()
-    assert served_n == len(q) and launches >= 1
-    ref = oracle_results(oi, q, ks, efs, fids, bank, nbits)
-    for i, (keys, dist, status, lat) in enumerate(results):
-        assert status == 0
-        c = int(ref[2][i])
-        np.testing.assert_array_equal(keys, ref[0][i, :c])
-        np.testing.assert_array_equal(dist.view(np.uint32), ref[1][i, :c].view(np.uint32))
-        assert lat >= 0
-
-
-def test_resident_kernel_open_loop_and_relaunch_after_idle(served):
-    import time
-
-    base, queries, data = served
-    gi = H.HnswIndex.from_bytes(data)
-    oi = O.Index(data)
-    nbits = 20000
-    ks, efs, fids, bank = make_requests(queries, nbits, 5)
-    rng = np.random.default_rng(6)
-    arrivals = np.cumsum(rng.exponential(1e6 / 100000.0, len(queries)))  # 100k requests/s
-    # A short idle budget: the kernel leaves between the two replays and is
-    # launched again for the second.
-    srv = H.Server(gi, max_batch=64, max_inflight=1, filter_nbits=nbits, filter_bank=bank, resident=True,
-                   idle_us=2000)
-    try:
-        keys, dist, cnt, st, lat = srv.replay(queries, arrivals, ks, efs, fids)
-        time.sleep(0.05)
-        keys2, dist2, cnt2, st2, _ = srv.replay(queries[:50], arrivals[:50], ks[:50], efs[:50], fids[:50])
-        launches, served_n = srv.stats()
-    finally:
-        srv.stop()
-    assert (st == 0).all() and (st2 == 0).all()
-    assert launches >= 2 and served_n == len(queries) + 50
-    ref = oracle_results(oi, queries, ks, efs, fids, bank, nbits)
-    for i in range(len(queries)):
-        c = int(ref[2][i])
-        assert cnt[i] == c
-        np.testing.assert_array_equal(keys[i, :c], ref[0][i, :c])
-        np.testing.assert_array_equal(dist[i, :c].view(np.uint32), ref[1][i, :c].view(np.uint32))
-    for i in range(50):
-        c = int(ref[2][i])
-        np.testing.assert_array_equal(keys2[i, :c], ref[0][i, :c])
-
-
-def test_resident_kernel_with_tombstones_and_int8():
-    base, queries = H.mixture(8000, 200, 24, 20, 0.4, 41)
-    dead = list(range(0, 8000, 13))
-    data = build_index(base, metric=1, m=12, seed=5, deleted_keys=dead, quantize=True)
-    gi = H.HnswIndex.from_bytes(data)
-    oi = O.Index(data)
-    srv = H.Server(gi, max_batch=32, max_inflight=1, max_k=20, max_ef=128, quantized=True, resident=True)
-    try:
-        tickets = [srv.submit(queries[i], 10, 40 + (i % 5) * 20) for i in range(len(queries))]
-        results = [srv.wait(t, timeout_ms=20000) for t in tickets]
-    finally:
-        srv.stop()
-    for i, (keys, dist, status, _) in enumerate(results):
-        ref = oi.search(queries[i:i + 1], 10, 40 + (i % 5) * 20, quantized=True)
-        assert status == 0
-        c = int(ref[2][0])
-        np.testing.assert_array_equal(keys, ref[0][0, :c])
-        np.testing.assert_array_equal(dist.view(np.uint32), ref[1][0, :c].view(np.uint32))
-        assert not np.isin(keys, np.array(dead, np.uint64)).any()
