@@ -132,6 +132,27 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
           "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) asm volatile("" : "+r"(v[i]));
+}
+// tcgen05.ld without the wait: the registers are valid only after
+// tmem_wait_regs on the same array.
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+// Waits for this thread's tcgen05.ld and re-defines v after the wait, so
+// that no use of v is scheduled before it.
+__device__ __forceinline__ void tmem_wait_regs(uint32_t (&v)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) asm volatile("" : "+r"(v[i]));
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -207,6 +228,71 @@ __device__ __forceinline__ void epilogue_tile(const TcScoreArgs& a, uint32_t tad
     }
 }
 
+// Candidate-mode staging: per epilogue warp kStageDepth entries per lane in
+// shared memory, entry i of lane l at [i * 32 + l] (consecutive lanes hit
+// consecutive words).
+constexpr uint32_t kStageDepth = 16;
+constexpr uint32_t kStageBytesPerWarp = kStageDepth * 32 * 8;  // 4 KB
+
+// Appends this lane's n staged entries to its query's candidates (one
+// reservation). Out of line: the per-entry path calls it only when a lane
+// has staged kStageDepth entries of one tile.
+__device__ __noinline__ void flush_stage(const TcScoreArgs& a, const uint64_t* stage, uint32_t q, uint32_t n) {
+    const int lane = threadIdx.x & 31;
+    uint32_t slot = atomicAdd(a.cand_count + q, n);
+    for (uint32_t i = 0; i < n; ++i, ++slot)
+        if (slot < a.cand_cap) a.cand[size_t(q) * a.cand_cap + slot] = stage[i * 32 + lane];
+}
+
+// The 32 accumulator columns v (rows row0 .. row0 + 31) of this lane's query:
+// entries at or below the threshold go to the lane's staging slots.
+__device__ __forceinline__ void stage_chunk(const TcScoreArgs& a, const uint32_t (&v)[32], uint32_t row0, bool qvalid,
+                                            float thr, float qn, uint64_t* stage, uint32_t q, uint32_t& n) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const uint32_t row = row0 + uint32_t(j);
+        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
+        if (qvalid && row < a.n && dist <= thr) {
+            if (n == kStageDepth) {
+                flush_stage(a, stage, q, n);
+                n = 0;
+            }
+            stage[n * 32 + uint32_t(lane)] = (uint64_t(__float_as_uint(dist)) << 32) | row;
+            ++n;
+        }
+    }
+}
+
+// Candidate mode, one pass: the accumulator's eight 32-column chunks are
+// read with the next load in flight while the current chunk is scanned;
+// `release` runs as soon as the last chunk is in registers (the MMA warp may
+// then reuse the accumulator), and the staged entries are appended after.
+template <typename Release>
+__device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32_t taddr, uint32_t q,
+                                                    uint32_t row_base, float thr, float qn, uint64_t* stage,
+                                                    Release release) {
+    const bool qvalid = q < a.nq;
+    uint32_t n = 0;
+    uint32_t va[32], vb[32];
+    tmem_ld32_async(taddr, va);
+    tmem_wait_regs(va);
+#pragma unroll 1
+    for (uint32_t c = 0; c < kTileN / 32; c += 2) {
+        tmem_ld32_async(taddr + (c + 1) * 32, vb);
+        stage_chunk(a, va, row_base + c * 32, qvalid, thr, qn, stage, q, n);
+        __syncwarp();
+        tmem_wait_regs(vb);
+        if (c + 2 < kTileN / 32) tmem_ld32_async(taddr + (c + 2) * 32, va);
+        else release();
+        stage_chunk(a, vb, row_base + (c + 1) * 32, qvalid, thr, qn, stage, q, n);
+        __syncwarp();
+        if (c + 2 < kTileN / 32) tmem_wait_regs(va);
+    }
+    if (n) flush_stage(a, stage, q, n);
+    __syncwarp();
+}
+
 template <bool SPLIT3>
 __global__ void __launch_bounds__(kThreads, 1)
     score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
@@ -224,6 +310,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* mma_done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    // Candidate staging of the four epilogue warps, after 256 bytes of barriers.
+    unsigned char* stage_base = smem + kStages * kStageBytes + 256;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t q_tiles = a.q_tiles;
@@ -333,18 +421,30 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else {
         // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, i.e. those query rows.
         const uint32_t lane_base = 32u * uint32_t(warp & 3);
+        uint64_t* stage = reinterpret_cast<uint64_t*>(stage_base + size_t(warp - 2) * kStageBytesPerWarp);
         uint32_t tile_it = 0;
         for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
             const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
             const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+            const uint32_t q = qt * kTileM + lane_base + uint32_t(lane);
+            // The query's threshold and norm load while the MMAs run.
+            const float thr = (q < a.nq && a.thr) ? a.thr[q] : 0.0f;
+            const float qn = (q < a.nq && a.qnorm2) ? a.qnorm2[q] : 0.0f;
             const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err, a.wait_budget));
             if (!got) break;
             tc_fence_after();
-            epilogue_tile(a, tmem_base + (lane_base << 16) + b * kTileN, qt * kTileM + lane_base + uint32_t(lane),
-                          nt * kTileN);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[b]);
+            const uint32_t taddr = tmem_base + (lane_base << 16) + b * kTileN;
+            auto release = [&]() {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[b]);
+            };
+            if (a.dense) {
+                epilogue_tile(a, taddr, q, nt * kTileN);
+                release();
+            } else {
+                epilogue_candidates(a, taddr, q, nt * kTileN, thr, qn, stage, release);
+            }
         }
     }
     tc_fence_before();
@@ -458,6 +558,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* mma_done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    // Candidate staging of the four epilogue warps, after 256 bytes of barriers.
+    unsigned char* stage_base = smem + kStages * kStageBytes + 256;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
@@ -584,20 +686,31 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     } else {
         // Epilogue (both CTAs): this CTA's 128 query rows x the tile's 256 rows.
         const uint32_t lane_base = 32u * uint32_t(warp & 3);
+        uint64_t* stage = reinterpret_cast<uint64_t*>(stage_base + size_t(warp - 2) * kStageBytesPerWarp);
         uint32_t tile_it = 0;
         for (uint32_t t = pair; t < total; t += npairs, ++tile_it) {
             const uint32_t nt = a.n_tile_begin + t / q_pairs, qp2 = t % q_pairs;
             const uint32_t b = tile_it & 1u, use = tile_it >> 1;
+            const uint32_t q = (2 * qp2 + rank) * kTileM + lane_base + uint32_t(lane);
+            const float thr = (q < a.nq && a.thr) ? a.thr[q] : 0.0f;
+            const float qn = (q < a.nq && a.qnorm2) ? a.qnorm2[q] : 0.0f;
             const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(&acc_full[b], use & 1u, a.err, a.wait_budget));
             if (!got) break;
             tc_fence_after();
-            epilogue_tile(a, tmem_base + (lane_base << 16) + b * kTileN,
-                          (2 * qp2 + rank) * kTileM + lane_base + uint32_t(lane), nt * kTileN);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                if (leader) mbar_arrive(&acc_empty[b]);
-                else mbar_arrive_remote(&acc_empty[b], 0);
+            const uint32_t taddr = tmem_base + (lane_base << 16) + b * kTileN;
+            auto release = [&]() {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    if (leader) mbar_arrive(&acc_empty[b]);
+                    else mbar_arrive_remote(&acc_empty[b], 0);
+                }
+            };
+            if (a.dense) {
+                epilogue_tile(a, taddr, q, nt * kTileN);
+                release();
+            } else {
+                epilogue_candidates(a, taddr, q, nt * kTileN, thr, qn, stage, release);
             }
         }
     }
@@ -781,7 +894,7 @@ cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B
     if (pairs) {
         const size_t smem2 = 1024 + size_t(split ? tc::Ring2<true>::kStages * tc::Ring2<true>::kStageBytes
                                                  : tc::Ring2<false>::kStages * tc::Ring2<false>::kStageBytes) +
-                             256;
+                             256 + 4 * tc::kStageBytesPerWarp;
         auto kern2 = split ? tc::score_pair_kernel<true> : tc::score_pair_kernel<false>;
         cudaError_t e2 = raise_smem_limit(reinterpret_cast<const void*>(kern2));
         if (e2 != cudaSuccess) return e2;
@@ -793,7 +906,7 @@ cudaError_t tc_score(const __nv_bfloat16* A, uint32_t qp, const __nv_bfloat16* B
     }
     const size_t smem = 1024 + size_t(split ? tc::Ring<true>::kStages * tc::Ring<true>::kStageBytes
                                             : tc::Ring<false>::kStages * tc::Ring<false>::kStageBytes) +
-                        256;
+                        256 + 4 * tc::kStageBytesPerWarp;
     auto kern = split ? tc::score_kernel<true> : tc::score_kernel<false>;
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
     if (e != cudaSuccess) return e;
