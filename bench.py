@@ -1222,9 +1222,11 @@ def run_case(args):
         bank = random_bitmaps(rng, nb, np.exp(rng.uniform(np.log(0.01), np.log(0.9), 64)))
         fids = rng.integers(0, 64, nq).astype(np.uint32)
         for _ in range(3):
+            # --case-exact-below > 0 turns on the selectivity planner
+            # (plan_kernel, and exact_scan inside the search kernel).
             r = timed_call(lambda: index.search_arrays(queries, 100, 16, quantized=True, ks=ks, efs=efs,
                                                        filter_bits=bank, filter_nbits=nb, filter_stride=words,
-                                                       filter_ids=fids, mode=1))
+                                                       filter_ids=fids, mode=1, exact_below=args.case_exact_below))
     elif args.workload == "case-retry-200kx64":
         # search_retry_kernel: a 1% filter at ef=256 in plain mode, so most
         # queries outgrow the shared scratch and finish in the retry pass.
@@ -1253,11 +1255,12 @@ def run_case(args):
         return 0
     else:  # case-brute-200kx768
         # Brute-force kernels: 200k x 768 cosine, 1000 queries, k=100; FP32
-        # twice, then BF16x3 twice.
+        # twice, then the tensor-core precision (--case-precision) twice.
         base, queries = H.mixture_split(200_000, 1000, 768, 4096, 0.5, 3, 4)
         bf = H.BruteForceIndex(768, H.Metric.Cosine)
         bf.insert_batch(np.arange(200_000, dtype=np.uint64), base)
-        for prec in (H.Precision.FP32, H.Precision.FP32, H.Precision.BF16X3, H.Precision.BF16X3):
+        tcp = H.Precision.BF16 if args.case_precision == "bf16" else H.Precision.BF16X3
+        for prec in (H.Precision.FP32, H.Precision.FP32, tcp, tcp):
             r = timed_call(lambda: bf.search_arrays(queries, 100, prec))
     print(json.dumps({"workload": args.workload, "host_ms_per_call": times, "results": int(r[2].sum())}))
     return 0
@@ -1277,6 +1280,8 @@ def main():
     ap.add_argument("--case-mode", type=int, default=1)
     ap.add_argument("--case-hash", type=int, default=0)
     ap.add_argument("--case-wpb", type=int, default=1)
+    ap.add_argument("--case-exact-below", type=float, default=0.0)
+    ap.add_argument("--case-precision", default="bf16x3", choices=["bf16", "bf16x3"])
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
     ap.add_argument("--brute-pairs", type=int, default=0, help="also time the paired (cta_group::2) kernel")
