@@ -12,6 +12,7 @@
 // result equals the result of the same search run alone. The kernel writes
 // each query's results into mapped host memory and publishes its status last,
 // so a request completes when its own query does, not when its batch does.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -41,6 +42,7 @@ struct Request {
     uint32_t count = 0;
     double t_arrival = 0, t_done = 0;
     uint64_t ticket = 0;
+    bool cancelled = false;  // in flight when cancelled: its results are discarded
 };
 
 // Host staging of one batch (pinned) plus its device scratch slot.
@@ -160,8 +162,8 @@ void complete_one(hnsw_gpu_server* s, BatchSlot& b, size_t i, int32_t status, do
     const uint32_t K = s->cfg.max_k;
     Request& r = s->at(b.tickets[i]);
     const uint64_t row = b.tickets[i] % s->cap;
-    r.status = status;
-    r.count = status == 0 ? std::min(b.h_count[i], r.k) : 0;
+    r.status = r.cancelled ? HNSW_ERR_CANCELLED : status;
+    r.count = r.status == 0 ? std::min(b.h_count[i], r.k) : 0;
     std::memcpy(&s->keys[row * K], b.h_keys + i * K, size_t(r.count) * 8);
     std::memcpy(&s->dist[row * K], b.h_dist + i * K, size_t(r.count) * 4);
     r.t_done = t;
@@ -379,6 +381,7 @@ static int submit_locked(hnsw_gpu_server* s, const float* query, uint32_t k, uin
     r.filter_id = filter_id;
     r.status = 0;
     r.count = 0;
+    r.cancelled = false;
     r.t_arrival = arrival_us >= 0 ? arrival_us : now_us();
     std::memcpy(&s->q[(t % s->cap) * s->dim], query, size_t(s->dim) * 4);
     s->pending.push_back(t);
@@ -397,6 +400,28 @@ int hnsw_gpu_submit(hnsw_gpu_server* s, const float* query, uint32_t k, uint32_t
     }
     if (r == HNSW_OK) s->cv_work.notify_one();
     return r;
+}
+
+int hnsw_gpu_cancel(hnsw_gpu_server* s, uint64_t ticket, int* cancelled) {
+    if (!s || !cancelled) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(s->mu);
+    Request& r = s->at(ticket);
+    if (r.ticket != ticket || r.state == ReqState::Free) return set_error(HNSW_ERR_INVALID_ARGUMENT, "unknown ticket");
+    *cancelled = 0;
+    if (r.state == ReqState::Pending) {
+        auto it = std::find(s->pending.begin(), s->pending.end(), ticket);
+        if (it != s->pending.end()) s->pending.erase(it);
+        r.status = HNSW_ERR_CANCELLED;
+        r.count = 0;
+        r.t_done = now_us();
+        r.state = ReqState::Done;
+        *cancelled = 1;
+        s->cv_done.notify_all();
+    } else if (r.state == ReqState::Inflight) {
+        r.cancelled = true;
+        *cancelled = 1;
+    }
+    return HNSW_OK;
 }
 
 int hnsw_gpu_poll(hnsw_gpu_server* s, uint64_t ticket, int* done) {

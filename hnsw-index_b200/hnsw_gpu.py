@@ -63,6 +63,7 @@ class Status(enum.IntEnum):
     ADMISSION_REJECTED = 23
     INVALID_ARGUMENT = 24
     SCRATCH_OVERFLOW = 25
+    CANCELLED = 26
 
 
 class Error(Exception):
@@ -638,6 +639,7 @@ _lib.hnsw_gpu_server_stop.argtypes = [_vp]
 _lib.hnsw_gpu_server_stop.restype = None
 _lib.hnsw_gpu_submit.argtypes = [_vp, _vp, C.c_uint32, C.c_uint32, C.c_int32, C.POINTER(C.c_uint64)]
 _lib.hnsw_gpu_poll.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_int)]
+_lib.hnsw_gpu_cancel.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_int)]
 _lib.hnsw_gpu_wait.argtypes = [_vp, C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_uint32),
                                C.POINTER(C.c_int32), C.POINTER(C.c_double)]
 _lib.hnsw_gpu_server_replay.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
@@ -673,6 +675,13 @@ class Server:
         t = C.c_uint64()
         _check(_lib.hnsw_gpu_submit(self._h, _ptr(q), k, ef, filter_id, C.byref(t)))
         return t.value
+
+    def cancel(self, ticket: int) -> bool:
+        """hnsw_gpu_cancel: True if the request will report CANCELLED, False
+        if it had already completed (its results stand)."""
+        c = C.c_int()
+        _check(_lib.hnsw_gpu_cancel(self._h, ticket, C.byref(c)))
+        return bool(c.value)
 
     def wait(self, ticket: int, timeout_ms: int = 60000):
         keys = np.zeros(self.max_k, np.uint64)

@@ -50,7 +50,8 @@ typedef enum hnsw_status {
     HNSW_ERR_TIMEOUT = 22,             /* a bounded device wait ran out */
     HNSW_ERR_ADMISSION_REJECTED = 23,  /* no scratch slot free for a request */
     HNSW_ERR_INVALID_ARGUMENT = 24,    /* null pointer, size out of the device path's range */
-    HNSW_ERR_SCRATCH_OVERFLOW = 25     /* a query outgrew its device scratch; retried internally */
+    HNSW_ERR_SCRATCH_OVERFLOW = 25,    /* a query outgrew its device scratch; retried internally */
+    HNSW_ERR_CANCELLED = 26            /* the request was cancelled (hnsw_gpu_cancel) */
 } hnsw_status;
 
 /* Metric tags, as in the file format (src/metric.rs:44-60). */
@@ -268,6 +269,13 @@ void hnsw_gpu_server_stop(hnsw_gpu_server* server);
 int hnsw_gpu_submit(hnsw_gpu_server* server, const float* query, uint32_t k, uint32_t ef, int32_t filter_id,
                     uint64_t* ticket);
 int hnsw_gpu_poll(hnsw_gpu_server* server, uint64_t ticket, int* done);
+/* Cancels a request. A queued request leaves the queue at once; a request
+ * whose batch is already on the device runs to the end there (kernels are
+ * not interrupted) and its results are discarded. Either way *cancelled = 1
+ * and hnsw_gpu_wait reports HNSW_ERR_CANCELLED with no results. A request
+ * that has already completed keeps its results (*cancelled = 0). The ticket
+ * must still be waited for to free it. */
+int hnsw_gpu_cancel(hnsw_gpu_server* server, uint64_t ticket, int* cancelled);
 /* Waits up to timeout_ms; copies the results (keys/dist: k entries) and the
  * request's latency (arrival to completion, microseconds), and frees the
  * ticket. */

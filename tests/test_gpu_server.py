@@ -122,3 +122,36 @@ def test_admission_rejects_when_queue_is_full(served):
         assert status == 0
     srv.stop()
     assert rejected > 0 and len(accepted) >= 16
+
+
+def test_cancelled_requests_report_cancelled_and_others_stand(served):
+    """hnsw_gpu_cancel on queued requests (one batch slot of 8 queries, so
+    most wait on the host) and on requests already launched: a cancelled
+    request reports CANCELLED with no results; every other request returns
+    the oracle's answer, and the server keeps serving afterwards."""
+    base, queries, data = served
+    gi = H.HnswIndex.from_bytes(data)
+    oi = O.Index(data)
+    q = queries[:200]
+    srv = H.Server(gi, max_batch=8, max_inflight=1, linger_us=0)
+    try:
+        tickets = [srv.submit(q[i], 10, 256) for i in range(len(q))]
+        # Every third request, from the first (likely launched) to the last (queued).
+        cancelled = {i: srv.cancel(tickets[i]) for i in range(0, len(q), 3)}
+        results = [srv.wait(t, timeout_ms=20000) for t in tickets]
+        after = [srv.wait(srv.submit(q[i], 10, 256), timeout_ms=20000) for i in range(8)]
+    finally:
+        srv.stop()
+    assert sum(cancelled.values()) >= len(cancelled) // 2
+    ref = oi.search(q, 10, 256)
+    for i, (keys, dist, status, _) in enumerate(results):
+        if cancelled.get(i):
+            assert status == H.Status.CANCELLED and len(keys) == 0
+        else:
+            assert status == 0
+            c = int(ref[2][i])
+            np.testing.assert_array_equal(keys, ref[0][i, :c])
+            np.testing.assert_array_equal(dist.view(np.uint32), ref[1][i, :c].view(np.uint32))
+    for i, (keys, _, status, _) in enumerate(after):
+        assert status == 0
+        np.testing.assert_array_equal(keys, ref[0][i, :int(ref[2][i])])
