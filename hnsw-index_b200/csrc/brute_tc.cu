@@ -164,6 +164,19 @@ __device__ __forceinline__ float tile_distance(const TcScoreArgs& a, float s, fl
     return 1.0f - s;
 }
 
+// The epilogue's per-row constants in registers (the scan loop then reads
+// no kernel argument, which a store could otherwise force it to reload).
+struct EpiConsts {
+    int metric;
+    uint32_t n;
+    const float* xnorm2;
+};
+__device__ __forceinline__ float row_distance(const EpiConsts& e, float s, float qn, uint32_t row) {
+    if (e.metric == 0) return qn + (row < e.n ? __ldg(e.xnorm2 + row) : 0.0f) - 2.0f * s;
+    if (e.metric == 1) return -s;
+    return 1.0f - s;
+}
+
 // Epilogue of one accumulator: this lane's query q against the 256 rows
 // row_base .. row_base + 255 held in TMEM columns taddr .. taddr + 255 of its
 // lane. Dense mode writes every distance of the sample's row range;
@@ -246,14 +259,15 @@ __device__ __noinline__ void flush_stage(const TcScoreArgs& a, const uint64_t* s
 
 // The 32 accumulator columns v (rows row0 .. row0 + 31) of this lane's query:
 // entries at or below the threshold go to the lane's staging slots.
-__device__ __forceinline__ void stage_chunk(const TcScoreArgs& a, const uint32_t (&v)[32], uint32_t row0, bool qvalid,
-                                            float thr, float qn, uint64_t* stage, uint32_t q, uint32_t& n) {
+__device__ __forceinline__ void stage_chunk(const TcScoreArgs& a, const EpiConsts& e, const uint32_t (&v)[32],
+                                            uint32_t row0, bool qvalid, float thr, float qn, uint64_t* stage,
+                                            uint32_t q, uint32_t& n) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
         const uint32_t row = row0 + uint32_t(j);
-        const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-        if (qvalid && row < a.n && dist <= thr) {
+        const float dist = row_distance(e, __uint_as_float(v[j]), qn, row);
+        if (qvalid && row < e.n && dist <= thr) {
             if (n == kStageDepth) {
                 flush_stage(a, stage, q, n);
                 n = 0;
@@ -273,6 +287,7 @@ __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32
                                                     uint32_t row_base, float thr, float qn, uint64_t* stage,
                                                     Release release) {
     const bool qvalid = q < a.nq;
+    const EpiConsts e{a.metric, a.n, a.xnorm2};
     uint32_t n = 0;
     uint32_t va[32], vb[32];
     tmem_ld32_async(taddr, va);
@@ -280,12 +295,12 @@ __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32
 #pragma unroll 1
     for (uint32_t c = 0; c < kTileN / 32; c += 2) {
         tmem_ld32_async(taddr + (c + 1) * 32, vb);
-        stage_chunk(a, va, row_base + c * 32, qvalid, thr, qn, stage, q, n);
+        stage_chunk(a, e, va, row_base + c * 32, qvalid, thr, qn, stage, q, n);
         __syncwarp();
         tmem_wait_regs(vb);
         if (c + 2 < kTileN / 32) tmem_ld32_async(taddr + (c + 2) * 32, va);
         else release();
-        stage_chunk(a, vb, row_base + (c + 1) * 32, qvalid, thr, qn, stage, q, n);
+        stage_chunk(a, e, vb, row_base + (c + 1) * 32, qvalid, thr, qn, stage, q, n);
         __syncwarp();
         if (c + 2 < kTileN / 32) tmem_wait_regs(va);
     }
@@ -295,7 +310,8 @@ __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32
 
 template <bool SPLIT3>
 __global__ void __launch_bounds__(kThreads, 1)
-    score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcScoreArgs a) {
+    score_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const __grid_constant__ TcScoreArgs a) {
     constexpr int kStages = Ring<SPLIT3>::kStages, kT = Ring<SPLIT3>::kTiles;
     constexpr uint32_t kStageBytes = Ring<SPLIT3>::kStageBytes;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -542,7 +558,7 @@ __device__ __forceinline__ void cluster_sync() {
 template <bool SPLIT3>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     score_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                      TcScoreArgs a) {
+                      const __grid_constant__ TcScoreArgs a) {
     constexpr int kStages = Ring2<SPLIT3>::kStages, kT = Ring2<SPLIT3>::kTiles;
     constexpr uint32_t kStageBytes = Ring2<SPLIT3>::kStageBytes;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
