@@ -999,6 +999,18 @@ def run_serve(args, emit=True):
             lat.append(time.perf_counter() - t)
         floor[e] = {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "max_ms": 1e3 * float(max(lat))}
     log(f"single-request latency by ef: {floor}")
+    # The floor of the filtered part of the mix: one request alone, k = 100,
+    # ef = 512, through a bank bitmap of about the given selectivity.
+    sel_bank = random_bitmaps(rq, nb, [0.05, 0.2, 0.5])
+    floor_filtered = {}
+    for j, sel in enumerate((0.05, 0.2, 0.5)):
+        lat = []
+        for i in range(20):
+            t = time.perf_counter()
+            index.search_arrays(queries[i:i + 1], 100, 512, quantized=True, filter_bits=sel_bank[j], filter_nbits=nb)
+            lat.append(time.perf_counter() - t)
+        floor_filtered[sel] = {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "max_ms": 1e3 * float(max(lat))}
+    log(f"single filtered request (k=100, ef=512) latency by selectivity: {floor_filtered}")
 
     def sweep(srv, rates):
         out, clocks = [], None
@@ -1045,6 +1057,7 @@ def run_serve(args, emit=True):
                    "open_s": open_s, "host_validate_s": host_validate_s,
                    "batched_qps_same_requests": batched_qps, "max_batch": args.serve_batch,
                    "p99_within_2ms_at_headline": bool(ok2), "latency_floor_single_request": floor,
+                   "latency_floor_single_filtered_request_ef512_k100": floor_filtered,
                    "batch_launches": launches, "served": served_n, "sweep_batches": batch},
         "clocks": clocks,
     }
