@@ -241,40 +241,45 @@ __device__ __forceinline__ void epilogue_tile(const TcScoreArgs& a, uint32_t tad
     }
 }
 
-// Candidate-mode staging: per epilogue warp kStageDepth entries per lane in
-// shared memory, entry i of lane l at [i * 32 + l] (consecutive lanes hit
-// consecutive words).
-constexpr uint32_t kStageDepth = 16;
-constexpr uint32_t kStageBytesPerWarp = kStageDepth * 32 * 8;  // 4 KB
+// Candidate-mode staging: per epilogue warp and lane up to kStageDepth
+// entries in shared memory, as the f32 distance and the row's column within
+// the tile (entry i of lane l at [i * 32 + l], so consecutive lanes hit
+// consecutive words). A chunk of 32 columns adds at most 32, so a warp
+// appends its staged entries before a chunk whenever a lane holds more than
+// kStageDepth - 32.
+constexpr uint32_t kStageDepth = 48;
+constexpr uint32_t kStageBytesPerWarp = kStageDepth * 32 * 5;  // 7.5 KB
 
 // Appends this lane's n staged entries to its query's candidates (one
-// reservation). Out of line: the per-entry path calls it only when a lane
-// has staged kStageDepth entries of one tile.
-__device__ __noinline__ void flush_stage(const TcScoreArgs& a, const uint64_t* stage, uint32_t q, uint32_t n) {
+// reservation).
+__device__ __forceinline__ void flush_stage(const TcScoreArgs& a, const float* sd, const uint8_t* sr, uint32_t q,
+                                            uint32_t row_base, uint32_t n) {
     const int lane = threadIdx.x & 31;
+    if (n == 0) return;
     uint32_t slot = atomicAdd(a.cand_count + q, n);
+    uint64_t* out = a.cand + size_t(q) * a.cand_cap;
     for (uint32_t i = 0; i < n; ++i, ++slot)
-        if (slot < a.cand_cap) a.cand[size_t(q) * a.cand_cap + slot] = stage[i * 32 + lane];
+        if (slot < a.cand_cap)
+            out[slot] = (uint64_t(__float_as_uint(sd[i * 32 + lane])) << 32) | (row_base + sr[i * 32 + lane]);
 }
 
-// The 32 accumulator columns v (rows row0 .. row0 + 31) of this lane's query:
-// entries at or below the threshold go to the lane's staging slots.
-__device__ __forceinline__ void stage_chunk(const TcScoreArgs& a, const EpiConsts& e, const uint32_t (&v)[32],
-                                            uint32_t row0, bool qvalid, float thr, float qn, uint64_t* stage,
-                                            uint32_t q, uint32_t& n) {
+// The 32 accumulator columns v (tile columns col0 .. col0 + 31) of this
+// lane's query: entries at or below the threshold are staged, without
+// branches (predicated stores). `lim` is the number of valid columns (0 for
+// a padding query).
+__device__ __forceinline__ void stage_chunk(const EpiConsts& e, const uint32_t (&v)[32], uint32_t row_base,
+                                            uint32_t col0, uint32_t lim, float thr, float qn, float* sd, uint8_t* sr,
+                                            uint32_t& n) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-        const uint32_t row = row0 + uint32_t(j);
-        const float dist = row_distance(e, __uint_as_float(v[j]), qn, row);
-        if (qvalid && row < e.n && dist <= thr) {
-            if (n == kStageDepth) {
-                flush_stage(a, stage, q, n);
-                n = 0;
-            }
-            stage[n * 32 + uint32_t(lane)] = (uint64_t(__float_as_uint(dist)) << 32) | row;
-            ++n;
+        const float dist = row_distance(e, __uint_as_float(v[j]), qn, row_base + col0 + uint32_t(j));
+        const bool pass = uint32_t(j) < lim && dist <= thr;
+        if (pass) {
+            sd[n * 32 + uint32_t(lane)] = dist;
+            sr[n * 32 + uint32_t(lane)] = uint8_t(col0 + uint32_t(j));
         }
+        n += pass ? 1u : 0u;
     }
 }
 
@@ -284,10 +289,13 @@ __device__ __forceinline__ void stage_chunk(const TcScoreArgs& a, const EpiConst
 // then reuse the accumulator), and the staged entries are appended after.
 template <typename Release>
 __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32_t taddr, uint32_t q,
-                                                    uint32_t row_base, float thr, float qn, uint64_t* stage,
+                                                    uint32_t row_base, float thr, float qn, unsigned char* stage,
                                                     Release release) {
-    const bool qvalid = q < a.nq;
     const EpiConsts e{a.metric, a.n, a.xnorm2};
+    float* sd = reinterpret_cast<float*>(stage);
+    uint8_t* sr = stage + kStageDepth * 32 * 4;
+    // Valid columns of this tile for this lane's query.
+    const uint32_t valid = q < a.nq ? (row_base < e.n ? min(e.n - row_base, kTileN) : 0u) : 0u;
     uint32_t n = 0;
     uint32_t va[32], vb[32];
     tmem_ld32_async(taddr, va);
@@ -295,16 +303,27 @@ __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32
 #pragma unroll 1
     for (uint32_t c = 0; c < kTileN / 32; c += 2) {
         tmem_ld32_async(taddr + (c + 1) * 32, vb);
-        stage_chunk(a, e, va, row_base + c * 32, qvalid, thr, qn, stage, q, n);
+        if (__any_sync(0xFFFFFFFFu, n > kStageDepth - 32)) {
+            flush_stage(a, sd, sr, q, row_base, n);
+            n = 0;
+        }
+        __syncwarp();
+        stage_chunk(e, va, row_base, c * 32, valid > c * 32 ? min(valid - c * 32, 32u) : 0u, thr, qn, sd, sr, n);
         __syncwarp();
         tmem_wait_regs(vb);
         if (c + 2 < kTileN / 32) tmem_ld32_async(taddr + (c + 2) * 32, va);
         else release();
-        stage_chunk(a, e, vb, row_base + (c + 1) * 32, qvalid, thr, qn, stage, q, n);
+        if (__any_sync(0xFFFFFFFFu, n > kStageDepth - 32)) {
+            flush_stage(a, sd, sr, q, row_base, n);
+            n = 0;
+        }
+        __syncwarp();
+        stage_chunk(e, vb, row_base, (c + 1) * 32, valid > (c + 1) * 32 ? min(valid - (c + 1) * 32, 32u) : 0u, thr,
+                    qn, sd, sr, n);
         __syncwarp();
         if (c + 2 < kTileN / 32) tmem_wait_regs(va);
     }
-    if (n) flush_stage(a, stage, q, n);
+    flush_stage(a, sd, sr, q, row_base, n);
     __syncwarp();
 }
 
@@ -437,7 +456,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else {
         // Epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, i.e. those query rows.
         const uint32_t lane_base = 32u * uint32_t(warp & 3);
-        uint64_t* stage = reinterpret_cast<uint64_t*>(stage_base + size_t(warp - 2) * kStageBytesPerWarp);
+        unsigned char* stage = stage_base + size_t(warp - 2) * kStageBytesPerWarp;
         uint32_t tile_it = 0;
         for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++tile_it) {
             const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
@@ -702,7 +721,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     } else {
         // Epilogue (both CTAs): this CTA's 128 query rows x the tile's 256 rows.
         const uint32_t lane_base = 32u * uint32_t(warp & 3);
-        uint64_t* stage = reinterpret_cast<uint64_t*>(stage_base + size_t(warp - 2) * kStageBytesPerWarp);
+        unsigned char* stage = stage_base + size_t(warp - 2) * kStageBytesPerWarp;
         uint32_t tile_it = 0;
         for (uint32_t t = pair; t < total; t += npairs, ++tile_it) {
             const uint32_t nt = a.n_tile_begin + t / q_pairs, qp2 = t % q_pairs;
