@@ -89,6 +89,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     }
 }
 
+// Brings one box of the tensor map into L2 (no shared memory, no barrier).
+__device__ __forceinline__ void tma_prefetch_l2(const CUtensorMap* map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
+}
+
+// The base-row operand of a CTA's next tile, into L2 while the current tile
+// runs: the CTAs of one round work on one or two n-tiles and reach each K
+// chunk together, so without it every one of them waits on the same DRAM
+// fetch. A CTA prefetches the chunks k = its index mod 4, 4 + that, ... of
+// its next tile when the next tile's n-tile differs from the current one
+// (the CTAs sharing that n-tile cover all chunks between them).
+__device__ __forceinline__ void prefetch_next_b(const CUtensorMap* map, uint32_t nt, uint32_t nt_next, uint32_t k_chunks,
+                                                int kT, uint32_t lo_col, int rows, int row_off, uint32_t who) {
+    if (nt_next == nt) return;
+    for (uint32_t k = who & 3u; k < k_chunks; k += 4)
+        for (int tt = 0; tt < kT; ++tt)
+            tma_prefetch_l2(map, int(k * kTileK + uint32_t(tt) * lo_col), int(nt_next) * rows + row_off);
+}
+
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
@@ -381,6 +402,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             for (uint32_t t = blockIdx.x; ok && t < total; t += gridDim.x) {
                 const uint32_t nt = a.n_tile_begin + t / q_tiles, qt = t % q_tiles;
+                if (t + gridDim.x < total)
+                    prefetch_next_b(&tmB, nt, a.n_tile_begin + (t + gridDim.x) / q_tiles, a.k_chunks, kT, a.lo_col,
+                                    int(kTileN), 0, blockIdx.x);
                 for (uint32_t k = 0; k < a.k_chunks; ++k) {
                     const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
                     if (!mbar_wait(&empty[s], ph ^ 1u, a.err, a.wait_budget)) {
@@ -635,6 +659,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             bool ok = true;
             for (uint32_t t = pair; ok && t < total; t += npairs) {
                 const uint32_t nt = a.n_tile_begin + t / q_pairs, qp2 = t % q_pairs;
+                if (t + npairs < total)
+                    prefetch_next_b(&tmB, nt, a.n_tile_begin + (t + npairs) / q_pairs, a.k_chunks, kT, a.lo_col,
+                                    int(kTileN), int(rank * kHalfN), pair);
                 for (uint32_t k = 0; k < a.k_chunks; ++k) {
                     const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
                     if (!mbar_wait(&empty[s], ph ^ 1u, a.err, a.wait_budget)) {
