@@ -269,7 +269,9 @@ __device__ __forceinline__ void epilogue_tile(const TcScoreArgs& a, uint32_t tad
 // appends its staged entries before a chunk whenever a lane holds more than
 // kStageDepth - 32.
 constexpr uint32_t kStageDepth = 48;
-constexpr uint32_t kStageBytesPerWarp = kStageDepth * 32 * 5;  // 7.5 KB
+// One more row per lane takes the stores of entries that do not pass, so the
+// scan has no branch per element.
+constexpr uint32_t kStageBytesPerWarp = (kStageDepth + 1) * 32 * 5;  // 7.7 KB
 
 // Appends this lane's n staged entries to its query's candidates (one
 // reservation).
@@ -285,23 +287,40 @@ __device__ __forceinline__ void flush_stage(const TcScoreArgs& a, const float* s
 }
 
 // The 32 accumulator columns v (tile columns col0 .. col0 + 31) of this
-// lane's query: entries at or below the threshold are staged, without
-// branches (predicated stores). `lim` is the number of valid columns (0 for
-// a padding query).
+// lane's query: entries at or below the threshold are staged. Straight-line
+// code: every entry is stored, one that does not pass into the spare row
+// kStageDepth, and only a passing one advances n. `lim` is the number of
+// valid columns (0 for a padding query). METRIC as in tile_distance.
+template <int METRIC>
+__device__ __forceinline__ void stage_chunk_m(const EpiConsts& e, const uint32_t (&v)[32], uint32_t row_base,
+                                              uint32_t col0, uint32_t lim, float thr, float qn, float* sd,
+                                              uint8_t* sr, uint32_t& n) {
+    const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const float s = __uint_as_float(v[j]);
+        float dist;
+        if (METRIC == 0) {
+            const uint32_t row = row_base + col0 + uint32_t(j);
+            dist = qn + (row < e.n ? __ldg(e.xnorm2 + row) : 0.0f) - 2.0f * s;
+        } else if (METRIC == 1) {
+            dist = -s;
+        } else {
+            dist = 1.0f - s;
+        }
+        const bool pass = uint32_t(j) < lim && dist <= thr;
+        const uint32_t at = (pass ? n : kStageDepth) * 32 + lane;
+        sd[at] = dist;
+        sr[at] = uint8_t(col0 + uint32_t(j));
+        n += pass ? 1u : 0u;
+    }
+}
 __device__ __forceinline__ void stage_chunk(const EpiConsts& e, const uint32_t (&v)[32], uint32_t row_base,
                                             uint32_t col0, uint32_t lim, float thr, float qn, float* sd, uint8_t* sr,
                                             uint32_t& n) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        const float dist = row_distance(e, __uint_as_float(v[j]), qn, row_base + col0 + uint32_t(j));
-        const bool pass = uint32_t(j) < lim && dist <= thr;
-        if (pass) {
-            sd[n * 32 + uint32_t(lane)] = dist;
-            sr[n * 32 + uint32_t(lane)] = uint8_t(col0 + uint32_t(j));
-        }
-        n += pass ? 1u : 0u;
-    }
+    if (e.metric == 0) stage_chunk_m<0>(e, v, row_base, col0, lim, thr, qn, sd, sr, n);
+    else if (e.metric == 1) stage_chunk_m<1>(e, v, row_base, col0, lim, thr, qn, sd, sr, n);
+    else stage_chunk_m<2>(e, v, row_base, col0, lim, thr, qn, sd, sr, n);
 }
 
 // Candidate mode, one pass: the accumulator's eight 32-column chunks are
@@ -314,7 +333,7 @@ __device__ __forceinline__ void epilogue_candidates(const TcScoreArgs& a, uint32
                                                     Release release) {
     const EpiConsts e{a.metric, a.n, a.xnorm2};
     float* sd = reinterpret_cast<float*>(stage);
-    uint8_t* sr = stage + kStageDepth * 32 * 4;
+    uint8_t* sr = stage + (kStageDepth + 1) * 32 * 4;
     // Valid columns of this tile for this lane's query.
     const uint32_t valid = q < a.nq ? (row_base < e.n ? min(e.n - row_base, kTileN) : 0u) : 0u;
     uint32_t n = 0;
