@@ -896,18 +896,35 @@ def run_batch(args, emit=True):
     alive[dead.astype(np.int64)] = False
     hits = [0, 0]
     tot = 0
+    # FP64 check of the returned results on the same sample: the distance of
+    # every returned key against -(x . q) in float64, and the returned keys
+    # outside the FP64 filtered top-k (the int8 walk is approximate; the
+    # re-ranked distances are exact f32).
+    max_abs = max_rel = 0.0
+    outside = 0
     for i in range(samp):
         allowed = np.unpackbits(bank[fids[i]].view(np.uint8), bitorder="little")[:nb].astype(bool)
         mask = allowed & alive
         idx = np.nonzero(mask)[0]
         sc = base[idx].astype(np.float64) @ queries[i].astype(np.float64)
         kk = min(10, int(ks[i]), idx.size)
-        truth = idx[np.argsort(-sc, kind="stable")[:kk]].astype(np.uint64)
+        order = np.argsort(-sc, kind="stable")
+        truth = idx[order[:kk]].astype(np.uint64)
         for j, r in enumerate((res, plan_res)):
             hits[j] += np.isin(r[0][i, :min(kk, int(r[2][i]))], truth).sum()
         tot += kk
+        c = int(res[2][i])
+        if c:
+            keys_i = res[0][i, :c].astype(np.int64)
+            d64 = -(base[keys_i].astype(np.float64) @ queries[i].astype(np.float64))
+            err = np.abs(res[1][i, :c].astype(np.float64) - d64)
+            max_abs = max(max_abs, float(err.max()))
+            max_rel = max(max_rel, float((err / np.maximum(np.abs(d64), 1e-30)).max()))
+            outside += len(set(keys_i.tolist()) - set(idx[order[:c]].tolist()))
     out["recall_at_10_sample"] = hits[0] / max(tot, 1)
     out["planner_recall_at_10_sample"] = hits[1] / max(tot, 1)
+    out["fp64_sample"] = {"queries": samp, "max_abs_distance_error": max_abs, "max_rel_distance_error": max_rel,
+                          "topk_disagreement_per_query": outside / samp}
     # CPU baseline: the oracle with quantized traversal and the same filters.
     oi = O.Index(data)
     cs = 1000
