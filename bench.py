@@ -1056,7 +1056,11 @@ def run_serve(args, emit=True):
     rates = tuple(int(r) for r in args.serve_rates.split(",")) if emit else (10_000, 30_000, 100_000)
     srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 17, max_k=100, max_ef=512,
                    linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
-    srv.replay(queries[:5000], np.cumsum(rq.exponential(1e6 / 30_000, 5000)), ks[:5000], efs[:5000], fids[:5000])
+    # Warm-up at a high rate so that every batch slot is driven with full
+    # batches and sizes its device buffers (growing one frees the old, which
+    # synchronises the device) before the sweep.
+    nw = min(pool, 40_000)
+    srv.replay(queries[:nw], np.cumsum(rq.exponential(1e6 / 300_000, nw)), ks[:nw], efs[:nw], fids[:nw])
     batch, clocks = sweep(srv, rates)
     launches, served_n = srv.stats()
     srv.stop()
