@@ -198,66 +198,32 @@ __device__ __forceinline__ float row_distance(const EpiConsts& e, float s, float
     return 1.0f - s;
 }
 
-// Epilogue of one accumulator: this lane's query q against the 256 rows
-// row_base .. row_base + 255 held in TMEM columns taddr .. taddr + 255 of its
-// lane. Dense mode writes every distance of the sample's row range;
-// candidate mode appends the (row, distance) pairs at or below the query's
-// threshold, with one reservation per (query, tile). All 32 lanes call.
-__device__ __forceinline__ void epilogue_tile(const TcScoreArgs& a, uint32_t taddr, uint32_t q, uint32_t row_base) {
+// Dense epilogue (threshold sample pass): this lane's query q against the
+// 256 rows row_base .. row_base + 255 held in TMEM columns taddr .. taddr +
+// 255 of its lane; every distance of the sample's row range is written,
+// four at a time (+inf past the last row). All 32 lanes call.
+__device__ __forceinline__ void epilogue_dense(const TcScoreArgs& a, uint32_t taddr, uint32_t q, uint32_t row_base) {
     const bool qvalid = q < a.nq;
-    const float thr = (qvalid && a.thr) ? a.thr[q] : 0.0f;
     const float qn = (qvalid && a.qnorm2) ? a.qnorm2[q] : 0.0f;
-    if (a.dense) {
-        for (uint32_t c = 0; c < kTileN / 32; ++c) {
-            uint32_t v[32];
-            __syncwarp();
-            tmem_ld32(taddr + c * 32, v);
-            const uint32_t row0 = row_base + c * 32;
-#pragma unroll
-            for (int j = 0; j < 32 && qvalid; ++j) {
-                const uint32_t row = row0 + uint32_t(j);
-                const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-                if (row >= a.row0 && row < a.row0 + a.ld)
-                    a.dense[size_t(q) * a.ld + (row - a.row0)] = row < a.n ? dist : __int_as_float(0x7f800000);
-            }
-        }
-        return;
-    }
-    // Pass 1: how many of this query's 256 rows pass the threshold.
-    uint32_t total_pass = 0;
-#pragma unroll 1
+    const EpiConsts e{a.metric, a.n, a.xnorm2};
     for (uint32_t c = 0; c < kTileN / 32; ++c) {
         uint32_t v[32];
         __syncwarp();
         tmem_ld32(taddr + c * 32, v);
         const uint32_t row0 = row_base + c * 32;
+        // The sample range starts at a.row0 (a multiple of 256) and holds a.ld
+        // (a multiple of 256) rows, so a chunk lies wholly inside or outside.
+        if (!qvalid || row0 < a.row0 || row0 >= a.row0 + a.ld) continue;
+        float4* out = reinterpret_cast<float4*>(a.dense + size_t(q) * a.ld + (row0 - a.row0));
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const uint32_t row = row0 + uint32_t(j);
-            const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-            total_pass += (qvalid && row < a.n && dist <= thr) ? 1u : 0u;
-        }
-    }
-    // One reservation per (query, tile); pass 2 writes the entries.
-    uint32_t slot = 0;
-    if (total_pass) slot = atomicAdd(a.cand_count + q, total_pass);
-    if (__any_sync(0xFFFFFFFFu, total_pass != 0)) {
-#pragma unroll 1
-        for (uint32_t c = 0; c < kTileN / 32; ++c) {
-            uint32_t v[32];
-            __syncwarp();
-            tmem_ld32(taddr + c * 32, v);
-            const uint32_t row0 = row_base + c * 32;
+        for (int j = 0; j < 32; j += 4) {
+            float d[4];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const uint32_t row = row0 + uint32_t(j);
-                const float dist = tile_distance(a, __uint_as_float(v[j]), qn, row);
-                if (qvalid && row < a.n && dist <= thr) {
-                    if (slot < a.cand_cap)
-                        a.cand[size_t(q) * a.cand_cap + slot] = (uint64_t(__float_as_uint(dist)) << 32) | row;
-                    ++slot;
-                }
+            for (int i = 0; i < 4; ++i) {
+                const uint32_t row = row0 + uint32_t(j + i);
+                d[i] = row < e.n ? row_distance(e, __uint_as_float(v[j + i]), qn, row) : __int_as_float(0x7f800000);
             }
+            out[j / 4] = make_float4(d[0], d[1], d[2], d[3]);
         }
     }
 }
@@ -518,7 +484,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (lane == 0) mbar_arrive(&acc_empty[b]);
             };
             if (a.dense) {
-                epilogue_tile(a, taddr, q, nt * kTileN);
+                epilogue_dense(a, taddr, q, nt * kTileN);
                 release();
             } else {
                 epilogue_candidates(a, taddr, q, nt * kTileN, thr, qn, stage, release);
@@ -788,7 +754,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 }
             };
             if (a.dense) {
-                epilogue_tile(a, taddr, q, nt * kTileN);
+                epilogue_dense(a, taddr, q, nt * kTileN);
                 release();
             } else {
                 epilogue_candidates(a, taddr, q, nt * kTileN, thr, qn, stage, release);
