@@ -1235,7 +1235,8 @@ def run_case(args):
             # workload: 4096-entry hash, one warp per block, plain mode).
             index.set_schedule(ef_cap=64, hash_cap=args.case_hash, warps_per_block=args.case_wpb)
         for _ in range(3):
-            r = timed_call(lambda: index.search_arrays(queries, K, 64, mode=args.case_mode))
+            r = timed_call(lambda: index.search_arrays(queries, K, 64, mode=args.case_mode,
+                                                       traversal=args.case_traversal))
     elif args.workload == "case-cold-500kx96":
         # search_kernel<1>: 500k x 96 inner product, int8 traversal, per-query
         # filters (1-90%), uneven k/ef, persistent mode.
@@ -1316,6 +1317,7 @@ def main():
     ap.add_argument("--case-wpb", type=int, default=1)
     ap.add_argument("--case-exact-below", type=float, default=0.0)
     ap.add_argument("--case-precision", default="bf16x3", choices=["bf16", "bf16x3"])
+    ap.add_argument("--case-traversal", type=int, default=0, help="0 f32, 1 BF16, 2 BF16x3 tensor-core traversal")
     ap.add_argument("--brute-n", type=int, default=1_000_000)
     ap.add_argument("--brute-nq", type=int, default=10_000)
     ap.add_argument("--brute-pairs", type=int, default=0, help="also time the paired (cta_group::2) kernel")
