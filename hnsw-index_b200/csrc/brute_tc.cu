@@ -21,7 +21,8 @@
 //   warps 2..5  epilogue: tcgen05.ld of a 128 x 256 FP32 accumulator (two
 //               accumulators alternate so the epilogue overlaps the next tile).
 // Every mbarrier wait is bounded by a clock budget; on expiry the CTA sets an
-// error word, drains, frees its TMEM and returns. No cluster multicast.
+// error word, drains, frees its TMEM and returns. No load is shared across a
+// cluster.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -510,7 +511,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ring (6 stages of 32 KB, or 3 of 64 KB with the split). Each CTA's TMA
 // loads complete on its own barrier; CTA 1's warp 1 relays each completed
 // stage to CTA 0 with a remote arrive. MMA completions are committed to both
-// CTAs' barriers (multicast commit). No load uses cluster multicast. Every
+// CTAs' barriers (one commit per CTA). Each CTA loads only its own tiles. Every
 // wait is bounded as in score_kernel; the CTAs meet at a cluster barrier
 // before tensor memory is freed, after CTA 0's MMAs and each CTA's copies
 // have completed.
@@ -534,12 +535,16 @@ __device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, 
         ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc2), "r"(accumulate));
 }
 // Arrives (once) on the barrier at `bar`'s offset in every CTA of `mask`
-// when this thread's MMAs so far have completed.
+// when this thread's MMAs so far have completed: one commit per CTA, each to
+// that CTA's barrier by its shared::cluster address (mapa).
 __device__ __forceinline__ void umma_commit_pair(uint64_t* bar, uint16_t mask) {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
-        ::"r"(smem_u32(bar)), "h"(mask)
-        : "memory");
+    for (uint32_t r = 0; r < 2; ++r) {
+        if (!((mask >> r) & 1u)) continue;
+        uint32_t addr;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(smem_u32(bar)), "r"(r));
+        asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(addr)
+                     : "memory");
+    }
 }
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
