@@ -240,6 +240,13 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     a.out_status = d_status;
     a.out_stride = out_stride;
     a.publish = publish ? 1 : 0;
+#ifdef HNSW_DEVICE_CHECKS
+    if (!gi->chk.p) {
+        CU(gi->chk.ensure(16), "cudaMalloc check word");
+        CU(cudaMemset(gi->chk.p, 0, 16), "clear check word");
+    }
+    a.chk = gi->chk.as<uint32_t>();
+#endif
     if (gi->counters) {
         CU(s->counters.ensure(std::max<size_t>(nq, 1) * 16), "cudaMalloc counters");
         a.counters = s->counters.as<uint32_t>();
@@ -1383,6 +1390,25 @@ int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* b, int enabled) {
 }
 
 void hnsw_gpu_debug_fail_allocations(int count) { g_fail_allocations.store(count > 0 ? count : 0); }
+
+int hnsw_gpu_check_word(hnsw_gpu_index* gi, uint32_t out[2], int clear) {
+    if (!gi || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");
+    out[0] = out[1] = 0;
+    if (!gi->chk.p) return HNSW_OK;
+    DeviceGuard dg(gi->device);
+    CU(cudaDeviceSynchronize(), "check word");
+    CU(cudaMemcpy(out, gi->chk.p, 8, cudaMemcpyDeviceToHost), "copy check word");
+    if (clear) CU(cudaMemset(gi->chk.p, 0, 16), "clear check word");
+    return HNSW_OK;
+}
+
+int hnsw_gpu_checked_build(void) {
+#ifdef HNSW_DEVICE_CHECKS
+    return 1;
+#else
+    return 0;
+#endif
+}
 
 int hnsw_gpu_brute_search_batch_noalloc(hnsw_gpu_brute* b, const float* d_queries, size_t nq, size_t dim,
                                         uint32_t k, uint64_t* d_keys, float* d_dist, uint32_t* d_count,

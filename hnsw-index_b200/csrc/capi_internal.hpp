@@ -188,6 +188,7 @@ struct hnsw_gpu_index {
     // parts, low parts (BF16X3), f32 squared norms (L2).
     std::mutex tc_mu;
     DBuf tc_hi, tc_lo, tc_norm;
+    DBuf chk;  // bounds-check word of the checked build (2 x u32)
     bool tc_hi_ready = false, tc_lo_ready = false;
     ~hnsw_gpu_index() {
         DeviceGuard g(device);
@@ -196,7 +197,7 @@ struct hnsw_gpu_index {
             cudaEventDestroy(dev_done);
         }
         dev_slot.reset();
-        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead, &tc_hi, &tc_lo, &tc_norm})
+        for (DBuf* b : {&vec, &codes, &norms, &offset, &adj0, &upoff, &adjU, &keys, &dead, &tc_hi, &tc_lo, &tc_norm, &chk})
             b->release();
         std::lock_guard<std::mutex> l(slots.mu);
         slots.free.clear();

@@ -129,6 +129,10 @@ struct SearchArgs {
     // completion flag: the status is written last, after a system-scope
     // fence, so a host thread that sees it can read the query's results.
     int publish = 0;
+    // Checked builds (HNSW_DEVICE_CHECKS): the first violated bounds check
+    // writes its site into chk[0] and the offending value into chk[1], and
+    // the access is skipped; unused otherwise.
+    uint32_t* chk = nullptr;
 };
 
 // Kernels of the tensor-core traversal (search_tc.cu): variant v (0 lean,

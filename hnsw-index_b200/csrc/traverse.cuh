@@ -32,6 +32,21 @@
 namespace hnswgpu {
 namespace dev {
 
+// Bounds checks of the checked build (-DHNSW_DEVICE_CHECKS, the
+// libhnsw_gpu_checked.so target): HNSW_CHK(word, cond, site, value) is cond;
+// when it fails, the first failure's site and value go to word[0], word[1]
+// and the caller skips the access. In the normal build it is `true` and
+// compiles away.
+#ifdef HNSW_DEVICE_CHECKS
+__device__ __forceinline__ bool chk_fail(uint32_t* word, uint32_t site, uint32_t value) {
+    if (word && atomicCAS(word, 0u, site) == 0u) word[1] = value;
+    return false;
+}
+#define HNSW_CHK(word, cond, site, value) ((cond) ? true : ::hnswgpu::dev::chk_fail((word), (site), uint32_t(value)))
+#else
+#define HNSW_CHK(word, cond, site, value) true
+#endif
+
 enum : int32_t { ST_OK = 0, ST_NON_FINITE = 3, ST_ZERO = 4, ST_QDISABLED = 7, ST_BAD_ARGUMENT = 24, ST_OVERFLOW = 25 };
 
 struct Counters {
@@ -79,6 +94,9 @@ struct Ws {
     uint32_t* pool_next;
     uint32_t pool_chunks;
     uint32_t* tab;          // chunk ids owned by this warp (kept across its queries)
+#ifdef HNSW_DEVICE_CHECKS
+    uint32_t* chk;          // bounds-check word (checked build)
+#endif
     uint32_t tab_cap;
     uint32_t b_chunks, b_count;
     uint64_t b_min, b_max;
@@ -88,6 +106,9 @@ struct Ws {
 // *full is set when the hash passes its load limit.
 __device__ __forceinline__ bool visit(Ws& w, uint32_t id) {
     if (w.bitmap_mode) {
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, (id >> 5) < w.bitmap_words, 1, id)) return false;
+#endif
         uint32_t bit = 1u << (id & 31);
         uint32_t old = atomicOr(&w.H[id >> 5], bit);
         return (old & bit) == 0;
@@ -388,12 +409,18 @@ __device__ __forceinline__ uint64_t greedy_layer(QueryCtx& c, uint64_t best, uin
     const int lane = lane_id();
     for (;;) {
         const uint32_t from = pid(best);
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, from < ix.n, 4, from)) return best;
+#endif
         const uint32_t* blk = ix.adjU + size_t(__ldg(ix.up_off + from) + (layer - 1)) * ix.mp;
         c.cnt.exp_up++;
         float bd = pdist(best);
         uint32_t bid = from;
         for (uint32_t base = 0; base < ix.m; base += 32) {
             uint32_t id = (base + lane < ix.m) ? __ldg(blk + base + lane) : kEmpty;
+#ifdef HNSW_DEVICE_CHECKS
+            if (!HNSW_CHK(w.chk, id == kEmpty || id < ix.n, 2, id)) id = kEmpty;
+#endif
             uint32_t V = __ballot_sync(kFull, id != kEmpty);
             if (V == 0) break;
             chunk_distances<DK>(c, id, V);
@@ -430,6 +457,11 @@ __device__ __forceinline__ int nth_set(uint32_t m, int r) {
 }
 
 __device__ __forceinline__ uint64_t* cold_slot(const Ws& w, uint32_t pos) {
+#ifdef HNSW_DEVICE_CHECKS
+    if (!HNSW_CHK(w.chk, (pos >> kColdChunkShift) < w.b_chunks, 7, pos) ||
+        !HNSW_CHK(w.chk, w.tab[pos >> kColdChunkShift] < w.pool_chunks, 8, w.tab[pos >> kColdChunkShift]))
+        return w.pool;
+#endif
     return w.pool + (size_t(w.tab[pos >> kColdChunkShift]) << kColdChunkShift) + (pos & (kColdChunk - 1));
 }
 
@@ -716,11 +748,19 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
         const float worst0 = rs > 0 ? pdist(w.R[rs - 1]) : 0.0f;
         if (rs >= ef && pdist(cur) > worst0) break;
         c.cnt.exp0++;
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, pid(cur) < ix.n, 3, pid(cur))) return -1;
+#endif
         const uint32_t* row = ix.adj0 + size_t(pid(cur)) * ix.m0p;
         // The next candidate in the queue is usually the next expansion.
         if (lane == 0 && head < tail) prefetch_l2(ix.adj0 + size_t(pid(w.C[head])) * ix.m0p, ix.m0p * 4);
         for (uint32_t base = 0; base < ix.m0; base += 32) {
+#ifdef HNSW_DEVICE_CHECKS
             uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+            if (!HNSW_CHK(w.chk, id == kEmpty || id < ix.n, 2, id)) id = kEmpty;
+#else
+            uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+#endif
             const bool valid = id != kEmpty;
             const uint32_t V = __ballot_sync(kFull, valid);
             if (V == 0) break;
@@ -833,6 +873,9 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                         if (COLD && cold) {
                             if (!cold_append(w, 1u, x)) return -1;
                         } else {
+#ifdef HNSW_DEVICE_CHECKS
+                            if (!HNSW_CHK(w.chk, tail < w.cand_cap + 1, 5, tail)) return -1;
+#endif
                             sorted_insert(w.C, head, tail, x);
                             ++tail;
                         }
@@ -921,9 +964,17 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
         }
         __syncwarp();
         c.cnt.exp0++;
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, (uint32_t(cur) >> 1) < ix.n, 3, uint32_t(cur) >> 1)) return -1;
+#endif
         const uint32_t* row = ix.adj0 + size_t(uint32_t(cur) >> 1) * ix.m0p;
         for (uint32_t base = 0; base < ix.m0; base += 32) {
+#ifdef HNSW_DEVICE_CHECKS
+            uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+            if (!HNSW_CHK(w.chk, id == kEmpty || id < ix.n, 2, id)) id = kEmpty;
+#else
             const uint32_t id = (base + lane < ix.m0) ? __ldg(row + base + lane) : kEmpty;
+#endif
             const bool valid = id != kEmpty;
             const uint32_t V = __ballot_sync(kFull, valid);
             if (V == 0) break;
@@ -982,6 +1033,9 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
                     }
                     const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
                     if (I) {
+#ifdef HNSW_DEVICE_CHECKS
+                        if (!HNSW_CHK(w.chk, rs + uint32_t(__popc(I)) <= w.cand_cap + 1, 6, rs)) return -1;
+#endif
                         nx = min(nx, merge_all(U, rs, I, my_x, pr));
                         const uint32_t total = rs + uint32_t(__popc(I));
                         if (total > ef) {
@@ -1216,6 +1270,9 @@ __device__ __forceinline__ int32_t run_query(const SearchArgs& a, Ws& w, uint32_
         __syncwarp();
     }
     if (lane == 0) {
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, qo < a.nq, 9, qo)) return st;
+#endif
         a.out_count[qo] = st == ST_OK ? count : 0u;
         if (a.publish) __threadfence_system();
         a.out_status[qo] = st;
@@ -1295,6 +1352,9 @@ static __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const
     w.tab = nullptr;
     w.tab_cap = 0;
     w.b_chunks = 0;
+#ifdef HNSW_DEVICE_CHECKS
+    w.chk = nullptr;
+#endif
     cold_reset(w);
 }
 
@@ -1338,6 +1398,9 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     const uint32_t warp = threadIdx.x >> 5;
     Ws w;
     carve(w, smem + size_t(warp) * g.bytes_per_warp, a.ix, g);
+#ifdef HNSW_DEVICE_CHECKS
+    w.chk = a.chk;
+#endif
     const int lane = lane_id();
     if (a.persistent) {
         const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -1422,6 +1485,9 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.H0 = w.H;
     w.C0 = w.C;
     w.cand_cap0 = w.cand_cap;
+#ifdef HNSW_DEVICE_CHECKS
+    w.chk = a.chk;
+#endif
     w.spilled_bits = w.spilled_cands = false;
     w.pool = nullptr;
     w.pool_next = nullptr;
@@ -1434,6 +1500,9 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     const uint32_t total = *a.overflow_count;
     for (uint32_t t = gw; t < total; t += nwarps) {
         const uint32_t qi = a.overflow_list[t];
+#ifdef HNSW_DEVICE_CHECKS
+        if (!HNSW_CHK(w.chk, qi < a.nq, 10, qi)) continue;
+#endif
         // Writes ST_OVERFLOW again if even this scratch is too small; the
         // last-resort pass then takes the query.
         if (run_query<1, DK>(a, w, qi, qi) == ST_OVERFLOW && a.overflow_list2 && lane_id() == 0)

@@ -25,7 +25,10 @@ from typing import Callable, NamedTuple, Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "libhnsw_gpu.so")
+# HNSW_GPU_LIB=checked loads the checked build (bounds checks in the
+# traversal kernels, libhnsw_gpu_checked.so from `make -C <package> checked`).
+_LIB_NAME = "libhnsw_gpu_checked.so" if os.environ.get("HNSW_GPU_LIB") == "checked" else "libhnsw_gpu.so"
+_LIB_PATH = os.path.join(_HERE, _LIB_NAME)
 if not os.path.exists(_LIB_PATH):
     raise ImportError(
         f"{_LIB_PATH} is missing: build it with `make -C {_HERE}` "
@@ -104,6 +107,11 @@ class Metric(enum.IntEnum):
     L2 = 0
     InnerProduct = 1
     Cosine = 2
+
+
+def checked_build() -> bool:
+    """True when the loaded library is the checked build."""
+    return bool(_lib.hnsw_gpu_checked_build())
 
 
 class Traversal(enum.IntEnum):
@@ -205,6 +213,8 @@ _lib.hnsw_gpu_brute_set_wait_limits.argtypes = [_vp, C.c_uint64, C.c_int]
 _lib.hnsw_gpu_brute_set_pairs.argtypes = [_vp, C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.argtypes = [C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.restype = None
+_lib.hnsw_gpu_check_word.argtypes = [_vp, C.c_void_p, C.c_int]
+_lib.hnsw_gpu_checked_build.argtypes = []
 
 
 class _BruteFilter(C.Structure):
@@ -587,6 +597,13 @@ class HnswIndex:
 
     def clear_tuning(self):
         _check(_lib.hnsw_gpu_clear_tuning(self._h))
+
+    def check_word(self, clear: bool = True):
+        """(site, value) of the first bounds-check violation of the checked
+        build (hnsw_gpu_check_word); (0, 0) when none or in the normal build."""
+        out = (C.c_uint32 * 2)()
+        _check(_lib.hnsw_gpu_check_word(self._h, out, int(clear)))
+        return int(out[0]), int(out[1])
 
     def set_counters(self, enabled: bool):
         _check(_lib.hnsw_gpu_set_counters(self._h, int(enabled)))

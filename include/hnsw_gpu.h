@@ -376,6 +376,17 @@ int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* brute, int enabled);
  * counterpart in the reference. */
 void hnsw_gpu_debug_fail_allocations(int count);
 
+/* Bounds checks of the checked build (libhnsw_gpu_checked.so, compiled with
+ * HNSW_DEVICE_CHECKS): the traversal kernels check node ids, array
+ * capacities, cold-list chunks and output rows before each use; the first
+ * violation writes its site (nonzero) and the offending value into the
+ * index's check word, and the access is skipped instead of faulting.
+ * hnsw_gpu_check_word copies that word (site, value) and clears it when
+ * `clear` is set; the normal build returns zeros. hnsw_gpu_checked_build
+ * returns 1 in the checked build, else 0. No counterpart in the reference. */
+int hnsw_gpu_check_word(hnsw_gpu_index* index, uint32_t out[2], int clear);
+int hnsw_gpu_checked_build(void);
+
 /* Allocation-free variant of hnsw_gpu_brute_search_batch, FP32 precision,
  * for callers that cannot allocate device memory while they run: code on a
  * latency-critical path, in a process whose memory policy forbids cudaMalloc
