@@ -345,6 +345,7 @@ class SearchOptions:
         self._ef = ef
         self._filter = None
         self._quantized = False
+        self._traversal = Traversal.F32
 
     def filter(self, f) -> "SearchOptions":
         self._filter = f
@@ -352,6 +353,12 @@ class SearchOptions:
 
     def quantized(self, q: bool) -> "SearchOptions":
         self._quantized = bool(q)
+        return self
+
+    def traversal(self, t: "Traversal") -> "SearchOptions":
+        """Distances while walking the graph (hnsw_search_opts.traversal); no
+        counterpart in the reference, whose search is Traversal.F32."""
+        self._traversal = Traversal(t)
         return self
 
     def ef(self) -> int:
@@ -542,7 +549,8 @@ class HnswIndex:
         bits, nbits, by_node = self._filter_bits(options._filter)
         keys, dist, count, _ = self.search_arrays(q.reshape(1, -1), k, options.ef(),
                                                   quantized=options._quantized,
-                                                  filter_bits=bits, filter_nbits=nbits, filter_by_node=by_node)
+                                                  filter_bits=bits, filter_nbits=nbits, filter_by_node=by_node,
+                                                  traversal=int(options._traversal))
         return self._to_lists(keys, dist, count)[0]
 
     def search_batch(self, queries, k: int, ef: int):
