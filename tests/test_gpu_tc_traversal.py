@@ -137,3 +137,16 @@ def test_rejects_quantized_and_unknown_traversal():
     got = gi.search_arrays(queries, 5, 20)
     ref = oi.search(queries, 5, 20)
     np.testing.assert_array_equal(got[0], ref[0])
+
+
+def test_search_with_options_traversal():
+    """SearchOptions.traversal reaches the device path through search_with."""
+    base, queries = H.gaussian(3000, 20, 48, 12)
+    data = build_index(base, metric=2, m=12, seed=6)
+    gi = H.HnswIndex.from_bytes(data)
+    arr = gi.search_arrays(queries, 10, 64, traversal=H.Traversal.BF16X3)
+    for i in range(len(queries)):
+        got = gi.search_with(queries[i], 10, H.SearchOptions(64).traversal(H.Traversal.BF16X3))
+        c = int(arr[2][i])
+        assert [n.key for n in got] == arr[0][i, :c].tolist()
+        assert [np.float32(n.distance).view(np.uint32) for n in got] == arr[1][i, :c].view(np.uint32).tolist()
