@@ -1054,8 +1054,9 @@ def run_serve(args, emit=True):
 
     # The default run (emit=False) sweeps three loads to stay within minutes.
     rates = tuple(int(r) for r in args.serve_rates.split(",")) if emit else (10_000, 30_000, 100_000)
-    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=8, max_pending=1 << 17, max_k=100, max_ef=512,
-                   linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank, quantized=True)
+    srv = H.Server(index, max_batch=args.serve_batch, max_inflight=args.serve_inflight, max_pending=1 << 17,
+                   max_k=100, max_ef=512, linger_us=args.serve_linger, filter_nbits=nb, filter_bank=bank,
+                   quantized=True)
     # Warm-up at a high rate so that every batch slot is driven with full
     # batches and sizes its device buffers (growing one frees the old, which
     # synchronises the device) before the sweep.
@@ -1077,6 +1078,7 @@ def run_serve(args, emit=True):
         "config": {"workload": "serve-10Mx128", "n_base": nb, "index_build_s": build_s, "file_gb": file_gb,
                    "open_s": open_s, "host_validate_s": host_validate_s,
                    "batched_qps_same_requests": batched_qps, "max_batch": args.serve_batch,
+                   "batch_slots": args.serve_inflight,
                    "p99_within_2ms_at_headline": bool(ok2), "latency_floor_single_request": floor,
                    "latency_floor_single_filtered_request_ef512_k100": floor_filtered,
                    "batch_launches": launches, "served": served_n, "sweep_batches": batch},
@@ -1326,6 +1328,7 @@ def main():
     ap.add_argument("--serve-n", type=int, default=10_000_000)
     ap.add_argument("--serve-batch", type=int, default=1024)
     ap.add_argument("--serve-linger", type=int, default=100)
+    ap.add_argument("--serve-inflight", type=int, default=8, help="batch slots of the 10M serving workload")
     ap.add_argument("--serve-rates", default="10000,30000,100000,300000,1000000")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-ref", type=int, default=20000)
