@@ -204,6 +204,7 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
             geo.hash_cap >>= 1;
     }
     if (!persistent) geo.cold = 0;  // cold lists need the persistent warps' chunk tables
+    set_hash_tags(geo, gi->view.n, g_visit_tag_bits.load());
     // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
     // out by the fast (cold variant) and retry kernels, [4] last-resort count.
     CU(s->work.ensure(32), "cudaMalloc work counters");
@@ -1390,6 +1391,8 @@ int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* b, int enabled) {
 }
 
 void hnsw_gpu_debug_fail_allocations(int count) { g_fail_allocations.store(count > 0 ? count : 0); }
+
+void hnsw_gpu_debug_visit_tags(int mode) { g_visit_tag_bits.store(mode < 0 ? -1 : std::min(mode, 32)); }
 
 int hnsw_gpu_check_word(hnsw_gpu_index* gi, uint32_t out[2], int clear) {
     if (!gi || !out) return set_error(HNSW_ERR_INVALID_ARGUMENT, "null argument");

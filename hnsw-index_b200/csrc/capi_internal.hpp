@@ -40,6 +40,9 @@ inline uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 // Device allocations still to fail on purpose (hnsw_gpu_debug_fail_allocations):
 // a host-side test hook for the out-of-device-memory paths.
 inline std::atomic<int> g_fail_allocations{0};
+// Visited-hash tags (hnsw_gpu_debug_visit_tags): 0 automatic, -1 off (32-bit
+// ids), k > 0 an id space of at least k bits.
+inline std::atomic<int> g_visit_tag_bits{0};
 inline bool injected_alloc_failure() {
     int n = g_fail_allocations.load(std::memory_order_relaxed);
     while (n > 0)

@@ -59,7 +59,34 @@ struct SearchGeometry {
     // Fast-kernel variant with the cold candidate list (persistent warps
     // move queue overflow there directly instead of to a global array).
     uint32_t cold = 0;
+    // Visited hash of 16-bit tags instead of 32-bit ids (set per launch by
+    // set_hash_tags from the node count): half the shared memory, so more
+    // warps fit on an SM. tag_sh = id bits kept in a tag, tag_mask = the id
+    // space 2^B - 1.
+    uint32_t tag16 = 0, tag_sh = 0, tag_mask = 0;
 };
+
+// 16-bit visited tags apply when the hash has 2^b entries (b >= 6) and node
+// ids below n need B = max(b, ceil(log2 n)) bits with B - b <= 10: the id is
+// mapped by a bijection of [0, 2^B), its home slot is the top b bits, and a
+// tag holds the low B - b bits beside the probe distance from home (at least
+// 6 bits, so probes up to 62 long). Otherwise the hash stores 32-bit ids.
+// `min_bits` > 0 widens the id space (any B >= the ids' bits is exact; a
+// wider one leaves fewer distance bits, down to 1, i.e. probes of length 1:
+// a test setting), negative turns the tags off.
+inline void set_hash_tags(SearchGeometry& g, uint32_t n, int min_bits = 0) {
+    g.tag16 = g.tag_sh = g.tag_mask = 0;
+    const uint32_t cap = g.hash_cap;
+    if (min_bits < 0 || cap < 64 || (cap & (cap - 1)) != 0) return;
+    const uint32_t b = 31u - uint32_t(__builtin_clz(cap));
+    uint32_t B = n > 1 ? 32u - uint32_t(__builtin_clz(n - 1)) : 1u;
+    if (B < uint32_t(min_bits)) B = uint32_t(min_bits > 32 ? 32 : min_bits);
+    if (B < b) B = b;
+    if (B - b > (min_bits > 0 ? 15u : 10u)) return;
+    g.tag16 = 1;
+    g.tag_sh = B - b;
+    g.tag_mask = B >= 32 ? 0xFFFFFFFFu : (1u << B) - 1u;
+}
 
 struct SearchArgs {
     DeviceIndexView ix;

@@ -56,7 +56,7 @@ __global__ void encode_codes_kernel(const float* __restrict__ vec, uint32_t n, u
 uint32_t geometry_bytes_per_warp(const SearchGeometry& g, uint32_t dp, uint32_t dc) {
     auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
     size_t b = al(size_t(dp) * 4) + al(dc) + al(g.tc_bytes) + al(size_t(g.ef_cap + 1) * 8) +
-               al(size_t(g.cand_cap + 1) * 8) + 256 + size_t(g.hash_cap) * 4;
+               al(size_t(g.cand_cap + 1) * 8) + 256 + size_t(g.hash_cap) * (g.tag16 ? 2 : 4);
     if (g.stage_rows) {
         const size_t rb = g.stage_row_bytes ? g.stage_row_bytes : size_t(dp) * 4;
         b += 256 + al(size_t(g.stage_rows) * rb);

@@ -71,6 +71,10 @@ struct Ws {
     uint32_t* fi;
     int32_t* fnorm;
     uint32_t ef_cap, cand_cap, hash_cap;
+    // 16-bit tags in H (SearchGeometry::tag16): tag_sh id bits per tag,
+    // tag_mask the id space.
+    bool tag16;
+    uint32_t tag_sh, tag_mask;
     bool bitmap_mode;  // H is a bitmap over node ids (retry kernel, or after a spill)
     uint32_t bitmap_words;
     // Persistent warps own spill areas in global memory: when the shared
@@ -102,27 +106,124 @@ struct Ws {
     uint64_t b_min, b_max;
 };
 
-// Visited test-and-set. Returns true if id was not visited before.
-// *full is set when the hash passes its load limit.
-__device__ __forceinline__ bool visit(Ws& w, uint32_t id) {
+// The bijection of the 16-bit-tag hash: x = id * kTagMul mod 2^B, inverted
+// by kTagMulInv (kTagMul * kTagMulInv = 1 mod 2^32).
+constexpr uint32_t kTagMul = 0x9E3779B1u;
+constexpr uint32_t tag_mul_inverse(uint32_t k) {
+    uint32_t x = k;
+    for (int i = 0; i < 5; ++i) x *= 2u - k * x;
+    return x;
+}
+constexpr uint32_t kTagMulInv = tag_mul_inverse(kTagMul);
+static_assert(kTagMul * kTagMulInv == 1u, "tag bijection");
+enum : uint32_t { VISIT_SEEN = 0, VISIT_FRESH = 1, VISIT_FULL = 2 };
+
+// Visited test-and-set: VISIT_FRESH if id was not visited before (it is
+// recorded now), VISIT_SEEN if it was, VISIT_FULL if a 16-bit-tag hash found
+// no free slot within the longest probe a tag can record (id is then not in
+// the set; the caller moves the set to its spill bitmap).
+//
+// 16-bit tags: with x = bijection(id), the home slot is x >> tag_sh and the
+// tag is (x mod 2^tag_sh) << dbits | d for the probe distance d < 2^dbits - 1
+// (dbits = 16 - tag_sh), so a tag never equals the empty value 0xFFFF. Slot
+// s holding tag (r, d) stores the id whose x is ((s - d) << tag_sh) | r: a
+// probe of id at distance d matches exactly its own tag. Slots are never
+// freed during a query, so linear probing finds an id before any empty slot.
+__device__ __forceinline__ uint32_t visit(Ws& w, uint32_t id) {
     if (w.bitmap_mode) {
 #ifdef HNSW_DEVICE_CHECKS
-        if (!HNSW_CHK(w.chk, (id >> 5) < w.bitmap_words, 1, id)) return false;
+        if (!HNSW_CHK(w.chk, (id >> 5) < w.bitmap_words, 1, id)) return VISIT_SEEN;
 #endif
         uint32_t bit = 1u << (id & 31);
         uint32_t old = atomicOr(&w.H[id >> 5], bit);
-        return (old & bit) == 0;
+        return (old & bit) == 0 ? VISIT_FRESH : VISIT_SEEN;
+    }
+    if (w.tag16) {
+        const uint32_t x = (id * kTagMul) & w.tag_mask;
+        const uint32_t dbits = 16u - w.tag_sh;
+        const uint32_t base = (x & ((1u << w.tag_sh) - 1u)) << dbits;
+        const uint32_t dlim = min((1u << dbits) - 1u, w.hash_cap);
+        unsigned short* H16 = reinterpret_cast<unsigned short*>(w.H);
+        uint32_t h = x >> w.tag_sh;
+        for (uint32_t d = 0; d < dlim; ++d) {
+            const unsigned short tag = (unsigned short)(base | d);
+            const unsigned short old = atomicCAS(H16 + h, (unsigned short)0xFFFFu, tag);
+            if (old == (unsigned short)0xFFFFu) return VISIT_FRESH;
+            if (old == tag) return VISIT_SEEN;
+            h = (h + 1u) & (w.hash_cap - 1u);
+        }
+        return VISIT_FULL;
     }
     // Any capacity (not only powers of two): the multiplicative hash maps
     // ids onto [0, hash_cap) and probing wraps around at the end.
     uint32_t h = uint32_t((uint64_t(id * 0x9E3779B1u) * w.hash_cap) >> 32);
     for (uint32_t probe = 0; probe < w.hash_cap; ++probe) {
         uint32_t old = atomicCAS(&w.H[h], kEmpty, id);
-        if (old == kEmpty) return true;
-        if (old == id) return false;
+        if (old == kEmpty) return VISIT_FRESH;
+        if (old == id) return VISIT_SEEN;
         h = h + 1 == w.hash_cap ? 0u : h + 1;
     }
-    return true;  // unreachable while the load limit holds
+    return VISIT_FRESH;  // unreachable while the load limit holds
+}
+
+// Empties the shared visited hash (all lanes).
+__device__ __forceinline__ void clear_hash(Ws& w) {
+    const int lane = lane_id();
+    if (w.tag16) {
+        uint4* h4 = reinterpret_cast<uint4*>(w.H);
+        const uint4 e = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+        for (uint32_t i = lane; i < (w.hash_cap >> 3); i += 32) h4[i] = e;
+    } else {
+        for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
+    }
+}
+
+// Moves the visited set from the shared hash into the warp's spill bitmap
+// (all lanes; w.spill_bits non-null) and continues in bitmap mode.
+__device__ __forceinline__ void spill_visited(Ws& w) {
+    const int lane = lane_id();
+    if (w.tag16) {
+        const unsigned short* H16 = reinterpret_cast<const unsigned short*>(w.H);
+        const uint32_t dbits = 16u - w.tag_sh, dmask = (1u << dbits) - 1u;
+        for (uint32_t i = lane; i < w.hash_cap; i += 32) {
+            const uint32_t t = H16[i];
+            if (t == 0xFFFFu) continue;
+            const uint32_t home = (i - (t & dmask)) & (w.hash_cap - 1u);
+            const uint32_t v = (((home << w.tag_sh) | (t >> dbits)) * kTagMulInv) & w.tag_mask;
+            atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
+        }
+    } else {
+        for (uint32_t i = lane; i < w.hash_cap; i += 32) {
+            const uint32_t v = w.H[i];
+            if (v != kEmpty) atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
+        }
+    }
+    __syncwarp();
+    w.H = w.spill_bits;
+    w.bitmap_mode = true;
+    w.bitmap_words = w.spill_words;
+    w.spilled_bits = true;
+}
+
+// Visited test of one neighbor list chunk (every lane, `valid` lanes hold
+// ids). A tag hash that cannot place an id moves the set to the spill
+// bitmap, where the id is then recorded; without a spill area the query
+// goes to the retry pass (*retry).
+__device__ __forceinline__ bool visit_chunk(Ws& w, uint32_t id, bool valid, bool* retry) {
+    uint32_t vr = valid ? visit(w, id) : VISIT_SEEN;
+    if (w.tag16 && !w.bitmap_mode && __any_sync(kFull, vr == VISIT_FULL)) {
+        if (!w.spill_bits) {
+            *retry = true;
+            return false;
+        }
+        spill_visited(w);
+        if (vr == VISIT_FULL) {
+            atomicOr(&w.H[id >> 5], 1u << (id & 31));
+            vr = VISIT_FRESH;
+        }
+        __syncwarp();
+    }
+    return vr == VISIT_FRESH;
 }
 
 struct QueryCtx {
@@ -721,7 +822,7 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
     if (w.bitmap_mode) {
         for (uint32_t i = lane; i < w.bitmap_words; i += 32) w.H[i] = 0;
     } else {
-        for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
+        clear_hash(w);
     }
     __syncwarp();
     const uint32_t hash_limit = (w.hash_cap >> 2) * 3;
@@ -767,17 +868,11 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
             if (!w.bitmap_mode && visited + __popc(V) > hash_limit) {
                 if (!w.spill_bits) return -1;
                 // Move the visited set into the warp's global bitmap.
-                for (uint32_t i = lane; i < w.hash_cap; i += 32) {
-                    const uint32_t v = w.H[i];
-                    if (v != kEmpty) atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
-                }
-                __syncwarp();
-                w.H = w.spill_bits;
-                w.bitmap_mode = true;
-                w.bitmap_words = w.spill_words;
-                w.spilled_bits = true;
+                spill_visited(w);
             }
-            const bool fresh = valid && visit(w, id);
+            bool retry = false;
+            const bool fresh = visit_chunk(w, id, valid, &retry);
+            if (retry) return -1;
             if (is_tc(DK)) {
                 if (fresh) {
                     prefetch_l2(ix.tc_hi + size_t(id) * (ix.dt >> 3), ix.dt * 2);
@@ -915,7 +1010,7 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
     if (w.bitmap_mode) {
         for (uint32_t i = lane; i < w.bitmap_words; i += 32) w.H[i] = 0;
     } else {
-        for (uint32_t i = lane; i < w.hash_cap; i += 32) w.H[i] = kEmpty;
+        clear_hash(w);
     }
     __syncwarp();
     const uint32_t hash_limit = (w.hash_cap >> 2) * 3;
@@ -980,17 +1075,12 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
             if (V == 0) break;
             if (!w.bitmap_mode && visited + __popc(V) > hash_limit) {
                 if (!w.spill_bits) return -1;
-                for (uint32_t i = lane; i < w.hash_cap; i += 32) {
-                    const uint32_t v = w.H[i];
-                    if (v != kEmpty) atomicOr(&w.spill_bits[v >> 5], 1u << (v & 31));
-                }
-                __syncwarp();
-                w.H = w.spill_bits;
-                w.bitmap_mode = true;
-                w.bitmap_words = w.spill_words;
-                w.spilled_bits = true;
+                // Move the visited set into the warp's global bitmap.
+                spill_visited(w);
             }
-            const bool fresh = valid && visit(w, id);
+            bool retry = false;
+            const bool fresh = visit_chunk(w, id, valid, &retry);
+            if (retry) return -1;
             if (is_tc(DK)) {
                 if (fresh) {
                     prefetch_l2(ix.tc_hi + size_t(id) * (ix.dt >> 3), ix.dt * 2);
@@ -1336,6 +1426,9 @@ static __device__ void carve(Ws& w, char* base, const DeviceIndexView& ix, const
     w.ef_cap = ef_cap;
     w.cand_cap = cand_cap;
     w.hash_cap = hash_cap;
+    w.tag16 = g.tag16 != 0;
+    w.tag_sh = g.tag_sh;
+    w.tag_mask = g.tag_mask;
     w.bitmap_mode = false;
     w.bitmap_words = 0;
     w.spill_bits = nullptr;
@@ -1476,6 +1569,8 @@ __global__ void __launch_bounds__(128) search_retry_kernel(SearchArgs a) {
     w.H = a.g_visited + size_t(gw) * a.g_visited_words;
     w.ef_cap = a.g_ef_cap;
     w.hash_cap = 0;
+    w.tag16 = false;
+    w.tag_sh = w.tag_mask = 0;
     w.bitmap_mode = true;
     w.bitmap_words = uint32_t(a.g_visited_words);
     w.spill_bits = nullptr;

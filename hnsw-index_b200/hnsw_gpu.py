@@ -213,6 +213,8 @@ _lib.hnsw_gpu_brute_set_wait_limits.argtypes = [_vp, C.c_uint64, C.c_int]
 _lib.hnsw_gpu_brute_set_pairs.argtypes = [_vp, C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.argtypes = [C.c_int]
 _lib.hnsw_gpu_debug_fail_allocations.restype = None
+_lib.hnsw_gpu_debug_visit_tags.argtypes = [C.c_int]
+_lib.hnsw_gpu_debug_visit_tags.restype = None
 _lib.hnsw_gpu_check_word.argtypes = [_vp, C.c_void_p, C.c_int]
 _lib.hnsw_gpu_checked_build.argtypes = []
 
@@ -775,6 +777,14 @@ class SearchGraph:
 def debug_fail_allocations(count: int):
     """Test hook: the next `count` device allocations fail as out of memory."""
     _lib.hnsw_gpu_debug_fail_allocations(int(count))
+
+
+def debug_visit_tags(mode: int):
+    """Visited-hash storage of the traversal kernels: 0 automatic (16-bit
+    tags where they fit), -1 always 32-bit ids, k > 0 ids treated as at least
+    k bits wide (shorter recordable probes). Results are the same in every
+    mode."""
+    _lib.hnsw_gpu_debug_visit_tags(int(mode))
 
 
 def validate_bytes(data: bytes, max_memory: Optional[int] = None) -> _Info:

@@ -376,6 +376,19 @@ int hnsw_gpu_brute_set_pairs(hnsw_gpu_brute* brute, int enabled);
  * counterpart in the reference. */
 void hnsw_gpu_debug_fail_allocations(int count);
 
+/* Tuning and test hook for the visited hash of the traversal kernels. By
+ * default (mode 0) a power-of-two hash over an index whose node ids need at
+ * most 10 bits more than the hash's log2 stores 16-bit tags (a slot holds
+ * the id's low bits beside its probe distance; half the shared memory of
+ * 32-bit ids, so more warps fit on an SM). mode -1 stores 32-bit ids
+ * always; mode k > 0 treats ids as k bits wide at least, which leaves fewer
+ * bits for probe distances, so tests can reach the path where a probe is
+ * longer than a tag records (the set then moves to the warp's spill bitmap,
+ * or the query to the retry pass). Results are identical in every mode.
+ * Process-wide; applies to searches enqueued after the call. No counterpart
+ * in the reference. */
+void hnsw_gpu_debug_visit_tags(int mode);
+
 /* Bounds checks of the checked build (libhnsw_gpu_checked.so, compiled with
  * HNSW_DEVICE_CHECKS): the traversal kernels check node ids, array
  * capacities, cold-list chunks and output rows before each use; the first
