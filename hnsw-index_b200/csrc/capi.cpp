@@ -80,8 +80,9 @@ int cuda_fail(cudaError_t e, const char* where) {
 // Persistent warps spill to global memory instead of restarting, so their
 // visited hash is sized near the typical visit count (about 12 per unit of
 // ef on the 1M x 128 workload, p99 about 25); plain warps size it for the tail.
-SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent, bool filtered) {
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent, bool filtered, uint32_t n) {
     constexpr uint32_t kSmemBudget = 220 * 1024;
+    const int tags = g_visit_tag_bits.load();
     SearchGeometry g;
     g.ef_cap = std::min<uint32_t>(1024, std::max<uint32_t>(32, round_up(ef_max, 32)));
     g.cand_cap = 2 * g.ef_cap + 32;
@@ -89,13 +90,28 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
     uint32_t h = 2048;
     while (h < want && h < 32768) h <<= 1;
     g.hash_cap = h;
+    // A persistent hash of 16-bit tags gets twice the slots for the bytes of
+    // 32-bit ids, up to 8192 slots (fewer spills; measured on the 1M x 128
+    // workload: ef = 64 2.35 ms with 4096 slots against 3.64 ms with 2048;
+    // at ef = 256 a 16384-slot hash costs more residency than it saves).
+    if (persistent && 2 * h <= 8192) {
+        SearchGeometry t = g;
+        t.hash_cap = 2 * h;
+        set_hash_tags(t, n, tags);
+        if (t.tag16) g.hash_cap = 2 * h;
+    }
+    // The sizing rules below count 32-bit slots (measured: they pick 4096
+    // slots at ef = 64 and 8192 at ef = 256 for plain warps, the fastest
+    // sizes with tags as well).
     while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget && g.hash_cap > 1024) g.hash_cap >>= 1;
     // Keep at least four warps per SM: a query that outgrows a smaller hash
     // continues in its spill bitmap (persistent) or the retry pass (plain),
     // which costs less than idle SMs (measured: a 64 KB hash at ef = 512 left
     // two warps per SM).
     while (geometry_bytes_per_warp(g, dp, dc) > kSmemBudget / 4 && g.hash_cap > 4096) g.hash_cap >>= 1;
-    // Warps per block that maximise resident warps per SM.
+    set_hash_tags(g, n, tags);
+    // Warps per block that maximise resident warps per SM, the fewest on a
+    // tie (a plain block holds its SM slot until its slowest query ends).
     uint32_t best_warps = 0, best_wpb = 1;
     for (uint32_t wpb : {1u, 2u, 4u, 8u}) {
         SearchGeometry t = g;
@@ -103,7 +119,7 @@ SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool per
         if (size_t(geometry_bytes_per_warp(t, dp, dc)) * wpb > kSmemBudget) continue;
         uint32_t warps = 0;
         if (persistent_warps(t, dp, dc, 1, &warps) != cudaSuccess) continue;
-        if (warps >= best_warps) {
+        if (warps > best_warps) {
             best_warps = warps;
             best_wpb = wpb;
         }
@@ -189,22 +205,26 @@ int hnswgpu::enqueue_search(hnsw_gpu_index* gi, Slot* s, const float* d_q, size_
     }
     if (o.mode == HNSW_MODE_AUTO) o.mode = HNSW_MODE_PERSISTENT;
     const bool persistent = o.mode == HNSW_MODE_PERSISTENT, filtered = d_fbits != nullptr;
-    if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
+    if (!geo.ef_cap) geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered, gi->view.n);
     geo.stage_row_bytes =
         geo.stage_rows ? ((o.quantized && gi->view.quantized) ? gi->view.dc : gi->view.dp * 4) : 0;
     geo.tc_bytes = tcb;
+    const int tags = g_visit_tag_bits.load();
+    set_hash_tags(geo, gi->view.n, tags);
     // A schedule tuned on int8 rows may not fit f32 rows (or the tensor-core
     // query operands): the heuristic's, with the visited hash halved until
     // it fits.
     if (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024) {
-        geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered);
+        geo = pick_geometry(ef_max, gi->view.dp, gi->view.dc, persistent, filtered, gi->view.n);
         geo.tc_bytes = tcb;
+        set_hash_tags(geo, gi->view.n, tags);
         while (size_t(geometry_bytes_per_warp(geo, gi->view.dp, gi->view.dc)) * geo.warps_per_block > 220 * 1024 &&
-               geo.hash_cap > 1024)
+               geo.hash_cap > 1024) {
             geo.hash_cap >>= 1;
+            set_hash_tags(geo, gi->view.n, tags);
+        }
     }
     if (!persistent) geo.cold = 0;  // cold lists need the persistent warps' chunk tables
-    set_hash_tags(geo, gi->view.n, g_visit_tag_bits.load());
     // work: [0] next query, [1] overflow count, [2] [3] cold chunks handed
     // out by the fast (cold variant) and retry kernels, [4] last-resort count.
     CU(s->work.ensure(32), "cudaMalloc work counters");
@@ -847,12 +867,13 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
     };
     for (int32_t mode : {HNSW_MODE_PLAIN, HNSW_MODE_PERSISTENT}) {
         const bool pers = mode == HNSW_MODE_PERSISTENT;
-        SearchGeometry cur = pick_geometry(ef_bound, gi->view.dp, gi->view.dc, pers, filtered);
+        SearchGeometry cur = pick_geometry(ef_bound, gi->view.dp, gi->view.dc, pers, filtered, gi->view.n);
         cur.stage_row_bytes = cur.stage_rows ? row_bytes : 0;
         float best_ms = 0.0f;
         if (!timed(cur, mode, 1, &best_ms)) return r;
         auto consider = [&](SearchGeometry g) {
             g.stage_row_bytes = g.stage_rows ? row_bytes : 0;
+            set_hash_tags(g, gi->view.n, g_visit_tag_bits.load());
             if (size_t(geometry_bytes_per_warp(g, gi->view.dp, gi->view.dc)) * g.warps_per_block > 220 * 1024)
                 return true;
             for (const Trial& t : trials)
@@ -878,8 +899,9 @@ int hnsw_gpu_autotune(hnsw_gpu_index* gi, const float* queries, size_t nq, size_
             }
             if (pass == 1) break;
             // Hash sizes need not be powers of two: 24 or 40 entries per
-            // result slot can fit one more warp per SM than 32 or 48.
-            for (uint32_t per : {16u, 24u, 32u, 40u, 48u, 64u}) {
+            // result slot can fit one more warp per SM than 32 or 48 (a
+            // power of two may store 16-bit tags, which halves its bytes).
+            for (uint32_t per : {16u, 24u, 32u, 40u, 48u, 64u, 128u}) {
                 const uint32_t hc = std::min<uint32_t>(32768, std::max<uint32_t>(1024, round_up(ef_cap * per, 64)));
                 SearchGeometry g = cur;
                 g.ef_cap = ef_cap;

@@ -148,7 +148,7 @@ struct DeviceGuard {
 // Scratch geometry per (ef bound): results, candidates and the visited
 // hash sized so that a typical traversal at that ef stays in shared memory.
 // Queries whose ef exceeds the fast kernel's 1024 go to the retry pass.
-SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent, bool filtered);
+SearchGeometry pick_geometry(uint32_t ef_max, uint32_t dp, uint32_t dc, bool persistent, bool filtered, uint32_t n);
 
 }  // namespace hnswgpu
 

@@ -167,7 +167,7 @@ struct SearchArgs {
 // or 2 (BF16x3); and the builder of the BF16 rows and f32 squared norms.
 using SearchKernel = void (*)(SearchArgs, SearchGeometry);
 using RetryKernel = void (*)(SearchArgs);
-SearchKernel tc_search_kernel(int v, int traversal);
+SearchKernel tc_search_kernel(int v, int traversal, bool persistent);
 RetryKernel tc_retry_kernel(int traversal);
 cudaError_t launch_tc_rows(const float* vec, uint32_t n, uint32_t dim, uint32_t dp, uint32_t dt, uint4* hi, uint4* lo,
                            float* xnorm, cudaStream_t stream);

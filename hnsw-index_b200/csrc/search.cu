@@ -78,11 +78,18 @@ static bool single_array_batch(const SearchArgs& args, const SearchGeometry& g) 
 static SearchKernel pick_search_kernel(const SearchArgs& args, const SearchGeometry& g) {
     if (args.traversal) {
         const int v = single_array_batch(args, g) ? 2 : (g.cold ? 1 : 0);
-        return tc_search_kernel(v, args.traversal);
+        return tc_search_kernel(v, args.traversal, args.persistent != 0);
     }
-    if (!single_array_batch(args, g)) return g.cold ? dev::search_kernel<1> : dev::search_kernel<0>;
-    if (args.quantized || g.stage_rows) return dev::search_kernel<2, dev::DK_ANY>;
-    return args.ix.metric == 0 ? dev::search_kernel<2, dev::DK_L2> : dev::search_kernel<2, dev::DK_DOT>;
+    using namespace dev;
+    if (args.persistent) {
+        if (!single_array_batch(args, g)) return g.cold ? search_kernel<1, DK_ANY, true> : search_kernel<0, DK_ANY, true>;
+        if (args.quantized || g.stage_rows) return search_kernel<2, DK_ANY, true>;
+        return args.ix.metric == 0 ? search_kernel<2, DK_L2, true> : search_kernel<2, DK_DOT, true>;
+    }
+    // Cold lists need persistent warps' chunk tables: plain batches use V = 0.
+    if (!single_array_batch(args, g)) return search_kernel<0>;
+    if (args.quantized || g.stage_rows) return search_kernel<2, DK_ANY>;
+    return args.ix.metric == 0 ? search_kernel<2, DK_L2> : search_kernel<2, DK_DOT>;
 }
 
 cudaError_t launch_search(const SearchArgs& args, const SearchGeometry& geo_in, int num_sms, cudaStream_t stream) {
@@ -116,12 +123,15 @@ cudaError_t persistent_warps(const SearchGeometry& g_in, uint32_t dp, uint32_t d
     const size_t smem = size_t(g.bytes_per_warp) * g.warps_per_block;
     // Spill slots for whichever variant a batch takes: the larger residency.
     int best = 1;
-    std::initializer_list<SearchKernel> kerns = {g.cold ? dev::search_kernel<1> : dev::search_kernel<0>,
-                                                 dev::search_kernel<2, dev::DK_ANY>, dev::search_kernel<2, dev::DK_L2>,
-                                                 dev::search_kernel<2, dev::DK_DOT>};
+    using namespace dev;
+    std::initializer_list<SearchKernel> kerns = {
+        g.cold ? search_kernel<1, DK_ANY, true> : search_kernel<0, DK_ANY, true>, search_kernel<2, DK_ANY, true>,
+        search_kernel<2, DK_L2, true>, search_kernel<2, DK_DOT, true>};
     // A geometry with tensor-core query operands is launched with those kernels.
-    std::initializer_list<SearchKernel> tc_kerns = {tc_search_kernel(g.cold ? 1 : 0, 1), tc_search_kernel(2, 1),
-                                                    tc_search_kernel(g.cold ? 1 : 0, 2), tc_search_kernel(2, 2)};
+    std::initializer_list<SearchKernel> tc_kerns = {tc_search_kernel(g.cold ? 1 : 0, 1, true),
+                                                    tc_search_kernel(2, 1, true),
+                                                    tc_search_kernel(g.cold ? 1 : 0, 2, true),
+                                                    tc_search_kernel(2, 2, true)};
     for (SearchKernel kern : g.tc_bytes ? tc_kerns : kerns) {
         cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(kern));
         if (e != cudaSuccess) return e;

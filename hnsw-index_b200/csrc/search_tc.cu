@@ -40,13 +40,19 @@ __global__ void tc_rows_kernel(const float* __restrict__ vec, uint32_t n, uint32
 
 }  // namespace dev
 
-SearchKernel tc_search_kernel(int v, int traversal) {
-    if (traversal == 2) {
-        if (v == 2) return dev::search_kernel<2, dev::DK_TC3>;
-        return v == 1 ? dev::search_kernel<1, dev::DK_TC3> : dev::search_kernel<0, dev::DK_TC3>;
+template <int DK>
+static SearchKernel tc_kernel_for(int v, bool persistent) {
+    using namespace dev;
+    if (persistent) {
+        if (v == 2) return search_kernel<2, DK, true>;
+        return v == 1 ? search_kernel<1, DK, true> : search_kernel<0, DK, true>;
     }
-    if (v == 2) return dev::search_kernel<2, dev::DK_TC1>;
-    return v == 1 ? dev::search_kernel<1, dev::DK_TC1> : dev::search_kernel<0, dev::DK_TC1>;
+    // Plain warps have no cold lists (V = 1 is persistent only).
+    return v == 2 ? search_kernel<2, DK> : search_kernel<0, DK>;
+}
+
+SearchKernel tc_search_kernel(int v, int traversal, bool persistent) {
+    return traversal == 2 ? tc_kernel_for<dev::DK_TC3>(v, persistent) : tc_kernel_for<dev::DK_TC1>(v, persistent);
 }
 
 RetryKernel tc_retry_kernel(int traversal) {

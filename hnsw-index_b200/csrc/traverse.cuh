@@ -1115,18 +1115,31 @@ __device__ __forceinline__ int layer0_single(QueryCtx& c, uint64_t ep, uint32_t 
                     if (pr > 0 && pdist(U[pr - 1]) == my_d) tie = true;
                 }
                 if (!__any_sync(kFull, tie)) {
-                    uint32_t before = 0;
+                    // before: entries of P earlier in the list and below this
+                    // one (the sequential admission test); below: all entries
+                    // of P below this one (its rank among them).
+                    uint32_t before = 0, below = 0;
                     for (uint32_t bits = P; bits; bits &= bits - 1) {
                         const int j = __ffs(bits) - 1;
                         const uint64_t xj = __shfl_sync(kFull, my_x, j);
-                        before += (j < lane && xj < my_x) ? 1u : 0u;
+                        const bool lt = xj < my_x;
+                        below += lt ? 1u : 0u;
+                        before += (lt && j < lane) ? 1u : 0u;
                     }
                     const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
                     if (I) {
 #ifdef HNSW_DEVICE_CHECKS
                         if (!HNSW_CHK(w.chk, rs + uint32_t(__popc(I)) <= w.cand_cap + 1, 6, rs)) return -1;
 #endif
-                        nx = min(nx, merge_all(U, rs, I, my_x, pr));
+                        // Rank among I: the entries of P below, less those
+                        // left out of I.
+                        for (uint32_t bits = P & ~I; bits; bits &= bits - 1) {
+                            const int j = __ffs(bits) - 1;
+                            below -= (__shfl_sync(kFull, my_x, j) < my_x) ? 1u : 0u;
+                        }
+                        // fr/fd (256 bytes, dead until the next chunk's
+                        // distances) hold the merge's new entries.
+                        nx = min(nx, merge_gather(U, rs, I, my_x, pr, below, reinterpret_cast<uint64_t*>(w.fr)));
                         const uint32_t total = rs + uint32_t(__popc(I));
                         if (total > ef) {
                             const float wd = pdist(U[ef - 1]);
@@ -1482,11 +1495,20 @@ static __device__ void end_spill(Ws& w) {
     }
 }
 
-// The fast kernel. COLD = false: candidate queues spill to a per-warp global
-// array and, beyond it, to the retry pass. COLD = true: the shared array's
-// upper half moves to the cold list directly.
-template <int V, int DK = DK_ANY>
-__global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometry g) {
+// The fast kernel. V = 0: candidate queues spill to a per-warp global array
+// and, beyond it, to the retry pass; V = 1: the shared array's upper half
+// moves to the cold list directly (persistent warps only); V = 2: the
+// single-array layer 0. PERSIST: persistent warps drain the work counter;
+// otherwise a warp runs its block's query once. Each mode is its own kernel
+// with one inlined traversal (measured at 1M x 128, ef = 64: a kernel
+// carrying both modes' copies ran persistent warps at 3.18 ms against
+// 2.34 ms plain, and one copy inside the persistent loop cost plain warps
+// 4 %). The bounds (256 threads, 2 blocks per SM: at most 128 registers)
+// steer the register allocation: with the thread bound alone the plain
+// kernels were built with 64 registers and spills (2.71 ms), without
+// bounds with 72 (2.64 ms); with both they take 124-128 and run 2.26 ms.
+template <int V, int DK = DK_ANY, bool PERSIST = false>
+__global__ void __launch_bounds__(256, 2) search_kernel(SearchArgs a, SearchGeometry g) {
     extern __shared__ __align__(16) char smem[];
     const uint32_t warp = threadIdx.x >> 5;
     Ws w;
@@ -1495,7 +1517,7 @@ __global__ void __launch_bounds__(256) search_kernel(SearchArgs a, SearchGeometr
     w.chk = a.chk;
 #endif
     const int lane = lane_id();
-    if (a.persistent) {
+    if constexpr (PERSIST) {
         const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + warp;
         if (a.spill_bits && slot < a.spill_slots) {
             w.spill_bits = a.spill_bits + size_t(slot) * a.spill_words;

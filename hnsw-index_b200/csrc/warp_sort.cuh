@@ -140,6 +140,43 @@ __device__ __forceinline__ uint32_t merge_all(uint64_t* A, uint32_t hi, uint32_t
     return pmin;
 }
 
+// merge_all with the positions known: the lanes of S (distinct entries x,
+// none in A) give their lower bound `pa` in the ascending A[0, hi) and their
+// rank `rk` among S, so each new entry's final position is pa + rk. Every
+// output position then gathers its entry instead of every old entry
+// counting the new ones below it: per 32-position chunk one OR reduction
+// collects the new entries' positions, an old entry at output o comes from
+// A[o - (new entries at or below o)] and a new one from `scratch` (32
+// entries, by rank). Chunks are rewritten from the top down and each is
+// read before it is written; a source never lies above its output, so
+// every source is read before its slot is overwritten. Room for hi + |S|
+// entries. Returns the lowest position written. All lanes call.
+__device__ __forceinline__ uint32_t merge_gather(uint64_t* A, uint32_t hi, uint32_t S, uint64_t x, uint32_t pa,
+                                                 uint32_t rk, uint64_t* scratch) {
+    const int lane = lane_id();
+    const bool in = (S >> lane) & 1u;
+    const uint32_t q = pa + rk;
+    if (in) scratch[rk] = x;
+    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
+    const uint32_t total = hi + uint32_t(__popc(S));
+    const uint32_t upto = (2u << lane) - 1u;  // lanes at or below this one
+    __syncwarp();
+    for (int c = int((total - 1) >> 5); c >= int(pmin >> 5); --c) {
+        const uint32_t b = uint32_t(c) << 5;
+        const uint32_t M = __reduce_or_sync(kFull, (in && q >= b && q < b + 32) ? 1u << (q - b) : 0u);
+        const uint32_t nb = __reduce_add_sync(kFull, (in && q < b) ? 1u : 0u);
+        const uint32_t o = b + uint32_t(lane);
+        const uint32_t nle = nb + uint32_t(__popc(M & upto));
+        const bool act = o >= pmin && o < total;
+        uint64_t v = 0;
+        if (act) v = ((M >> lane) & 1u) ? scratch[nle - 1] : A[o - nle];
+        __syncwarp();
+        if (act) A[o] = v;
+        __syncwarp();
+    }
+    return pmin;
+}
+
 constexpr uint32_t kTieCap = 32;
 
 // A result evicted while unexpanded stays a candidate of the reference's
