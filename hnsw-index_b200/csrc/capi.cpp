@@ -726,6 +726,22 @@ static int stage_batch(Slot* s, const float* queries, size_t nq, size_t dim, con
     return HNSW_OK;
 }
 
+// The first non-OK query status of a finished batch becomes the call's error.
+static int batch_status(const int32_t* out_status, size_t nq) {
+    for (size_t i = 0; i < nq; ++i)
+        if (out_status[i] != HNSW_OK) {
+            const int32_t code = out_status[i];
+            std::string msg = code == HNSW_ERR_NON_FINITE_VECTOR ? "vector contains NaN or infinite values"
+                              : code == HNSW_ERR_ZERO_VECTOR     ? "zero vector has no direction under cosine distance"
+                              : code == HNSW_ERR_QUANTIZATION_DISABLED
+                                  ? "quantized search requested but quantization is not enabled"
+                              : code == HNSW_ERR_SCRATCH_OVERFLOW ? "a query outgrew the device scratch"
+                                                                  : "query failed";
+            return set_error(code, msg);
+        }
+    return HNSW_OK;
+}
+
 int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, size_t dim,
                           const hnsw_search_opts* opts, uint64_t* out_keys, float* out_dist, uint32_t* out_count,
                           int32_t* out_status) {
@@ -761,18 +777,7 @@ int hnsw_gpu_search_batch(hnsw_gpu_index* gi, const float* queries, size_t nq, s
         gi->last_counters.resize(nq * 4);
         CU(cudaMemcpy(gi->last_counters.data(), s->counters.p, nq * 16, cudaMemcpyDeviceToHost), "copy counters");
     }
-    for (size_t i = 0; i < nq; ++i)
-        if (out_status[i] != HNSW_OK) {
-            const int32_t code = out_status[i];
-            std::string msg = code == HNSW_ERR_NON_FINITE_VECTOR ? "vector contains NaN or infinite values"
-                              : code == HNSW_ERR_ZERO_VECTOR     ? "zero vector has no direction under cosine distance"
-                              : code == HNSW_ERR_QUANTIZATION_DISABLED
-                                  ? "quantized search requested but quantization is not enabled"
-                              : code == HNSW_ERR_SCRATCH_OVERFLOW ? "a query outgrew the device scratch"
-                                                                  : "query failed";
-            return set_error(code, msg);
-        }
-    return HNSW_OK;
+    return batch_status(out_status, nq);
 }
 
 int hnsw_gpu_clear_tuning(hnsw_gpu_index* gi) {
