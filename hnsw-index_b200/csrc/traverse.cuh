@@ -927,7 +927,9 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                     const uint32_t I = __ballot_sync(kFull, inP && pr + before < ef);
                     const uint32_t IR = I & A;
                     if (IR) {
-                        batch_merge(w.R, 0, rs, IR, my_x, ef);
+                        // fr/fd (dead until the next chunk's distances) hold
+                        // the merges' new entries.
+                        batch_merge_gather(w.R, 0, rs, IR, my_x, ef, reinterpret_cast<uint64_t*>(w.fr));
                         rs = min(rs + uint32_t(__popc(IR)), ef);
                     }
                     if (I) {
@@ -945,7 +947,8 @@ __device__ __forceinline__ int layer0(QueryCtx& c, uint64_t ep, uint32_t ef) {
                                 IB |= mv;
                             }
                             if (IA) {
-                                batch_merge(w.C, head, tail, IA, my_x, w.cand_cap);
+                                batch_merge_gather(w.C, head, tail, IA, my_x, w.cand_cap,
+                                                   reinterpret_cast<uint64_t*>(w.fr));
                                 tail += uint32_t(__popc(IA));
                             }
                         }

@@ -177,6 +177,43 @@ __device__ __forceinline__ uint32_t merge_gather(uint64_t* A, uint32_t hi, uint3
     return pmin;
 }
 
+// batch_merge by gathering (as merge_gather): the lanes of S (distinct
+// entries x, none in A[lo, hi)) merge into the ascending A[lo, hi), and
+// positions at or above `limit` are dropped. `scratch` holds 32 entries.
+// All lanes call.
+__device__ __forceinline__ void batch_merge_gather(uint64_t* A, uint32_t lo, uint32_t hi, uint32_t S, uint64_t x,
+                                                   uint32_t limit, uint64_t* scratch) {
+    const int lane = lane_id();
+    const bool in = (S >> lane) & 1u;
+    uint32_t rk = 0;
+    for (uint32_t bits = S; bits; bits &= bits - 1) {
+        const int j = __ffs(bits) - 1;
+        rk += (__shfl_sync(kFull, x, j) < x) ? 1u : 0u;
+    }
+    const uint32_t pa = in ? lower_bound(A, lo, hi, x) : hi;
+    const uint32_t q = pa + rk;
+    if (in) scratch[rk] = x;
+    const uint32_t pmin = __reduce_min_sync(kFull, in ? pa : 0xFFFFFFFFu);
+    const uint32_t end = min(hi + uint32_t(__popc(S)), limit);
+    const uint32_t upto = (2u << lane) - 1u;
+    __syncwarp();
+    if (pmin < end) {
+        for (int c = int((end - 1) >> 5); c >= int(pmin >> 5); --c) {
+            const uint32_t b = uint32_t(c) << 5;
+            const uint32_t M = __reduce_or_sync(kFull, (in && q >= b && q < b + 32) ? 1u << (q - b) : 0u);
+            const uint32_t nb = __reduce_add_sync(kFull, (in && q < b) ? 1u : 0u);
+            const uint32_t o = b + uint32_t(lane);
+            const uint32_t nle = nb + uint32_t(__popc(M & upto));
+            const bool act = o >= pmin && o < end;
+            uint64_t v = 0;
+            if (act) v = ((M >> lane) & 1u) ? scratch[nle - 1] : A[o - nle];
+            __syncwarp();
+            if (act) A[o] = v;
+            __syncwarp();
+        }
+    }
+}
+
 constexpr uint32_t kTieCap = 32;
 
 // A result evicted while unexpanded stays a candidate of the reference's
